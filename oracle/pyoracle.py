@@ -1,0 +1,233 @@
+"""ctypes front end to the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and bench.py's
+CPU-baseline leg, never by the product package.  Arrays are numpy complex128;
+2-transverse-dim fields are (Ny, Nx) arrays stored Fortran-order so that the
+memory layout is the reference's Armadillo column-major cx_mat.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REFPIN = None
+
+
+class Grid(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "xmin", "xmax", "dx", "ymin", "ymax", "dy", "zmin", "zmax", "dz",
+        "wavenumber")]
+
+
+class Sphere(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("cx", "cy", "cz", "radius", "delta", "beta")]
+
+
+class Material(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("core_half_width", C.c_double), ("delta_clad", C.c_double),
+        ("beta_clad", C.c_double), ("ramp_beta", C.c_double),
+        ("ramp_points", C.c_int), ("n_transverse", C.c_int),
+        ("spheres", C.POINTER(Sphere)), ("n_spheres", C.c_int),
+        ("delta_table", C.POINTER(C.c_double)), ("beta_table", C.POINTER(C.c_double)),
+    ]
+
+
+MAT_VACUUM, MAT_WAVEGUIDE, MAT_SPHERES, MAT_XTABLE = 0, 1, 2, 3
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _LIB = C.CDLL(path)
+        d = C.POINTER(C.c_double)
+        _LIB.orc_node_count.restype = C.c_uint
+        _LIB.orc_node_count.argtypes = [C.c_double] * 3
+        _LIB.orc_fft1d.argtypes = [d, C.c_int, C.c_int]
+        _LIB.orc_thomas.argtypes = [d, d, d, C.c_int]
+        for name in ("orc_fft2d_run",):
+            getattr(_LIB, name).argtypes = [C.POINTER(Grid), C.POINTER(Material), d,
+                                            C.c_int, C.c_int, d, d]
+        for name in ("orc_cn2d_run", "orc_adi3d_run"):
+            getattr(_LIB, name).argtypes = [C.POINTER(Grid), C.POINTER(Material), C.c_int,
+                                            d, C.c_int, C.c_int, d, d]
+        _LIB.orc_fft3d_run.argtypes = [C.POINTER(Grid), C.POINTER(Material), C.c_double,
+                                       C.c_double, d, C.c_int, C.c_int, d, d]
+        _LIB.orc_gaussian_beam_2d.argtypes = [C.POINTER(Grid)] + [C.c_double] * 5 + [d]
+        _LIB.orc_gaussian_beam_3d.argtypes = [C.POINTER(Grid)] + [C.c_double] * 6 + [d]
+        _LIB.orc_material_eval.argtypes = [C.POINTER(Material), C.POINTER(Grid)] + \
+            [C.c_double] * 3 + [d, d]
+        _LIB.orc_set_threads.argtypes = [C.c_int]
+    return _LIB
+
+
+def refpin():
+    """The reference's own ThomasAlgorithm / ParaxialEquation, compiled from its
+    sources (None when that library was not built)."""
+    global _REFPIN
+    if _REFPIN is None:
+        path = os.path.join(_HERE, "_ref", "libpaxpro_refpin.so")
+        if not os.path.exists(path):
+            return None
+        _REFPIN = C.CDLL(path)
+        d = C.POINTER(C.c_double)
+        _REFPIN.ref_thomas_solve.argtypes = [d, d, d, C.c_int]
+        _REFPIN.ref_paraxial_equation.argtypes = [C.c_double] * 3 + [d]
+    return _REFPIN
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def grid(xmin, xmax, dx, zmin, zmax, dz, wavenumber, ymin=None, ymax=None, dy=None):
+    g = Grid()
+    g.xmin, g.xmax, g.dx = xmin, xmax, dx
+    g.ymin = xmin if ymin is None else ymin
+    g.ymax = xmax if ymax is None else ymax
+    g.dy = dx if dy is None else dy
+    g.zmin, g.zmax, g.dz = zmin, zmax, dz
+    g.wavenumber = wavenumber
+    return g
+
+
+class MaterialSpec:
+    """Keeps the ctypes Material and the arrays it points into alive."""
+
+    def __init__(self, kind=MAT_VACUUM, **kw):
+        self.m = Material()
+        self.m.kind = kind
+        self._keep = []
+        for key in ("core_half_width", "delta_clad", "beta_clad", "ramp_beta"):
+            setattr(self.m, key, float(kw.get(key, 0.0)))
+        self.m.ramp_points = int(kw.get("ramp_points", 0))
+        self.m.n_transverse = int(kw.get("n_transverse", 0))
+        sph = kw.get("spheres")
+        if sph is not None and len(sph):
+            arr = (Sphere * len(sph))()
+            for i, s in enumerate(sph):
+                arr[i] = Sphere(*[float(v) for v in s])
+            self._keep.append(arr)
+            self.m.spheres = C.cast(arr, C.POINTER(Sphere))
+            self.m.n_spheres = len(sph)
+        if kw.get("delta_table") is not None:
+            dt = np.ascontiguousarray(kw["delta_table"], dtype=np.float64)
+            bt = np.ascontiguousarray(kw["beta_table"], dtype=np.float64)
+            self._keep += [dt, bt]
+            self.m.delta_table, self.m.beta_table = _p(dt), _p(bt)
+            self.m.n_transverse = len(dt)
+
+
+def node_count(mn, mx, step) -> int:
+    return int(lib().orc_node_count(mn, mx, step))
+
+
+def fft1d(x: np.ndarray, sign: int) -> np.ndarray:
+    a = np.ascontiguousarray(x, dtype=np.complex128).copy()
+    rc = lib().orc_fft1d(_p(a), len(a), sign)
+    if rc:
+        raise ValueError("length must be a power of two")
+    return a
+
+
+def thomas(diag, sub, rhs) -> np.ndarray:
+    d = np.ascontiguousarray(diag, dtype=np.complex128).copy()
+    s = np.ascontiguousarray(sub, dtype=np.complex128).copy()
+    r = np.ascontiguousarray(rhs, dtype=np.complex128).copy()
+    lib().orc_thomas(_p(d), _p(s), _p(r), len(d))
+    return d
+
+
+def ref_thomas(diag, sub, rhs):
+    rp = refpin()
+    if rp is None:
+        return None
+    d = np.ascontiguousarray(diag, dtype=np.complex128).copy()
+    s = np.ascontiguousarray(sub, dtype=np.complex128).copy()
+    r = np.ascontiguousarray(rhs, dtype=np.complex128).copy()
+    rp.ref_thomas_solve(_p(d), _p(s), _p(r), len(d))
+    return d
+
+
+def material_eval(spec: MaterialSpec, g: Grid, x, y, z):
+    d = np.zeros(1)
+    b = np.zeros(1)
+    lib().orc_material_eval(C.byref(spec.m), C.byref(g), x, y, z, _p(d), _p(b))
+    return float(d[0]), float(b[0])
+
+
+def _run2d(fn, g, spec, u0, nsteps, save_every, *extra):
+    u0 = np.ascontiguousarray(u0, dtype=np.complex128)
+    n = len(u0)
+    nsave = nsteps // save_every if save_every > 0 else 0
+    saves = np.zeros((max(nsave, 1), n), dtype=np.complex128)
+    out = np.zeros(n, dtype=np.complex128)
+    rc = fn(C.byref(g), C.byref(spec.m), *extra, _p(u0), nsteps, save_every,
+            _p(saves), _p(out))
+    if rc:
+        raise ValueError(f"oracle rejected the problem (rc={rc})")
+    return out, saves[:nsave]
+
+
+def fft2d_run(g, spec, u0, nsteps, save_every=0):
+    return _run2d(lib().orc_fft2d_run, g, spec, u0, nsteps, save_every)
+
+
+def cn2d_run(g, spec, u0, nsteps, save_every=0, transparent=False):
+    return _run2d(lib().orc_cn2d_run, g, spec, u0, nsteps, save_every, int(transparent))
+
+
+def _run3d(fn, g, spec, u0, nsteps, save_every, *extra):
+    u0 = np.asfortranarray(u0, dtype=np.complex128)
+    ny, nx = u0.shape
+    nsave = nsteps // save_every if save_every > 0 else 0
+    saves = np.zeros((max(nsave, 1), nx * ny), dtype=np.complex128)
+    out = np.zeros((ny, nx), dtype=np.complex128, order="F")
+    flat_in = u0.reshape(-1, order="F")
+    rc = fn(C.byref(g), C.byref(spec.m), *extra, _p(flat_in), nsteps, save_every,
+            _p(saves), out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc:
+        raise ValueError(f"oracle rejected the problem (rc={rc})")
+    return out, [s.reshape((ny, nx), order="F") for s in saves[:nsave]]
+
+
+def fft3d_run(g, spec, u0, nsteps, save_every=0, absorber_width=0.0, absorber_damping=0.0):
+    return _run3d(lib().orc_fft3d_run, g, spec, u0, nsteps, save_every,
+                  float(absorber_width), float(absorber_damping))
+
+
+def adi3d_run(g, spec, u0, nsteps, save_every=0, use_tbc=False):
+    return _run3d(lib().orc_adi3d_run, g, spec, u0, nsteps, save_every, int(use_tbc))
+
+
+def gaussian_beam_2d(g, wavelength, waist, center=0.0, amplitude=1.0, z=0.0):
+    n = node_count(g.xmin, g.xmax, g.dx)
+    out = np.zeros(n, dtype=np.complex128)
+    lib().orc_gaussian_beam_2d(C.byref(g), wavelength, waist, center, amplitude, z, _p(out))
+    return out
+
+
+def gaussian_beam_3d(g, wavelength, waist, cx=0.0, cy=0.0, amplitude=1.0, z=0.0):
+    nx = node_count(g.xmin, g.xmax, g.dx)
+    ny = node_count(g.ymin, g.ymax, g.dy)
+    out = np.zeros((ny, nx), dtype=np.complex128, order="F")
+    lib().orc_gaussian_beam_3d(C.byref(g), wavelength, waist, cx, cy, amplitude, z,
+                               out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
