@@ -1,0 +1,164 @@
+/*
+ * paxpro_b200.h -- C ABI of the B200 propagation solvers.
+ *
+ * The reference exposes its solvers through C++ classes (include/solver.hpp,
+ * include/solver2D.hpp, include/solver3D.hpp, include/paraxialSimulation.hpp)
+ * and a SWIG module (pypaxpro/pypaxpro.i).  This header is the plain-C
+ * boundary those classes sit on in this build: opaque handles, plain
+ * pointers and sizes, int status codes, no exceptions and no C++ or torch
+ * types.  The C++ mirror of the reference API (include/paxpro/*.hpp) and the
+ * Python package call only these functions.
+ *
+ * Conventions
+ *  - Complex arrays are interleaved (re, im) doubles on the host.
+ *  - 1-transverse-dim fields are Nx values (arma::cx_vec).  2-transverse-dim
+ *    fields are Ny x Nx in Armadillo column-major order: element (row = y
+ *    index, col = x index) at col*Ny + row (arma::cx_mat, as the reference's
+ *    Solver3D stores prevSolution/currentSolution, src/solver3D.cpp:33-34).
+ *  - Steps are numbered from 1 as Solver::currentStep (include/solver.hpp:73).
+ *  - Every function returns PXP_OK (0) or a negative status; the handle keeps
+ *    a message for pxp_last_error.
+ */
+#ifndef PAXPRO_B200_H
+#define PAXPRO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PXP_OK 0
+#define PXP_ERR_INVALID (-1)     /* bad argument / call order */
+#define PXP_ERR_NOMEM (-2)       /* device or host allocation failed */
+#define PXP_ERR_CUDA (-3)        /* CUDA runtime error */
+#define PXP_ERR_ABORTED (-4)     /* job cancelled */
+#define PXP_ERR_BUDGET (-5)      /* step / wait budget exceeded */
+#define PXP_ERR_NOT_READY (-6)   /* result not available yet */
+#define PXP_ERR_UNSUPPORTED (-7) /* size/precision this build does not run */
+
+/* ---- solver kinds (the reference's Solver2D / Solver3D subclasses) ------ */
+#define PXP_FFT_SOLVER_2D 1   /* FFTSolver2D, include/fftSolver2D.hpp:13 */
+#define PXP_CRANK_NICHOLSON 2 /* CrankNicholson, include/crankNicholson.hpp:16 */
+#define PXP_FFT_SOLVER_3D 3   /* FFTSolver3D, include/fftSolver3D.hpp:16 */
+#define PXP_ADI 4             /* ADI, include/alternatingDirectionSolver.hpp:15 */
+
+#define PXP_FP64 0 /* plain mode: complex128 fields, reference parity */
+#define PXP_FP32 1 /* served mode: complex64 fields, FP64-reduced phase tables */
+
+/* Disctretization (include/paraxialSimulation.hpp:20-26). */
+typedef struct {
+  double min, max, step;
+  unsigned downsampling_ratio;
+} pxp_discretization;
+
+/* Everything ParaxialSimulation hands a solver in setSolver/solve
+ * (src/paraxialSimulation.cpp:67-131, 398). */
+typedef struct {
+  int kind;            /* PXP_FFT_SOLVER_2D ... PXP_ADI */
+  int precision;       /* PXP_FP64 / PXP_FP32 */
+  pxp_discretization x; /* setTransverseDiscretization */
+  pxp_discretization y; /* setVerticalDiscretization (3-D kinds) */
+  pxp_discretization z; /* setLongitudinalDiscretization */
+  double wavenumber;   /* setWavenumber / setWaveLength: k = 2 pi / lambda */
+  int transparent_bc;  /* CrankNicholson BC_t::TRANSPARENT; ADI::useTBC */
+  double absorber_width, absorber_damping; /* FFTSolver3D::absorbingBC (0 = off) */
+  int save_every;      /* save a field every n steps (0 = never; the
+                          reference's 2-D solvers keep every step, its 3-D
+                          solvers every z.downsampling_ratio steps) */
+  int device;          /* CUDA device ordinal */
+} pxp_problem;
+
+/* One sphere of a first-hit sphere material (sphere r^2 < R^2 test as in
+ * Examples/sphere.cpp:13-14, shapes evaluated in list order as
+ * CSGMaterial::getXrayMatProp, src/materialFunction.cpp:3-13). */
+typedef struct {
+  double cx, cy, cz, radius, delta, beta;
+} pxp_sphere;
+
+typedef struct pxp_solver_s *pxp_solver;
+
+/* Node count exactly as ParaxialSimulation::nodeNumber* computes it
+ * (src/paraxialSimulation.cpp:107-120). */
+unsigned pxp_node_count(double min, double max, double step);
+
+/* Solver::setSimulator + ParaxialSimulation::setSolver
+ * (src/paraxialSimulation.cpp:122-131, src/solver2D.cpp:21-42,
+ * src/solver3D.cpp:19-44): allocate device state for the problem. */
+int pxp_solver_create(const pxp_problem *problem, pxp_solver *out);
+
+/* Solver destructor (src/solver2D.cpp:10-19, src/solver3D.cpp:11-17). */
+int pxp_solver_destroy(pxp_solver s);
+
+/* Material hook, z-invariant medium sampled per transverse point
+ * (ParaxialSimulation::getXrayMatProp, src/paraxialSimulation.cpp:513-537):
+ * delta[i], beta[i] at x_i for the 2-D kinds (n = Nx), or at (x_col, y_row)
+ * column-major for the 3-D kinds (n = Nx*Ny). */
+int pxp_set_material_table(pxp_solver s, const double *delta, const double *beta, size_t n);
+
+/* Material hook, sampled per step for z-varying 2-D media: for each step
+ * s = first_step .. first_step+nsteps-1, plane (s - first_step) holds
+ * delta/beta at the step's sampling plane(s): FFTSolver2D uses
+ * z = getZ(s) + dz/2 (src/fftSolver2D.cpp:38); CrankNicholson uses z and
+ * z - dz (src/crancNicholson.cpp:37-38), passed as two planes per step
+ * (z first).  Layout [plane][x]. */
+int pxp_set_material_planes(pxp_solver s, const double *delta, const double *beta,
+                            int first_step, int nsteps);
+
+/* Material hook, first-hit sphere list evaluated on the device
+ * (3-D kinds; 2-D kinds take y = 0). */
+int pxp_set_material_spheres(pxp_solver s, const pxp_sphere *spheres, int n);
+
+/* Solver::setInitialConditions (include/solver.hpp:54,57): the field at
+ * z = zmin; host array.  Resets the step counter to 1 and clears saves. */
+int pxp_set_initial_conditions(pxp_solver s, const double *field);
+/* Same from a device array of the solver's storage precision. */
+int pxp_set_initial_conditions_device(pxp_solver s, const void *dfield);
+
+/* Solver::step repeated nsteps times (src/solver2D.cpp:243-250,
+ * src/solver3D.cpp:148-166).  Asynchronous on the solver's stream. */
+int pxp_step(pxp_solver s, int nsteps);
+
+/* Solver::solve: all remaining steps up to nodeNumberLongitudinal()-1
+ * (src/solver2D.cpp:224-241, src/solver3D.cpp:168-199). */
+int pxp_solve(pxp_solver s);
+
+/* Wait for the solver's queued work; returns the first error seen. */
+int pxp_synchronize(pxp_solver s);
+
+/* Solver::getLastSolution / getLastSolution3D (include/solver2D.hpp:78,
+ * include/solver3D.hpp:38): copy the current field to the host (complex128). */
+int pxp_get_last_solution(pxp_solver s, double *field);
+/* Device pointer to the resident field (solver precision), valid until the
+ * next call on the handle. */
+int pxp_get_field_device(pxp_solver s, void **dfield, int *precision);
+
+/* Saved fields (the columns of Solver2D::solution / slices of
+ * Solver3D::solution, include/solver2D.hpp:121, include/solver3D.hpp:52):
+ * number of slots filled and one slot copied to the host. */
+int pxp_num_saved(pxp_solver s, int *count);
+int pxp_get_saved(pxp_solver s, int slot, double *field);
+
+/* Solver::reset (include/solver.hpp:30): step counter back to 1. */
+int pxp_reset(pxp_solver s);
+
+/* Next step index (Solver::currentStep). */
+int pxp_current_step(pxp_solver s, unsigned *step);
+
+/* Grid shape of the handle: Nx, Ny (1 for 2-D kinds), Nz. */
+int pxp_shape(pxp_solver s, unsigned *nx, unsigned *ny, unsigned *nz);
+
+/* Last error message of the handle (NULL handle: last global error). */
+int pxp_last_error(pxp_solver s, char *buf, size_t len);
+
+/* Static text for a status code. */
+const char *pxp_status_string(int status);
+
+/* Build information: kernel architecture and version string. */
+const char *pxp_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PAXPRO_B200_H */

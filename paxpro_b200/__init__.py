@@ -1,0 +1,204 @@
+"""paxpro_b200 -- B200-native paraxial propagation solvers.
+
+Python face of the C ABI (include/paxpro_b200.h), shaped like the reference's
+Solver / ParaxialSimulation API (include/solver.hpp, include/
+paraxialSimulation.hpp): a solver is created for a discretised problem, given
+a material and an initial field, then stepped; fields come back as numpy
+arrays in the reference's layouts (cx_vec for one transverse dimension,
+column-major Ny x Nx cx_mat for two).
+
+All compute runs in the CUDA library; importing this package without the
+built library raises ImportError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import (ADI, CRANK_NICHOLSON, FFT_SOLVER_2D, FFT_SOLVER_3D, FP32, FP64,  # noqa: F401
+                    PxpError)
+
+_capi.lib()  # fail loudly at import when the CUDA library is absent
+
+KIND_NAMES = {FFT_SOLVER_2D: "FFTSolver2D", CRANK_NICHOLSON: "CrankNicholson",
+              FFT_SOLVER_3D: "FFTSolver3D", ADI: "ADI"}
+
+
+def node_count(mn: float, mx: float, step: float) -> int:
+    """ParaxialSimulation::nodeNumber* (src/paraxialSimulation.cpp:107-120)."""
+    return int(_capi.lib().pxp_node_count(mn, mx, step))
+
+
+@dataclass
+class Disc:
+    """Disctretization record (include/paraxialSimulation.hpp:20-26)."""
+    min: float
+    max: float
+    step: float
+    downsampling_ratio: int = 1
+
+
+@dataclass
+class Sphere:
+    cx: float
+    cy: float
+    cz: float
+    radius: float
+    delta: float
+    beta: float
+
+
+@dataclass
+class ProblemSpec:
+    kind: int
+    x: Disc
+    z: Disc
+    wavenumber: float
+    y: Optional[Disc] = None
+    precision: int = FP64
+    transparent_bc: bool = False
+    absorber_width: float = 0.0
+    absorber_damping: float = 0.0
+    save_every: int = 0
+    device: int = 0
+
+    def to_c(self) -> _capi.Problem:
+        p = _capi.Problem()
+        p.kind, p.precision = self.kind, self.precision
+        for name in ("x", "y", "z"):
+            d = getattr(self, name) or self.x
+            setattr(p, name, _capi.Discretization(d.min, d.max, d.step, d.downsampling_ratio))
+        p.wavenumber = self.wavenumber
+        p.transparent_bc = int(self.transparent_bc)
+        p.absorber_width, p.absorber_damping = self.absorber_width, self.absorber_damping
+        p.save_every, p.device = self.save_every, self.device
+        return p
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Solver:
+    """One propagation problem resident on the GPU (a C-ABI handle)."""
+
+    def __init__(self, spec: ProblemSpec):
+        self.spec = spec
+        self._h = C.c_void_p()
+        L = _capi.lib()
+        _capi.check(L.pxp_solver_create(C.byref(spec.to_c()), C.byref(self._h)))
+        nx, ny, nz = C.c_uint(), C.c_uint(), C.c_uint()
+        L.pxp_shape(self._h, C.byref(nx), C.byref(ny), C.byref(nz))
+        self.nx, self.ny, self.nz = nx.value, ny.value, nz.value
+        self.three_d = spec.kind in (FFT_SOLVER_3D, ADI)
+
+    # -- lifetime
+    def close(self) -> None:
+        if self._h:
+            _capi.lib().pxp_solver_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status: int) -> None:
+        _capi.check(status, self._h)
+
+    @property
+    def name(self) -> str:
+        return KIND_NAMES[self.spec.kind]
+
+    @property
+    def shape(self):
+        return (self.ny, self.nx) if self.three_d else (self.nx,)
+
+    # -- material hook
+    def set_material_table(self, delta: np.ndarray, beta: np.ndarray) -> None:
+        d = np.ascontiguousarray(np.asarray(delta, dtype=np.float64).reshape(-1, order="F"))
+        b = np.ascontiguousarray(np.asarray(beta, dtype=np.float64).reshape(-1, order="F"))
+        self._check(_capi.lib().pxp_set_material_table(self._h, _dptr(d), _dptr(b), d.size))
+
+    def set_material_planes(self, delta: np.ndarray, beta: np.ndarray, first_step: int,
+                            nsteps: int) -> None:
+        d = np.ascontiguousarray(delta, dtype=np.float64)
+        b = np.ascontiguousarray(beta, dtype=np.float64)
+        self._check(_capi.lib().pxp_set_material_planes(self._h, _dptr(d), _dptr(b),
+                                                        int(first_step), int(nsteps)))
+
+    def set_material_spheres(self, spheres: Sequence[Sphere]) -> None:
+        arr = (_capi.SphereC * max(len(spheres), 1))()
+        for i, s in enumerate(spheres):
+            arr[i] = _capi.SphereC(s.cx, s.cy, s.cz, s.radius, s.delta, s.beta)
+        self._check(_capi.lib().pxp_set_material_spheres(self._h, arr, len(spheres)))
+
+    # -- field
+    def set_initial_conditions(self, field0: np.ndarray) -> None:
+        a = np.asarray(field0, dtype=np.complex128)
+        if a.shape != self.shape:
+            raise ValueError(f"initial field shape {a.shape} != {self.shape}")
+        flat = np.ascontiguousarray(a.reshape(-1, order="F"))
+        self._check(_capi.lib().pxp_set_initial_conditions(self._h, _dptr(flat.view(np.float64))))
+
+    def set_initial_conditions_device(self, ptr: int) -> None:
+        self._check(_capi.lib().pxp_set_initial_conditions_device(self._h, C.c_void_p(ptr)))
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(_capi.lib().pxp_step(self._h, int(nsteps)))
+
+    def solve(self) -> None:
+        self._check(_capi.lib().pxp_solve(self._h))
+
+    def synchronize(self) -> None:
+        self._check(_capi.lib().pxp_synchronize(self._h))
+
+    def _unflatten(self, flat: np.ndarray) -> np.ndarray:
+        if self.three_d:
+            return flat.reshape((self.ny, self.nx), order="F")
+        return flat
+
+    def get_last_solution(self) -> np.ndarray:
+        out = np.empty(self.nx * self.ny, dtype=np.complex128)
+        self._check(_capi.lib().pxp_get_last_solution(self._h, _dptr(out.view(np.float64))))
+        return self._unflatten(out)
+
+    def field_device_ptr(self) -> int:
+        p = C.c_void_p()
+        prec = C.c_int()
+        self._check(_capi.lib().pxp_get_field_device(self._h, C.byref(p), C.byref(prec)))
+        return p.value
+
+    def num_saved(self) -> int:
+        c = C.c_int()
+        self._check(_capi.lib().pxp_num_saved(self._h, C.byref(c)))
+        return c.value
+
+    def get_saved(self, slot: int) -> np.ndarray:
+        out = np.empty(self.nx * self.ny, dtype=np.complex128)
+        self._check(_capi.lib().pxp_get_saved(self._h, int(slot), _dptr(out.view(np.float64))))
+        return self._unflatten(out)
+
+    def reset(self) -> None:
+        self._check(_capi.lib().pxp_reset(self._h))
+
+    @property
+    def current_step(self) -> int:
+        s = C.c_uint()
+        self._check(_capi.lib().pxp_current_step(self._h, C.byref(s)))
+        return s.value
+
+
+__all__ = ["Solver", "ProblemSpec", "Disc", "Sphere", "node_count", "PxpError",
+           "FFT_SOLVER_2D", "CRANK_NICHOLSON", "FFT_SOLVER_3D", "ADI", "FP64", "FP32"]

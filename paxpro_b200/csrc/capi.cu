@@ -1,0 +1,584 @@
+// capi.cu -- the C ABI (include/paxpro_b200.h): solver handles, device state,
+// host-side FP64 tables and kernel launches.
+//
+// A handle owns one CUDA stream, the resident field, the per-solver tables
+// and the save slots.  Nothing here throws across the ABI: every entry point
+// catches, records a message on the handle and returns a status.
+//
+// Host tables that the reference evaluates with std::complex (the FFTSolver2D
+// propagator, src/fftSolver2D.cpp:15-19, and the transmission factor,
+// src/fftSolver2D.cpp:46-48) are built here with the same std::complex
+// expressions (this file's host code is compiled with -ffp-contract=off), so
+// the FP64 device path multiplies by exactly the reference's values.  FP32
+// served mode rounds the FP64 values (phase reduced in FP64) to complex64.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/paxpro_b200.h"
+#include "pxp_kernels.h"
+
+using cd = std::complex<double>;
+
+namespace {
+
+const double PI = std::acos(-1.0);
+std::mutex g_err_mutex;
+std::string g_last_error;
+
+void set_global_error(const std::string &m) {
+  std::lock_guard<std::mutex> lk(g_err_mutex);
+  g_last_error = m;
+}
+
+bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
+
+}  // namespace
+
+struct pxp_solver_s {
+  pxp_problem prob{};
+  unsigned nx = 0, ny = 1, nz = 0;
+  long long npts = 0;
+  pxp::Precision prec = pxp::kFP64;
+  size_t csize = 16;
+  cudaStream_t stream = nullptr;
+  // resident state
+  void *d_field = nullptr;
+  void *d_saves = nullptr;
+  int max_slots = 0;
+  int save_every = 0;
+  // FFT 1-D tables
+  void *d_kern = nullptr, *d_trans = nullptr, *d_tw = nullptr;
+  long long trans_stride = 0;
+  int trans_step0 = 1;
+  // CN material planes (FP64)
+  double *d_mat = nullptr;  // [delta | beta | delta_prev | beta_prev] planes
+  long long mat_block = 0;  // doubles per block of d_mat
+  long long mat_stride = 0;
+  int mat_step0 = 1;
+  // job descriptors in device memory
+  void *d_job = nullptr;
+  // host copies
+  std::vector<double> h_delta, h_beta;
+  int plane_first = 1, plane_count = 0;  // per-step material planes (0 = z-invariant)
+  bool material_set = false;
+  bool ic_set = false;
+  unsigned current_step = 1;
+  std::string err;
+
+  int fail(int code, const std::string &m) {
+    err = m;
+    set_global_error(m);
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char *what) {
+    return fail(PXP_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+};
+
+namespace {
+
+#define PXP_TRY_CUDA(h, expr)                        \
+  do {                                               \
+    cudaError_t e_ = (expr);                         \
+    if (e_ != cudaSuccess) return (h)->cuda_fail(e_, #expr); \
+  } while (0)
+
+template <typename T> void free_dev(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+// Twiddles exp(-2 pi i m / n), m < n, in extended precision.
+std::vector<cd> twiddles(int n) {
+  std::vector<cd> w(n);
+  const long double pi_l = 3.141592653589793238462643383279502884L;
+  for (int m = 0; m < n; ++m) {
+    long double a = -2.0L * pi_l * (long double)m / (long double)n;
+    w[m] = cd((double)cosl(a), (double)sinl(a));
+  }
+  return w;
+}
+
+// FFTSolver2D::spatialFreq (src/fftSolver2D.cpp:52-59).
+double spatial_freq(unsigned indx, unsigned size, double step) {
+  if (indx > size / 2) indx = size - indx;
+  return 2.0 * PI * indx / (step * size);
+}
+
+// FFTSolver2D::kernel (src/fftSolver2D.cpp:15-19).
+cd kernel_2d(double kx, double dz, double k) {
+  cd A(0.0, 0.5 * dz / k);
+  return std::exp(-A * kx * kx);
+}
+
+// Transmission factor of FFTSolver2D::refraction (src/fftSolver2D.cpp:46-48).
+cd transmission(double k, double beta, double delta, double dz) {
+  cd im(0.0, 1.0);
+  return std::exp(-k * (beta + im * delta) * dz);
+}
+
+// Upload complex128 host values in the solver's precision.
+int upload_complex(pxp_solver_s *h, void *dst, const cd *src, long long n) {
+  if (h->prec == pxp::kFP64) {
+    PXP_TRY_CUDA(h, cudaMemcpy(dst, src, sizeof(cd) * n, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> tmp(2 * n);
+    for (long long i = 0; i < n; ++i) {
+      tmp[2 * i] = (float)src[i].real();
+      tmp[2 * i + 1] = (float)src[i].imag();
+    }
+    PXP_TRY_CUDA(h, cudaMemcpy(dst, tmp.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice));
+  }
+  return PXP_OK;
+}
+
+int alloc(pxp_solver_s *h, void **p, size_t bytes, const char *what) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return h->fail(e == cudaErrorMemoryAllocation ? PXP_ERR_NOMEM : PXP_ERR_CUDA,
+                   std::string("allocating ") + what + ": " + cudaGetErrorString(e));
+  }
+  return PXP_OK;
+}
+
+// ---- FFT 1-D -------------------------------------------------------------
+int fft1d_setup(pxp_solver_s *h) {
+  const unsigned n = h->nx;
+  std::vector<cd> ker(n);
+  for (unsigned i = 0; i < n; ++i)
+    ker[i] = kernel_2d(spatial_freq(i, n, h->prob.x.step), h->prob.z.step, h->prob.wavenumber);
+  int rc;
+  if ((rc = alloc(h, &h->d_kern, h->csize * n, "propagator table"))) return rc;
+  if ((rc = upload_complex(h, h->d_kern, ker.data(), n))) return rc;
+  std::vector<cd> tw = twiddles((int)n);
+  if ((rc = alloc(h, &h->d_tw, h->csize * n, "twiddle table"))) return rc;
+  if ((rc = upload_complex(h, h->d_tw, tw.data(), n))) return rc;
+  return alloc(h, &h->d_job, sizeof(pxp::Fft1dJob), "job descriptor");
+}
+
+// Transmission tables t (FP64) or t/N (FP32) from delta/beta planes.
+int fft1d_set_trans(pxp_solver_s *h, const double *delta, const double *beta, int nplanes,
+                    int first_step) {
+  const unsigned n = h->nx;
+  std::vector<cd> t((size_t)n * nplanes);
+  const double k = h->prob.wavenumber, dz = h->prob.z.step;
+  for (int p = 0; p < nplanes; ++p)
+    for (unsigned i = 0; i < n; ++i) {
+      size_t j = (size_t)p * n + i;
+      cd v = transmission(k, beta[j], delta[j], dz);
+      if (h->prec == pxp::kFP32) v = v / (double)n;
+      t[j] = v;
+    }
+  free_dev(h->d_trans);
+  int rc;
+  if ((rc = alloc(h, &h->d_trans, h->csize * t.size(), "transmission table"))) return rc;
+  if ((rc = upload_complex(h, h->d_trans, t.data(), (long long)t.size()))) return rc;
+  h->trans_stride = nplanes > 1 ? n : 0;
+  h->trans_step0 = first_step;
+  h->material_set = true;
+  return PXP_OK;
+}
+
+int fft1d_write_job(pxp_solver_s *h) {
+  pxp::Fft1dJob j{};
+  j.field = h->d_field;
+  j.kern = h->d_kern;
+  j.trans = h->d_trans;
+  j.trans_stride = h->trans_stride;
+  j.twiddle = h->d_tw;
+  j.saves = h->d_saves;
+  j.n = (int)h->nx;
+  j.save_every = h->save_every;
+  j.max_slots = h->max_slots;
+  j.trans_step0 = h->trans_step0;
+  PXP_TRY_CUDA(h, cudaMemcpy(h->d_job, &j, sizeof(j), cudaMemcpyHostToDevice));
+  return PXP_OK;
+}
+
+// ---- CN --------------------------------------------------------------------
+int cn_set_planes(pxp_solver_s *h, const double *delta, const double *beta, int nsteps,
+                  int first_step, bool two_planes_per_step) {
+  // Device layout: 4 blocks [delta | beta | delta_prev | beta_prev], each
+  // nsteps * n doubles; per-step stride n.
+  const unsigned n = h->nx;
+  const size_t per = (size_t)n * nsteps;
+  std::vector<double> buf(4 * per);
+  for (int s = 0; s < nsteps; ++s) {
+    const size_t src0 = (size_t)(two_planes_per_step ? 2 * s : s) * n;
+    const size_t src1 = (size_t)(two_planes_per_step ? 2 * s + 1 : s) * n;
+    std::memcpy(&buf[0 * per + (size_t)s * n], delta + src0, sizeof(double) * n);
+    std::memcpy(&buf[1 * per + (size_t)s * n], beta + src0, sizeof(double) * n);
+    std::memcpy(&buf[2 * per + (size_t)s * n], delta + src1, sizeof(double) * n);
+    std::memcpy(&buf[3 * per + (size_t)s * n], beta + src1, sizeof(double) * n);
+  }
+  free_dev(h->d_mat);
+  int rc;
+  if ((rc = alloc(h, (void **)&h->d_mat, sizeof(double) * buf.size(), "material planes")))
+    return rc;
+  PXP_TRY_CUDA(h, cudaMemcpy(h->d_mat, buf.data(), sizeof(double) * buf.size(),
+                             cudaMemcpyHostToDevice));
+  h->mat_block = (long long)per;
+  h->mat_stride = nsteps > 1 ? n : 0;
+  h->mat_step0 = first_step;
+  h->material_set = true;
+  return PXP_OK;
+}
+
+int cn_write_job(pxp_solver_s *h) {
+  pxp::CnJob j{};
+  const unsigned n = h->nx;
+  const double dx = h->prob.x.step, dz = h->prob.z.step, k = h->prob.wavenumber;
+  j.field = h->d_field;
+  j.delta = h->d_mat;
+  j.beta = h->d_mat + h->mat_block;
+  j.delta_prev = h->d_mat + 2 * h->mat_block;
+  j.beta_prev = h->d_mat + 3 * h->mat_block;
+  j.mat_stride = h->mat_stride;
+  j.saves = h->d_saves;
+  j.rho = dz / (k * dx * dx);  // CrankNicholson::solveStep (src/crancNicholson.cpp:25-26)
+  j.r = k * dz;
+  j.n = (int)n;
+  j.save_every = h->save_every;
+  j.max_slots = h->max_slots;
+  j.mat_step0 = h->mat_step0;
+  j.transparent = h->prob.transparent_bc ? 1 : 0;
+  PXP_TRY_CUDA(h, cudaMemcpy(h->d_job, &j, sizeof(j), cudaMemcpyHostToDevice));
+  return PXP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+unsigned pxp_node_count(double mn, double mx, double step) {
+  return (unsigned)((mx - mn) / step + 1.0);
+}
+
+const char *pxp_status_string(int status) {
+  switch (status) {
+    case PXP_OK: return "ok";
+    case PXP_ERR_INVALID: return "invalid argument";
+    case PXP_ERR_NOMEM: return "out of memory";
+    case PXP_ERR_CUDA: return "CUDA error";
+    case PXP_ERR_ABORTED: return "aborted";
+    case PXP_ERR_BUDGET: return "step or wait budget exceeded";
+    case PXP_ERR_NOT_READY: return "not ready";
+    case PXP_ERR_UNSUPPORTED: return "unsupported size or precision";
+    default: return "unknown status";
+  }
+}
+
+const char *pxp_build_info(void) { return "paxpro_b200 sm_100a"; }
+
+int pxp_last_error(pxp_solver s, char *buf, size_t len) {
+  if (buf == nullptr || len == 0) return PXP_ERR_INVALID;
+  std::string m;
+  if (s) {
+    m = s->err;
+  } else {
+    std::lock_guard<std::mutex> lk(g_err_mutex);
+    m = g_last_error;
+  }
+  std::snprintf(buf, len, "%s", m.c_str());
+  return PXP_OK;
+}
+
+int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
+  if (problem == nullptr || out == nullptr) {
+    set_global_error("pxp_solver_create: null argument");
+    return PXP_ERR_INVALID;
+  }
+  *out = nullptr;
+  pxp_solver_s *h = new (std::nothrow) pxp_solver_s();
+  if (h == nullptr) return PXP_ERR_NOMEM;
+  h->prob = *problem;
+  const pxp_problem &p = h->prob;
+  auto bad = [&](const std::string &m) {
+    set_global_error(m);
+    delete h;
+    return PXP_ERR_INVALID;
+  };
+  if (p.kind < PXP_FFT_SOLVER_2D || p.kind > PXP_ADI) return bad("unknown solver kind");
+  if (p.precision != PXP_FP64 && p.precision != PXP_FP32) return bad("unknown precision");
+  if (!(p.x.step > 0.0) || !(p.z.step > 0.0) || !(p.wavenumber > 0.0))
+    return bad("discretisation steps and wavenumber must be positive");
+  const bool three_d = p.kind == PXP_FFT_SOLVER_3D || p.kind == PXP_ADI;
+  if (three_d && !(p.y.step > 0.0)) return bad("vertical step must be positive");
+  h->nx = pxp_node_count(p.x.min, p.x.max, p.x.step);
+  h->nz = pxp_node_count(p.z.min, p.z.max, p.z.step);
+  h->ny = three_d ? h->nx : 1;  // Solver3D::setSimulator forces Ny = Nx (src/solver3D.cpp:24)
+  h->npts = (long long)h->nx * h->ny;
+  h->prec = p.precision == PXP_FP64 ? pxp::kFP64 : pxp::kFP32;
+  h->csize = h->prec == pxp::kFP64 ? 16 : 8;
+  if (h->nx < 4 || h->nz < 2) return bad("grid too small (need Nx >= 4, Nz >= 2)");
+  bool supported = false;
+  switch (p.kind) {
+    case PXP_FFT_SOLVER_2D: supported = pxp::fft1d_supported(h->prec, (int)h->nx); break;
+    case PXP_CRANK_NICHOLSON: supported = pxp::cn_supported(h->prec, (int)h->nx); break;
+    default: supported = false;
+  }
+  if (!supported) {
+    set_global_error("solver kind / size / precision not supported by this build (Nx=" +
+                     std::to_string(h->nx) + ")");
+    delete h;
+    return PXP_ERR_UNSUPPORTED;
+  }
+  cudaError_t e = cudaSetDevice(p.device);
+  if (e == cudaSuccess) e = cudaStreamCreate(&h->stream);
+  if (e != cudaSuccess) {
+    set_global_error(std::string("CUDA initialisation: ") + cudaGetErrorString(e));
+    delete h;
+    return PXP_ERR_CUDA;
+  }
+  int rc = PXP_OK;
+  auto cleanup_fail = [&](int code) {
+    std::string m = h->err;
+    pxp_solver_destroy(h);
+    set_global_error(m);
+    return code;
+  };
+  if ((rc = alloc(h, &h->d_field, h->csize * h->npts, "field"))) return cleanup_fail(rc);
+  PXP_TRY_CUDA(h, cudaMemset(h->d_field, 0, h->csize * h->npts));
+  h->save_every = p.save_every > 0 ? p.save_every : 0;
+  if (h->save_every) {
+    h->max_slots = (int)((h->nz - 1) / (unsigned)h->save_every);
+    if (h->max_slots > 0 &&
+        (rc = alloc(h, &h->d_saves, h->csize * h->npts * (size_t)h->max_slots, "save slots")))
+      return cleanup_fail(rc);
+  }
+  std::vector<double> zeros(h->npts, 0.0);
+  switch (p.kind) {
+    case PXP_FFT_SOLVER_2D:
+      if ((rc = fft1d_setup(h))) return cleanup_fail(rc);
+      if ((rc = fft1d_set_trans(h, zeros.data(), zeros.data(), 1, 1))) return cleanup_fail(rc);
+      if ((rc = fft1d_write_job(h))) return cleanup_fail(rc);
+      break;
+    case PXP_CRANK_NICHOLSON:
+      if ((rc = alloc(h, &h->d_job, sizeof(pxp::CnJob), "job descriptor"))) return cleanup_fail(rc);
+      if ((rc = cn_set_planes(h, zeros.data(), zeros.data(), 1, 1, false))) return cleanup_fail(rc);
+      if ((rc = cn_write_job(h))) return cleanup_fail(rc);
+      break;
+  }
+  *out = h;
+  return PXP_OK;
+}
+
+int pxp_solver_destroy(pxp_solver h) {
+  if (h == nullptr) return PXP_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_dev(h->d_field);
+  free_dev(h->d_saves);
+  free_dev(h->d_kern);
+  free_dev(h->d_trans);
+  free_dev(h->d_tw);
+  free_dev(h->d_mat);
+  free_dev(h->d_job);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return PXP_OK;
+}
+
+static int rewrite_job(pxp_solver_s *h) {
+  switch (h->prob.kind) {
+    case PXP_FFT_SOLVER_2D: return fft1d_write_job(h);
+    case PXP_CRANK_NICHOLSON: return cn_write_job(h);
+    default: return PXP_OK;
+  }
+}
+
+int pxp_set_material_table(pxp_solver h, const double *delta, const double *beta, size_t n) {
+  if (h == nullptr || delta == nullptr || beta == nullptr) return PXP_ERR_INVALID;
+  if (n != (size_t)h->npts)
+    return h->fail(PXP_ERR_INVALID, "material table length " + std::to_string(n) +
+                                        " != grid points " + std::to_string(h->npts));
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  int rc;
+  switch (h->prob.kind) {
+    case PXP_FFT_SOLVER_2D:
+      if ((rc = fft1d_set_trans(h, delta, beta, 1, 1))) return rc;
+      break;
+    case PXP_CRANK_NICHOLSON:
+      if ((rc = cn_set_planes(h, delta, beta, 1, 1, false))) return rc;
+      break;
+    default:
+      return h->fail(PXP_ERR_UNSUPPORTED, "material tables not supported for this kind");
+  }
+  h->h_delta.assign(delta, delta + n);
+  h->h_beta.assign(beta, beta + n);
+  h->plane_count = 0;
+  return rewrite_job(h);
+}
+
+int pxp_set_material_planes(pxp_solver h, const double *delta, const double *beta,
+                            int first_step, int nsteps) {
+  if (h == nullptr || delta == nullptr || beta == nullptr || nsteps <= 0 || first_step < 1)
+    return PXP_ERR_INVALID;
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  int rc;
+  switch (h->prob.kind) {
+    case PXP_FFT_SOLVER_2D:
+      if ((rc = fft1d_set_trans(h, delta, beta, nsteps, first_step))) return rc;
+      if (nsteps == 1) h->trans_stride = 0;
+      break;
+    case PXP_CRANK_NICHOLSON:
+      if ((rc = cn_set_planes(h, delta, beta, nsteps, first_step, true))) return rc;
+      break;
+    default:
+      return h->fail(PXP_ERR_UNSUPPORTED, "material planes apply to the 2-D kinds");
+  }
+  h->plane_first = first_step;
+  h->plane_count = nsteps;
+  return rewrite_job(h);
+}
+
+int pxp_set_material_spheres(pxp_solver h, const pxp_sphere *spheres, int n) {
+  if (h == nullptr || (n > 0 && spheres == nullptr) || n < 0) return PXP_ERR_INVALID;
+  return h->fail(PXP_ERR_UNSUPPORTED, "sphere materials are not supported for this kind");
+}
+
+static int upload_field(pxp_solver_s *h, void *dst, const double *src) {
+  if (h->prec == pxp::kFP64) {
+    PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, 16 * h->npts, cudaMemcpyHostToDevice, h->stream));
+  } else {
+    std::vector<float> tmp(2 * h->npts);
+    for (long long i = 0; i < 2 * h->npts; ++i) tmp[i] = (float)src[i];
+    PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, tmp.data(), 8 * h->npts, cudaMemcpyHostToDevice, h->stream));
+    PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  }
+  return PXP_OK;
+}
+
+static int download_field(pxp_solver_s *h, double *dst, const void *src) {
+  if (h->prec == pxp::kFP64) {
+    PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, 16 * h->npts, cudaMemcpyDeviceToHost, h->stream));
+    PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  } else {
+    std::vector<float> tmp(2 * h->npts);
+    PXP_TRY_CUDA(h, cudaMemcpyAsync(tmp.data(), src, 8 * h->npts, cudaMemcpyDeviceToHost, h->stream));
+    PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (long long i = 0; i < 2 * h->npts; ++i) dst[i] = (double)tmp[i];
+  }
+  return PXP_OK;
+}
+
+int pxp_set_initial_conditions(pxp_solver h, const double *field) {
+  if (h == nullptr || field == nullptr) return PXP_ERR_INVALID;
+  int rc = upload_field(h, h->d_field, field);
+  if (rc) return rc;
+  h->current_step = 1;
+  h->ic_set = true;
+  return PXP_OK;
+}
+
+int pxp_set_initial_conditions_device(pxp_solver h, const void *dfield) {
+  if (h == nullptr || dfield == nullptr) return PXP_ERR_INVALID;
+  PXP_TRY_CUDA(h, cudaMemcpyAsync(h->d_field, dfield, h->csize * h->npts,
+                                  cudaMemcpyDeviceToDevice, h->stream));
+  h->current_step = 1;
+  h->ic_set = true;
+  return PXP_OK;
+}
+
+int pxp_step(pxp_solver h, int nsteps) {
+  if (h == nullptr) return PXP_ERR_INVALID;
+  if (nsteps < 0) return h->fail(PXP_ERR_INVALID, "negative step count");
+  if (!h->ic_set)
+    return h->fail(PXP_ERR_INVALID, "setInitialConditions must be called before stepping");
+  if (nsteps == 0) return PXP_OK;
+  const long long first = h->current_step, last = first + nsteps - 1;
+  if (h->plane_count > 0 &&
+      (first < h->plane_first || last >= (long long)h->plane_first + h->plane_count))
+    return h->fail(PXP_ERR_INVALID, "steps " + std::to_string(first) + ".." + std::to_string(last) +
+                                        " are outside the material planes provided");
+  cudaError_t e = cudaSuccess;
+  switch (h->prob.kind) {
+    case PXP_FFT_SOLVER_2D:
+      e = pxp::launch_fft1d(h->prec, (const pxp::Fft1dJob *)h->d_job, 1, (int)h->nx,
+                            (int)first, nsteps, h->stream);
+      break;
+    case PXP_CRANK_NICHOLSON:
+      e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first, nsteps,
+                         h->stream);
+      break;
+    default:
+      return h->fail(PXP_ERR_UNSUPPORTED, "kind not available");
+  }
+  if (e != cudaSuccess) return h->cuda_fail(e, "kernel launch");
+  h->current_step += (unsigned)nsteps;
+  return PXP_OK;
+}
+
+int pxp_solve(pxp_solver h) {
+  if (h == nullptr) return PXP_ERR_INVALID;
+  if (h->current_step >= h->nz) return PXP_OK;
+  return pxp_step(h, (int)(h->nz - h->current_step));
+}
+
+int pxp_synchronize(pxp_solver h) {
+  if (h == nullptr) return PXP_ERR_INVALID;
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  return PXP_OK;
+}
+
+int pxp_get_last_solution(pxp_solver h, double *field) {
+  if (h == nullptr || field == nullptr) return PXP_ERR_INVALID;
+  return download_field(h, field, h->d_field);
+}
+
+int pxp_get_field_device(pxp_solver h, void **dfield, int *precision) {
+  if (h == nullptr || dfield == nullptr) return PXP_ERR_INVALID;
+  *dfield = h->d_field;
+  if (precision) *precision = h->prob.precision;
+  return PXP_OK;
+}
+
+int pxp_num_saved(pxp_solver h, int *count) {
+  if (h == nullptr || count == nullptr) return PXP_ERR_INVALID;
+  int c = 0;
+  if (h->save_every > 0 && h->ic_set) c = (int)((h->current_step - 1) / (unsigned)h->save_every);
+  if (c > h->max_slots) c = h->max_slots;
+  *count = c;
+  return PXP_OK;
+}
+
+int pxp_get_saved(pxp_solver h, int slot, double *field) {
+  if (h == nullptr || field == nullptr) return PXP_ERR_INVALID;
+  int c = 0;
+  pxp_num_saved(h, &c);
+  if (slot < 0 || slot >= c)
+    return h->fail(PXP_ERR_INVALID, "save slot " + std::to_string(slot) + " not filled");
+  const char *base = (const char *)h->d_saves + (size_t)slot * h->csize * h->npts;
+  return download_field(h, field, base);
+}
+
+int pxp_reset(pxp_solver h) {
+  if (h == nullptr) return PXP_ERR_INVALID;
+  h->current_step = 1;
+  return PXP_OK;
+}
+
+int pxp_current_step(pxp_solver h, unsigned *step) {
+  if (h == nullptr || step == nullptr) return PXP_ERR_INVALID;
+  *step = h->current_step;
+  return PXP_OK;
+}
+
+int pxp_shape(pxp_solver h, unsigned *nx, unsigned *ny, unsigned *nz) {
+  if (h == nullptr) return PXP_ERR_INVALID;
+  if (nx) *nx = h->nx;
+  if (ny) *ny = h->ny;
+  if (nz) *nz = h->nz;
+  return PXP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,308 @@
+// cn.cu -- K-CN: Crank-Nicolson step with a fused tridiagonal solve.
+//
+// Replaces CrankNicholson::solveStep (src/crancNicholson.cpp:17-105) with the
+// default ParaxialEquation (F = G = H = 1, J = 0, src/paraxialEquation.cpp:
+// 3-21) and ThomasAlgorithm::solve (include/thomasAlgorithm.tpp:2-32).
+//
+// One CTA owns one problem; the field stays in shared memory for every step
+// of the launch.  Per step:
+//   1. each thread builds the matrix rows of its chunk of M consecutive points
+//      (diag, rhs; sub-diagonal constant) with the reference's operation
+//      order, rounded op by op, so the coefficients equal the reference's;
+//   2. each thread eliminates its chunk interior in registers (a partition
+//      method: interior x_i = y_i + p_i x_first + q_i x_last) and writes the
+//      two boundary equations of its chunk into a reduced system of 2T
+//      unknowns;
+//   3. the CTA solves the reduced system by cyclic reduction in shared memory;
+//   4. each thread reconstructs its interior.
+// The solve runs in FP64 in both storage precisions: with rho = dz/(k dx^2)
+// of a few hundred the system is only weakly diagonally dominant.
+// The split into chunks changes the rounding relative to the reference's
+// serial Thomas sweep; the step matrix is well conditioned (Cayley transform,
+// condition ~ rho), so the difference stays near machine precision.
+#include "pxp_complex.cuh"
+#include "pxp_kernels.h"
+
+namespace pxp {
+
+// Coefficients of row i (exact FP64, reference operation order).
+struct CnRow {
+  double2 diag, rhs;
+};
+
+__device__ __forceinline__ double2 cn_diag(double delta, double beta, double rho, double r) {
+  // fval*1.0 + 0.25*(H+ + H-)*g*i*rho + 0.5*(beta*r + i*delta*r)
+  double im_a = __dmul_rn(0.5, rho);              // 0.25*(1+1)*1 = 0.5, *i, *rho
+  double br = __dmul_rn(beta, r);
+  double dr = __dmul_rn(delta, r);
+  double2 t = mk(__dmul_rn(0.5, br), __dmul_rn(0.5, dr));
+  return mk(__dadd_rn(1.0, t.x), __dadd_rn(im_a, t.y));
+}
+
+__device__ __forceinline__ double2 cn_rhs(double2 left, double2 center, double2 right,
+                                          double deltaPrev, double betaPrev, double rho,
+                                          double r) {
+  // rhs = left*H-'*g' + right*H+'*g'; rhs *= 0.25*i*rho
+  double2 s = cx_add_rn(left, right);
+  double q = __dmul_rn(0.25, rho);
+  double2 rhs = cx_mul_rn(s, mk(0.0, q));
+  // rhs -= 0.25*center*i*rho*(H+' + H-')*g
+  double2 c4 = cx_scale_rn(center, 0.25);
+  double2 t = cx_mul_rn(c4, mk(0.0, 1.0));
+  t = cx_scale_rn(t, rho);
+  t = cx_scale_rn(t, 2.0);
+  rhs = cx_sub_rn(rhs, t);
+  // rhs += (1.0*f' - 0.5*(beta'*r + i*delta'*r)) * center
+  double2 h = mk(__dmul_rn(0.5, __dmul_rn(betaPrev, r)), __dmul_rn(0.5, __dmul_rn(deltaPrev, r)));
+  // libstdc++ evaluates (double - complex) as (-y) + x
+  double2 coef = mk(__dadd_rn(-h.x, 1.0), -h.y);
+  return cx_add_rn(rhs, cx_mul_rn(coef, center));
+}
+
+// Transparent boundary (CrankNicholson::applyTBCOneSide,
+// src/crancNicholson.cpp:136-148) with H- = g = 1.
+__device__ __forceinline__ void cn_tbc(double2 outer, double2 inner, double rho, double2 &diag,
+                                       double2 &rhs) {
+  double2 ratio = cx_div_rn(outer, inner);
+  double lr = log(hypot(ratio.x, ratio.y));
+  double ar = atan2(ratio.y, ratio.x);
+  double2 kdx = cx_div_rn(mk(lr, ar), mk(0.0, 1.0));
+  if (kdx.x < 0.0) kdx.x = 0.0;
+  double2 ik = cx_mul_rn(mk(0.0, 1.0), kdx);
+  double e = exp(ik.x);
+  double sn, cs;
+  sincos(ik.y, &sn, &cs);
+  double2 ex = mk(e * cs, e * sn);
+  double2 coef = cx_mul_rn(mk(0.0, __dmul_rn(0.25, rho)), ex);
+  diag = cx_sub_rn(diag, coef);
+  rhs = cx_add_rn(rhs, cx_mul_rn(coef, outer));
+}
+
+// Cyclic reduction on n = 2^L equations held in shared memory
+// (a = coupling to x_{i-1}, b = diagonal, c = coupling to x_{i+1}, d = rhs);
+// the solution overwrites d.  T threads.
+template <int T>
+__device__ void cyclic_reduction(double2 *a, double2 *b, double2 *c, double2 *d, int n) {
+  const int tid = threadIdx.x;
+  int s = 1;
+  for (; 4 * s <= n; s <<= 1) {
+    const int cnt = n / (2 * s);
+    for (int k = tid; k < cnt; k += T) {
+      int i = 2 * s * k + 2 * s - 1;
+      int il = i - s, ir = i + s;
+      double2 k1 = cx_div_rn(a[i], b[il]);
+      double2 ai = cx_sub_rn(mk(0.0, 0.0), cx_mul_rn(a[il], k1));
+      double2 bi = cx_sub_rn(b[i], cx_mul_rn(c[il], k1));
+      double2 di = cx_sub_rn(d[i], cx_mul_rn(d[il], k1));
+      double2 ci = mk(0.0, 0.0);
+      if (ir < n) {
+        double2 k2 = cx_div_rn(c[i], b[ir]);
+        ci = cx_sub_rn(mk(0.0, 0.0), cx_mul_rn(c[ir], k2));
+        bi = cx_sub_rn(bi, cx_mul_rn(a[ir], k2));
+        di = cx_sub_rn(di, cx_mul_rn(d[ir], k2));
+      }
+      a[i] = ai;
+      b[i] = bi;
+      c[i] = ci;
+      d[i] = di;
+    }
+    __syncthreads();
+  }
+  // two remaining unknowns: i1 = n/2 - 1, i2 = n - 1
+  if (tid == 0) {
+    int i1 = n / 2 - 1, i2 = n - 1;
+    double2 det = cx_sub_rn(cx_mul_rn(b[i1], b[i2]), cx_mul_rn(c[i1], a[i2]));
+    double2 x1 = cx_div_rn(cx_sub_rn(cx_mul_rn(b[i2], d[i1]), cx_mul_rn(c[i1], d[i2])), det);
+    double2 x2 = cx_div_rn(cx_sub_rn(cx_mul_rn(b[i1], d[i2]), cx_mul_rn(a[i2], d[i1])), det);
+    d[i1] = x1;
+    d[i2] = x2;
+  }
+  __syncthreads();
+  for (s >>= 1; s >= 1; s >>= 1) {
+    const int cnt = n / (2 * s);
+    for (int k = tid; k < cnt; k += T) {
+      int i = 2 * s * k + s - 1;
+      double2 acc = d[i];
+      if (i - s >= 0) acc = cx_sub_rn(acc, cx_mul_rn(a[i], d[i - s]));
+      if (i + s < n) acc = cx_sub_rn(acc, cx_mul_rn(c[i], d[i + s]));
+      d[i] = cx_div_rn(acc, b[i]);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename R, int M, int T>
+__global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, int step0_ov,
+                                              int nsteps_ov) {
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CnJob job = jobs[blockIdx.x];
+  if (nsteps_ov >= 0) {
+    job.step0 = step0_ov;
+    job.nsteps = nsteps_ov;
+  }
+  const int n = job.n;  // == M * T
+  const int nr = 2 * T;
+  double2 *ra = reinterpret_cast<double2 *>(smem_raw);
+  double2 *rb = ra + nr;
+  double2 *rc = rb + nr;
+  double2 *rd = rc + nr;
+  C *u = reinterpret_cast<C *>(rd + nr);
+  const int t = threadIdx.x;
+  C *field = reinterpret_cast<C *>(job.field);
+  for (int i = t; i < n; i += T) u[i] = field[i];
+  __syncthreads();
+  const double rho = job.rho, r = job.r;
+  const double2 sub = mk(-0.0, __dmul_rn(-0.25, rho));  // -0.25*i*rho*H-*g
+  C *saves = reinterpret_cast<C *>(job.saves);
+  const int s0 = t * M;
+
+  for (int st = 0; st < job.nsteps; ++st) {
+    const int step = job.step0 + st;
+    const long long moff = job.mat_stride * (long long)(step - job.mat_step0);
+    // ---- 1. rows of this chunk
+    double2 dg[M], rh[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      int i = s0 + m;
+      double2 center = to_d(u[i]);
+      double2 left = i > 0 ? to_d(u[i - 1]) : mk(0.0, 0.0);
+      double2 right = i < n - 1 ? to_d(u[i + 1]) : mk(0.0, 0.0);
+      double de = job.delta[moff + i], be = job.beta[moff + i];
+      double dp = job.delta_prev[moff + i], bp = job.beta_prev[moff + i];
+      dg[m] = cn_diag(de, be, rho, r);
+      rh[m] = cn_rhs(left, center, right, dp, bp, rho, r);
+    }
+    if (job.transparent) {
+      const double ZERO = 1e-16;
+      if (t == 0) {
+        double2 o = to_d(u[0]), in = to_d(u[1]);
+        if (hypot(in.x, in.y) > ZERO) cn_tbc(o, in, rho, dg[0], rh[0]);
+      }
+      if (t == T - 1) {
+        double2 o = to_d(u[n - 1]), in = to_d(u[n - 2]);
+        if (hypot(in.x, in.y) > ZERO) cn_tbc(o, in, rho, dg[M - 1], rh[M - 1]);
+      }
+    }
+    // ---- 2. interior elimination (rows 1..M-2 of the chunk), three RHS:
+    // y (rhs), p (coupling to x_first), q (coupling to x_last).
+    double2 y[M > 2 ? M - 2 : 1], p[M > 2 ? M - 2 : 1], q[M > 2 ? M - 2 : 1];
+    double2 ea, eb, ec, ed, fa, fb, fc, fd;  // reduced rows (first, last)
+    if constexpr (M > 2) {
+      double2 cp[M - 2];
+      // forward sweep
+#pragma unroll
+      for (int m = 1; m <= M - 2; ++m) {
+        int j = m - 1;
+        double2 den = dg[m];
+        if (j > 0) den = cx_sub_rn(den, cx_mul_rn(sub, cp[j - 1]));
+        if (m < M - 2) cp[j] = cx_div_rn(sub, den);
+        double2 ry = rh[m];
+        double2 rp = (m == 1) ? cx_sub_rn(mk(0.0, 0.0), sub) : mk(0.0, 0.0);
+        double2 rq = (m == M - 2) ? cx_sub_rn(mk(0.0, 0.0), sub) : mk(0.0, 0.0);
+        if (j > 0) {
+          ry = cx_sub_rn(ry, cx_mul_rn(sub, y[j - 1]));
+          rp = cx_sub_rn(rp, cx_mul_rn(sub, p[j - 1]));
+          rq = cx_sub_rn(rq, cx_mul_rn(sub, q[j - 1]));
+        }
+        y[j] = cx_div_rn(ry, den);
+        p[j] = cx_div_rn(rp, den);
+        q[j] = cx_div_rn(rq, den);
+      }
+      // back substitution
+#pragma unroll
+      for (int j = M - 4; j >= 0; --j) {
+        y[j] = cx_sub_rn(y[j], cx_mul_rn(cp[j], y[j + 1]));
+        p[j] = cx_sub_rn(p[j], cx_mul_rn(cp[j], p[j + 1]));
+        q[j] = cx_sub_rn(q[j], cx_mul_rn(cp[j], q[j + 1]));
+      }
+      // first row: a x_{s-1} + (b + c p_1) x_s + c q_1 x_e = d - c y_1
+      ea = (s0 > 0) ? sub : mk(0.0, 0.0);
+      eb = cx_add_rn(dg[0], cx_mul_rn(sub, p[0]));
+      ec = cx_mul_rn(sub, q[0]);
+      ed = cx_sub_rn(rh[0], cx_mul_rn(sub, y[0]));
+      // last row: a p_{M-2} x_s + (b + a q_{M-2}) x_e + c x_{e+1} = d - a y_{M-2}
+      fa = cx_mul_rn(sub, p[M - 3]);
+      fb = cx_add_rn(dg[M - 1], cx_mul_rn(sub, q[M - 3]));
+      fc = (s0 + M < n) ? sub : mk(0.0, 0.0);
+      fd = cx_sub_rn(rh[M - 1], cx_mul_rn(sub, y[M - 3]));
+    } else {
+      ea = (s0 > 0) ? sub : mk(0.0, 0.0);
+      eb = dg[0];
+      ec = sub;
+      ed = rh[0];
+      fa = sub;
+      fb = dg[M - 1];
+      fc = (s0 + M < n) ? sub : mk(0.0, 0.0);
+      fd = rh[M - 1];
+    }
+    ra[2 * t] = ea; rb[2 * t] = eb; rc[2 * t] = ec; rd[2 * t] = ed;
+    ra[2 * t + 1] = fa; rb[2 * t + 1] = fb; rc[2 * t + 1] = fc; rd[2 * t + 1] = fd;
+    __syncthreads();
+    // ---- 3. reduced system
+    cyclic_reduction<T>(ra, rb, rc, rd, nr);
+    // ---- 4. reconstruct
+    const double2 xf = rd[2 * t], xl = rd[2 * t + 1];
+    const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
+                      (step / job.save_every - 1) < job.max_slots;
+    C *slot = save ? saves + (long long)(step / job.save_every - 1) * n : nullptr;
+    C outv[M];
+    outv[0] = from_d<R>(xf);
+    outv[M - 1] = from_d<R>(xl);
+    if constexpr (M > 2) {
+#pragma unroll
+      for (int j = 0; j < M - 2; ++j)
+        outv[j + 1] = from_d<R>(cx_add_rn(cx_add_rn(y[j], cx_mul_rn(p[j], xf)), cx_mul_rn(q[j], xl)));
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      u[s0 + m] = outv[m];
+      if (save) slot[s0 + m] = outv[m];
+    }
+    __syncthreads();
+  }
+  for (int i = t; i < n; i += T) field[i] = u[i];
+}
+
+static constexpr int kCnM = 8;
+
+template <typename R, int T>
+static cudaError_t cn_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
+                               cudaStream_t s) {
+  using C = typename Cx<R>::T;
+  size_t smem = sizeof(double2) * 4 * 2 * T + sizeof(C) * kCnM * T;
+  auto k = cn_kernel<R, kCnM, T>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);
+  return cudaGetLastError();
+}
+
+bool cn_supported(Precision p, int n) {
+  if (n < 2 * kCnM || (n & (n - 1))) return false;
+  return p == kFP64 ? n <= 4096 : n <= 8192;
+}
+
+cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0, int nsteps,
+                      cudaStream_t s) {
+  if (nj <= 0) return cudaSuccess;
+  const int T = n / kCnM;
+#define PXP_CN(TT)                                                                 \
+  case TT:                                                                         \
+    return p == kFP64 ? cn_launch_t<double, TT>(d_jobs, nj, step0, nsteps, s)      \
+                      : cn_launch_t<float, TT>(d_jobs, nj, step0, nsteps, s);
+  switch (T) {
+    PXP_CN(2) PXP_CN(4) PXP_CN(8) PXP_CN(16) PXP_CN(32) PXP_CN(64) PXP_CN(128) PXP_CN(256)
+    PXP_CN(512)
+    case 1024:
+      if (p == kFP32) return cn_launch_t<float, 1024>(d_jobs, nj, step0, nsteps, s);
+      return cudaErrorInvalidValue;
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef PXP_CN
+}
+
+}  // namespace pxp

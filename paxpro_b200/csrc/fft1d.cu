@@ -1,0 +1,126 @@
+// fft1d.cu -- K-FFT1: fused split-step kernel for one transverse dimension.
+//
+// Replaces FFTSolver2D::solveStep (src/fftSolver2D.cpp:61-73): forward FFT,
+// propagator multiply (:21-34), backward FFT, transmission multiply and 1/N
+// normalisation (:36-50).  One CTA owns one problem and keeps its field in
+// shared memory for all steps of the launch, so HBM sees the field once per
+// launch plus the save slots; the only per-step global reads are the
+// propagator and transmission tables, which stay in L2.
+//
+// FP64 mode reproduces the reference's pointwise arithmetic exactly:
+// curr *= kernel is a rounded complex product and the refraction update is
+// (prev * t) / N with t taken from a host table built with std::exp, as the
+// reference evaluates it.  FP32 mode multiplies by a table holding t/N.
+#include "fft_smem.cuh"
+#include "pxp_kernels.h"
+
+namespace pxp {
+
+template <typename R> __device__ __forceinline__ void refract(typename Cx<R>::T &u,
+                                                              typename Cx<R>::T t, R n);
+template <> __device__ __forceinline__ void refract<double>(double2 &u, double2 t, double n) {
+  u = cx_div_real_rn(cx_mul_rn(u, t), n);
+}
+template <> __device__ __forceinline__ void refract<float>(float2 &u, float2 t, float) {
+  u = cmul(u, t);
+}
+template <typename R> __device__ __forceinline__ typename Cx<R>::T kmul(typename Cx<R>::T u,
+                                                                       typename Cx<R>::T k);
+template <> __device__ __forceinline__ double2 kmul<double>(double2 u, double2 k) {
+  return cx_mul_rn(u, k);
+}
+template <> __device__ __forceinline__ float2 kmul<float>(float2 u, float2 k) { return cmul(u, k); }
+
+template <typename R, int N, int T, bool TW_SMEM>
+__global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ jobs, int step0_ov,
+                                                 int nsteps_ov) {
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *u = reinterpret_cast<C *>(smem_raw);
+  Fft1dJob job = jobs[blockIdx.x];
+  if (nsteps_ov >= 0) {
+    job.step0 = step0_ov;
+    job.nsteps = nsteps_ov;
+  }
+  const int lane = threadIdx.x;
+  const C *gtw = reinterpret_cast<const C *>(job.twiddle);
+  const C *tw = gtw;
+  if constexpr (TW_SMEM) {
+    C *stw = u + N;
+    for (int i = lane; i < N; i += T) stw[i] = gtw[i];
+    tw = stw;
+  }
+  C *field = reinterpret_cast<C *>(job.field);
+  for (int i = lane; i < N; i += T) u[i] = field[i];
+  __syncthreads();
+  const C *kern = reinterpret_cast<const C *>(job.kern);
+  const C *trans0 = reinterpret_cast<const C *>(job.trans);
+  C *saves = reinterpret_cast<C *>(job.saves);
+  const R nreal = (R)N;
+  for (int s = 0; s < job.nsteps; ++s) {
+    const int step = job.step0 + s;
+    fft_smem<C, N, T, -1>(u, tw, lane);
+    for (int i = lane; i < N; i += T) u[i] = kmul<R>(u[i], kern[i]);
+    __syncthreads();
+    fft_smem<C, N, T, +1>(u, tw, lane);
+    const C *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
+    const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
+                      (step / job.save_every - 1) < job.max_slots;
+    C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
+    for (int i = lane; i < N; i += T) {
+      C v = u[i];
+      refract<R>(v, trans[i], nreal);
+      u[i] = v;
+      if (save) slot[i] = v;
+    }
+    __syncthreads();
+  }
+  for (int i = lane; i < N; i += T) field[i] = u[i];
+}
+
+template <typename R> constexpr int fft1d_threads(int n) {
+  return n >= 8192 ? 512 : (n >= 2048 ? 256 : (n >= 512 ? 64 : 32));
+}
+
+template <typename R, int N>
+static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nsteps,
+                            cudaStream_t s) {
+  using C = typename Cx<R>::T;
+  constexpr int T = fft1d_threads<R>(N);
+  constexpr size_t field_bytes = sizeof(C) * N;
+  constexpr bool tw_smem = 2 * field_bytes <= 160 * 1024;
+  constexpr size_t smem = tw_smem ? 2 * field_bytes : field_bytes;
+  auto k = fft1d_kernel<R, N, T, tw_smem>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);
+  return cudaGetLastError();
+}
+
+bool fft1d_supported(Precision p, int n) {
+  if (n < 8 || (n & (n - 1))) return false;
+  return p == kFP64 ? n <= 8192 : n <= 16384;
+}
+
+cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
+                         int nsteps, cudaStream_t s) {
+  if (nj <= 0) return cudaSuccess;
+#define PXP_CASE(NN)                                                              \
+  case NN:                                                                        \
+    return p == kFP64 ? launch_n<double, NN>(d_jobs, nj, step0, nsteps, s)            \
+                      : launch_n<float, NN>(d_jobs, nj, step0, nsteps, s);
+  switch (n) {
+    PXP_CASE(8) PXP_CASE(16) PXP_CASE(32) PXP_CASE(64) PXP_CASE(128) PXP_CASE(256)
+    PXP_CASE(512) PXP_CASE(1024) PXP_CASE(2048) PXP_CASE(4096) PXP_CASE(8192)
+    case 16384:
+      if (p == kFP32) return launch_n<float, 16384>(d_jobs, nj, step0, nsteps, s);
+      return cudaErrorInvalidValue;
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef PXP_CASE
+}
+
+}  // namespace pxp

@@ -1,0 +1,113 @@
+// fft_smem.cuh -- power-of-two complex FFT held in shared memory.
+//
+// Stockham autosort passes, radix 8 while it divides the remaining length,
+// then one radix-4 or radix-2 pass.  Each pass: every thread loads its
+// butterflies' R inputs into registers, the CTA synchronises, then every
+// thread applies twiddles and an R-point DFT and stores in place.  Twiddles
+// come from a table tw[m] = exp(-2 pi i m / N), m < N, computed on the host
+// in extended precision; the inverse transform uses their conjugates.
+// SIGN = -1 is the forward transform exp(-2 pi i jk/N), +1 the backward one,
+// both unnormalised (the FFTW convention the reference relies on,
+// src/fftSolver2D.cpp:68-69).
+#pragma once
+#include "pxp_complex.cuh"
+
+namespace pxp {
+
+// In-register R-point DFT, R in {2, 4, 8}.
+template <int SIGN, typename C>
+__device__ __forceinline__ void dft2(C &a, C &b) {
+  C t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+template <int SIGN, typename C>
+__device__ __forceinline__ void dft4(C &v0, C &v1, C &v2, C &v3) {
+  C a0 = cadd(v0, v2), a1 = csub(v0, v2);
+  C a2 = cadd(v1, v3), a3 = mul_i<SIGN>(csub(v1, v3));
+  v0 = cadd(a0, a2);
+  v2 = csub(a0, a2);
+  v1 = cadd(a1, a3);
+  v3 = csub(a1, a3);
+}
+
+template <int SIGN, typename C>
+__device__ __forceinline__ void dft8(C *v) {
+  using Rt = decltype(v[0].x);
+  const Rt h = (Rt)0.70710678118654752440084436210484903928;  // 1/sqrt(2)
+  C a0 = cadd(v[0], v[4]), b0 = csub(v[0], v[4]);
+  C a1 = cadd(v[1], v[5]), b1 = csub(v[1], v[5]);
+  C a2 = cadd(v[2], v[6]), b2 = csub(v[2], v[6]);
+  C a3 = cadd(v[3], v[7]), b3 = csub(v[3], v[7]);
+  // b_r *= W8^(r) (forward) or its conjugate (inverse)
+  if (SIGN < 0) {
+    b1 = mk((b1.x + b1.y) * h, (b1.y - b1.x) * h);
+    b2 = mk(b2.y, -b2.x);
+    b3 = mk((b3.y - b3.x) * h, -(b3.x + b3.y) * h);
+  } else {
+    b1 = mk((b1.x - b1.y) * h, (b1.x + b1.y) * h);
+    b2 = mk(-b2.y, b2.x);
+    b3 = mk(-(b3.x + b3.y) * h, (b3.x - b3.y) * h);
+  }
+  dft4<SIGN>(a0, a1, a2, a3);
+  dft4<SIGN>(b0, b1, b2, b3);
+  v[0] = a0; v[2] = a1; v[4] = a2; v[6] = a3;
+  v[1] = b0; v[3] = b1; v[5] = b2; v[7] = b3;
+}
+
+template <int R, int SIGN, typename C>
+__device__ __forceinline__ void dft_r(C *v) {
+  if constexpr (R == 2) dft2<SIGN>(v[0], v[1]);
+  else if constexpr (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
+  else dft8<SIGN>(v);
+}
+
+// One Stockham pass over x (length N) with T threads; NS = length of the
+// sub-transforms already done.  `lane` is this thread's index in [0, T).
+template <typename C, int N, int T, int SIGN, int R, int NS>
+__device__ __forceinline__ void stockham_pass(C *x, const C *tw, int lane) {
+  constexpr int NB = N / R;
+  constexpr int PER = (NB + T - 1) / T;
+  C v[PER][R];
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    int j = lane + b * T;
+    if (NB % T == 0 || j < NB) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = x[j + r * NB];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    int j = lane + b * T;
+    if (NB % T == 0 || j < NB) {
+      int k = j & (NS - 1);
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C w = tw[r * k * (N / (NS * R))];
+          v[b][r] = SIGN < 0 ? cmul(v[b][r], w) : cmulc(v[b][r], w);
+        }
+      }
+      dft_r<R, SIGN>(v[b]);
+      int base = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[base + r * NS] = v[b][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <typename C, int N, int T, int SIGN, int NS = 1>
+__device__ __forceinline__ void fft_smem(C *x, const C *tw, int lane) {
+  if constexpr (NS < N) {
+    constexpr int REM = N / NS;
+    constexpr int R = REM >= 8 ? 8 : REM;
+    stockham_pass<C, N, T, SIGN, R, NS>(x, tw, lane);
+    fft_smem<C, N, T, SIGN, NS * R>(x, tw, lane);
+  }
+}
+
+}  // namespace pxp

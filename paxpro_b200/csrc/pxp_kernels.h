@@ -1,0 +1,56 @@
+// pxp_kernels.h -- host-side launch interface of the CUDA kernels.
+// Plain structs of device pointers; shared by the C-ABI layer (capi.cu) and
+// the kernel translation units.  No torch types anywhere.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace pxp {
+
+enum Precision { kFP64 = 0, kFP32 = 1 };
+
+// ---------------------------------------------------------------- FFT 1-D --
+// One split-step problem with one transverse dimension (FFTSolver2D).
+// All complex arrays are interleaved and in the solver's precision.
+struct Fft1dJob {
+  void *field;             // N complex: field after the previous step
+  const void *kern;        // N complex: propagator exp(-i (dz/2k) kx^2)
+  const void *trans;       // N complex per table: transmission (FP64: t,
+                           // applied as (u*t)/N; FP32: t/N, applied as u*t)
+  long long trans_stride;  // complex elements between per-step tables; 0 =
+                           // z-invariant medium (one table)
+  const void *twiddle;     // N complex: exp(-2 pi i m/N)
+  void *saves;             // save slots, N complex each (may be null)
+  int n;                   // transverse points (power of two)
+  int step0;               // 1-based index of the first step of this launch
+  int nsteps;              // steps to take
+  int save_every;          // save when step % save_every == 0 (0 = never)
+  int max_slots;           // capacity of saves
+  int trans_step0;         // step that per-step table 0 belongs to
+};
+
+// Launch nj jobs that all share one transform length n (one CTA per job).
+// step0/nsteps >= 0 override every job's own values (single-problem use).
+cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n,
+                         int step0, int nsteps, cudaStream_t s);
+bool fft1d_supported(Precision p, int n);
+
+// ------------------------------------------------------------ CN 1-D ------
+// Crank-Nicolson problem (CrankNicholson with default F=G=H=1, J=0).
+struct CnJob {
+  void *field;                 // N complex (solver precision)
+  const double *delta, *beta;  // material at z (per x), FP64
+  const double *delta_prev, *beta_prev;  // material at z - dz
+  long long mat_stride;        // doubles between per-step planes (0 = z-invariant)
+  void *saves;
+  double rho, r;               // dz/(k dx^2), k dz
+  int n;
+  int step0, nsteps, save_every, max_slots, mat_step0;
+  int transparent;             // BC_t::TRANSPARENT
+  int status;                  // unused (reserved)
+};
+cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
+                      int nsteps, cudaStream_t s);
+bool cn_supported(Precision p, int n);
+
+}  // namespace pxp

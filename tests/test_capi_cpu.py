@@ -1,0 +1,41 @@
+"""CPU checks of the drop-in boundary: the in-tree CUDA library loads and
+exports every entry point include/paxpro_b200.h declares.  No compute calls:
+this container has no GPU."""
+import ctypes as C
+import os
+
+from paxpro_b200 import _capi
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(_capi.LIB_PATH)
+    declared = _capi.declared_symbols()
+    assert len(declared) >= 20
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert missing == []
+
+
+def test_every_header_under_include_is_covered():
+    inc = os.path.join(os.path.dirname(_capi.HEADER))
+    headers = [f for f in os.listdir(inc) if f.endswith(".h")]
+    assert "paxpro_b200.h" in headers
+
+
+def test_node_count_matches_reference_expression():
+    lib = _capi.lib()
+    for mn, mx, st in [(-250.0, 250.0, 500.0 / 2047), (0.0, 4e6, 1000.0), (-1.0, 1.0, 0.3)]:
+        assert lib.pxp_node_count(mn, mx, st) == int((mx - mn) / st + 1.0)
+
+
+def test_status_strings():
+    lib = _capi.lib()
+    assert lib.pxp_status_string(0) == b"ok"
+    assert b"unsupported" in lib.pxp_status_string(-7)
+    assert b"sm_100a" in lib.pxp_build_info()
+
+
+def test_null_arguments_are_rejected_without_a_device():
+    lib = _capi.lib()
+    assert lib.pxp_solver_create(None, None) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_step(None, 1) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_solver_destroy(None) == _capi.PXP_OK

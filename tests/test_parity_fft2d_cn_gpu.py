@@ -1,0 +1,176 @@
+"""GPU parity of the 1-transverse-dim solvers (FFTSolver2D, CrankNicholson)
+against the CPU oracle, through the C ABI.
+
+Tolerances: FP64 plain mode <= 1e-10 relative L2 at every saved step (the
+target stated for the reference path); FP32 served mode <= 1e-4 relative L2
+of the intensity |u|^2 against the FP64 oracle."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from paxpro_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_INT_TOL = 1e-4
+
+
+def _pxp():
+    import paxpro_b200 as pxp
+    return pxp
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _int_rel(a, b):
+    ia, ib = np.abs(a) ** 2, np.abs(b) ** 2
+    return np.linalg.norm(ia - ib) / np.linalg.norm(ib)
+
+
+def _oracle_2d(p, delta, beta, u0, nsteps, save_every, transparent=False):
+    g = po.grid(p.xmin, p.xmax, p.dx, p.zmin, p.zmax, p.dz, wl.K)
+    spec = po.MaterialSpec(po.MAT_XTABLE, delta_table=delta, beta_table=beta)
+    if p.kind == "fft":
+        return po.fft2d_run(g, spec, u0, nsteps, save_every)
+    return po.cn2d_run(g, spec, u0, nsteps, save_every, transparent)
+
+
+def _gpu_2d(p, delta, beta, u0, nsteps, save_every, precision, transparent=False, chunks=1):
+    pxp = _pxp()
+    kind = pxp.FFT_SOLVER_2D if p.kind == "fft" else pxp.CRANK_NICHOLSON
+    spec = pxp.ProblemSpec(kind=kind, x=pxp.Disc(p.xmin, p.xmax, p.dx),
+                           z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K,
+                           precision=precision, save_every=save_every,
+                           transparent_bc=transparent)
+    with pxp.Solver(spec) as s:
+        s.set_material_table(delta, beta)
+        s.set_initial_conditions(u0)
+        done = 0
+        for c in range(chunks):
+            k = nsteps // chunks if c < chunks - 1 else nsteps - done
+            s.step(k)
+            done += k
+        s.synchronize()
+        out = s.get_last_solution()
+        saves = [s.get_saved(i) for i in range(s.num_saved())]
+    return out, saves
+
+
+def test_cfg0_fft2d_fp64_every_save_within_1e10():
+    p = wl.cfg0()
+    d, b = p.material()
+    u0 = p.initial_field()
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, p.nsteps, 100)
+    out, saves = _gpu_2d(p, d, b, u0, p.nsteps, 100, 0)
+    assert len(saves) == len(ref_saves) == 40
+    errs = [_rel(g, r) for g, r in zip(saves, ref_saves)]
+    assert max(errs) <= FP64_TOL, errs
+    assert _rel(out, ref_out) <= FP64_TOL
+
+
+@pytest.mark.parametrize("n", [16, 256, 1024, 4096, 8192])
+def test_fft2d_fp64_sizes(n):
+    p = wl.Problem2D("t", "fft", -250.0, 250.0, wl.step_for_nodes(-250.0, 250.0, n),
+                     0.0, 1e6, 1000.0, 60, 15.0, wl.Waveguide())
+    d, b = p.material()
+    rng = np.random.default_rng(n)
+    u0 = p.initial_field() + 0.01 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, 60, 20)
+    out, saves = _gpu_2d(p, d, b, u0, 60, 20, 0, chunks=3)
+    assert max(_rel(g, r) for g, r in zip(saves, ref_saves)) <= FP64_TOL
+    assert _rel(out, ref_out) <= FP64_TOL
+
+
+def test_cfg1_cn_fp64_every_save_within_1e10():
+    p = wl.cfg1_cn()
+    d, b = p.material()
+    u0 = p.initial_field()
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, p.nsteps, 100)
+    out, saves = _gpu_2d(p, d, b, u0, p.nsteps, 100, 0)
+    assert len(saves) == 80
+    errs = [_rel(g, r) for g, r in zip(saves, ref_saves)]
+    assert max(errs) <= FP64_TOL, max(errs)
+
+
+@pytest.mark.parametrize("n", [16, 64, 512, 2048])
+@pytest.mark.parametrize("transparent", [False, True])
+def test_cn_fp64_sizes_and_boundaries(n, transparent):
+    p = wl.Problem2D("t", "cn", -250.0, 250.0, wl.step_for_nodes(-250.0, 250.0, n),
+                     0.0, 1e6, 500.0, 50, 15.0, wl.Waveguide(), center=60.0)
+    d, b = p.material()
+    u0 = p.initial_field()
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, 50, 10, transparent)
+    out, saves = _gpu_2d(p, d, b, u0, 50, 10, 0, transparent=transparent, chunks=2)
+    assert max(_rel(g, r) for g, r in zip(saves, ref_saves)) <= FP64_TOL
+    assert _rel(out, ref_out) <= FP64_TOL
+
+
+def test_fft2d_fp32_served_intensity_within_1e4():
+    p = wl.cfg0()
+    d, b = p.material()
+    u0 = p.initial_field()
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, p.nsteps, 100)
+    out, saves = _gpu_2d(p, d, b, u0, p.nsteps, 100, 1)
+    errs = [_int_rel(g, r) for g, r in zip(saves, ref_saves)]
+    assert max(errs) <= FP32_INT_TOL, max(errs)
+
+
+def test_cn_fp32_served_intensity_within_1e4():
+    p = wl.cfg1_cn(nsteps=2000)
+    d, b = p.material()
+    u0 = p.initial_field()
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, p.nsteps, 100)
+    out, saves = _gpu_2d(p, d, b, u0, p.nsteps, 100, 1)
+    errs = [_int_rel(g, r) for g, r in zip(saves, ref_saves)]
+    assert max(errs) <= FP32_INT_TOL, max(errs)
+
+
+def test_z_varying_planes_fft2d_and_cn():
+    # material switched on for a band of steps, supplied as per-step planes
+    for kind in ("fft", "cn"):
+        n, nsteps = 512, 40
+        p = wl.Problem2D("t", kind, -250.0, 250.0, wl.step_for_nodes(-250.0, 250.0, n),
+                         0.0, 1e6, 500.0, nsteps, 15.0, wl.Waveguide())
+        d, b = p.material()
+        u0 = p.initial_field()
+        # oracle with the z-invariant table for reference trajectory
+        ref_out, _ = _oracle_2d(p, d, b, u0, nsteps, 0)
+        pxp = _pxp()
+        kd = pxp.FFT_SOLVER_2D if kind == "fft" else pxp.CRANK_NICHOLSON
+        spec = pxp.ProblemSpec(kind=kd, x=pxp.Disc(p.xmin, p.xmax, p.dx),
+                               z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K)
+        per = 1 if kind == "fft" else 2
+        with pxp.Solver(spec) as s:
+            s.set_material_planes(np.tile(d, nsteps * per), np.tile(b, nsteps * per), 1, nsteps)
+            s.set_initial_conditions(u0)
+            s.step(nsteps)
+            out = s.get_last_solution()
+            with pytest.raises(pxp.PxpError):
+                s.step(1)  # beyond the planes provided
+        assert _rel(out, ref_out) <= FP64_TOL
+
+
+def test_api_errors_and_counters():
+    pxp = _pxp()
+    p = wl.cfg0(nsteps=10)
+    spec = pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(p.xmin, p.xmax, p.dx),
+                           z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K, save_every=5)
+    with pxp.Solver(spec) as s:
+        with pytest.raises(pxp.PxpError):
+            s.step(1)  # no initial conditions yet
+        s.set_initial_conditions(p.initial_field())
+        assert s.current_step == 1
+        s.step(10)
+        assert s.current_step == 11 and s.num_saved() == 2
+        with pytest.raises(pxp.PxpError):
+            s.get_saved(2)
+        s.reset()
+        assert s.current_step == 1
+    with pytest.raises(pxp.PxpError):
+        pxp.Solver(pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(0, 10, 1.0),
+                                   z=pxp.Disc(0, 10, 1.0), wavenumber=wl.K))  # Nx = 11
