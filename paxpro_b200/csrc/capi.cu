@@ -140,6 +140,15 @@ int upload_complex(pxp_solver_s *h, void *dst, const cd *src, long long n) {
   return PXP_OK;
 }
 
+// Per-step factor tables and twiddles are complex128 in both precisions;
+// served mode rounds only the field to complex64.
+size_t table_entry_bytes(const pxp_solver_s *) { return 16; }
+
+int upload_table(pxp_solver_s *h, void *dst, const cd *src, long long n) {
+  PXP_TRY_CUDA(h, cudaMemcpy(dst, src, sizeof(cd) * n, cudaMemcpyHostToDevice));
+  return PXP_OK;
+}
+
 int alloc(pxp_solver_s *h, void **p, size_t bytes, const char *what) {
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) {
@@ -158,11 +167,11 @@ int fft1d_setup(pxp_solver_s *h) {
   for (unsigned i = 0; i < n; ++i)
     ker[i] = kernel_2d(spatial_freq(i, n, h->prob.x.step), h->prob.z.step, h->prob.wavenumber);
   int rc;
-  if ((rc = alloc(h, &h->d_kern, h->csize * n, "propagator table"))) return rc;
-  if ((rc = upload_complex(h, h->d_kern, ker.data(), n))) return rc;
+  if ((rc = alloc(h, &h->d_kern, table_entry_bytes(h) * n, "propagator table"))) return rc;
+  if ((rc = upload_table(h, h->d_kern, ker.data(), n))) return rc;
   std::vector<cd> tw = twiddles((int)n);
-  if ((rc = alloc(h, &h->d_tw, h->csize * n, "twiddle table"))) return rc;
-  if ((rc = upload_complex(h, h->d_tw, tw.data(), n))) return rc;
+  if ((rc = alloc(h, &h->d_tw, sizeof(cd) * n, "twiddle table"))) return rc;
+  if ((rc = upload_table(h, h->d_tw, tw.data(), n))) return rc;
   return alloc(h, &h->d_job, sizeof(pxp::Fft1dJob), "job descriptor");
 }
 
@@ -181,8 +190,9 @@ int fft1d_set_trans(pxp_solver_s *h, const double *delta, const double *beta, in
     }
   free_dev(h->d_trans);
   int rc;
-  if ((rc = alloc(h, &h->d_trans, h->csize * t.size(), "transmission table"))) return rc;
-  if ((rc = upload_complex(h, h->d_trans, t.data(), (long long)t.size()))) return rc;
+  if ((rc = alloc(h, &h->d_trans, table_entry_bytes(h) * t.size(), "transmission table")))
+    return rc;
+  if ((rc = upload_table(h, h->d_trans, t.data(), (long long)t.size()))) return rc;
   h->trans_stride = nplanes > 1 ? n : 0;
   h->trans_step0 = first_step;
   h->material_set = true;

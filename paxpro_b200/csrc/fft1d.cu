@@ -10,26 +10,33 @@
 // FP64 mode reproduces the reference's pointwise arithmetic exactly:
 // curr *= kernel is a rounded complex product and the refraction update is
 // (prev * t) / N with t taken from a host table built with std::exp, as the
-// reference evaluates it.  FP32 mode multiplies by a table holding t/N.
+// reference evaluates it.  FP32 mode multiplies by t/N, the product formed
+// in FP64 and rounded once.
 #include "fft_smem.cuh"
 #include "pxp_kernels.h"
 
 namespace pxp {
 
-template <typename R> __device__ __forceinline__ void refract(typename Cx<R>::T &u,
-                                                              typename Cx<R>::T t, R n);
+// Per-step factor tables hold complex128 values in both precisions.  FP64
+// mode reproduces the reference's rounding (rounded complex product, then
+// division by N); FP32 served mode forms the product with t/N in FP64 and
+// rounds once to complex64.
+template <typename R> __device__ __forceinline__ void refract(typename Cx<R>::T &u, double2 t,
+                                                              R n);
 template <> __device__ __forceinline__ void refract<double>(double2 &u, double2 t, double n) {
   u = cx_div_real_rn(cx_mul_rn(u, t), n);
 }
-template <> __device__ __forceinline__ void refract<float>(float2 &u, float2 t, float) {
-  u = cmul(u, t);
+template <> __device__ __forceinline__ void refract<float>(float2 &u, double2 t, float) {
+  u = tw_mul(u, t);
 }
 template <typename R> __device__ __forceinline__ typename Cx<R>::T kmul(typename Cx<R>::T u,
-                                                                       typename Cx<R>::T k);
+                                                                       double2 k);
 template <> __device__ __forceinline__ double2 kmul<double>(double2 u, double2 k) {
   return cx_mul_rn(u, k);
 }
-template <> __device__ __forceinline__ float2 kmul<float>(float2 u, float2 k) { return cmul(u, k); }
+template <> __device__ __forceinline__ float2 kmul<float>(float2 u, double2 k) {
+  return tw_mul(u, k);
+}
 
 template <typename R, int N, int T, bool TW_SMEM>
 __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ jobs, int step0_ov,
@@ -43,18 +50,19 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     job.nsteps = nsteps_ov;
   }
   const int lane = threadIdx.x;
-  const C *gtw = reinterpret_cast<const C *>(job.twiddle);
-  const C *tw = gtw;
+  const double2 *gtw = reinterpret_cast<const double2 *>(job.twiddle);
+  const double2 *tw = gtw;
   if constexpr (TW_SMEM) {
-    C *stw = u + N;
+    // twiddles after the field, 16-byte aligned
+    double2 *stw = reinterpret_cast<double2 *>(smem_raw + ((sizeof(C) * N + 15) & ~size_t(15)));
     for (int i = lane; i < N; i += T) stw[i] = gtw[i];
     tw = stw;
   }
   C *field = reinterpret_cast<C *>(job.field);
   for (int i = lane; i < N; i += T) u[i] = field[i];
   __syncthreads();
-  const C *kern = reinterpret_cast<const C *>(job.kern);
-  const C *trans0 = reinterpret_cast<const C *>(job.trans);
+  const double2 *kern = reinterpret_cast<const double2 *>(job.kern);
+  const double2 *trans0 = reinterpret_cast<const double2 *>(job.trans);
   C *saves = reinterpret_cast<C *>(job.saves);
   const R nreal = (R)N;
   for (int s = 0; s < job.nsteps; ++s) {
@@ -63,7 +71,7 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     for (int i = lane; i < N; i += T) u[i] = kmul<R>(u[i], kern[i]);
     __syncthreads();
     fft_smem<C, N, T, +1>(u, tw, lane);
-    const C *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
+    const double2 *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
@@ -88,8 +96,9 @@ static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nstep
   using C = typename Cx<R>::T;
   constexpr int T = fft1d_threads<R>(N);
   constexpr size_t field_bytes = sizeof(C) * N;
-  constexpr bool tw_smem = 2 * field_bytes <= 160 * 1024;
-  constexpr size_t smem = tw_smem ? 2 * field_bytes : field_bytes;
+  constexpr size_t tw_bytes = sizeof(double2) * N;
+  constexpr bool tw_smem = field_bytes + tw_bytes <= 200 * 1024;
+  constexpr size_t smem = tw_smem ? field_bytes + tw_bytes : field_bytes;
   auto k = fft1d_kernel<R, N, T, tw_smem>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

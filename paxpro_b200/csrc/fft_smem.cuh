@@ -14,6 +14,27 @@
 
 namespace pxp {
 
+// v * w and v * conj(w) with FP64 twiddles.
+__device__ __forceinline__ double2 tw_mul(double2 v, double2 w) { return cmul(v, w); }
+__device__ __forceinline__ double2 tw_mulc(double2 v, double2 w) { return cmulc(v, w); }
+__device__ __forceinline__ float2 tw_mul(float2 v, double2 w) {
+  double x = v.x, y = v.y;
+  return make_float2((float)fma(x, w.x, -y * w.y), (float)fma(x, w.y, y * w.x));
+}
+__device__ __forceinline__ float2 tw_mulc(float2 v, double2 w) {
+  double x = v.x, y = v.y;
+  return make_float2((float)fma(x, w.x, y * w.y), (float)fma(y, w.x, -x * w.y));
+}
+// (a, b) * 1/sqrt(2), the product formed in FP64 for complex64 data.
+__device__ __forceinline__ double2 scale_h(double a, double b) {
+  const double h = 0.70710678118654752440084436210484903928;
+  return make_double2(a * h, b * h);
+}
+__device__ __forceinline__ float2 scale_h(float a, float b) {
+  const double h = 0.70710678118654752440084436210484903928;
+  return make_float2((float)((double)a * h), (float)((double)b * h));
+}
+
 // In-register R-point DFT, R in {2, 4, 8}.
 template <int SIGN, typename C>
 __device__ __forceinline__ void dft2(C &a, C &b) {
@@ -34,21 +55,19 @@ __device__ __forceinline__ void dft4(C &v0, C &v1, C &v2, C &v3) {
 
 template <int SIGN, typename C>
 __device__ __forceinline__ void dft8(C *v) {
-  using Rt = decltype(v[0].x);
-  const Rt h = (Rt)0.70710678118654752440084436210484903928;  // 1/sqrt(2)
   C a0 = cadd(v[0], v[4]), b0 = csub(v[0], v[4]);
   C a1 = cadd(v[1], v[5]), b1 = csub(v[1], v[5]);
   C a2 = cadd(v[2], v[6]), b2 = csub(v[2], v[6]);
   C a3 = cadd(v[3], v[7]), b3 = csub(v[3], v[7]);
   // b_r *= W8^(r) (forward) or its conjugate (inverse)
   if (SIGN < 0) {
-    b1 = mk((b1.x + b1.y) * h, (b1.y - b1.x) * h);
+    b1 = scale_h(b1.x + b1.y, b1.y - b1.x);
     b2 = mk(b2.y, -b2.x);
-    b3 = mk((b3.y - b3.x) * h, -(b3.x + b3.y) * h);
+    b3 = scale_h(b3.y - b3.x, -(b3.x + b3.y));
   } else {
-    b1 = mk((b1.x - b1.y) * h, (b1.x + b1.y) * h);
+    b1 = scale_h(b1.x - b1.y, b1.x + b1.y);
     b2 = mk(-b2.y, b2.x);
-    b3 = mk(-(b3.x + b3.y) * h, (b3.x - b3.y) * h);
+    b3 = scale_h(-(b3.x + b3.y), b3.x - b3.y);
   }
   dft4<SIGN>(a0, a1, a2, a3);
   dft4<SIGN>(b0, b1, b2, b3);
@@ -66,7 +85,7 @@ __device__ __forceinline__ void dft_r(C *v) {
 // One Stockham pass over x (length N) with T threads; NS = length of the
 // sub-transforms already done.  `lane` is this thread's index in [0, T).
 template <typename C, int N, int T, int SIGN, int R, int NS>
-__device__ __forceinline__ void stockham_pass(C *x, const C *tw, int lane) {
+__device__ __forceinline__ void stockham_pass(C *x, const double2 *tw, int lane) {
   constexpr int NB = N / R;
   constexpr int PER = (NB + T - 1) / T;
   C v[PER][R];
@@ -87,8 +106,8 @@ __device__ __forceinline__ void stockham_pass(C *x, const C *tw, int lane) {
       if constexpr (NS > 1) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          C w = tw[r * k * (N / (NS * R))];
-          v[b][r] = SIGN < 0 ? cmul(v[b][r], w) : cmulc(v[b][r], w);
+          double2 w = tw[r * k * (N / (NS * R))];
+          v[b][r] = SIGN < 0 ? tw_mul(v[b][r], w) : tw_mulc(v[b][r], w);
         }
       }
       dft_r<R, SIGN>(v[b]);
@@ -101,7 +120,7 @@ __device__ __forceinline__ void stockham_pass(C *x, const C *tw, int lane) {
 }
 
 template <typename C, int N, int T, int SIGN, int NS = 1>
-__device__ __forceinline__ void fft_smem(C *x, const C *tw, int lane) {
+__device__ __forceinline__ void fft_smem(C *x, const double2 *tw, int lane) {
   if constexpr (NS < N) {
     constexpr int REM = N / NS;
     constexpr int R = REM >= 8 ? 8 : REM;

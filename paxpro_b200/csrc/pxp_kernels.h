@@ -14,12 +14,13 @@ enum Precision { kFP64 = 0, kFP32 = 1 };
 // All complex arrays are interleaved and in the solver's precision.
 struct Fft1dJob {
   void *field;             // N complex: field after the previous step
-  const void *kern;        // N complex: propagator exp(-i (dz/2k) kx^2)
-  const void *trans;       // N complex per table: transmission (FP64: t,
-                           // applied as (u*t)/N; FP32: t/N, applied as u*t)
+  const void *kern;        // N complex128: propagator exp(-i (dz/2k) kx^2)
+  const void *trans;       // N complex128 per table: transmission (FP64: t,
+                           // applied as (u*t)/N; FP32: t/N, applied as u*t
+                           // with the product formed in FP64)
   long long trans_stride;  // complex elements between per-step tables; 0 =
                            // z-invariant medium (one table)
-  const void *twiddle;     // N complex: exp(-2 pi i m/N)
+  const void *twiddle;     // N complex128: exp(-2 pi i m/N)
   void *saves;             // save slots, N complex each (may be null)
   int n;                   // transverse points (power of two)
   int step0;               // 1-based index of the first step of this launch
