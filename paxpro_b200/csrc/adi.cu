@@ -1,0 +1,231 @@
+// adi.cu -- K-ADI: one alternating-direction half step with the right-hand
+// side stencil fused with a parallel complex tridiagonal solve.
+//
+// Replaces ADI::xImplicit / ADI::yImplicit / ADI::applyTBC
+// (src/alternatingDirectionSolver.cpp:8-234) and the ThomasAlgorithm sweep
+// over the chain of n*n unknowns (include/thomasAlgorithm.tpp:2-32), whose
+// zero sub-diagonal entries at every system start make the n systems of a
+// half step independent.
+//
+// A CTA owns G consecutive systems.  It stages them, plus one halo system on
+// each side for the explicit stencil, in shared memory with loads that are
+// coalesced for either layout (systems interleaved in memory for the x half
+// step, contiguous for the y half step).  Each system is split into
+// P = n/M chunks, one per thread; the chunk rows are built with the
+// reference's operation order (matrix coefficients equal the reference's),
+// the chunk interior is eliminated in registers, and the 2P-unknown reduced
+// system is solved by cyclic reduction in shared memory.  The solution goes
+// back through shared memory for coalesced stores.
+//
+// Materials: a first-hit sphere list evaluated per point with rounded FP64
+// operations (the same r^2 < R^2 test as the oracle); the host culls, per
+// half step, spheres whose dz^2 alone is >= R^2, which cannot contain any
+// point of the plane.
+#include "pxp_complex.cuh"
+#include "pxp_kernels.h"
+#include "tridiag.cuh"
+
+namespace pxp {
+
+__device__ __forceinline__ void sphere_material(const AdiHalf &h, double x, double y,
+                                                double &delta, double &beta) {
+  delta = 0.0;
+  beta = 0.0;
+  const int n = h.nspheres;
+  const Sphere *list = n > kInlineSpheres ? h.spheres_all : h.spheres;
+  for (int i = 0; i < n; ++i) {
+    const Sphere sp = list[i];
+    double ddx = __dsub_rn(x, sp.cx), ddy = __dsub_rn(y, sp.cy), ddz = __dsub_rn(h.z, sp.cz);
+    double rsq = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
+    if (rsq < __dmul_rn(sp.r, sp.r)) {
+      delta = sp.delta;
+      beta = sp.beta;
+      return;
+    }
+  }
+}
+
+// Transparent-boundary factor 0.5*i*exp(i*kd)/kd2 with kd = -i*log(ratio),
+// Re(kd) clamped at 0 (src/alternatingDirectionSolver.cpp:157-234).
+__device__ __forceinline__ double2 tbc_factor(double2 num, double2 den) {
+  double2 ratio = cx_div_rn(num, den);
+  double2 lg = mk(log(hypot(ratio.x, ratio.y)), atan2(ratio.y, ratio.x));
+  double2 kd = cx_mul_rn(mk(-0.0, -1.0), lg);
+  if (kd.x < 0.0) kd.x = 0.0;
+  double2 ik = cx_mul_rn(mk(0.0, 1.0), kd);
+  double e = exp(ik.x), sn, cs;
+  sincos(ik.y, &sn, &cs);
+  return cx_mul_rn(mk(0.0, 0.5), mk(e * cs, e * sn));
+}
+
+template <typename R, int M, int G>
+__global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = h.n;
+  const int P = n / M;        // chunks per system
+  const int T = G * P;        // threads
+  const int ld = n + 1;       // padded row of the staging tile
+  C *tile = reinterpret_cast<C *>(smem_raw);                  // (G+2) x ld
+  double2 *red = reinterpret_cast<double2 *>(
+      smem_raw + ((sizeof(C) * (G + 2) * ld + 15) & ~size_t(15)));  // 4 x G x 2P
+  const int nr = 2 * P;
+  const int tid = threadIdx.x;
+  const int s_base = blockIdx.x * G;  // first system of this CTA
+  const C *in = reinterpret_cast<const C *>(h.in);
+  C *out = reinterpret_cast<C *>(h.out);
+  const bool interleaved = h.stride_sys == 1;
+
+  // ---- stage systems s_base-1 .. s_base+G (out-of-range halo rows zero)
+  const int rows = G + 2;
+  for (int idx = tid; idx < rows * n; idx += T) {
+    int g, p;
+    if (interleaved) {
+      p = idx / rows;
+      g = idx - p * rows;
+    } else {
+      g = idx / n;
+      p = idx - g * n;
+    }
+    const int s = s_base - 1 + g;
+    C v = from_d<R>(mk(0.0, 0.0));
+    if (s >= 0 && s < n) v = in[(long long)p * h.stride_pos + (long long)s * h.stride_sys];
+    tile[g * ld + p] = v;
+  }
+  __syncthreads();
+
+  const int g = tid / P;          // system within the CTA
+  const int c = tid - g * P;      // chunk
+  const int s = s_base + g;       // global system index
+  const int p0 = c * M;
+  const double2 sub = mk(-0.0, __ddiv_rn(-0.5, h.kd2_impl));  // -0.5*i/(k d^2)
+  const C *ctr = tile + (g + 1) * ld;
+  const C *lft = tile + g * ld;
+  const C *rgt = tile + (g + 2) * ld;
+
+  double2 dg[M], rh[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int p = p0 + m;
+    // coordinates: position runs along x in the x half step, along y in the y half step
+    double x, y;
+    const double pos_c = (double)p, sys_c = (double)s;
+    if (!h.y_implicit) {
+      x = __dadd_rn(h.xmin, __dmul_rn(pos_c, h.dx));
+      y = __dadd_rn(h.ymin, __dmul_rn(sys_c, h.dy));
+    } else {
+      x = __dadd_rn(h.xmin, __dmul_rn(sys_c, h.dx));
+      y = __dadd_rn(h.ymin, __dmul_rn(pos_c, h.dy));
+    }
+    double delta, beta;
+    sphere_material(h, x, y, delta, beta);
+    if (!h.y_implicit) {
+      // 1.0/dz + i/(k dx dx) + beta*k + i*delta*k   (reference :38)
+      dg[m] = mk(__dadd_rn(h.inv_dzh, __dmul_rn(beta, h.k)),
+                 __dadd_rn(__ddiv_rn(1.0, h.kd2_impl), __dmul_rn(delta, h.k)));
+    } else {
+      // 1.0/dz + i/(k dy dy + beta*k + i*delta*k)   (reference :103, as written)
+      double2 q = cx_div_rn(mk(0.0, 1.0), mk(__dadd_rn(h.kd2_impl, __dmul_rn(beta, h.k)),
+                                              __dmul_rn(delta, h.k)));
+      dg[m] = mk(__dadd_rn(q.x, h.inv_dzh), q.y);
+    }
+    // rhs = (1/dz - i/(k d_e^2)) u + 0.5 i u_left/(k d_e^2) + 0.5 i u_right/(k d_e^2)
+    const double2 uc = to_d(ctr[p]);
+    double2 r = cx_mul_rn(mk(h.inv_dzh, -__ddiv_rn(1.0, h.kd2_expl)), uc);
+    if (s > 0) r = cx_add_rn(r, cx_div_real_rn(cx_mul_rn(mk(0.0, 0.5), to_d(lft[p])), h.kd2_expl));
+    if (s < n - 1)
+      r = cx_add_rn(r, cx_div_real_rn(cx_mul_rn(mk(0.0, 0.5), to_d(rgt[p])), h.kd2_expl));
+    rh[m] = r;
+  }
+  if (h.use_tbc) {
+    const double zero = 1e-6;
+    // along the system (implicit direction): diagonal at both ends
+    if (c == P - 1) {
+      double2 inner = to_d(ctr[n - 2]);
+      if (hypot(inner.x, inner.y) > zero)
+        dg[M - 1] = cx_sub_rn(dg[M - 1], cx_div_real_rn(tbc_factor(to_d(ctr[n - 1]), inner), h.kd2_impl));
+    }
+    if (c == 0) {
+      double2 inner = to_d(ctr[1]);
+      if (hypot(inner.x, inner.y) > zero)
+        dg[0] = cx_sub_rn(dg[0], cx_div_real_rn(tbc_factor(to_d(ctr[0]), inner), h.kd2_impl));
+    }
+    // across systems (explicit direction): rhs of the first and last system
+    if (s == n - 1 || s == 0) {
+      const C *inner_row = (s == n - 1) ? lft : rgt;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int p = p0 + m;
+        double2 inner = to_d(inner_row[p]);
+        if (hypot(inner.x, inner.y) > zero) {
+          double2 edge = to_d(ctr[p]);
+          double2 f = cx_mul_rn(tbc_factor(edge, inner), edge);
+          rh[m] = cx_add_rn(rh[m], cx_div_real_rn(f, h.kd2_expl));
+        }
+      }
+    }
+  }
+
+  double2 yv[M > 2 ? M - 2 : 1], pv[M > 2 ? M - 2 : 1], qv[M > 2 ? M - 2 : 1];
+  const ReducedRows rr = chunk_eliminate<M>(dg, rh, sub, p0 > 0, p0 + M < n, yv, pv, qv);
+  double2 *ra = red + (0 * G + g) * nr;
+  double2 *rb = red + (1 * G + g) * nr;
+  double2 *rc = red + (2 * G + g) * nr;
+  double2 *rd = red + (3 * G + g) * nr;
+  ra[2 * c] = rr.ea; rb[2 * c] = rr.eb; rc[2 * c] = rr.ec; rd[2 * c] = rr.ed;
+  ra[2 * c + 1] = rr.fa; rb[2 * c + 1] = rr.fb; rc[2 * c + 1] = rr.fc; rd[2 * c + 1] = rr.fd;
+  __syncthreads();  // also: every read of the staged tile is done
+  cyclic_reduction(ra, rb, rc, rd, nr, c, P);
+  const double2 xf = rd[2 * c], xl = rd[2 * c + 1];
+  C *dst = tile + (g + 1) * ld;
+#pragma unroll
+  for (int m = 0; m < M; ++m) dst[p0 + m] = from_d<R>(chunk_value<M>(m, xf, xl, yv, pv, qv));
+  __syncthreads();
+  C *save = reinterpret_cast<C *>(h.save);
+  for (int idx = tid; idx < G * n; idx += T) {
+    int gg, p;
+    if (interleaved) {
+      p = idx / G;
+      gg = idx - p * G;
+    } else {
+      gg = idx / n;
+      p = idx - gg * n;
+    }
+    const long long off = (long long)p * h.stride_pos + (long long)(s_base + gg) * h.stride_sys;
+    const C v = tile[(gg + 1) * ld + p];
+    out[off] = v;
+    if (save) save[off] = v;
+  }
+}
+
+static constexpr int kAdiM = 8;
+
+template <int G> constexpr int adi_threads(int n) { return G * (n / kAdiM); }
+
+template <typename R, int G>
+static cudaError_t adi_launch_g(const AdiHalf &h, cudaStream_t s) {
+  using C = typename Cx<R>::T;
+  const int n = h.n;
+  const int T = adi_threads<G>(n);
+  const size_t tile = (sizeof(C) * (G + 2) * (n + 1) + 15) & ~size_t(15);
+  const size_t smem = tile + sizeof(double2) * 4 * G * 2 * (n / kAdiM);
+  auto k = adi_half_kernel<R, kAdiM, G>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<n / G, T, smem, s>>>(h);
+  return cudaGetLastError();
+}
+
+bool adi_supported(Precision p, int n) {
+  if (n < 64 || (n & (n - 1))) return false;
+  return p == kFP64 ? n <= 2048 : n <= 2048;
+}
+
+cudaError_t launch_adi_half(Precision p, const AdiHalf &h, cudaStream_t s) {
+  if (!adi_supported(p, h.n)) return cudaErrorInvalidValue;
+  // G systems per CTA so that G * n/8 <= 512 threads
+  if (h.n <= 1024) return p == kFP64 ? adi_launch_g<double, 4>(h, s) : adi_launch_g<float, 4>(h, s);
+  return p == kFP64 ? adi_launch_g<double, 2>(h, s) : adi_launch_g<float, 2>(h, s);
+}
+
+}  // namespace pxp

@@ -65,6 +65,10 @@ struct pxp_solver_s {
   int mat_step0 = 1;
   // job descriptors in device memory
   void *d_job = nullptr;
+  // 2-transverse-dim solvers
+  void *d_field2 = nullptr;                  // ping-pong buffer
+  std::vector<pxp_sphere> spheres;           // first-hit sphere material
+  pxp::Sphere *d_spheres = nullptr;
   // host copies
   std::vector<double> h_delta, h_beta;
   int plane_first = 1, plane_count = 0;  // per-step material planes (0 = z-invariant)
@@ -244,6 +248,89 @@ int cn_set_planes(pxp_solver_s *h, const double *delta, const double *beta, int 
   return PXP_OK;
 }
 
+// ---- ADI -------------------------------------------------------------------
+// getZ (src/paraxialSimulation.cpp:250-253)
+double get_z(const pxp_solver_s *h, unsigned iz) { return h->prob.z.min + iz * h->prob.z.step; }
+
+// Spheres that can contain a point of the plane z: the oracle's and the
+// kernel's test is ((dx^2 + dy^2) + dz^2) < R^2 with rounded operations, and
+// the rounded sum of non-negative terms is never below dz^2, so a sphere
+// with fl(dz^2) >= fl(R^2) is never hit and may be dropped (list order kept).
+void active_spheres(const pxp_solver_s *h, double z, std::vector<pxp::Sphere> &out) {
+  out.clear();
+  for (const pxp_sphere &sp : h->spheres) {
+    volatile double dz = z - sp.cz;
+    volatile double dz2 = dz * dz;
+    volatile double r2 = sp.radius * sp.radius;
+    if (dz2 < r2) out.push_back({sp.cx, sp.cy, sp.cz, sp.radius, sp.delta, sp.beta});
+  }
+}
+
+int adi_fill_spheres(pxp_solver_s *h, pxp::AdiHalf &a, double z) {
+  std::vector<pxp::Sphere> act;
+  active_spheres(h, z, act);
+  a.nspheres = (int)act.size();
+  if (a.nspheres <= pxp::kInlineSpheres) {
+    for (int i = 0; i < a.nspheres; ++i) a.spheres[i] = act[i];
+    a.spheres_all = nullptr;
+  } else {
+    // too many active spheres for the parameter block: the full list
+    a.nspheres = (int)h->spheres.size();
+    a.spheres_all = h->d_spheres;
+  }
+  return PXP_OK;
+}
+
+int adi_steps(pxp_solver_s *h, unsigned first, int nsteps) {
+  const pxp_problem &p = h->prob;
+  const double dzh = p.z.step / 2.0;  // ADI::xImplicit (src/alternatingDirectionSolver.cpp:18)
+  const double k = p.wavenumber;
+  const double kdx2 = k * p.x.step * p.x.step, kdy2 = k * p.y.step * p.y.step;
+  const long long n = h->nx;
+  for (int i = 0; i < nsteps; ++i) {
+    const unsigned step = first + (unsigned)i;
+    pxp::AdiHalf a{};
+    a.n = (int)n;
+    a.use_tbc = p.transparent_bc ? 1 : 0;
+    a.inv_dzh = 1.0 / dzh;
+    a.k = k;
+    a.xmin = p.x.min;
+    a.dx = p.x.step;
+    a.ymin = p.y.min;
+    a.dy = p.y.step;
+    // x implicit: systems are rows (y), positions run along x (stride Ny)
+    a.in = h->d_field;
+    a.out = h->d_field2;
+    a.save = nullptr;
+    a.stride_pos = n;
+    a.stride_sys = 1;
+    a.y_implicit = 0;
+    a.kd2_impl = kdx2;
+    a.kd2_expl = kdy2;
+    a.z = get_z(h, step);
+    adi_fill_spheres(h, a, a.z);
+    cudaError_t e = pxp::launch_adi_half(h->prec, a, h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "ADI x half step");
+    // y implicit: systems are columns (x), positions run along y (stride 1)
+    a.in = h->d_field2;
+    a.out = h->d_field;
+    const bool save = h->save_every > 0 && step % (unsigned)h->save_every == 0 &&
+                      (int)(step / (unsigned)h->save_every) - 1 < h->max_slots;
+    a.save = save ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
+                  : nullptr;
+    a.stride_pos = 1;
+    a.stride_sys = n;
+    a.y_implicit = 1;
+    a.kd2_impl = kdy2;
+    a.kd2_expl = kdx2;
+    a.z = get_z(h, step) + dzh;
+    adi_fill_spheres(h, a, a.z);
+    e = pxp::launch_adi_half(h->prec, a, h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
+  }
+  return PXP_OK;
+}
+
 int cn_write_job(pxp_solver_s *h) {
   pxp::CnJob j{};
   const unsigned n = h->nx;
@@ -335,6 +422,7 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
   switch (p.kind) {
     case PXP_FFT_SOLVER_2D: supported = pxp::fft1d_supported(h->prec, (int)h->nx); break;
     case PXP_CRANK_NICHOLSON: supported = pxp::cn_supported(h->prec, (int)h->nx); break;
+    case PXP_ADI: supported = pxp::adi_supported(h->prec, (int)h->nx); break;
     default: supported = false;
   }
   if (!supported) {
@@ -378,6 +466,10 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
       if ((rc = cn_set_planes(h, zeros.data(), zeros.data(), 1, 1, false))) return cleanup_fail(rc);
       if ((rc = cn_write_job(h))) return cleanup_fail(rc);
       break;
+    case PXP_ADI:
+      if ((rc = alloc(h, &h->d_field2, h->csize * h->npts, "second field buffer")))
+        return cleanup_fail(rc);
+      break;
   }
   *out = h;
   return PXP_OK;
@@ -393,6 +485,8 @@ int pxp_solver_destroy(pxp_solver h) {
   free_dev(h->d_tw);
   free_dev(h->d_mat);
   free_dev(h->d_job);
+  free_dev(h->d_field2);
+  free_dev(h->d_spheres);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return PXP_OK;
@@ -453,7 +547,23 @@ int pxp_set_material_planes(pxp_solver h, const double *delta, const double *bet
 
 int pxp_set_material_spheres(pxp_solver h, const pxp_sphere *spheres, int n) {
   if (h == nullptr || (n > 0 && spheres == nullptr) || n < 0) return PXP_ERR_INVALID;
-  return h->fail(PXP_ERR_UNSUPPORTED, "sphere materials are not supported for this kind");
+  if (h->prob.kind != PXP_ADI && h->prob.kind != PXP_FFT_SOLVER_3D)
+    return h->fail(PXP_ERR_UNSUPPORTED, "sphere materials apply to the 3-D kinds");
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->spheres.assign(spheres, spheres + n);
+  free_dev(h->d_spheres);
+  if (n > 0) {
+    std::vector<pxp::Sphere> dev(n);
+    for (int i = 0; i < n; ++i)
+      dev[i] = {spheres[i].cx, spheres[i].cy, spheres[i].cz, spheres[i].radius, spheres[i].delta,
+                spheres[i].beta};
+    int rc;
+    if ((rc = alloc(h, (void **)&h->d_spheres, sizeof(pxp::Sphere) * n, "sphere list"))) return rc;
+    PXP_TRY_CUDA(h, cudaMemcpy(h->d_spheres, dev.data(), sizeof(pxp::Sphere) * n,
+                               cudaMemcpyHostToDevice));
+  }
+  h->material_set = true;
+  return PXP_OK;
 }
 
 static int upload_field(pxp_solver_s *h, void *dst, const double *src) {
@@ -520,6 +630,11 @@ int pxp_step(pxp_solver h, int nsteps) {
       e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first, nsteps,
                          h->stream);
       break;
+    case PXP_ADI: {
+      int rc = adi_steps(h, (unsigned)first, nsteps);
+      if (rc) return rc;
+      break;
+    }
     default:
       return h->fail(PXP_ERR_UNSUPPORTED, "kind not available");
   }

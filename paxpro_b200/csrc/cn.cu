@@ -22,6 +22,7 @@
 // condition ~ rho), so the difference stays near machine precision.
 #include "pxp_complex.cuh"
 #include "pxp_kernels.h"
+#include "tridiag.cuh"
 
 namespace pxp {
 
@@ -78,59 +79,6 @@ __device__ __forceinline__ void cn_tbc(double2 outer, double2 inner, double rho,
   rhs = cx_add_rn(rhs, cx_mul_rn(coef, outer));
 }
 
-// Cyclic reduction on n = 2^L equations held in shared memory
-// (a = coupling to x_{i-1}, b = diagonal, c = coupling to x_{i+1}, d = rhs);
-// the solution overwrites d.  T threads.
-template <int T>
-__device__ void cyclic_reduction(double2 *a, double2 *b, double2 *c, double2 *d, int n) {
-  const int tid = threadIdx.x;
-  int s = 1;
-  for (; 4 * s <= n; s <<= 1) {
-    const int cnt = n / (2 * s);
-    for (int k = tid; k < cnt; k += T) {
-      int i = 2 * s * k + 2 * s - 1;
-      int il = i - s, ir = i + s;
-      double2 k1 = cx_div_rn(a[i], b[il]);
-      double2 ai = cx_sub_rn(mk(0.0, 0.0), cx_mul_rn(a[il], k1));
-      double2 bi = cx_sub_rn(b[i], cx_mul_rn(c[il], k1));
-      double2 di = cx_sub_rn(d[i], cx_mul_rn(d[il], k1));
-      double2 ci = mk(0.0, 0.0);
-      if (ir < n) {
-        double2 k2 = cx_div_rn(c[i], b[ir]);
-        ci = cx_sub_rn(mk(0.0, 0.0), cx_mul_rn(c[ir], k2));
-        bi = cx_sub_rn(bi, cx_mul_rn(a[ir], k2));
-        di = cx_sub_rn(di, cx_mul_rn(d[ir], k2));
-      }
-      a[i] = ai;
-      b[i] = bi;
-      c[i] = ci;
-      d[i] = di;
-    }
-    __syncthreads();
-  }
-  // two remaining unknowns: i1 = n/2 - 1, i2 = n - 1
-  if (tid == 0) {
-    int i1 = n / 2 - 1, i2 = n - 1;
-    double2 det = cx_sub_rn(cx_mul_rn(b[i1], b[i2]), cx_mul_rn(c[i1], a[i2]));
-    double2 x1 = cx_div_rn(cx_sub_rn(cx_mul_rn(b[i2], d[i1]), cx_mul_rn(c[i1], d[i2])), det);
-    double2 x2 = cx_div_rn(cx_sub_rn(cx_mul_rn(b[i1], d[i2]), cx_mul_rn(a[i2], d[i1])), det);
-    d[i1] = x1;
-    d[i2] = x2;
-  }
-  __syncthreads();
-  for (s >>= 1; s >= 1; s >>= 1) {
-    const int cnt = n / (2 * s);
-    for (int k = tid; k < cnt; k += T) {
-      int i = 2 * s * k + s - 1;
-      double2 acc = d[i];
-      if (i - s >= 0) acc = cx_sub_rn(acc, cx_mul_rn(a[i], d[i - s]));
-      if (i + s < n) acc = cx_sub_rn(acc, cx_mul_rn(c[i], d[i + s]));
-      d[i] = cx_div_rn(acc, b[i]);
-    }
-    __syncthreads();
-  }
-}
-
 template <typename R, int M, int T>
 __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, int step0_ov,
                                               int nsteps_ov) {
@@ -184,80 +132,26 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
         if (hypot(in.x, in.y) > ZERO) cn_tbc(o, in, rho, dg[M - 1], rh[M - 1]);
       }
     }
-    // ---- 2. interior elimination (rows 1..M-2 of the chunk), three RHS:
-    // y (rhs), p (coupling to x_first), q (coupling to x_last).
+    // ---- 2. interior elimination (partition method)
     double2 y[M > 2 ? M - 2 : 1], p[M > 2 ? M - 2 : 1], q[M > 2 ? M - 2 : 1];
-    double2 ea, eb, ec, ed, fa, fb, fc, fd;  // reduced rows (first, last)
-    if constexpr (M > 2) {
-      double2 cp[M - 2];
-      // forward sweep
-#pragma unroll
-      for (int m = 1; m <= M - 2; ++m) {
-        int j = m - 1;
-        double2 den = dg[m];
-        if (j > 0) den = cx_sub_rn(den, cx_mul_rn(sub, cp[j - 1]));
-        if (m < M - 2) cp[j] = cx_div_rn(sub, den);
-        double2 ry = rh[m];
-        double2 rp = (m == 1) ? cx_sub_rn(mk(0.0, 0.0), sub) : mk(0.0, 0.0);
-        double2 rq = (m == M - 2) ? cx_sub_rn(mk(0.0, 0.0), sub) : mk(0.0, 0.0);
-        if (j > 0) {
-          ry = cx_sub_rn(ry, cx_mul_rn(sub, y[j - 1]));
-          rp = cx_sub_rn(rp, cx_mul_rn(sub, p[j - 1]));
-          rq = cx_sub_rn(rq, cx_mul_rn(sub, q[j - 1]));
-        }
-        y[j] = cx_div_rn(ry, den);
-        p[j] = cx_div_rn(rp, den);
-        q[j] = cx_div_rn(rq, den);
-      }
-      // back substitution
-#pragma unroll
-      for (int j = M - 4; j >= 0; --j) {
-        y[j] = cx_sub_rn(y[j], cx_mul_rn(cp[j], y[j + 1]));
-        p[j] = cx_sub_rn(p[j], cx_mul_rn(cp[j], p[j + 1]));
-        q[j] = cx_sub_rn(q[j], cx_mul_rn(cp[j], q[j + 1]));
-      }
-      // first row: a x_{s-1} + (b + c p_1) x_s + c q_1 x_e = d - c y_1
-      ea = (s0 > 0) ? sub : mk(0.0, 0.0);
-      eb = cx_add_rn(dg[0], cx_mul_rn(sub, p[0]));
-      ec = cx_mul_rn(sub, q[0]);
-      ed = cx_sub_rn(rh[0], cx_mul_rn(sub, y[0]));
-      // last row: a p_{M-2} x_s + (b + a q_{M-2}) x_e + c x_{e+1} = d - a y_{M-2}
-      fa = cx_mul_rn(sub, p[M - 3]);
-      fb = cx_add_rn(dg[M - 1], cx_mul_rn(sub, q[M - 3]));
-      fc = (s0 + M < n) ? sub : mk(0.0, 0.0);
-      fd = cx_sub_rn(rh[M - 1], cx_mul_rn(sub, y[M - 3]));
-    } else {
-      ea = (s0 > 0) ? sub : mk(0.0, 0.0);
-      eb = dg[0];
-      ec = sub;
-      ed = rh[0];
-      fa = sub;
-      fb = dg[M - 1];
-      fc = (s0 + M < n) ? sub : mk(0.0, 0.0);
-      fd = rh[M - 1];
-    }
+    const ReducedRows rr = chunk_eliminate<M>(dg, rh, sub, s0 > 0, s0 + M < n, y, p, q);
+    const double2 ea = rr.ea, eb = rr.eb, ec = rr.ec, ed = rr.ed;
+    const double2 fa = rr.fa, fb = rr.fb, fc = rr.fc, fd = rr.fd;
     ra[2 * t] = ea; rb[2 * t] = eb; rc[2 * t] = ec; rd[2 * t] = ed;
     ra[2 * t + 1] = fa; rb[2 * t + 1] = fb; rc[2 * t + 1] = fc; rd[2 * t + 1] = fd;
     __syncthreads();
     // ---- 3. reduced system
-    cyclic_reduction<T>(ra, rb, rc, rd, nr);
+    cyclic_reduction(ra, rb, rc, rd, nr, t, T);
     // ---- 4. reconstruct
     const double2 xf = rd[2 * t], xl = rd[2 * t + 1];
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * n : nullptr;
-    C outv[M];
-    outv[0] = from_d<R>(xf);
-    outv[M - 1] = from_d<R>(xl);
-    if constexpr (M > 2) {
-#pragma unroll
-      for (int j = 0; j < M - 2; ++j)
-        outv[j + 1] = from_d<R>(cx_add_rn(cx_add_rn(y[j], cx_mul_rn(p[j], xf)), cx_mul_rn(q[j], xl)));
-    }
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-      u[s0 + m] = outv[m];
-      if (save) slot[s0 + m] = outv[m];
+      const C v = from_d<R>(chunk_value<M>(m, xf, xl, y, p, q));
+      u[s0 + m] = v;
+      if (save) slot[s0 + m] = v;
     }
     __syncthreads();
   }

@@ -54,4 +54,36 @@ cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0
                       int nsteps, cudaStream_t s);
 bool cn_supported(Precision p, int n);
 
+// ------------------------------------------------------------- ADI ------
+struct Sphere {
+  double cx, cy, cz, r, delta, beta;
+};
+constexpr int kInlineSpheres = 16;
+
+// One half step of ADI (ADI::xImplicit / yImplicit,
+// src/alternatingDirectionSolver.cpp:8-134) on an n x n field.  Systems run
+// along the implicit direction ("position"); the explicit stencil couples
+// neighbouring systems.  Element (system s, position p) is at
+// p * stride_pos + s * stride_sys.
+struct AdiHalf {
+  const void *in;
+  void *out;
+  void *save;              // optional extra copy of the output (save slot)
+  long long stride_pos, stride_sys;
+  int n;
+  int y_implicit;          // 1: y-implicit diagonal formula (reference :103)
+  int use_tbc;             // ADI::useTBC
+  int nspheres;            // active spheres; > kInlineSpheres: use spheres_all
+  double inv_dzh;          // 1.0 / (dz/2)
+  double kd2_impl;         // k*d*d along the implicit direction
+  double kd2_expl;         // k*d*d along the explicit direction
+  double k;
+  double xmin, dx, ymin, dy;
+  double z;                // material plane of this half step
+  const Sphere *spheres_all;
+  Sphere spheres[kInlineSpheres];
+};
+cudaError_t launch_adi_half(Precision p, const AdiHalf &h, cudaStream_t s);
+bool adi_supported(Precision p, int n);
+
 }  // namespace pxp
