@@ -1,0 +1,428 @@
+"""Benchmark of the paraxial propagation step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cfg1|cfg0|cfg2]
+
+Metric: grid-point * steps per second (whole job, all ranks).  A bench
+"step" is one pass of the workload over its synthetic input:
+
+  cfg1 (default)  CrankNicholson Nx=4096, 8000 steps of 0.5 um  +  ADI 1024^2,
+                  2000 steps of 1 um (unit plane wave, sphere R = 200 nm at
+                  z = 1 mm), plain FP64; the two problems run concurrently on
+                  two streams.  2.13e9 grid-point-steps per bench step.
+  cfg0            FFTSolver2D Nx=2048, 4000 steps, FP64 (8.19e6 pt-steps).
+
+Each rank runs its own replica (the path does not shard one field; weak
+scaling).  Timing: CUDA events on the solvers' own streams, warm-up first,
+L2 flushed (256 MB write) before every timed step, barrier +
+synchronize around the timed region, max over ranks.
+
+--impl reference times the CPU restatement of the reference (oracle/, the
+reference cannot be built here: Armadillo/FFTW3/HDF5 are absent) on all host
+cores, on a bounded sample of the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from paxpro_b200 import workloads as wl  # noqa: E402
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------ workloads --
+class Cfg1:
+    """CN (Nx = 4096, 8000 steps) + ADI (1024^2, 2000 steps), FP64."""
+    name = "cfg1: CrankNicholson Nx=4096 x 8000 steps + ADI 1024^2 x 2000 steps, FP64"
+
+    def __init__(self, device: int, precision: int = 0):
+        import paxpro_b200 as pxp
+        self.pxp = pxp
+        self.cn = wl.cfg1_cn()
+        self.adi = wl.cfg1_adi()
+        c, a = self.cn, self.adi
+        self.s_cn = pxp.Solver(pxp.ProblemSpec(
+            kind=pxp.CRANK_NICHOLSON, x=pxp.Disc(c.xmin, c.xmax, c.dx),
+            z=pxp.Disc(c.zmin, c.zmax, c.dz), wavenumber=wl.K, precision=precision,
+            save_every=100, device=device))
+        d, b = c.material()
+        self.s_cn.set_material_table(d, b)
+        self.s_adi = pxp.Solver(pxp.ProblemSpec(
+            kind=pxp.ADI, x=pxp.Disc(a.xmin, a.xmax, a.dx), y=pxp.Disc(a.xmin, a.xmax, a.dx),
+            z=pxp.Disc(a.zmin, a.zmax, a.dz), wavenumber=wl.K, precision=precision,
+            save_every=100, device=device))
+        self.s_adi.set_material_spheres([pxp.Sphere(*s) for s in a.spheres])
+        self.u_cn = c.initial_field()
+        self.u_adi = a.initial_field()
+        self.pts_steps = c.nx * c.nsteps + a.nx * a.nx * a.nsteps
+        self.solvers = [self.s_cn, self.s_adi]
+        # per-step algorithmic bytes (2 x complex128 per point per CN step, per
+        # ADI half step)
+        self.adi_launches_per_step = 2 * a.nsteps
+        self.adi_bytes_per_launch = 2 * 16 * a.nx * a.nx
+        self.gpu_launches_per_step = 1 + 2 * a.nsteps
+        self.h2d_bytes = 16 * (c.nx + a.nx * a.nx)
+        self.d2h_bytes = 16 * (c.nx + a.nx * a.nx)
+
+    def load_device_inputs(self):
+        # inputs resident on the device (uploaded before the timed region)
+        self.s_cn.set_initial_conditions(self.u_cn)
+        self.s_adi.set_initial_conditions(self.u_adi)
+
+    def run(self):
+        self.s_cn.step(self.cn.nsteps)
+        self.s_adi.step(self.adi.nsteps)
+
+    def close(self):
+        for s in self.solvers:
+            s.close()
+
+
+class Cfg0:
+    name = "cfg0: FFTSolver2D Nx=2048 x 4000 steps, FP64"
+
+    def __init__(self, device: int, precision: int = 0):
+        import paxpro_b200 as pxp
+        self.pxp = pxp
+        self.p = wl.cfg0()
+        p = self.p
+        self.s = pxp.Solver(pxp.ProblemSpec(
+            kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(p.xmin, p.xmax, p.dx),
+            z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K, precision=precision,
+            save_every=100, device=device))
+        d, b = p.material()
+        self.s.set_material_table(d, b)
+        self.u = p.initial_field()
+        self.pts_steps = p.nx * p.nsteps
+        self.solvers = [self.s]
+        self.adi_launches_per_step = 0
+        self.gpu_launches_per_step = 1
+        self.h2d_bytes = 16 * p.nx
+        self.d2h_bytes = 16 * p.nx
+
+    def load_device_inputs(self):
+        self.s.set_initial_conditions(self.u)
+
+    def run(self):
+        self.s.step(self.p.nsteps)
+
+    def close(self):
+        self.s.close()
+
+
+WORKLOADS = {"cfg1": Cfg1, "cfg0": Cfg0}
+
+
+# ------------------------------------------------------------- GPU arm --
+def run_ours(args, rank, world, device):
+    import torch
+    torch.cuda.set_device(device)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    W = WORKLOADS[args.workload](device)
+    streams = [torch.cuda.ExternalStream(s.stream_ptr(), device=device) for s in W.solvers]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    def one_step(timed):
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        W.load_device_inputs()
+        torch.cuda.synchronize(device)
+        ev0 = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        ev1 = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        for e, st in zip(ev0, streams):
+            e.record(st)
+        W.run()
+        for e, st in zip(ev1, streams):
+            e.record(st)
+        torch.cuda.synchronize(device)
+        # the region: from the first start to the last end
+        per_stream = [ev0[0].elapsed_time(e) for e in ev1]
+        return max(per_stream), [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
+
+    for _ in range(args.warmup):
+        one_step(False)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    times, stream_times = [], []
+    with ClockSampler(device) as clk:
+        for _ in range(args.steps):
+            t, st = one_step(True)
+            times.append(t)
+            stream_times.append(st)
+    torch.cuda.synchronize(device)
+    if dist:
+        dist.barrier()
+    total_ms = sum(times)
+
+    # end-to-end through the public API: host (pinned) inputs, H2D, steps, D2H
+    pinned_in = [torch.from_numpy(np.ascontiguousarray(u.reshape(-1, order="F")).view(np.float64)).pin_memory()
+                 for u in ([W.u_cn, W.u_adi] if args.workload == "cfg1" else [W.u])]
+    pinned_out = [torch.empty_like(t).pin_memory() for t in pinned_in]
+    e2e_times = []
+    for it in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        ev0 = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        ev1 = [torch.cuda.Event(enable_timing=True) for _ in streams]
+        for e, st in zip(ev0, streams):
+            e.record(st)
+        for s, buf in zip(W.solvers, pinned_in):
+            s.set_initial_conditions_ptr(buf.data_ptr())
+        W.run()
+        for s, buf in zip(W.solvers, pinned_out):
+            s.get_last_solution_ptr(buf.data_ptr())
+        for e, st in zip(ev1, streams):
+            e.record(st)
+        torch.cuda.synchronize(device)
+        if it >= args.warmup:
+            e2e_times.append(max(ev0[0].elapsed_time(e) for e in ev1))
+    e2e_ms = sum(e2e_times) / len(e2e_times)
+
+    t_max = total_ms
+    e2e_max = e2e_ms
+    if dist:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64)
+        if dist.get_backend() == "nccl":
+            t = t.to(device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max, e2e_max = float(t[0]), float(t[1])
+    W.close()
+    if rank != 0:
+        return None
+    ms_per_step = t_max / args.steps
+    value = world * W.pts_steps / (ms_per_step / 1e3)
+    e2e_value = world * W.pts_steps / (e2e_max / 1e3)
+    peak, peak_kind = measured_peaks()
+    roofline = None
+    if args.workload == "cfg1":
+        adi_ms = sum(st[1] for st in stream_times) / len(stream_times)
+        per_launch_s = adi_ms / 1e3 / W.adi_launches_per_step
+        achieved = W.adi_bytes_per_launch / per_launch_s / 1e9
+        roofline = {"kernel": "adi_half_kernel (FP64, 1024^2, one half step)",
+                    "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(achieved / peak, 4),
+                    "peak_kind": peak_kind,
+                    "traffic": None,
+                    "note": "algorithmic bytes 2 x 16 B per point per half step; the 16 MB "
+                            "field stays in the 126 MB L2 across half steps, so this is "
+                            "effective bandwidth (see profiles/)"}
+    return {
+        "metric": "grid-pt*steps/s (plain FP64)",
+        "value": value,
+        "unit": "grid-pt*steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded inputs with the benchmark configuration's shapes)",
+        "config": {"workload": W.name, "grid_pt_steps_per_step": W.pts_steps,
+                   "parallelism": f"replicas x{world}", "l2": "flushed before every step"},
+        "e2e": {"value": e2e_value, "unit": "grid-pt*steps/s",
+                "h2d_bytes_per_step": W.h2d_bytes, "d2h_bytes_per_step": W.d2h_bytes},
+        "gpu_launches": W.gpu_launches_per_step * args.steps,
+        "roofline": roofline,
+        "clocks": clk.summary(),
+    }
+
+
+# ------------------------------------------------------------- CPU arms --
+def cpu_rate(workload: str, threads: int, scale: float = 1.0):
+    """Oracle (CPU restatement of the reference) on a bounded sample of the
+    workload; returns (pt-steps/s extrapolated to the whole workload,
+    description of the sample)."""
+    from oracle import pyoracle as po
+    po.set_threads(threads)
+    if workload == "cfg1":
+        c, a = wl.cfg1_cn(), wl.cfg1_adi()
+        n_cn = max(20, int(800 * scale))
+        n_adi = max(1, int(4 * scale))
+        g = po.grid(c.xmin, c.xmax, c.dx, c.zmin, c.zmax, c.dz, wl.K)
+        d, b = c.material()
+        spec = po.MaterialSpec(po.MAT_XTABLE, delta_table=d, beta_table=b)
+        t0 = time.perf_counter()
+        po.cn2d_run(g, spec, c.initial_field(), n_cn, 0)
+        t_cn = time.perf_counter() - t0
+        ga = po.grid(a.xmin, a.xmax, a.dx, a.zmin, a.zmax, a.dz, wl.K)
+        sph = po.MaterialSpec(po.MAT_SPHERES, spheres=a.spheres)
+        t0 = time.perf_counter()
+        po.adi3d_run(ga, sph, a.initial_field(), n_adi, 0)
+        t_adi = time.perf_counter() - t0
+        total = t_cn * c.nsteps / n_cn + t_adi * a.nsteps / n_adi
+        pts = c.nx * c.nsteps + a.nx * a.nx * a.nsteps
+        return pts / total, (f"CN {n_cn} of {c.nsteps} steps ({t_cn:.2f} s) + ADI {n_adi} of "
+                             f"{a.nsteps} steps ({t_adi:.2f} s), extrapolated linearly")
+    p = wl.cfg0()
+    n = max(50, int(1000 * scale))
+    g = po.grid(p.xmin, p.xmax, p.dx, p.zmin, p.zmax, p.dz, wl.K)
+    d, b = p.material()
+    spec = po.MaterialSpec(po.MAT_XTABLE, delta_table=d, beta_table=b)
+    t0 = time.perf_counter()
+    po.fft2d_run(g, spec, p.initial_field(), n, 0)
+    t = time.perf_counter() - t0
+    return p.nx * p.nsteps / (t * p.nsteps / n), f"FFTSolver2D {n} of {p.nsteps} steps ({t:.2f} s)"
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    rates, sample = [], ""
+    for i in range(args.warmup + args.steps):
+        r, sample = cpu_rate(args.workload, threads, scale=0.5)
+        if i >= args.warmup:
+            rates.append(r)
+    value = statistics.median(rates)
+    W = {"cfg1": Cfg1.name, "cfg0": Cfg0.name}[args.workload]
+    return {
+        "impl": "reference",
+        "metric": "grid-pt*steps/s (plain FP64)",
+        "value": value,
+        "unit": "grid-pt*steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": W, "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "grid-pt*steps/s", "cores": threads,
+                         "kind": "port", "sample": sample + f"; {cpu_model()}"},
+        "e2e": {"value": value, "unit": "grid-pt*steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "the reference cannot be built here (Armadillo, FFTW3, HDF5, jsoncpp, VISA "
+                "absent); this is the oracle's C++ restatement of the reference path",
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfg1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out:
+            print(json.dumps(out), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out = run_ours(args, rank, world, local)
+    if out is not None and not args.no_cpu_baseline:
+        rate, sample = cpu_rate(args.workload, 1, scale=1.0)
+        out["cpu_baseline"] = {"value": rate, "unit": "grid-pt*steps/s", "cores": 1,
+                               "kind": "port", "sample": sample + f"; {cpu_model()}"}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

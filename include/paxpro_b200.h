@@ -134,6 +134,11 @@ int pxp_get_last_solution(pxp_solver s, double *field);
  * next call on the handle. */
 int pxp_get_field_device(pxp_solver s, void **dfield, int *precision);
 
+/* The CUDA stream (cudaStream_t) the solver launches its kernels and copies
+ * on, for callers that order their own work or events against it.  No
+ * reference counterpart: the reference runs on the host. */
+int pxp_get_stream(pxp_solver s, void **stream);
+
 /* Saved fields (the columns of Solver2D::solution / slices of
  * Solver3D::solution, include/solver2D.hpp:121, include/solver3D.hpp:52):
  * number of slots filled and one slot copied to the host. */

@@ -180,6 +180,23 @@ class Solver:
         self._check(_capi.lib().pxp_get_field_device(self._h, C.byref(p), C.byref(prec)))
         return p.value
 
+    def stream_ptr(self) -> int:
+        """cudaStream_t of the solver (for events / interop)."""
+        p = C.c_void_p()
+        self._check(_capi.lib().pxp_get_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def set_initial_conditions_ptr(self, host_ptr: int) -> None:
+        """Initial field from host memory at host_ptr (interleaved complex128,
+        reference layout); pinned memory makes the copy asynchronous."""
+        self._check(_capi.lib().pxp_set_initial_conditions(
+            self._h, C.cast(C.c_void_p(host_ptr), C.POINTER(C.c_double))))
+
+    def get_last_solution_ptr(self, host_ptr: int) -> None:
+        """Current field into host memory at host_ptr (complex128)."""
+        self._check(_capi.lib().pxp_get_last_solution(
+            self._h, C.cast(C.c_void_p(host_ptr), C.POINTER(C.c_double))))
+
     def num_saved(self) -> int:
         c = C.c_int()
         self._check(_capi.lib().pxp_num_saved(self._h, C.byref(c)))

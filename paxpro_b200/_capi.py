@@ -86,6 +86,7 @@ def lib():
         "pxp_synchronize": (C.c_int, [h]),
         "pxp_get_last_solution": (C.c_int, [h, d]),
         "pxp_get_field_device": (C.c_int, [h, C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
+        "pxp_get_stream": (C.c_int, [h, C.POINTER(C.c_void_p)]),
         "pxp_num_saved": (C.c_int, [h, C.POINTER(C.c_int)]),
         "pxp_get_saved": (C.c_int, [h, C.c_int, d]),
         "pxp_reset": (C.c_int, [h]),

@@ -210,8 +210,13 @@ static cudaError_t adi_launch_g(const AdiHalf &h, cudaStream_t s) {
   const size_t tile = (sizeof(C) * (G + 2) * (n + 1) + 15) & ~size_t(15);
   const size_t smem = tile + sizeof(double2) * 4 * G * 2 * (n / kAdiM);
   auto k = adi_half_kernel<R, kAdiM, G>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
+  // raise the dynamic shared-memory limit once per instantiation to the largest
+  // size it can need (n = 2048 for G = 2, n = 1024 for G = 4)
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)(((sizeof(C) * (G + 2) * (G == 2 ? 2049 : 1025) + 15) & ~size_t(15)) +
+            sizeof(double2) * 4 * G * 2 * ((G == 2 ? 2048 : 1024) / kAdiM)));
+  if (attr != cudaSuccess) return attr;
   k<<<n / G, T, smem, s>>>(h);
   return cudaGetLastError();
 }

@@ -667,6 +667,12 @@ int pxp_get_field_device(pxp_solver h, void **dfield, int *precision) {
   return PXP_OK;
 }
 
+int pxp_get_stream(pxp_solver h, void **stream) {
+  if (h == nullptr || stream == nullptr) return PXP_ERR_INVALID;
+  *stream = (void *)h->stream;
+  return PXP_OK;
+}
+
 int pxp_num_saved(pxp_solver h, int *count) {
   if (h == nullptr || count == nullptr) return PXP_ERR_INVALID;
   int c = 0;

@@ -167,8 +167,9 @@ static cudaError_t cn_launch_t(const CnJob *d_jobs, int nj, int step0, int nstep
   size_t smem = sizeof(double2) * 4 * 2 * T + sizeof(C) * kCnM * T;
   auto k = cn_kernel<R, kCnM, T>;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return attr;
   }
   k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);
   return cudaGetLastError();

@@ -101,8 +101,9 @@ static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nstep
   constexpr size_t smem = tw_smem ? field_bytes + tw_bytes : field_bytes;
   auto k = fft1d_kernel<R, N, T, tw_smem>;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return attr;
   }
   k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);
   return cudaGetLastError();
