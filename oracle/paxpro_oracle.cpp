@@ -244,6 +244,7 @@ unsigned orc_node_count(double mn, double mx, double step) {
 }
 
 void orc_set_threads(int n) { g_threads = n; }
+void orc_set_fft_parallel(int on) { g_fft_parallel = on; }
 int orc_get_threads(void) { return nthreads(); }
 
 int orc_fft1d(double *data, int n, int sign) {

@@ -103,6 +103,11 @@ void orc_gaussian_beam_3d(const orc_grid *g, double wavelength, double waist,
                           double *out /* Ny x Nx column-major */);
 void orc_plane_wave(int n, double value_re, double value_im, double *out);
 
+/* Run the lines of 2-D transforms on all OpenMP threads (1) or on one
+ * thread as the reference's FFTW plans do (0, default).  Results are the
+ * same either way: each line's transform is computed identically. */
+void orc_set_fft_parallel(int on);
+
 /* Number of OpenMP threads the oracle uses (0 = library default). */
 void orc_set_threads(int n);
 int orc_get_threads(void);

@@ -71,6 +71,7 @@ def lib():
         _LIB.orc_material_eval.argtypes = [C.POINTER(Material), C.POINTER(Grid)] + \
             [C.c_double] * 3 + [d, d]
         _LIB.orc_set_threads.argtypes = [C.c_int]
+        _LIB.orc_set_fft_parallel.argtypes = [C.c_int]
     return _LIB
 
 
@@ -231,3 +232,7 @@ def gaussian_beam_3d(g, wavelength, waist, cx=0.0, cy=0.0, amplitude=1.0, z=0.0)
 
 def set_threads(n: int) -> None:
     lib().orc_set_threads(int(n))
+
+
+def set_fft_parallel(on: bool) -> None:
+    lib().orc_set_fft_parallel(int(bool(on)))

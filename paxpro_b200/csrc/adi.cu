@@ -99,6 +99,10 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
   const int s = s_base + g;       // global system index
   const int p0 = c * M;
   const double2 sub = mk(-0.0, __ddiv_rn(-0.5, h.kd2_impl));  // -0.5*i/(k d^2)
+  const double inv_kd2_impl = __ddiv_rn(1.0, h.kd2_impl);
+  const double inv_kd2_expl = __ddiv_rn(1.0, h.kd2_expl);
+  // y half step diagonal in vacuum: i/(k dy^2 + 0 + i 0) = (0, 1/(k dy^2))
+  // exactly (Smith's division with a zero imaginary part).
   const C *ctr = tile + (g + 1) * ld;
   const C *lft = tile + g * ld;
   const C *rgt = tile + (g + 2) * ld;
@@ -122,19 +126,25 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
     if (!h.y_implicit) {
       // 1.0/dz + i/(k dx dx) + beta*k + i*delta*k   (reference :38)
       dg[m] = mk(__dadd_rn(h.inv_dzh, __dmul_rn(beta, h.k)),
-                 __dadd_rn(__ddiv_rn(1.0, h.kd2_impl), __dmul_rn(delta, h.k)));
+                 __dadd_rn(inv_kd2_impl, __dmul_rn(delta, h.k)));
     } else {
       // 1.0/dz + i/(k dy dy + beta*k + i*delta*k)   (reference :103, as written)
-      double2 q = cx_div_rn(mk(0.0, 1.0), mk(__dadd_rn(h.kd2_impl, __dmul_rn(beta, h.k)),
-                                              __dmul_rn(delta, h.k)));
+      double2 q = mk(0.0, inv_kd2_impl);
+      if (delta != 0.0 || beta != 0.0)
+        q = cx_div_rn(mk(0.0, 1.0), mk(__dadd_rn(h.kd2_impl, __dmul_rn(beta, h.k)),
+                                       __dmul_rn(delta, h.k)));
       dg[m] = mk(__dadd_rn(q.x, h.inv_dzh), q.y);
     }
-    // rhs = (1/dz - i/(k d_e^2)) u + 0.5 i u_left/(k d_e^2) + 0.5 i u_right/(k d_e^2)
+    // rhs = (1/dz - i/(k d_e^2)) u + 0.5 i (u_left + u_right)/(k d_e^2); the
+    // reference divides each neighbour term by k d_e^2, here it is one
+    // multiplication by the reciprocal (a rounding-level difference).
     const double2 uc = to_d(ctr[p]);
-    double2 r = cx_mul_rn(mk(h.inv_dzh, -__ddiv_rn(1.0, h.kd2_expl)), uc);
-    if (s > 0) r = cx_add_rn(r, cx_div_real_rn(cx_mul_rn(mk(0.0, 0.5), to_d(lft[p])), h.kd2_expl));
-    if (s < n - 1)
-      r = cx_add_rn(r, cx_div_real_rn(cx_mul_rn(mk(0.0, 0.5), to_d(rgt[p])), h.kd2_expl));
+    double2 r = cmul(mk(h.inv_dzh, -inv_kd2_expl), uc);
+    double2 nb = mk(0.0, 0.0);
+    if (s > 0) nb = to_d(lft[p]);
+    if (s < n - 1) nb = cadd(nb, to_d(rgt[p]));
+    const double hk = 0.5 * inv_kd2_expl;
+    r = mk(fma(-hk, nb.y, r.x), fma(hk, nb.x, r.y));
     rh[m] = r;
   }
   if (h.use_tbc) {

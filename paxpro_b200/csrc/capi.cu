@@ -13,6 +13,7 @@
 // served mode rounds the FP64 values (phase reduced in FP64) to complex64.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -331,6 +332,78 @@ int adi_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   return PXP_OK;
 }
 
+// ---- FFT 3-D ---------------------------------------------------------------
+// Spheres that can contain any material sample of the step between planes z0
+// and z1 (the end points and the refraction-integral points between them):
+// the sphere's z extent, widened by a relative margin, must meet [z0, z1].
+// Dropping the others is exact: a sphere that contains no sample point
+// changes no first-hit lookup.
+void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::Sphere> &out) {
+  out.clear();
+  const double lo = std::min(z0, z1), hi = std::max(z0, z1);
+  const double margin = 1e-9 * (std::fabs(lo) + std::fabs(hi) + 1.0);
+  for (const pxp_sphere &sp : h->spheres)
+    if (sp.cz + sp.radius > lo - margin && sp.cz - sp.radius < hi + margin)
+      out.push_back({sp.cx, sp.cy, sp.cz, sp.radius, sp.delta, sp.beta});
+}
+
+int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
+  const pxp_problem &p = h->prob;
+  const int n = (int)h->nx;
+  pxp::Fft3dPass q{};
+  q.field = h->d_field;
+  q.twiddle = h->d_tw;
+  q.n = n;
+  q.a = 0.5 * p.z.step / p.wavenumber;  // FFTSolver3D::kernel (src/fftSolver3D.cpp:24-30)
+  q.two_pi = 2.0 * PI;
+  q.stepn_x = p.x.step * n;
+  q.stepn_y = p.y.step * n;
+  q.k = p.wavenumber;
+  q.dz = p.z.step;
+  q.xmin = p.x.min;
+  q.dx = p.x.step;
+  q.ymin = p.y.min;
+  q.dy = p.y.step;
+  q.norm = (double)((unsigned)n * (unsigned)n);
+  if (p.absorber_damping > 0.0) {  // FFTSolver3D::absorbingBC (src/fftSolver3D.cpp:327-349)
+    q.thick_x = (int)(unsigned)(p.absorber_width / p.x.step + 1);
+    q.thick_y = (int)(unsigned)(p.absorber_width / p.y.step + 1);
+    q.inv_damp_x = p.x.step / p.absorber_damping;
+    q.inv_damp_y = p.y.step / p.absorber_damping;
+  }
+  cudaError_t e;
+  q.mode = 0;  // forward transform along y of the real-space field
+  if ((e = pxp::launch_fft3d_pass(h->prec, q, h->stream)) != cudaSuccess)
+    return h->cuda_fail(e, "FFT3D forward y pass");
+  std::vector<pxp::Sphere> act;
+  for (int i = 0; i < nsteps; ++i) {
+    const unsigned step = first + (unsigned)i;
+    q.mode = 1;
+    q.save = nullptr;
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "FFT3D x pass");
+    q.mode = (i == nsteps - 1) ? 3 : 2;
+    q.z1 = get_z(h, step);
+    q.z0 = get_z(h, step - 1);
+    slab_spheres(h, q.z0, q.z1, act);
+    q.nspheres = (int)act.size();
+    if (q.nspheres <= pxp::kInlineSpheres) {
+      for (int j = 0; j < q.nspheres; ++j) q.spheres[j] = act[j];
+      q.spheres_all = nullptr;
+    } else {
+      q.nspheres = (int)h->spheres.size();
+      q.spheres_all = h->d_spheres;
+    }
+    const bool save = h->save_every > 0 && step % (unsigned)h->save_every == 0 &&
+                      (int)(step / (unsigned)h->save_every) - 1 < h->max_slots;
+    q.save = save ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
+                  : nullptr;
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, h->stream)) != cudaSuccess)
+      return h->cuda_fail(e, "FFT3D y pass");
+  }
+  return PXP_OK;
+}
+
 int cn_write_job(pxp_solver_s *h) {
   pxp::CnJob j{};
   const unsigned n = h->nx;
@@ -423,6 +496,7 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
     case PXP_FFT_SOLVER_2D: supported = pxp::fft1d_supported(h->prec, (int)h->nx); break;
     case PXP_CRANK_NICHOLSON: supported = pxp::cn_supported(h->prec, (int)h->nx); break;
     case PXP_ADI: supported = pxp::adi_supported(h->prec, (int)h->nx); break;
+    case PXP_FFT_SOLVER_3D: supported = pxp::fft3d_supported(h->prec, (int)h->nx); break;
     default: supported = false;
   }
   if (!supported) {
@@ -470,6 +544,12 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
       if ((rc = alloc(h, &h->d_field2, h->csize * h->npts, "second field buffer")))
         return cleanup_fail(rc);
       break;
+    case PXP_FFT_SOLVER_3D: {
+      std::vector<cd> tw = twiddles((int)h->nx);
+      if ((rc = alloc(h, &h->d_tw, sizeof(cd) * h->nx, "twiddle table"))) return cleanup_fail(rc);
+      if ((rc = upload_table(h, h->d_tw, tw.data(), h->nx))) return cleanup_fail(rc);
+      break;
+    }
   }
   *out = h;
   return PXP_OK;
@@ -632,6 +712,11 @@ int pxp_step(pxp_solver h, int nsteps) {
       break;
     case PXP_ADI: {
       int rc = adi_steps(h, (unsigned)first, nsteps);
+      if (rc) return rc;
+      break;
+    }
+    case PXP_FFT_SOLVER_3D: {
+      int rc = fft3d_steps(h, (unsigned)first, nsteps);
       if (rc) return rc;
       break;
     }

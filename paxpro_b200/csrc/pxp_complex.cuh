@@ -82,6 +82,15 @@ __device__ __forceinline__ double2 cx_div_rn(double2 a, double2 b) {
   }
 }
 
+// Complex reciprocal conj(b)/|b|^2: one real division.  Used inside the
+// tridiagonal solves, where the operands are O(1e-3..1e3) and well away from
+// overflow or underflow.
+__device__ __forceinline__ double2 crecip(double2 b) {
+  double m = fma(b.x, b.x, b.y * b.y);
+  double r = 1.0 / m;
+  return mk(b.x * r, -b.y * r);
+}
+
 // Plain complex division for FP32 served mode (Smith, contractible).
 __device__ __forceinline__ float2 cdiv(float2 a, float2 b) {
   if (fabsf(b.x) < fabsf(b.y)) {

@@ -86,4 +86,39 @@ struct AdiHalf {
 cudaError_t launch_adi_half(Precision p, const AdiHalf &h, cudaStream_t s);
 bool adi_supported(Precision p, int n);
 
+// --------------------------------------------------------------- FFT 3-D --
+// FFTSolver3D (src/fftSolver3D.cpp:52-156, 327-374) on an n x n field in the
+// reference's column-major layout (element (y, x) at x*n + y).  A step is two
+// line passes over HBM:
+//   x pass: each line of fixed y index (stride n): forward FFT along x,
+//           propagator multiply, backward FFT along x;
+//   y pass: each contiguous line of fixed x: backward FFT along y,
+//           transmission / normalisation / absorber (refraction of this
+//           step), then the next step's forward FFT along y.
+// The field between pxp_step calls is in real space; the first step of a call
+// starts with a forward-only y pass and the last ends without the forward.
+struct Fft3dPass {
+  void *field;             // n*n complex (solver precision), in place
+  void *save;              // optional: real-space copy after refraction
+  const void *twiddle;     // n complex128
+  int n;
+  int mode;                // 0: forward y only; 1: x pass; 2: y pass (inverse,
+                           // refraction, forward); 3: y pass without forward
+  // propagator (x pass): K = exp(-A (kx^2 + ky^2)), A = (0, 0.5*dz/k)
+  double a;                // 0.5*dz/k
+  double two_pi;           // 2.0*PI
+  double stepn_x, stepn_y; // step*n per axis (FFTSolver3D::spatialFreqX/Y)
+  // refraction (y pass)
+  double k, dz, xmin, dx, ymin, dy, z1, z0, norm;
+  int nspheres;
+  const Sphere *spheres_all;
+  Sphere spheres[kInlineSpheres];
+  // absorber (FFTSolver3D::absorbingBC): thickness in pixels and inverse
+  // damping length per axis (0 thickness = off)
+  int thick_x, thick_y;
+  double inv_damp_x, inv_damp_y;
+};
+cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, cudaStream_t s);
+bool fft3d_supported(Precision p, int n);
+
 }  // namespace pxp

@@ -10,7 +10,8 @@
 // sides through one Thomas factorisation) and emits the two boundary rows of
 // its chunk; those 2P rows form a tridiagonal reduced system that the
 // threads solve by cyclic reduction in shared memory.  All arithmetic is
-// FP64, rounded op by op.
+// FP64; each pivot is inverted once (complex reciprocal) and applied by
+// multiplication.
 #pragma once
 #include "pxp_complex.cuh"
 
@@ -37,34 +38,35 @@ __device__ __forceinline__ ReducedRows chunk_eliminate(const double2 (&dg)[M], c
     for (int m = 1; m <= M - 2; ++m) {
       const int j = m - 1;
       double2 den = dg[m];
-      if (j > 0) den = cx_sub_rn(den, cx_mul_rn(sub, cp[j - 1]));
-      if (m < M - 2) cp[j] = cx_div_rn(sub, den);
+      if (j > 0) den = csub(den, cmul(sub, cp[j - 1]));
+      const double2 inv = crecip(den);
+      if (m < M - 2) cp[j] = cmul(sub, inv);
       double2 ry = rh[m];
-      double2 rp = (m == 1) ? cx_sub_rn(zero, sub) : zero;
-      double2 rq = (m == M - 2) ? cx_sub_rn(zero, sub) : zero;
+      double2 rp = (m == 1) ? csub(zero, sub) : zero;
+      double2 rq = (m == M - 2) ? csub(zero, sub) : zero;
       if (j > 0) {
-        ry = cx_sub_rn(ry, cx_mul_rn(sub, y[j - 1]));
-        rp = cx_sub_rn(rp, cx_mul_rn(sub, p[j - 1]));
-        rq = cx_sub_rn(rq, cx_mul_rn(sub, q[j - 1]));
+        ry = csub(ry, cmul(sub, y[j - 1]));
+        rp = csub(rp, cmul(sub, p[j - 1]));
+        if (m == M - 2) rq = csub(rq, cmul(sub, q[j - 1]));
       }
-      y[j] = cx_div_rn(ry, den);
-      p[j] = cx_div_rn(rp, den);
-      q[j] = cx_div_rn(rq, den);
+      y[j] = cmul(ry, inv);
+      p[j] = cmul(rp, inv);
+      q[j] = (m == M - 2) ? cmul(rq, inv) : zero;
     }
 #pragma unroll
     for (int j = M - 4; j >= 0; --j) {
-      y[j] = cx_sub_rn(y[j], cx_mul_rn(cp[j], y[j + 1]));
-      p[j] = cx_sub_rn(p[j], cx_mul_rn(cp[j], p[j + 1]));
-      q[j] = cx_sub_rn(q[j], cx_mul_rn(cp[j], q[j + 1]));
+      y[j] = csub(y[j], cmul(cp[j], y[j + 1]));
+      p[j] = csub(p[j], cmul(cp[j], p[j + 1]));
+      q[j] = csub(q[j], cmul(cp[j], q[j + 1]));
     }
     o.ea = has_left ? sub : zero;
-    o.eb = cx_add_rn(dg[0], cx_mul_rn(sub, p[0]));
-    o.ec = cx_mul_rn(sub, q[0]);
-    o.ed = cx_sub_rn(rh[0], cx_mul_rn(sub, y[0]));
-    o.fa = cx_mul_rn(sub, p[M - 3]);
-    o.fb = cx_add_rn(dg[M - 1], cx_mul_rn(sub, q[M - 3]));
+    o.eb = cadd(dg[0], cmul(sub, p[0]));
+    o.ec = cmul(sub, q[0]);
+    o.ed = csub(rh[0], cmul(sub, y[0]));
+    o.fa = cmul(sub, p[M - 3]);
+    o.fb = cadd(dg[M - 1], cmul(sub, q[M - 3]));
     o.fc = has_right ? sub : zero;
-    o.fd = cx_sub_rn(rh[M - 1], cx_mul_rn(sub, y[M - 3]));
+    o.fd = csub(rh[M - 1], cmul(sub, y[M - 3]));
   } else {
     o.ea = has_left ? sub : zero;
     o.eb = dg[0];
@@ -86,7 +88,7 @@ __device__ __forceinline__ double2 chunk_value(int m, double2 xf, double2 xl,
                                                const double2 (&q)[M > 2 ? M - 2 : 1]) {
   if (m == 0) return xf;
   if (m == M - 1) return xl;
-  return cx_add_rn(cx_add_rn(y[m - 1], cx_mul_rn(p[m - 1], xf)), cx_mul_rn(q[m - 1], xl));
+  return cadd(cadd(y[m - 1], cmul(p[m - 1], xf)), cmul(q[m - 1], xl));
 }
 
 // Cyclic reduction on n = 2^L >= 4 equations (a: coupling to x_{i-1},
@@ -102,16 +104,16 @@ __device__ __forceinline__ void cyclic_reduction(double2 *a, double2 *b, double2
     for (int k = tid; k < cnt; k += nt) {
       const int i = 2 * s * k + 2 * s - 1;
       const int il = i - s, ir = i + s;
-      double2 k1 = cx_div_rn(a[i], b[il]);
-      double2 ai = cx_sub_rn(zero, cx_mul_rn(a[il], k1));
-      double2 bi = cx_sub_rn(b[i], cx_mul_rn(c[il], k1));
-      double2 di = cx_sub_rn(d[i], cx_mul_rn(d[il], k1));
+      double2 k1 = cmul(a[i], crecip(b[il]));
+      double2 ai = csub(zero, cmul(a[il], k1));
+      double2 bi = csub(b[i], cmul(c[il], k1));
+      double2 di = csub(d[i], cmul(d[il], k1));
       double2 ci = zero;
       if (ir < n) {
-        double2 k2 = cx_div_rn(c[i], b[ir]);
-        ci = cx_sub_rn(zero, cx_mul_rn(c[ir], k2));
-        bi = cx_sub_rn(bi, cx_mul_rn(a[ir], k2));
-        di = cx_sub_rn(di, cx_mul_rn(d[ir], k2));
+        double2 k2 = cmul(c[i], crecip(b[ir]));
+        ci = csub(zero, cmul(c[ir], k2));
+        bi = csub(bi, cmul(a[ir], k2));
+        di = csub(di, cmul(d[ir], k2));
       }
       a[i] = ai;
       b[i] = bi;
@@ -134,9 +136,9 @@ __device__ __forceinline__ void cyclic_reduction(double2 *a, double2 *b, double2
     for (int k = tid; k < cnt; k += nt) {
       const int i = 2 * s * k + s - 1;
       double2 acc = d[i];
-      if (i - s >= 0) acc = cx_sub_rn(acc, cx_mul_rn(a[i], d[i - s]));
-      if (i + s < n) acc = cx_sub_rn(acc, cx_mul_rn(c[i], d[i + s]));
-      d[i] = cx_div_rn(acc, b[i]);
+      if (i - s >= 0) acc = csub(acc, cmul(a[i], d[i - s]));
+      if (i + s < n) acc = csub(acc, cmul(c[i], d[i + s]));
+      d[i] = cmul(acc, crecip(b[i]));
     }
     __syncthreads();
   }
