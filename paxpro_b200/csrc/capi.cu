@@ -101,13 +101,23 @@ template <typename T> void free_dev(T *&p) {
   p = nullptr;
 }
 
-// Twiddles exp(-2 pi i m / n), m < n, in extended precision.
+// Twiddles of the shared-memory Stockham transform in pass order (layout of
+// fft_smem.cuh): for each pass (sub-transform length ns, radix r = 8 while it
+// divides the rest, then 4 or 2), entries (q-1)*ns + k = exp(-2 pi i q k /
+// (ns r)), in extended precision.  At least n entries are allocated.
 std::vector<cd> twiddles(int n) {
-  std::vector<cd> w(n);
+  std::vector<cd> w(std::max(n, 1));
   const long double pi_l = 3.141592653589793238462643383279502884L;
-  for (int m = 0; m < n; ++m) {
-    long double a = -2.0L * pi_l * (long double)m / (long double)n;
-    w[m] = cd((double)cosl(a), (double)sinl(a));
+  int off = 0;
+  for (int ns = 1; ns < n;) {
+    const int r = n / ns >= 8 ? 8 : n / ns;
+    for (int q = 1; q < r; ++q)
+      for (int k = 0; k < ns; ++k) {
+        long double a = -2.0L * pi_l * (long double)(q * k) / (long double)(ns * r);
+        w[off + (q - 1) * ns + k] = cd((double)cosl(a), (double)sinl(a));
+      }
+    off += (r - 1) * ns;
+    ns *= r;
   }
   return w;
 }
@@ -695,6 +705,7 @@ int pxp_step(pxp_solver h, int nsteps) {
   if (!h->ic_set)
     return h->fail(PXP_ERR_INVALID, "setInitialConditions must be called before stepping");
   if (nsteps == 0) return PXP_OK;
+  PXP_TRY_CUDA(h, cudaSetDevice(h->prob.device));
   const long long first = h->current_step, last = first + nsteps - 1;
   if (h->plane_count > 0 &&
       (first < h->plane_first || last >= (long long)h->plane_first + h->plane_count))

@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     tw = stw;
   }
   C *field = reinterpret_cast<C *>(job.field);
-  for (int i = lane; i < N; i += T) u[i] = field[i];
+  for (int i = lane; i < N; i += T) u[sw<C>(i)] = field[i];
   __syncthreads();
   const double2 *kern = reinterpret_cast<const double2 *>(job.kern);
   const double2 *trans0 = reinterpret_cast<const double2 *>(job.trans);
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
   for (int s = 0; s < job.nsteps; ++s) {
     const int step = job.step0 + s;
     fft_smem<C, N, T, -1>(u, tw, lane);
-    for (int i = lane; i < N; i += T) u[i] = kmul<R>(u[i], kern[i]);
+    for (int i = lane; i < N; i += T) u[sw<C>(i)] = kmul<R>(u[sw<C>(i)], kern[i]);
     __syncthreads();
     fft_smem<C, N, T, +1>(u, tw, lane);
     const double2 *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
@@ -76,14 +76,14 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
     for (int i = lane; i < N; i += T) {
-      C v = u[i];
+      C v = u[sw<C>(i)];
       refract<R>(v, trans[i], nreal);
-      u[i] = v;
+      u[sw<C>(i)] = v;
       if (save) slot[i] = v;
     }
     __syncthreads();
   }
-  for (int i = lane; i < N; i += T) field[i] = u[i];
+  for (int i = lane; i < N; i += T) field[i] = u[sw<C>(i)];
 }
 
 template <typename R> constexpr int fft1d_threads(int n) {

@@ -5,9 +5,10 @@
 // along y and regrouped so that each step reads and writes the field twice:
 //   x pass  (lines of fixed row index, stride n):  F_x, * K(kx, ky), F_x^-1
 //   y pass  (contiguous lines of fixed x):          F_y^-1, refraction, F_y
-// where the y pass's trailing F_y is the next step's first transform.  A CTA
-// keeps L whole lines in shared memory; loads and stores are coalesced in
-// runs of L elements for the strided pass and fully for the contiguous one.
+// where the y pass's trailing F_y is the next step's first transform.
+// Persistent CTAs stream lines through two shared-memory buffers with
+// cp.async prefetch of the next line; each line is transformed in place in a
+// bank-conflict-free swizzled layout with the twiddles held in shared memory.
 //
 // FP64 pointwise arithmetic follows the reference op by op: the propagator
 // argument fl(a * fl(fl(kx*kx) + fl(ky*ky))) with kx, ky from
@@ -84,7 +85,7 @@ template <> __device__ __forceinline__ float2 mul_k<float>(float2 u, double2 k) 
 // Refraction, absorber: u = (u * t) / (n*n), then absorber factors.
 template <typename R>
 __device__ __forceinline__ typename Cx<R>::T refract3(const Fft3dPass &q, typename Cx<R>::T uu,
-                                                      int ix, int iy) {
+                                                      int ix, int iy, double inv_norm) {
   const double x = __dadd_rn(q.xmin, __dmul_rn((double)ix, q.dx));
   const double y = __dadd_rn(q.ymin, __dmul_rn((double)iy, q.dy));
   double delta = 0.0, beta = 0.0;
@@ -104,7 +105,9 @@ __device__ __forceinline__ typename Cx<R>::T refract3(const Fft3dPass &q, typena
       u = cmul(u, t);
     }
   }
-  u = cx_div_real_rn(u, q.norm);
+  // (u * t) / (n*n): n*n is a power of two, so multiplying by its exact
+  // reciprocal rounds identically to the division
+  u = cx_scale_rn(u, inv_norm);
   if (q.thick_y > 0) {
     if (iy < q.thick_y) u = cx_scale_rn(u, exp(-(double)(q.thick_y - iy - 1) * q.inv_damp_y));
     if (q.n - 1 - iy < q.thick_y)
@@ -118,104 +121,137 @@ __device__ __forceinline__ typename Cx<R>::T refract3(const Fft3dPass &q, typena
   return from_d<R>(u);
 }
 
-template <typename R, int N, int L, int TPL>
-__global__ void __launch_bounds__(L *TPL) fft3d_pass_kernel(const Fft3dPass q) {
-  using C = typename Cx<R>::T;
-  constexpr int T = L * TPL;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *buf = reinterpret_cast<C *>(smem_raw);
-  const int tid = threadIdx.x;
-  const int line = tid / TPL, lane = tid - line * TPL;
-  C *u = buf + line * N;
-  const double2 *tw = reinterpret_cast<const double2 *>(q.twiddle);
-  C *field = reinterpret_cast<C *>(q.field);
-  const int l0 = blockIdx.x * L;  // first line of this CTA
-  const bool strided = q.mode == 1;
+// ---- asynchronous global -> shared copies (cp.async, 8 or 16 bytes)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-  // ---- load L lines
-  for (int idx = tid; idx < L * N; idx += T) {
-    int l, j;
-    long long off;
-    if (strided) {
-      l = idx % L;
-      j = idx / L;
-      off = (long long)j * N + (l0 + l);
-    } else {
-      l = idx / N;
-      j = idx - l * N;
-      off = (long long)(l0 + l) * N + j;
+// Issue the copy of line `line` into the swizzled buffer `dst`.
+template <typename C, int N, int T>
+__device__ __forceinline__ void load_line(C *dst, const C *field, int line, bool strided) {
+  if (strided) {
+    // element j of row `line` is at j*N + line
+    for (int j = threadIdx.x; j < N; j += T) {
+      if constexpr (sizeof(C) == 16) cp_async16(dst + sw<C>(j), field + (long long)j * N + line);
+      else cp_async8(dst + sw<C>(j), field + (long long)j * N + line);
     }
-    buf[l * N + j] = field[off];
-  }
-  __syncthreads();
-
-  if (q.mode == 1) {
-    // x pass: row index of these lines is the ky index
-    fft_smem<C, N, TPL, -1>(u, tw, lane);
-    const double ky = kfreq(l0 + line, N, q.two_pi, q.stepn_y);
-    const double ky2 = __dmul_rn(ky, ky);
-    for (int j = lane; j < N; j += TPL) {
-      const double kx = kfreq(j, N, q.two_pi, q.stepn_x);
-      const double phi = __dmul_rn(q.a, __dadd_rn(__dmul_rn(kx, kx), ky2));
-      double sn, cs;
-      sincos(phi, &sn, &cs);
-      u[j] = mul_k<R>(u[j], mk(cs, -sn));
-    }
-    __syncthreads();
-    fft_smem<C, N, TPL, +1>(u, tw, lane);
   } else {
-    if (q.mode >= 2) {
-      fft_smem<C, N, TPL, +1>(u, tw, lane);
-      C *save = reinterpret_cast<C *>(q.save);
-      const int ix = l0 + line;
-      for (int j = lane; j < N; j += TPL) {
-        const C v = refract3<R>(q, u[j], ix, j);
-        u[j] = v;
-        if (save) save[(long long)ix * N + j] = v;
+    const C *src = field + (long long)line * N;
+    constexpr int per16 = 16 / (int)sizeof(C);  // elements per 16-byte chunk
+    for (int c = threadIdx.x; c < N / per16; c += T)
+      cp_async16(dst + sw<C>(c * per16), src + c * per16);
+  }
+}
+
+template <typename C, int N, int T>
+__device__ __forceinline__ void store_line(const C *src, C *field, int line, bool strided) {
+  if (strided) {
+    for (int j = threadIdx.x; j < N; j += T) field[(long long)j * N + line] = src[sw<C>(j)];
+  } else {
+    C *dst = field + (long long)line * N;
+    for (int j = threadIdx.x; j < N; j += T) dst[j] = src[sw<C>(j)];
+  }
+}
+
+// Persistent CTAs walk the n lines of one pass.  Two line buffers: the copy
+// of the next line is in flight while the current one is transformed.  The
+// twiddle table (and for the x pass the kx^2 table) is loaded into shared
+// memory once per CTA.
+template <typename R, int N, int T>
+__global__ void __launch_bounds__(T) fft3d_pass_kernel(const Fft3dPass q) {
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf0 = reinterpret_cast<C *>(smem_raw);
+  C *buf1 = buf0 + N;
+  double2 *tw = reinterpret_cast<double2 *>(buf1 + N);
+  double *kx2 = reinterpret_cast<double *>(tw + N);
+  C *field = reinterpret_cast<C *>(q.field);
+  const bool strided = q.mode == 1;
+  const int tid = threadIdx.x;
+
+  int line = blockIdx.x;
+  if (line < N) load_line<C, N, T>(buf0, field, line, strided);
+  cp_async_commit();
+  const double2 *gtw = reinterpret_cast<const double2 *>(q.twiddle);
+  for (int i = tid; i < N; i += T) tw[i] = gtw[i];
+  if (strided) {
+    for (int i = tid; i < N; i += T) {
+      const double kx = kfreq(i, N, q.two_pi, q.stepn_x);
+      kx2[i] = __dmul_rn(kx, kx);
+    }
+  }
+  const double inv_norm = 1.0 / q.norm;  // n*n is a power of two: exact
+  C *save = reinterpret_cast<C *>(q.save);
+
+  for (int it = 0; line < N; ++it, line += gridDim.x) {
+    C *u = (it & 1) ? buf1 : buf0;
+    C *nxt = (it & 1) ? buf0 : buf1;
+    const int next = line + gridDim.x;
+    if (next < N) load_line<C, N, T>(nxt, field, next, strided);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+
+    if (q.mode == 1) {
+      fft_smem<C, N, T, -1>(u, tw, tid);
+      const double ky = kfreq(line, N, q.two_pi, q.stepn_y);
+      const double ky2 = __dmul_rn(ky, ky);
+      for (int j = tid; j < N; j += T) {
+        const double phi = __dmul_rn(q.a, __dadd_rn(kx2[j], ky2));
+        double sn, cs;
+        sincos(phi, &sn, &cs);
+        u[sw<C>(j)] = mul_k<R>(u[sw<C>(j)], mk(cs, -sn));
       }
       __syncthreads();
-    }
-    if (q.mode != 3) fft_smem<C, N, TPL, -1>(u, tw, lane);
-  }
-
-  // ---- store
-  for (int idx = tid; idx < L * N; idx += T) {
-    int l, j;
-    long long off;
-    if (strided) {
-      l = idx % L;
-      j = idx / L;
-      off = (long long)j * N + (l0 + l);
+      fft_smem<C, N, T, +1>(u, tw, tid);
     } else {
-      l = idx / N;
-      j = idx - l * N;
-      off = (long long)(l0 + l) * N + j;
+      if (q.mode >= 2) {
+        fft_smem<C, N, T, +1>(u, tw, tid);
+        for (int j = tid; j < N; j += T) {
+          const C v = refract3<R>(q, u[sw<C>(j)], line, j, inv_norm);
+          u[sw<C>(j)] = v;
+          if (save) save[(long long)line * N + j] = v;
+        }
+        __syncthreads();
+      }
+      if (q.mode != 3) fft_smem<C, N, T, -1>(u, tw, tid);
     }
-    field[off] = buf[l * N + j];
+    store_line<C, N, T>(u, field, line, strided);
+    __syncthreads();  // the buffer is refilled by the prefetch of iteration it+1
   }
+  cp_async_commit();
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// Lines per CTA: about 128 KB of line data; threads per line: N/16 (two
-// radix-8 butterflies per thread per pass), at least 16.
-template <typename R, int N> constexpr int lines_per_cta() {
-  constexpr int per = (int)((128 * 1024) / (sizeof(typename Cx<R>::T) * N));
-  return per < 1 ? 1 : (per > 8 ? 8 : per);
-}
-template <int N> constexpr int threads_per_line() { return N / 16 < 16 ? 16 : (N / 16 > 512 ? 512 : N / 16); }
+template <int N> constexpr int pass_threads() { return N / 8 < 32 ? 32 : (N / 8 > 1024 ? 1024 : N / 8); }
 
 template <typename R, int N>
 static cudaError_t fft3d_launch_n(const Fft3dPass &q, cudaStream_t s) {
   using C = typename Cx<R>::T;
-  constexpr int L = lines_per_cta<R, N>();
-  constexpr int TPL = threads_per_line<N>();
-  constexpr size_t smem = sizeof(C) * L * N;
-  auto k = fft3d_pass_kernel<R, N, L, TPL>;
-  if (smem > 48 * 1024) {
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (attr != cudaSuccess) return attr;
+  constexpr int T = pass_threads<N>();
+  constexpr size_t smem = 2 * sizeof(C) * N + sizeof(double2) * N + sizeof(double) * N;
+  auto k = fft3d_pass_kernel<R, N, T>;
+  static int grid = 0;
+  if (grid == 0) {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, T, smem);
+    if (e != cudaSuccess) return e;
+    grid = sms * (per > 0 ? per : 1);
   }
-  k<<<N / L, L * TPL, smem, s>>>(q);
+  k<<<grid < N ? grid : N, T, smem, s>>>(q);
   return cudaGetLastError();
 }
 

@@ -4,8 +4,16 @@
 // then one radix-4 or radix-2 pass.  Each pass: every thread loads its
 // butterflies' R inputs into registers, the CTA synchronises, then every
 // thread applies twiddles and an R-point DFT and stores in place.  Twiddles
-// come from a table tw[m] = exp(-2 pi i m / N), m < N, computed on the host
-// in extended precision; the inverse transform uses their conjugates.
+// come from a table in pass order: for the pass with sub-transform length NS
+// and radix R, entry stockham_offset(N, NS) + (r-1)*NS + k holds
+// exp(-2 pi i r k / (NS R)), r = 1..R-1, k < NS, so that the threads of a
+// warp read consecutive entries.  Values are FP64, computed on the host in
+// extended precision; the inverse transform uses their conjugates.  With
+// complex64 data (served mode) every product with a twiddle or with
+// 1/sqrt(2) is formed in FP64 and rounded once to FP32: an FP32 complex
+// product (ac - bd with a rounded factor and cancellation) leaves a bias that
+// the same transform, applied to a slowly changing field thousands of times,
+// would accumulate coherently.
 // SIGN = -1 is the forward transform exp(-2 pi i jk/N), +1 the backward one,
 // both unnormalised (the FFTW convention the reference relies on,
 // src/fftSolver2D.cpp:68-69).
@@ -13,6 +21,18 @@
 #include "pxp_complex.cuh"
 
 namespace pxp {
+
+// Shared-memory layout of a transform line: 16-byte chunks are XOR-swizzled,
+// chunk' = chunk ^ ((chunk >> 3) & 7), so that the eight threads of every
+// access phase hit eight different 16-byte bank groups in every Stockham pass
+// (stride-R stores of the first passes included).  sw() maps an element index
+// to its slot; every access to a line in shared memory goes through it.
+template <typename C> __device__ __forceinline__ int sw(int i);
+template <> __device__ __forceinline__ int sw<double2>(int i) { return i ^ ((i >> 3) & 7); }
+template <> __device__ __forceinline__ int sw<float2>(int i) {
+  const int c = i >> 1;
+  return ((c ^ ((c >> 3) & 7)) << 1) | (i & 1);
+}
 
 // v * w and v * conj(w) with FP64 twiddles.
 __device__ __forceinline__ double2 tw_mul(double2 v, double2 w) { return cmul(v, w); }
@@ -82,10 +102,22 @@ __device__ __forceinline__ void dft_r(C *v) {
   else dft8<SIGN>(v);
 }
 
-// One Stockham pass over x (length N) with T threads; NS = length of the
-// sub-transforms already done.  `lane` is this thread's index in [0, T).
+// One Stockham pass over x (length N, swizzled layout) with T threads; NS =
+// length of the sub-transforms already done.  `lane` is this thread's index
+// in [0, T).
+// Number of twiddle entries of all passes of a length-N transform, and the
+// offset of the pass with sub-transform length NS.
+__host__ __device__ constexpr int stockham_radix(int n, int ns) { return n / ns >= 8 ? 8 : n / ns; }
+__host__ __device__ constexpr int stockham_offset(int n, int ns) {
+  int off = 0;
+  for (int s = 1; s < ns; s *= stockham_radix(n, s)) off += (stockham_radix(n, s) - 1) * s;
+  return off;
+}
+__host__ __device__ constexpr int stockham_twiddle_count(int n) { return stockham_offset(n, n); }
+
 template <typename C, int N, int T, int SIGN, int R, int NS>
 __device__ __forceinline__ void stockham_pass(C *x, const double2 *tw, int lane) {
+  constexpr int OFF = stockham_offset(N, NS);
   constexpr int NB = N / R;
   constexpr int PER = (NB + T - 1) / T;
   C v[PER][R];
@@ -94,7 +126,7 @@ __device__ __forceinline__ void stockham_pass(C *x, const double2 *tw, int lane)
     int j = lane + b * T;
     if (NB % T == 0 || j < NB) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = x[j + r * NB];
+      for (int r = 0; r < R; ++r) v[b][r] = x[sw<C>(j + r * NB)];
     }
   }
   __syncthreads();
@@ -106,14 +138,14 @@ __device__ __forceinline__ void stockham_pass(C *x, const double2 *tw, int lane)
       if constexpr (NS > 1) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          double2 w = tw[r * k * (N / (NS * R))];
+          double2 w = tw[OFF + (r - 1) * NS + k];
           v[b][r] = SIGN < 0 ? tw_mul(v[b][r], w) : tw_mulc(v[b][r], w);
         }
       }
       dft_r<R, SIGN>(v[b]);
       int base = (j - k) * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) x[base + r * NS] = v[b][r];
+      for (int r = 0; r < R; ++r) x[sw<C>(base + r * NS)] = v[b][r];
     }
   }
   __syncthreads();
