@@ -23,6 +23,7 @@
 // point of the plane.
 #include "pxp_complex.cuh"
 #include "pxp_kernels.h"
+#include "scan_solve.cuh"
 #include "tridiag.cuh"
 
 namespace pxp {
@@ -206,6 +207,118 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
     out[off] = v;
     if (save) save[off] = v;
   }
+}
+
+// Same half step when the matrix is the vacuum one for every system: the
+// right-hand side stencil is fused with the two substitution scans of the
+// precomputed factorisation (scan_solve.cuh).  No material, no boundary terms.
+template <typename R, int N, int M, int G>
+__global__ void __launch_bounds__(G *(N / M)) adi_const_kernel(const AdiHalf h,
+                                                               const double2 *__restrict__ gtab,
+                                                               const double2 *__restrict__ htab) {
+  using C = typename Cx<R>::T;
+  constexpr int P = N / M;
+  constexpr int T = G * P;
+  constexpr int ld = N + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *tile = reinterpret_cast<C *>(smem_raw);
+  double2 *gs = reinterpret_cast<double2 *>(smem_raw + ((sizeof(C) * (G + 2) * ld + 15) & ~size_t(15)));
+  double2 *hs = gs + N;
+  Affine *scratch = reinterpret_cast<Affine *>(hs + N);
+  const int tid = threadIdx.x;
+  const int s_base = blockIdx.x * G;
+  const C *in = reinterpret_cast<const C *>(h.in);
+  C *out = reinterpret_cast<C *>(h.out);
+  const bool interleaved = h.stride_sys == 1;
+  constexpr int rows = G + 2;
+  for (int idx = tid; idx < rows * N; idx += T) {
+    int g, p;
+    if (interleaved) {
+      p = idx / rows;
+      g = idx - p * rows;
+    } else {
+      g = idx / N;
+      p = idx - g * N;
+    }
+    const int s = s_base - 1 + g;
+    C v = from_d<R>(mk(0.0, 0.0));
+    if (s >= 0 && s < N) v = in[(long long)p * h.stride_pos + (long long)s * h.stride_sys];
+    tile[g * ld + p] = v;
+  }
+  for (int i = tid; i < N; i += T) {
+    gs[i] = gtab[i];
+    hs[i] = htab[i];
+  }
+  __syncthreads();
+  const int g = tid / P, c = tid - g * P;
+  const int s = s_base + g;
+  const int p0 = c * M;
+  const double inv_kd2_expl = __ddiv_rn(1.0, h.kd2_expl);
+  const double hk = 0.5 * inv_kd2_expl;
+  const C *ctr = tile + (g + 1) * ld;
+  const C *lft = tile + g * ld;
+  const C *rgt = tile + (g + 2) * ld;
+  double2 r[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int p = p0 + m;
+    double2 rr = cmul(mk(h.inv_dzh, -inv_kd2_expl), to_d(ctr[p]));
+    double2 nb = mk(0.0, 0.0);
+    if (s > 0) nb = to_d(lft[p]);
+    if (s < N - 1) nb = cadd(nb, to_d(rgt[p]));
+    r[m] = mk(fma(-hk, nb.y, rr.x), fma(hk, nb.x, rr.y));
+  }
+  const_solve<M, P>(r, gs, hs, p0, scratch);
+  __syncthreads();  // every read of the staged tile is done
+  C *dst = tile + (g + 1) * ld;
+#pragma unroll
+  for (int m = 0; m < M; ++m) dst[p0 + m] = from_d<R>(r[m]);
+  __syncthreads();
+  C *save = reinterpret_cast<C *>(h.save);
+  for (int idx = tid; idx < G * N; idx += T) {
+    int gg, p;
+    if (interleaved) {
+      p = idx / G;
+      gg = idx - p * G;
+    } else {
+      gg = idx / N;
+      p = idx - gg * N;
+    }
+    const long long off = (long long)p * h.stride_pos + (long long)(s_base + gg) * h.stride_sys;
+    const C v = tile[(gg + 1) * ld + p];
+    out[off] = v;
+    if (save) save[off] = v;
+  }
+}
+
+template <typename R, int N, int G>
+static cudaError_t adi_const_launch(const AdiHalf &h, const void *g, const void *hh, cudaStream_t s) {
+  using C = typename Cx<R>::T;
+  constexpr int M = 8, P = N / M, T = G * P;
+  constexpr size_t smem = ((sizeof(C) * (G + 2) * (N + 1) + 15) & ~size_t(15)) +
+                          2 * sizeof(double2) * N + sizeof(Affine) * (T / 32 + 1);
+  auto k = adi_const_kernel<R, N, M, G>;
+  if (smem > 48 * 1024) {
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return attr;
+  }
+  k<<<N / G, T, smem, s>>>(h, (const double2 *)g, (const double2 *)hh);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, const void *hh,
+                                  cudaStream_t s) {
+#define PXP_AC(NN, GG)                                                                  \
+  case NN:                                                                              \
+    return p == kFP64 ? adi_const_launch<double, NN, GG>(h, g, hh, s)                   \
+                      : adi_const_launch<float, NN, GG>(h, g, hh, s);
+  switch (h.n) {
+    PXP_AC(64, 4) PXP_AC(128, 4) PXP_AC(256, 4) PXP_AC(512, 4) PXP_AC(1024, 4) PXP_AC(2048, 2)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef PXP_AC
 }
 
 static constexpr int kAdiM = 8;

@@ -68,6 +68,8 @@ struct pxp_solver_s {
   void *d_job = nullptr;
   // 2-transverse-dim solvers
   void *d_field2 = nullptr;                  // ping-pong buffer
+  void *d_lu = nullptr;                      // factor tables of step-invariant matrices
+  bool cn_const = false;                     // CN matrix step-invariant
   std::vector<pxp_sphere> spheres;           // first-hit sphere material
   pxp::Sphere *d_spheres = nullptr;
   // host copies
@@ -231,6 +233,8 @@ int fft1d_write_job(pxp_solver_s *h) {
 }
 
 // ---- CN --------------------------------------------------------------------
+int cn_build_lu(pxp_solver_s *h, const double *delta, const double *beta);
+
 int cn_set_planes(pxp_solver_s *h, const double *delta, const double *beta, int nsteps,
                   int first_step, bool two_planes_per_step) {
   // Device layout: 4 blocks [delta | beta | delta_prev | beta_prev], each
@@ -256,6 +260,73 @@ int cn_set_planes(pxp_solver_s *h, const double *delta, const double *beta, int 
   h->mat_stride = nsteps > 1 ? n : 0;
   h->mat_step0 = first_step;
   h->material_set = true;
+  // step-invariant matrix when the same plane serves every step
+  h->cn_const = false;
+  if (nsteps == 1 && pxp::cn_const_supported(h->prec, (int)n)) {
+    int rc2 = cn_build_lu(h, delta, beta);
+    if (rc2) return rc2;
+    h->cn_const = true;
+  }
+  return PXP_OK;
+}
+
+// ---- step-invariant matrices --------------------------------------------------
+// Thomas factor tables of a tridiagonal matrix with diagonal `diag` and
+// constant symmetric off-diagonal `sub` (include/thomasAlgorithm.tpp:2-32
+// forward sweep): g_i = 1/den_i, h_i = -sub * g_i, see scan_solve.cuh.
+void thomas_factor(const std::vector<cd> &diag, cd sub, std::vector<cd> &out_gh) {
+  const size_t n = diag.size();
+  out_gh.assign(2 * n, cd(0.0));
+  cd den = diag[0];
+  for (size_t i = 0; i < n; ++i) {
+    if (i > 0) den = diag[i] - sub * (sub * out_gh[i - 1]);
+    const cd g = cd(1.0) / den;
+    out_gh[i] = g;
+    out_gh[n + i] = -sub * g;
+  }
+}
+
+// CrankNicholson matrix for a z-invariant medium (src/crancNicholson.cpp:
+// 46-52 with F = G = H = 1, J = 0), evaluated with the reference's
+// std::complex expressions.
+int cn_build_lu(pxp_solver_s *h, const double *delta, const double *beta) {
+  const unsigned n = h->nx;
+  const cd IMAG_UNIT(0.0, 1.0);
+  const double dx = h->prob.x.step, dz = h->prob.z.step, k = h->prob.wavenumber;
+  const double rho = dz / (k * dx * dx), r = k * dz;
+  const double Hp = 1.0, Hm = 1.0, gval = 1.0, fval = 1.0;
+  std::vector<cd> diag(n);
+  for (unsigned i = 0; i < n; ++i)
+    diag[i] = fval * 1.0 + 0.25 * (Hp + Hm) * gval * IMAG_UNIT * rho +
+              0.5 * (beta[i] * r + IMAG_UNIT * delta[i] * r);
+  const cd sub = -0.25 * IMAG_UNIT * rho * Hm * gval;
+  std::vector<cd> gh;
+  thomas_factor(diag, sub, gh);
+  free_dev(h->d_lu);
+  int rc;
+  if ((rc = alloc(h, &h->d_lu, sizeof(cd) * 2 * n, "factor tables"))) return rc;
+  PXP_TRY_CUDA(h, cudaMemcpy(h->d_lu, gh.data(), sizeof(cd) * 2 * n, cudaMemcpyHostToDevice));
+  return PXP_OK;
+}
+
+// ADI vacuum matrices of the x and y half steps (src/alternatingDirection
+// Solver.cpp:38, :103 with beta = delta = 0): tables [gx | hx | gy | hy].
+int adi_build_lu(pxp_solver_s *h) {
+  const unsigned n = h->nx;
+  const cd im(0.0, 1.0);
+  const double dz = h->prob.z.step / 2.0, k = h->prob.wavenumber;
+  const double dx = h->prob.x.step, dy = h->prob.y.step;
+  const double beta = 0.0, delta = 0.0;
+  std::vector<cd> dgx(n, 1.0 / dz + im / (k * dx * dx) + beta * k + im * delta * k);
+  std::vector<cd> dgy(n, 1.0 / dz + im / (k * dy * dy + beta * k + im * delta * k));
+  std::vector<cd> gx, gy;
+  thomas_factor(dgx, -0.5 * im / (k * dx * dx), gx);
+  thomas_factor(dgy, -0.5 * im / (k * dy * dy), gy);
+  gx.insert(gx.end(), gy.begin(), gy.end());
+  free_dev(h->d_lu);
+  int rc;
+  if ((rc = alloc(h, &h->d_lu, sizeof(cd) * 4 * n, "factor tables"))) return rc;
+  PXP_TRY_CUDA(h, cudaMemcpy(h->d_lu, gx.data(), sizeof(cd) * 4 * n, cudaMemcpyHostToDevice));
   return PXP_OK;
 }
 
@@ -320,7 +391,10 @@ int adi_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     a.kd2_expl = kdy2;
     a.z = get_z(h, step);
     adi_fill_spheres(h, a, a.z);
-    cudaError_t e = pxp::launch_adi_half(h->prec, a, h->stream);
+    const cd *lu = (const cd *)h->d_lu;
+    cudaError_t e = (a.nspheres == 0 && !a.use_tbc && lu)
+                        ? pxp::launch_adi_half_const(h->prec, a, lu, lu + n, h->stream)
+                        : pxp::launch_adi_half(h->prec, a, h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "ADI x half step");
     // y implicit: systems are columns (x), positions run along y (stride 1)
     a.in = h->d_field2;
@@ -336,7 +410,9 @@ int adi_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     a.kd2_expl = kdx2;
     a.z = get_z(h, step) + dzh;
     adi_fill_spheres(h, a, a.z);
-    e = pxp::launch_adi_half(h->prec, a, h->stream);
+    e = (a.nspheres == 0 && !a.use_tbc && lu)
+            ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n, h->stream)
+            : pxp::launch_adi_half(h->prec, a, h->stream);
     if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
   }
   return PXP_OK;
@@ -432,6 +508,8 @@ int cn_write_job(pxp_solver_s *h) {
   j.max_slots = h->max_slots;
   j.mat_step0 = h->mat_step0;
   j.transparent = h->prob.transparent_bc ? 1 : 0;
+  j.lu_g = h->d_lu;
+  j.lu_h = h->d_lu ? (const void *)((const cd *)h->d_lu + n) : nullptr;
   PXP_TRY_CUDA(h, cudaMemcpy(h->d_job, &j, sizeof(j), cudaMemcpyHostToDevice));
   return PXP_OK;
 }
@@ -553,6 +631,7 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
     case PXP_ADI:
       if ((rc = alloc(h, &h->d_field2, h->csize * h->npts, "second field buffer")))
         return cleanup_fail(rc);
+      if ((rc = adi_build_lu(h))) return cleanup_fail(rc);
       break;
     case PXP_FFT_SOLVER_3D: {
       std::vector<cd> tw = twiddles((int)h->nx);
@@ -577,6 +656,7 @@ int pxp_solver_destroy(pxp_solver h) {
   free_dev(h->d_job);
   free_dev(h->d_field2);
   free_dev(h->d_spheres);
+  free_dev(h->d_lu);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return PXP_OK;
@@ -718,8 +798,12 @@ int pxp_step(pxp_solver h, int nsteps) {
                             (int)first, nsteps, h->stream);
       break;
     case PXP_CRANK_NICHOLSON:
-      e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first, nsteps,
-                         h->stream);
+      if (h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0)
+        e = pxp::launch_cn_const(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first,
+                                 nsteps, h->stream);
+      else
+        e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first,
+                           nsteps, h->stream);
       break;
     case PXP_ADI: {
       int rc = adi_steps(h, (unsigned)first, nsteps);

@@ -22,6 +22,7 @@
 // condition ~ rho), so the difference stays near machine precision.
 #include "pxp_complex.cuh"
 #include "pxp_kernels.h"
+#include "scan_solve.cuh"
 #include "tridiag.cuh"
 
 namespace pxp {
@@ -158,7 +159,119 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
   for (int i = t; i < n; i += T) field[i] = u[i];
 }
 
+// z-invariant medium, Dirichlet ends: the step matrix is fixed, so the
+// factor tables g, h (host-computed) are loaded into shared memory once and
+// each step is the right-hand-side stencil plus two substitution scans
+// (scan_solve.cuh).  The field stays in registers: thread t owns points
+// t*M .. t*M+M-1 and trades its two edge values with its neighbours through
+// shared memory.  The per-point right-hand-side coefficient
+// 1 - 0.5*(beta'*r + i*delta'*r) is formed once with the reference's
+// rounding and kept in shared memory.
+template <typename R, int M, int T>
+__global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ jobs, int step0_ov,
+                                                    int nsteps_ov) {
+  using C = typename Cx<R>::T;
+  constexpr int N = M * T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *gs = reinterpret_cast<double2 *>(smem_raw);
+  double2 *hs = gs + N;
+  double2 *coef = hs + N;
+  double2 *xch = coef + N;  // 2 per thread
+  Affine *scratch = reinterpret_cast<Affine *>(xch + 2 * T);
+  CnJob job = jobs[blockIdx.x];
+  if (nsteps_ov >= 0) {
+    job.step0 = step0_ov;
+    job.nsteps = nsteps_ov;
+  }
+  const int t = threadIdx.x;
+  const double rho = job.rho, r = job.r;
+  const double2 *gt = reinterpret_cast<const double2 *>(job.lu_g);
+  const double2 *ht = reinterpret_cast<const double2 *>(job.lu_h);
+  for (int i = t; i < N; i += T) {
+    gs[i] = gt[i];
+    hs[i] = ht[i];
+    const double bp = job.beta_prev[i], dp = job.delta_prev[i];
+    const double2 hh = mk(__dmul_rn(0.5, __dmul_rn(bp, r)), __dmul_rn(0.5, __dmul_rn(dp, r)));
+    coef[i] = mk(__dadd_rn(-hh.x, 1.0), -hh.y);
+  }
+  C *field = reinterpret_cast<C *>(job.field);
+  const int s0 = t * M;
+  double2 u[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) u[m] = to_d(field[s0 + m]);
+  const double q = __dmul_rn(0.25, rho);
+  C *saves = reinterpret_cast<C *>(job.saves);
+  __syncthreads();
+  for (int st = 0; st < job.nsteps; ++st) {
+    const int step = job.step0 + st;
+    xch[2 * t] = u[0];
+    xch[2 * t + 1] = u[M - 1];
+    __syncthreads();
+    const double2 lft = t > 0 ? xch[2 * t - 1] : mk(0.0, 0.0);
+    const double2 rgt = t < T - 1 ? xch[2 * t + 2] : mk(0.0, 0.0);
+    double2 rh[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const double2 left = m > 0 ? u[m - 1] : lft;
+      const double2 right = m < M - 1 ? u[m + 1] : rgt;
+      // cn_rhs with the coefficient precomputed (same operations)
+      double2 sum = cx_add_rn(left, right);
+      double2 v = cx_mul_rn(sum, mk(0.0, q));
+      double2 c4 = cx_scale_rn(u[m], 0.25);
+      double2 tt = cx_scale_rn(cx_scale_rn(cx_mul_rn(c4, mk(0.0, 1.0)), rho), 2.0);
+      v = cx_sub_rn(v, tt);
+      rh[m] = cx_add_rn(v, cx_mul_rn(coef[s0 + m], u[m]));
+    }
+    const_solve<M, T>(rh, gs, hs, s0, scratch);
+    const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
+                      (step / job.save_every - 1) < job.max_slots;
+    C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const C v = from_d<R>(rh[m]);
+      u[m] = to_d(v);
+      if (save) slot[s0 + m] = v;
+    }
+    __syncthreads();  // xch is rewritten next step
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) field[s0 + m] = from_d<R>(u[m]);
+}
+
 static constexpr int kCnM = 8;
+
+template <typename R, int T>
+static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
+                                     cudaStream_t s) {
+  constexpr int N = kCnM * T;
+  constexpr size_t smem = sizeof(double2) * (3 * N + 2 * T) + sizeof(Affine) * (T / 32 + 1);
+  auto k = cn_const_kernel<R, kCnM, T>;
+  if (smem > 48 * 1024) {
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return attr;
+  }
+  k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);
+  return cudaGetLastError();
+}
+
+bool cn_const_supported(Precision, int n) { return n >= 2 * kCnM && !(n & (n - 1)) && n <= 4096; }
+
+cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0, int nsteps,
+                            cudaStream_t s) {
+  if (nj <= 0) return cudaSuccess;
+#define PXP_CC(TT)                                                                     \
+  case TT:                                                                             \
+    return p == kFP64 ? cn_const_launch_t<double, TT>(d_jobs, nj, step0, nsteps, s)   \
+                      : cn_const_launch_t<float, TT>(d_jobs, nj, step0, nsteps, s);
+  switch (n / kCnM) {
+    PXP_CC(2) PXP_CC(4) PXP_CC(8) PXP_CC(16) PXP_CC(32) PXP_CC(64) PXP_CC(128) PXP_CC(256)
+    PXP_CC(512)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef PXP_CC
+}
 
 template <typename R, int T>
 static cudaError_t cn_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,

@@ -49,10 +49,16 @@ struct CnJob {
   int step0, nsteps, save_every, max_slots, mat_step0;
   int transparent;             // BC_t::TRANSPARENT
   int status;                  // unused (reserved)
+  const void *lu_g, *lu_h;     // factor tables of the step matrix (const path)
 };
 cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
                       int nsteps, cudaStream_t s);
 bool cn_supported(Precision p, int n);
+// z-invariant medium and Dirichlet ends: the step matrix never changes; the
+// job's lu_g / lu_h hold its Thomas factor tables (n complex128 each).
+cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
+                            int nsteps, cudaStream_t s);
+bool cn_const_supported(Precision p, int n);
 
 // ------------------------------------------------------------- ADI ------
 struct Sphere {
@@ -85,6 +91,11 @@ struct AdiHalf {
 };
 cudaError_t launch_adi_half(Precision p, const AdiHalf &h, cudaStream_t s);
 bool adi_supported(Precision p, int n);
+// Half step whose plane holds no material and no transparent boundary: the
+// matrix is the same for every system and every step; g/h are its Thomas
+// factor tables (n complex128 each, see scan_solve.cuh).
+cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, const void *hh,
+                                  cudaStream_t s);
 
 // --------------------------------------------------------------- FFT 3-D --
 // FFTSolver3D (src/fftSolver3D.cpp:52-156, 327-374) on an n x n field in the

@@ -1,0 +1,143 @@
+// scan_solve.cuh -- tridiagonal solve with a step-invariant matrix as two
+// parallel linear-recurrence scans.
+//
+// When the system matrix does not change between steps (CrankNicholson with a
+// z-invariant medium and Dirichlet ends; an ADI half step whose plane holds
+// no material), its Thomas factorisation (include/thomasAlgorithm.tpp:2-32)
+// is computed once on the host:
+//   den_0 = b_0,  den_i = b_i - s * c'_{i-1},  c'_i = s / den_i,
+// and stored per position as g_i = 1/den_i and h_i = -s * g_i (s = the
+// constant symmetric off-diagonal; h_i is zero at the last position).  Each
+// step then needs only the two substitutions, both first-order linear
+// recurrences:
+//   forward   y_i = g_i r_i + h_i y_{i-1}          (h_{-1} term absent)
+//   backward  x_i = y_i + h_i x_{i+1}
+// (with symmetric off-diagonals the forward multiplier -s g_i equals the
+// backward one -c'_i).  A system of L rows is split into P chunks of M rows,
+// one chunk per thread: each thread runs its chunk with a zero carry-in and
+// records the chunk's transfer (A, B) (y_out = A y_in + B); a scan of the
+// transfers across the P chunks (warp shuffles, then one shared-memory step
+// across warps) gives every chunk its carry-in, and a second sweep adds the
+// carry-in times the running product of multipliers.  No division occurs in
+// the step.  The scan reassociates the products, a rounding-level difference
+// from the serial sweep; the multipliers have modulus below one for these
+// diagonally dominant systems, so the products stay bounded.
+#pragma once
+#include "pxp_complex.cuh"
+
+namespace pxp {
+
+struct Affine {
+  double2 a, b;  // y_out = a * y_in + b
+};
+
+// after(first, second): apply `first`, then `second`.
+__device__ __forceinline__ Affine compose(Affine first, Affine second) {
+  return {cmul(second.a, first.a), cadd(cmul(second.a, first.b), second.b)};
+}
+
+template <bool DOWN>
+__device__ __forceinline__ Affine shfl(Affine v, int d) {
+  Affine o;
+  if (DOWN) {
+    o.a.x = __shfl_down_sync(0xffffffffu, v.a.x, d);
+    o.a.y = __shfl_down_sync(0xffffffffu, v.a.y, d);
+    o.b.x = __shfl_down_sync(0xffffffffu, v.b.x, d);
+    o.b.y = __shfl_down_sync(0xffffffffu, v.b.y, d);
+  } else {
+    o.a.x = __shfl_up_sync(0xffffffffu, v.a.x, d);
+    o.a.y = __shfl_up_sync(0xffffffffu, v.a.y, d);
+    o.b.x = __shfl_up_sync(0xffffffffu, v.b.x, d);
+    o.b.y = __shfl_up_sync(0xffffffffu, v.b.y, d);
+  }
+  return o;
+}
+
+// Exclusive scan of chunk transfers over the P threads of each system (the
+// P threads are contiguous in the CTA, chunk c at thread offset c, P a power
+// of two).  REVERSE = false scans in increasing chunk order (forward
+// substitution), true in decreasing order (back substitution).  Returns the
+// composition of the transfers of all chunks that precede this one in scan
+// order (identity for the first).  `scratch` holds one Affine per warp of the
+// CTA; every thread of the CTA must call with the same P.
+template <int P, bool REVERSE>
+__device__ __forceinline__ Affine exclusive_scan(Affine v, Affine *scratch) {
+  const int lane = threadIdx.x & 31;
+  constexpr int SEG = P < 32 ? P : 32;  // lanes per system inside a warp
+  const int seg_lane = lane & (SEG - 1);
+  const Affine ident = {mk(1.0, 0.0), mk(0.0, 0.0)};
+  Affine inc = v;
+#pragma unroll
+  for (int d = 1; d < SEG; d <<= 1) {
+    Affine o = shfl<REVERSE>(inc, d);
+    const bool take = REVERSE ? (seg_lane + d < SEG) : (seg_lane >= d);
+    if (take) inc = compose(o, inc);
+  }
+  Affine ex = shfl<REVERSE>(inc, 1);
+  if (REVERSE ? seg_lane == SEG - 1 : seg_lane == 0) ex = ident;
+  if constexpr (P > 32) {
+    constexpr int W = P / 32;  // warps per system
+    const int warp = threadIdx.x >> 5;
+    const int chunk_warp = (threadIdx.x % P) >> 5;  // warp index inside the system
+    const int first_warp = warp - chunk_warp;
+    __syncthreads();
+    // a warp's total is the inclusive value of its last lane in scan order
+    if (lane == (REVERSE ? 0 : 31)) scratch[warp] = inc;
+    __syncthreads();
+    Affine pre = ident;
+    if (REVERSE) {
+      for (int w = W - 1; w > chunk_warp; --w) pre = compose(pre, scratch[first_warp + w]);
+    } else {
+      for (int w = 0; w < chunk_warp; ++w) pre = compose(pre, scratch[first_warp + w]);
+    }
+    ex = compose(pre, ex);
+  }
+  return ex;
+}
+
+// Solve one system whose chunk rows this thread holds: r[m] is the right-hand
+// side of row p0 + m on entry and the solution on exit.  g, h: the factor
+// tables (global positions).  P threads per system, chunk c = thread offset.
+template <int M, int P>
+__device__ __forceinline__ void const_solve(double2 (&r)[M], const double2 *__restrict__ g,
+                                            const double2 *__restrict__ h, int p0,
+                                            Affine *scratch) {
+  const double2 one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
+  // forward, zero carry-in
+  double2 prod = one, y = zero;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const double2 hm = h[p0 + m];
+    y = cadd(cmul(g[p0 + m], r[m]), cmul(hm, y));
+    prod = cmul(hm, prod);
+    r[m] = y;
+  }
+  Affine ex = exclusive_scan<P, false>(Affine{prod, y}, scratch);
+  const double2 y_in = ex.b;
+  prod = one;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    prod = cmul(h[p0 + m], prod);
+    r[m] = cadd(r[m], cmul(prod, y_in));
+  }
+  // backward, zero carry-in: x_i = y_i + h_i x_{i+1}
+  double2 x = zero;
+  prod = one;
+#pragma unroll
+  for (int m = M - 1; m >= 0; --m) {
+    const double2 hm = h[p0 + m];
+    x = cadd(r[m], cmul(hm, x));
+    prod = cmul(hm, prod);
+    r[m] = x;
+  }
+  ex = exclusive_scan<P, true>(Affine{prod, x}, scratch);
+  const double2 x_in = ex.b;
+  prod = one;
+#pragma unroll
+  for (int m = M - 1; m >= 0; --m) {
+    prod = cmul(h[p0 + m], prod);
+    r[m] = cadd(r[m], cmul(prod, x_in));
+  }
+}
+
+}  // namespace pxp
