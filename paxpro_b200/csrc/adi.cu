@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
   const int n = h.n;
   const int P = n / M;        // chunks per system
   const int T = G * P;        // threads
-  const int ld = n + 1;       // padded row of the staging tile
+  const int ld = n + n / 8 + 2;  // padded row of the staging tile (pad8)
   C *tile = reinterpret_cast<C *>(smem_raw);                  // (G+2) x ld
   double2 *red = reinterpret_cast<double2 *>(
       smem_raw + ((sizeof(C) * (G + 2) * ld + 15) & ~size_t(15)));  // 4 x G x 2P
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
     const int s = s_base - 1 + g;
     C v = from_d<R>(mk(0.0, 0.0));
     if (s >= 0 && s < n) v = in[(long long)p * h.stride_pos + (long long)s * h.stride_sys];
-    tile[g * ld + p] = v;
+    tile[g * ld + pad8(p)] = v;
   }
   __syncthreads();
 
@@ -139,11 +139,11 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
     // rhs = (1/dz - i/(k d_e^2)) u + 0.5 i (u_left + u_right)/(k d_e^2); the
     // reference divides each neighbour term by k d_e^2, here it is one
     // multiplication by the reciprocal (a rounding-level difference).
-    const double2 uc = to_d(ctr[p]);
+    const double2 uc = to_d(ctr[pad8(p)]);
     double2 r = cmul(mk(h.inv_dzh, -inv_kd2_expl), uc);
     double2 nb = mk(0.0, 0.0);
-    if (s > 0) nb = to_d(lft[p]);
-    if (s < n - 1) nb = cadd(nb, to_d(rgt[p]));
+    if (s > 0) nb = to_d(lft[pad8(p)]);
+    if (s < n - 1) nb = cadd(nb, to_d(rgt[pad8(p)]));
     const double hk = 0.5 * inv_kd2_expl;
     r = mk(fma(-hk, nb.y, r.x), fma(hk, nb.x, r.y));
     rh[m] = r;
@@ -152,14 +152,14 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
     const double zero = 1e-6;
     // along the system (implicit direction): diagonal at both ends
     if (c == P - 1) {
-      double2 inner = to_d(ctr[n - 2]);
+      double2 inner = to_d(ctr[pad8(n - 2)]);
       if (hypot(inner.x, inner.y) > zero)
-        dg[M - 1] = cx_sub_rn(dg[M - 1], cx_div_real_rn(tbc_factor(to_d(ctr[n - 1]), inner), h.kd2_impl));
+        dg[M - 1] = cx_sub_rn(dg[M - 1], cx_div_real_rn(tbc_factor(to_d(ctr[pad8(n - 1)]), inner), h.kd2_impl));
     }
     if (c == 0) {
-      double2 inner = to_d(ctr[1]);
+      double2 inner = to_d(ctr[pad8(1)]);
       if (hypot(inner.x, inner.y) > zero)
-        dg[0] = cx_sub_rn(dg[0], cx_div_real_rn(tbc_factor(to_d(ctr[0]), inner), h.kd2_impl));
+        dg[0] = cx_sub_rn(dg[0], cx_div_real_rn(tbc_factor(to_d(ctr[pad8(0)]), inner), h.kd2_impl));
     }
     // across systems (explicit direction): rhs of the first and last system
     if (s == n - 1 || s == 0) {
@@ -167,9 +167,9 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         const int p = p0 + m;
-        double2 inner = to_d(inner_row[p]);
+        double2 inner = to_d(inner_row[pad8(p)]);
         if (hypot(inner.x, inner.y) > zero) {
-          double2 edge = to_d(ctr[p]);
+          double2 edge = to_d(ctr[pad8(p)]);
           double2 f = cx_mul_rn(tbc_factor(edge, inner), edge);
           rh[m] = cx_add_rn(rh[m], cx_div_real_rn(f, h.kd2_expl));
         }
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
   const double2 xf = rd[2 * c], xl = rd[2 * c + 1];
   C *dst = tile + (g + 1) * ld;
 #pragma unroll
-  for (int m = 0; m < M; ++m) dst[p0 + m] = from_d<R>(chunk_value<M>(m, xf, xl, yv, pv, qv));
+  for (int m = 0; m < M; ++m) dst[pad8(p0 + m)] = from_d<R>(chunk_value<M>(m, xf, xl, yv, pv, qv));
   __syncthreads();
   C *save = reinterpret_cast<C *>(h.save);
   for (int idx = tid; idx < G * n; idx += T) {
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
       p = idx - gg * n;
     }
     const long long off = (long long)p * h.stride_pos + (long long)(s_base + gg) * h.stride_sys;
-    const C v = tile[(gg + 1) * ld + p];
+    const C v = tile[(gg + 1) * ld + pad8(p)];
     out[off] = v;
     if (save) save[off] = v;
   }
@@ -219,12 +219,12 @@ __global__ void __launch_bounds__(G *(N / M)) adi_const_kernel(const AdiHalf h,
   using C = typename Cx<R>::T;
   constexpr int P = N / M;
   constexpr int T = G * P;
-  constexpr int ld = N + 1;
+  constexpr int ld = N + N / 8 + 2;  // padded row (pad8)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *tile = reinterpret_cast<C *>(smem_raw);
   double2 *gs = reinterpret_cast<double2 *>(smem_raw + ((sizeof(C) * (G + 2) * ld + 15) & ~size_t(15)));
-  double2 *hs = gs + N;
-  Affine *scratch = reinterpret_cast<Affine *>(hs + N);
+  double2 *hs = gs + (N + N / 8);
+  Affine *scratch = reinterpret_cast<Affine *>(hs + (N + N / 8));
   const int tid = threadIdx.x;
   const int s_base = blockIdx.x * G;
   const C *in = reinterpret_cast<const C *>(h.in);
@@ -243,11 +243,11 @@ __global__ void __launch_bounds__(G *(N / M)) adi_const_kernel(const AdiHalf h,
     const int s = s_base - 1 + g;
     C v = from_d<R>(mk(0.0, 0.0));
     if (s >= 0 && s < N) v = in[(long long)p * h.stride_pos + (long long)s * h.stride_sys];
-    tile[g * ld + p] = v;
+    tile[g * ld + pad8(p)] = v;
   }
   for (int i = tid; i < N; i += T) {
-    gs[i] = gtab[i];
-    hs[i] = htab[i];
+    gs[pad8(i)] = gtab[i];
+    hs[pad8(i)] = htab[i];
   }
   __syncthreads();
   const int g = tid / P, c = tid - g * P;
@@ -262,17 +262,17 @@ __global__ void __launch_bounds__(G *(N / M)) adi_const_kernel(const AdiHalf h,
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     const int p = p0 + m;
-    double2 rr = cmul(mk(h.inv_dzh, -inv_kd2_expl), to_d(ctr[p]));
+    double2 rr = cmul(mk(h.inv_dzh, -inv_kd2_expl), to_d(ctr[pad8(p)]));
     double2 nb = mk(0.0, 0.0);
-    if (s > 0) nb = to_d(lft[p]);
-    if (s < N - 1) nb = cadd(nb, to_d(rgt[p]));
+    if (s > 0) nb = to_d(lft[pad8(p)]);
+    if (s < N - 1) nb = cadd(nb, to_d(rgt[pad8(p)]));
     r[m] = mk(fma(-hk, nb.y, rr.x), fma(hk, nb.x, rr.y));
   }
   const_solve<M, P>(r, gs, hs, p0, scratch);
   __syncthreads();  // every read of the staged tile is done
   C *dst = tile + (g + 1) * ld;
 #pragma unroll
-  for (int m = 0; m < M; ++m) dst[p0 + m] = from_d<R>(r[m]);
+  for (int m = 0; m < M; ++m) dst[pad8(p0 + m)] = from_d<R>(r[m]);
   __syncthreads();
   C *save = reinterpret_cast<C *>(h.save);
   for (int idx = tid; idx < G * N; idx += T) {
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(G *(N / M)) adi_const_kernel(const AdiHalf h,
       p = idx - gg * N;
     }
     const long long off = (long long)p * h.stride_pos + (long long)(s_base + gg) * h.stride_sys;
-    const C v = tile[(gg + 1) * ld + p];
+    const C v = tile[(gg + 1) * ld + pad8(p)];
     out[off] = v;
     if (save) save[off] = v;
   }
@@ -295,8 +295,8 @@ template <typename R, int N, int G>
 static cudaError_t adi_const_launch(const AdiHalf &h, const void *g, const void *hh, cudaStream_t s) {
   using C = typename Cx<R>::T;
   constexpr int M = 8, P = N / M, T = G * P;
-  constexpr size_t smem = ((sizeof(C) * (G + 2) * (N + 1) + 15) & ~size_t(15)) +
-                          2 * sizeof(double2) * N + sizeof(Affine) * (T / 32 + 1);
+  constexpr size_t smem = ((sizeof(C) * (G + 2) * (N + N / 8 + 2) + 15) & ~size_t(15)) +
+                          2 * sizeof(double2) * (N + N / 8) + sizeof(Affine) * (T / 32 + 1);
   auto k = adi_const_kernel<R, N, M, G>;
   if (smem > 48 * 1024) {
     static const cudaError_t attr =
@@ -330,14 +330,14 @@ static cudaError_t adi_launch_g(const AdiHalf &h, cudaStream_t s) {
   using C = typename Cx<R>::T;
   const int n = h.n;
   const int T = adi_threads<G>(n);
-  const size_t tile = (sizeof(C) * (G + 2) * (n + 1) + 15) & ~size_t(15);
+  const size_t tile = (sizeof(C) * (G + 2) * (n + n / 8 + 2) + 15) & ~size_t(15);
   const size_t smem = tile + sizeof(double2) * 4 * G * 2 * (n / kAdiM);
   auto k = adi_half_kernel<R, kAdiM, G>;
   // raise the dynamic shared-memory limit once per instantiation to the largest
   // size it can need (n = 2048 for G = 2, n = 1024 for G = 4)
   static const cudaError_t attr = cudaFuncSetAttribute(
       k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      (int)(((sizeof(C) * (G + 2) * (G == 2 ? 2049 : 1025) + 15) & ~size_t(15)) +
+      (int)(((sizeof(C) * (G + 2) * (G == 2 ? 2048 + 258 : 1024 + 130) + 15) & ~size_t(15)) +
             sizeof(double2) * 4 * G * 2 * ((G == 2 ? 2048 : 1024) / kAdiM)));
   if (attr != cudaSuccess) return attr;
   k<<<n / G, T, smem, s>>>(h);

@@ -174,9 +174,9 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
   constexpr int N = M * T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2 *gs = reinterpret_cast<double2 *>(smem_raw);
-  double2 *hs = gs + N;
-  double2 *coef = hs + N;
-  double2 *xch = coef + N;  // 2 per thread
+  constexpr int NP = N + N / 8;  // padded length (pad8)
+  double2 *hs = gs + NP;
+  double2 *xch = hs + NP;  // 2 per thread
   Affine *scratch = reinterpret_cast<Affine *>(xch + 2 * T);
   CnJob job = jobs[blockIdx.x];
   if (nsteps_ov >= 0) {
@@ -188,11 +188,8 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
   const double2 *gt = reinterpret_cast<const double2 *>(job.lu_g);
   const double2 *ht = reinterpret_cast<const double2 *>(job.lu_h);
   for (int i = t; i < N; i += T) {
-    gs[i] = gt[i];
-    hs[i] = ht[i];
-    const double bp = job.beta_prev[i], dp = job.delta_prev[i];
-    const double2 hh = mk(__dmul_rn(0.5, __dmul_rn(bp, r)), __dmul_rn(0.5, __dmul_rn(dp, r)));
-    coef[i] = mk(__dadd_rn(-hh.x, 1.0), -hh.y);
+    gs[pad8(i)] = gt[i];
+    hs[pad8(i)] = ht[i];
   }
   C *field = reinterpret_cast<C *>(job.field);
   const int s0 = t * M;
@@ -204,6 +201,15 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
   __syncthreads();
   for (int st = 0; st < job.nsteps; ++st) {
     const int step = job.step0 + st;
+    // right-hand-side coefficient 1 - 0.5*(beta'*r + i*delta'*r) of this
+    // chunk (z-invariant medium: the same cached values every step)
+    double2 coef[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const double bp = job.beta_prev[s0 + m], dp = job.delta_prev[s0 + m];
+      const double2 hh = mk(__dmul_rn(0.5, __dmul_rn(bp, r)), __dmul_rn(0.5, __dmul_rn(dp, r)));
+      coef[m] = mk(__dadd_rn(-hh.x, 1.0), -hh.y);
+    }
     xch[2 * t] = u[0];
     xch[2 * t + 1] = u[M - 1];
     __syncthreads();
@@ -220,7 +226,7 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
       double2 c4 = cx_scale_rn(u[m], 0.25);
       double2 tt = cx_scale_rn(cx_scale_rn(cx_mul_rn(c4, mk(0.0, 1.0)), rho), 2.0);
       v = cx_sub_rn(v, tt);
-      rh[m] = cx_add_rn(v, cx_mul_rn(coef[s0 + m], u[m]));
+      rh[m] = cx_add_rn(v, cx_mul_rn(coef[m], u[m]));
     }
     const_solve<M, T>(rh, gs, hs, s0, scratch);
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
@@ -244,7 +250,7 @@ template <typename R, int T>
 static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
                                      cudaStream_t s) {
   constexpr int N = kCnM * T;
-  constexpr size_t smem = sizeof(double2) * (3 * N + 2 * T) + sizeof(Affine) * (T / 32 + 1);
+  constexpr size_t smem = sizeof(double2) * (2 * (N + N / 8) + 2 * T) + sizeof(Affine) * (T / 32 + 1);
   auto k = cn_const_kernel<R, kCnM, T>;
   if (smem > 48 * 1024) {
     static const cudaError_t attr =

@@ -105,6 +105,11 @@ __device__ __forceinline__ float2 cdiv(float2 a, float2 b) {
 }
 __device__ __forceinline__ double2 cdiv(double2 a, double2 b) { return cx_div_rn(a, b); }
 
+// Padded shared-memory position for arrays read in chunks of 8 consecutive
+// rows per thread: chunk c starts at 9c, so the eight threads of an access
+// phase (c .. c+7) hit eight different 16-byte bank groups.
+__host__ __device__ __forceinline__ int pad8(int p) { return p + (p >> 3); }
+
 // Conversions between storage precisions.
 __device__ __forceinline__ double2 to_d(float2 a) { return mk((double)a.x, (double)a.y); }
 __device__ __forceinline__ double2 to_d(double2 a) { return a; }

@@ -97,7 +97,8 @@ __device__ __forceinline__ Affine exclusive_scan(Affine v, Affine *scratch) {
 
 // Solve one system whose chunk rows this thread holds: r[m] is the right-hand
 // side of row p0 + m on entry and the solution on exit.  g, h: the factor
-// tables (global positions).  P threads per system, chunk c = thread offset.
+// tables in shared memory at padded positions pad8(p).  P threads per
+// system, chunk c = thread offset.
 template <int M, int P>
 __device__ __forceinline__ void const_solve(double2 (&r)[M], const double2 *__restrict__ g,
                                             const double2 *__restrict__ h, int p0,
@@ -107,8 +108,8 @@ __device__ __forceinline__ void const_solve(double2 (&r)[M], const double2 *__re
   double2 prod = one, y = zero;
 #pragma unroll
   for (int m = 0; m < M; ++m) {
-    const double2 hm = h[p0 + m];
-    y = cadd(cmul(g[p0 + m], r[m]), cmul(hm, y));
+    const double2 hm = h[pad8(p0 + m)];
+    y = cadd(cmul(g[pad8(p0 + m)], r[m]), cmul(hm, y));
     prod = cmul(hm, prod);
     r[m] = y;
   }
@@ -117,7 +118,7 @@ __device__ __forceinline__ void const_solve(double2 (&r)[M], const double2 *__re
   prod = one;
 #pragma unroll
   for (int m = 0; m < M; ++m) {
-    prod = cmul(h[p0 + m], prod);
+    prod = cmul(h[pad8(p0 + m)], prod);
     r[m] = cadd(r[m], cmul(prod, y_in));
   }
   // backward, zero carry-in: x_i = y_i + h_i x_{i+1}
@@ -125,7 +126,7 @@ __device__ __forceinline__ void const_solve(double2 (&r)[M], const double2 *__re
   prod = one;
 #pragma unroll
   for (int m = M - 1; m >= 0; --m) {
-    const double2 hm = h[p0 + m];
+    const double2 hm = h[pad8(p0 + m)];
     x = cadd(r[m], cmul(hm, x));
     prod = cmul(hm, prod);
     r[m] = x;
@@ -135,7 +136,7 @@ __device__ __forceinline__ void const_solve(double2 (&r)[M], const double2 *__re
   prod = one;
 #pragma unroll
   for (int m = M - 1; m >= 0; --m) {
-    prod = cmul(h[p0 + m], prod);
+    prod = cmul(h[pad8(p0 + m)], prod);
     r[m] = cadd(r[m], cmul(prod, x_in));
   }
 }
