@@ -154,6 +154,32 @@ int pxp_current_step(pxp_solver s, unsigned *step);
 /* Grid shape of the handle: Nx, Ny (1 for 2-D kinds), Nz. */
 int pxp_shape(pxp_solver s, unsigned *nx, unsigned *ny, unsigned *nz);
 
+/* ADI steps (Solver3D::step with the ADI solver) on a field the caller owns
+ * in device memory, without allocating any device memory.  This has no
+ * counterpart in the reference: it is for callers that must not allocate
+ * device memory while they run -- code whose device memory is already carved
+ * up by another allocator (a framework's caching allocator or a fixed pool),
+ * and latency-critical loops, where cudaMalloc/cudaFree can synchronise the
+ * device and stall other streams.
+ *
+ * dfield: Ny x Nx column-major field in the problem's precision (complex128
+ * for PXP_FP64, complex64 for PXP_FP32), advanced in place by steps
+ * first_step .. first_step+nsteps-1.  spheres: first-hit sphere material
+ * (at most 16 may meet any one half-step plane).  stream: cudaStream_t to
+ * launch on (NULL: the default stream); the call is asynchronous.
+ *
+ * The intermediate field between the x and y half steps lives in a fixed
+ * 4 MiB array compiled into the library (every GPU that loads the library
+ * holds it until the process exits): grids needing more (n*n*16 bytes in
+ * FP64, n*n*8 in FP32; at most 512^2 in FP64) are rejected with
+ * PXP_ERR_UNSUPPORTED and a message.  All calls on a device share that
+ * array, so calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on each device looks up the array's device
+ * address; make that first call before any stream capture.  Errors are
+ * reported through pxp_last_error(NULL, ...). */
+int pxp_adi_steps_noalloc(const pxp_problem *problem, const pxp_sphere *spheres, int nspheres,
+                          void *dfield, unsigned first_step, int nsteps, void *stream);
+
 /* Last error message of the handle (NULL handle: last global error). */
 int pxp_last_error(pxp_solver s, char *buf, size_t len);
 

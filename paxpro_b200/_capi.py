@@ -92,6 +92,8 @@ def lib():
         "pxp_reset": (C.c_int, [h]),
         "pxp_current_step": (C.c_int, [h, C.POINTER(C.c_uint)]),
         "pxp_shape": (C.c_int, [h, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),
+        "pxp_adi_steps_noalloc": (C.c_int, [C.POINTER(Problem), C.POINTER(SphereC), C.c_int,
+                                            C.c_void_p, C.c_uint, C.c_int, C.c_void_p]),
         "pxp_last_error": (C.c_int, [h, C.c_char_p, C.c_size_t]),
         "pxp_status_string": (C.c_char_p, [C.c_int]),
         "pxp_build_info": (C.c_char_p, []),

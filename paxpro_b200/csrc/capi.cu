@@ -43,6 +43,8 @@ bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
 
 }  // namespace
 
+void pxp::set_last_error(const char *msg) { set_global_error(msg ? msg : ""); }
+
 struct pxp_solver_s {
   pxp_problem prob{};
   unsigned nx = 0, ny = 1, nz = 0;

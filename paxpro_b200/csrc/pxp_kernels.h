@@ -9,6 +9,9 @@ namespace pxp {
 
 enum Precision { kFP64 = 0, kFP32 = 1 };
 
+// Record the message pxp_last_error(NULL, ...) returns (capi.cu).
+void set_last_error(const char *msg);
+
 // ---------------------------------------------------------------- FFT 1-D --
 // One split-step problem with one transverse dimension (FFTSolver2D).
 // All complex arrays are interleaved and in the solver's precision.
