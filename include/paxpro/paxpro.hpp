@@ -1,0 +1,700 @@
+// paxpro.hpp -- the reference's C++ solver API (ParaxialSimulation, Solver,
+// Solver2D/3D, FFTSolver2D, CrankNicholson, FFTSolver3D, ADI, sources and the
+// material hook) backed by the B200 solvers through the C ABI of
+// paxpro_b200.h.  Header only; link with libpaxpro_b200.so.
+//
+// Class names, members and call order follow the reference
+// (include/paraxialSimulation.hpp, include/solver.hpp, include/solver2D.hpp,
+// include/solver3D.hpp, include/fftSolver2D.hpp, include/crankNicholson.hpp,
+// include/fftSolver3D.hpp, include/alternatingDirectionSolver.hpp,
+// include/paraxialSource.hpp, include/gaussianBeam.hpp, include/planeWave.hpp,
+// include/materialFunction.hpp) so that user code written against them
+// (e.g. Examples/waveguide2D.cpp) builds against this header instead.
+// Errors surface as std::runtime_error, as in the reference
+// (src/solver.cpp:5-28).
+//
+// Not provided (no counterpart on the GPU path, or a third-party dependency
+// this build does not have): HDF5 save (save() throws), post-processing
+// modules, VISA visualisation and the VISA longitudinal low-pass filter
+// (solve() requires disableLongitudinalFilter() when the longitudinal
+// downsampling ratio is above 1), CSG geometry on the 3-D solvers (they take
+// SphereMaterial or no material).
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../paxpro_b200.h"
+#include "arma_lite.hpp"
+
+typedef std::complex<double> cdouble;
+
+/** Discretisation record (include/paraxialSimulation.hpp:20-26). */
+struct Disctretization {
+  double min{0.0};
+  double max{0.0};
+  double step{1.0};
+  unsigned int downsamplingRatio{1};
+};
+
+// ------------------------------------------------------------ material ----
+/** Material hook (include/materialFunction.hpp:6-10). */
+class MaterialFunction {
+ public:
+  virtual ~MaterialFunction() {}
+  virtual void getXrayMatProp(double x, double y, double z, double &delta,
+                              double &beta) const = 0;
+  /** Extension without a reference counterpart: return true when delta and
+   * beta do not depend on z, so the 2-D CUDA solvers sample the medium once
+   * instead of once per step.  The default (false) is always correct. */
+  virtual bool zInvariant() const { return false; }
+};
+
+/** First-hit list of spheres, r^2 < R^2 as Examples/sphere.cpp:13-14; the
+ * 3-D CUDA solvers evaluate it on the device. */
+class SphereMaterial : public MaterialFunction {
+ public:
+  struct Sphere {
+    double cx, cy, cz, radius, delta, beta;
+  };
+  void addSphere(double cx, double cy, double cz, double radius, double delta, double beta) {
+    spheres.push_back({cx, cy, cz, radius, delta, beta});
+  }
+  void getXrayMatProp(double x, double y, double z, double &delta,
+                      double &beta) const override {
+    for (const Sphere &s : spheres) {
+      double dx = x - s.cx, dy = y - s.cy, dz = z - s.cz;
+      if (dx * dx + dy * dy + dz * dz < s.radius * s.radius) {
+        delta = s.delta;
+        beta = s.beta;
+        return;
+      }
+    }
+    delta = 0.0;
+    beta = 0.0;
+  }
+  std::vector<Sphere> spheres;
+};
+
+// ------------------------------------------------------------- sources ----
+/** include/paraxialSource.hpp:10-59, src/paraxialSource.cpp. */
+class ParaxialSource {
+ public:
+  enum class Dim_t { TWO_D, THREE_D };
+  explicit ParaxialSource(const char *name) : name(name) {}
+  virtual ~ParaxialSource() {}
+  virtual cdouble get(double x, double z) const {
+    throw std::runtime_error("2D version of the ParaxialSorce get function is not implemented!");
+  }
+  virtual cdouble get(double x, double y, double z) const {
+    throw std::runtime_error("3D version of the ParaxialSource get function is not implemented!");
+  }
+  void setWavenumber(double k) { wavenumber = k; }
+  double getWavenumber() const { return wavenumber; }
+  void setWavelength(double lambda) { wavenumber = 2.0 * pi() / lambda; }
+  double getWavelength() const { return 2.0 * pi() / wavenumber; }
+  void setOrigin(double, double zOrig) { z0 = zOrig; }
+  void setAmplitude(double amp) { amplitude = amp; }
+  void setDim(Dim_t d) { dim = d; }
+  Dim_t getDim() const { return dim; }
+  std::string getName() const { return name; }
+
+ protected:
+  static double pi() { return std::acos(-1.0); }
+  double wavenumber{0.0};
+  double z0{0.0};
+  double x0{0.0};
+  double amplitude{1.0};
+  Dim_t dim{Dim_t::TWO_D};
+
+ private:
+  std::string name;
+};
+
+/** include/gaussianBeam.hpp:6-66, src/gaussianBeam.cpp:7-63. */
+class GaussianBeam : public ParaxialSource {
+ public:
+  GaussianBeam() : ParaxialSource("gaussianBeam") {}
+  cdouble get(double x, double z) const override {
+    x -= centerX;
+    cdouble im(0.0, 1.0);
+    double waistRatio = waist / spotSize(z - z0);
+    double gaussianFactor = std::exp(-std::pow(x / spotSize(z - z0), 2));
+    cdouble phaseFactor = std::exp(-im * wavenumber * z0 +
+                                   0.5 * im * wavenumber * x * x * invR(z - z0) -
+                                   im * guoy(z - z0));
+    return amplitude * waistRatio * gaussianFactor * phaseFactor * angleFactor(angleX, x);
+  }
+  cdouble get(double x, double y, double z) const override {
+    y -= centerY;
+    double gaussY = std::exp(-std::pow(y / spotSize(z - z0), 2));
+    return get(x, z) * gaussY * angleFactor(angleY, y);
+  }
+  void setWaist(double w) { waist = w; }
+  void setCenter(double xc, double yc) {
+    centerX = xc;
+    centerY = yc;
+  }
+  void setAngleX(double a) { angleX = a; }
+  void setAngleY(double a) { angleY = a; }
+  double getWaist() const { return waist; }
+
+ private:
+  double waist{1.0}, centerX{0.0}, centerY{0.0}, angleX{0.0}, angleY{0.0};
+  double zR() const { return pi() * waist * waist / getWavelength(); }
+  double guoy(double z) const { return std::atan(z / zR()); }
+  double invR(double z) const {
+    double r = zR();
+    return z / (z * z + r * r);
+  }
+  double spotSize(double z) const { return waist * std::sqrt(1.0 + std::pow(z / zR(), 2)); }
+  cdouble angleFactor(double angDeg, double x) const {
+    double a = angDeg * pi() / 180.0;
+    cdouble im(0.0, 1.0);
+    return std::exp(im * getWavenumber() * std::sin(a) * x);
+  }
+};
+
+/** include/planeWave.hpp:7-25, src/planeWave.cpp:5-14. */
+class PlaneWave : public ParaxialSource {
+ public:
+  PlaneWave() : ParaxialSource("planeWave") {}
+  cdouble get(double x, double z) const override {
+    cdouble im(0.0, 1.0);
+    return amplitude * std::exp(im * wavenumber * x * std::sin(angleWithZAxis) - im * wavenumber * z0);
+  }
+  cdouble get(double x, double y, double z) const override { return get(x, z); }
+  void setAngleDeg(double angle) { angleWithZAxis = angle * pi() / 180.0; }
+
+ private:
+  double angleWithZAxis{0.0};
+};
+
+/** include/arraySource.hpp: the values must match the transverse grid. */
+class ArraySource : public ParaxialSource {
+ public:
+  ArraySource() : ParaxialSource("arraySource") {}
+  void setData(const arma::cx_vec *data) { values = data; }
+  const arma::cx_vec &getVec() const { return *values; }
+
+ private:
+  const arma::cx_vec *values{nullptr};
+};
+
+class ParaxialSimulation;
+
+// -------------------------------------------------------------- solvers ----
+/** include/solver.hpp:10-74 */
+class Solver {
+ public:
+  enum class Dimension_t { TWO_D, THREE_D };
+  Solver(const char *name, Dimension_t dim) : dim(dim), name(name) {}
+  virtual ~Solver() { release(); }
+  Dimension_t getDim() const { return dim; }
+  std::string getName() const { return name; }
+  virtual void setSimulator(ParaxialSimulation &g) { guide = &g; }
+  const ParaxialSimulation &getSimulator() const { return *guide; }
+  virtual void reset() {
+    currentStep = 1;
+    if (handle) pxp_reset(handle);
+  }
+  virtual const arma::cx_cube &getSolution3D() const {
+    throw std::runtime_error("The 3D version of getSolution() is not implemented!");
+  }
+  virtual const arma::cx_mat &getSolution() const {
+    throw std::runtime_error("The 2D version of getSolution() is not implemented!");
+  }
+  virtual const arma::cx_vec &getLastSolution() const {
+    throw std::runtime_error("The 2D version of getLastSolution() is not implemented!");
+  }
+  virtual const arma::cx_mat &getLastSolution3D() const {
+    throw std::runtime_error("The 3D version of getLastSolution3D() is not implemented!");
+  }
+  virtual void solve() {}
+  virtual void step() = 0;
+  virtual void setInitialConditions(const arma::cx_vec &) {}
+  virtual void setInitialConditions(const arma::cx_mat &) {}
+  virtual void filterInLongitudinalDirection() {}
+  virtual void downSampleLongitudinalDirection() {}
+  virtual void updateDimensionsOfArrays() {}
+  /** Precision of the CUDA solver: PXP_FP64 (plain) or PXP_FP32 (served). */
+  void setPrecision(int p) { precision = p; }
+
+ protected:
+  Dimension_t dim;
+  std::string name;
+  ParaxialSimulation *guide{nullptr};
+  unsigned int currentStep{1};
+  pxp_solver handle{nullptr};
+  int precision{PXP_FP64};
+
+  void release() {
+    if (handle) pxp_solver_destroy(handle);
+    handle = nullptr;
+  }
+  void check(int status) const {
+    if (status != PXP_OK) {
+      char msg[1024];
+      pxp_last_error(handle, msg, sizeof(msg));
+      throw std::runtime_error(std::string(name) + ": " + msg + " (" +
+                               pxp_status_string(status) + ")");
+    }
+  }
+};
+
+/** include/paraxialSimulation.hpp:28-236 (minus HDF5 and post-processing). */
+class ParaxialSimulation {
+ public:
+  enum class Boundary_t { TOP, BOTTOM, LEFT, RIGHT };
+  explicit ParaxialSimulation(const char *name) : name(name) {}
+  ParaxialSimulation(const ParaxialSimulation &) = delete;
+  ParaxialSimulation &operator=(const ParaxialSimulation &) = delete;
+  virtual ~ParaxialSimulation() {}
+
+  void setTransverseDiscretization(double xmin, double xmax, double step) {
+    setTransverseDiscretization(xmin, xmax, step, 1);
+  }
+  void setTransverseDiscretization(double xmin, double xmax, double step, unsigned int ratio) {
+    xDisc = {xmin, xmax, step, ratio};
+    yDisc.downsamplingRatio = ratio;
+  }
+  void setLongitudinalDiscretization(double zmin, double zmax, double step) {
+    setLongitudinalDiscretization(zmin, zmax, step, 1);
+  }
+  void setLongitudinalDiscretization(double zmin, double zmax, double step, unsigned int ratio) {
+    zDisc = {zmin, zmax, step, ratio};
+  }
+  void setVerticalDiscretization(double ymin, double ymax, double step) {
+    yDisc.min = ymin;
+    yDisc.max = ymax;
+    yDisc.step = step;
+  }
+  unsigned int nodeNumberTransverse() const { return pxp_node_count(xDisc.min, xDisc.max, xDisc.step); }
+  unsigned int nodeNumberLongitudinal() const { return pxp_node_count(zDisc.min, zDisc.max, zDisc.step); }
+  unsigned int nodeNumberVertical() const { return pxp_node_count(yDisc.min, yDisc.max, yDisc.step); }
+  const Disctretization &transverseDiscretization() const { return xDisc; }
+  const Disctretization &longitudinalDiscretization() const { return zDisc; }
+  const Disctretization &verticalDiscretization() const { return yDisc; }
+
+  double getWavenumber() const { return wavenumber; }
+  void setWavenumber(double k) { wavenumber = k; }
+  double getWavelength() const { return 2.0 * std::acos(-1.0) / wavenumber; }
+  void setWaveLength(double lambda) { wavenumber = 2.0 * std::acos(-1.0) / lambda; }
+
+  void setSolver(Solver &s) {
+    solver = &s;
+    solver->setSimulator(*this);
+  }
+  std::string getName() const { return name; }
+  void step() { solver->step(); }
+  virtual void solve() { solver->solve(); }
+  void reset() {
+    if (solver) solver->reset();
+  }
+
+  double getZ(unsigned int iz) const { return zDisc.min + iz * zDisc.step; }
+  double getX(int ix) const { return xDisc.min + ix * xDisc.step; }
+  double getY(int iy) const { return yDisc.min + iy * yDisc.step; }
+
+  /** src/paraxialSimulation.cpp:356-399 */
+  virtual void setBoundaryConditions(const ParaxialSource &source) {
+    if (solver == nullptr) throw std::runtime_error("Solver needs to be set before boundary conditions!");
+    src = &source;
+    unsigned Nx = nodeNumberTransverse();
+    if (source.getDim() == ParaxialSource::Dim_t::TWO_D) {
+      arma::cx_vec values(Nx, 1.0);
+      for (unsigned i = 0; i < Nx; ++i) values[i] = src->get(getX(i), 0.0);
+      solver->setInitialConditions(values);
+    } else {
+      unsigned Ny = nodeNumberVertical();
+      arma::cx_mat values(Nx, Ny);
+      for (unsigned indx = 0; indx < Nx * Ny; ++indx) {
+        unsigned i = indx / Ny, j = indx % Ny;
+        values(j, i) = src->get(getX(i), getY(j), 0.0);
+      }
+      solver->setInitialConditions(values);
+    }
+    setWaveLength(source.getWavelength());
+  }
+  void setBoundaryConditions(const ArraySource &source) {
+    src = &source;
+    if (source.getVec().n_elem != nodeNumberTransverse())
+      throw std::runtime_error("The size of the given array does not match the number of transverse nodes!");
+    solver->setInitialConditions(source.getVec());
+  }
+
+  /** src/paraxialSimulation.cpp:513-537 */
+  virtual void getXrayMatProp(double x, double z, double &delta, double &beta) const {
+    if (material) {
+      material->getXrayMatProp(x, 0.0, z, delta, beta);
+    } else {
+      delta = 0.0;
+      beta = 0.0;
+    }
+  }
+  virtual void getXrayMatProp(double x, double y, double z, double &delta, double &beta) const {
+    if (material) {
+      material->getXrayMatProp(x, y, z, delta, beta);
+    } else {
+      delta = 0.0;
+      beta = 0.0;
+    }
+  }
+  void save(const char *) {
+    throw std::runtime_error("HDF5 export is not available in this build");
+  }
+  const Solver &getSolver() const { return *solver; }
+
+  std::string description{""};
+  const MaterialFunction *material{nullptr};
+
+ protected:
+  Solver *solver{nullptr};
+  Disctretization xDisc, zDisc, yDisc;
+  double wavenumber{1.0};
+  std::string name;
+  const ParaxialSource *src{nullptr};
+};
+
+/** Base of the 2-D (one transverse dimension) solvers, include/solver2D.hpp. */
+class Solver2D : public Solver {
+ public:
+  enum class Comp_t { REAL, IMAG };
+  enum class BC_t { DIRICHLET, TRANSPARENT };
+  Solver2D(const char *name, int kind) : Solver(name, Dimension_t::TWO_D), kind(kind) {}
+  Solver2D(const Solver2D &) = delete;
+
+  void setSimulator(ParaxialSimulation &g) override {
+    Solver::setSimulator(g);
+    release();
+    Nx = g.nodeNumberTransverse();
+    Nz = g.nodeNumberLongitudinal();
+    unsigned ds = Nx / g.transverseDiscretization().downsamplingRatio;
+    solution = arma::cx_mat(ds, Nz);
+    prevSolution = arma::cx_vec(Nx);
+    currentSolution = arma::cx_vec(Nx);
+    currentStep = 1;
+  }
+  const arma::cx_mat &getSolution() const override { return solution; }
+  const arma::cx_vec &getLastSolution() const override { return prevSolution; }
+  void setInitialConditions(const arma::cx_vec &vec) override {
+    for (unsigned i = 0; i < Nx; ++i) currentSolution(i) = vec(i);
+    copyCurrentSolution(0);
+    icPending = true;
+  }
+  void setBoundaryCondition(BC_t bc) { boundaryCondition = bc; }
+  void disableLongitudinalFilter() { longitudinalFilterDisabled = true; }
+
+  /** Solver2D::step (src/solver2D.cpp:243-250): one step, field copied back. */
+  void step() override {
+    initDevice();
+    runSteps(currentStep, 1);
+    check(pxp_get_last_solution(handle, reinterpret_cast<double *>(currentSolution.memptr())));
+    copyCurrentSolution(currentStep);
+    currentStep++;
+  }
+
+  /** Solver2D::solve (src/solver2D.cpp:224-241): all steps on the device,
+   * the saved columns copied back once at the end. */
+  void solve() override {
+    initDevice();
+    const unsigned first = currentStep, last = Nz - 1;
+    if (first > last) return;
+    runSteps(first, last - first + 1);
+    int nsaved = 0;
+    check(pxp_num_saved(handle, &nsaved));
+    for (unsigned s = first; s <= last && (int)(s - 1) < nsaved; ++s) {
+      check(pxp_get_saved(handle, (int)(s - 1), reinterpret_cast<double *>(currentSolution.memptr())));
+      copyCurrentSolution(s);
+    }
+    currentStep = last + 1;
+    if (!longitudinalFilterDisabled && guide->longitudinalDiscretization().downsamplingRatio > 1)
+      throw std::runtime_error(
+          "the longitudinal low-pass filter (VISA) is not available: call "
+          "disableLongitudinalFilter() or use a longitudinal downsampling ratio of 1");
+    if (!longitudinalFilterDisabled) downSampleLongitudinalDirection();
+  }
+
+  /** src/solver2D.cpp:267-282 */
+  void downSampleLongitudinalDirection() override {
+    unsigned nz = Nz / guide->longitudinalDiscretization().downsamplingRatio;
+    arma::cx_mat copy(solution.n_rows, nz);
+    double delta = static_cast<double>(solution.n_cols) / static_cast<double>(nz);
+    for (unsigned iz = 0; iz < nz; ++iz) {
+      unsigned indx = iz * delta + delta / 2.0;
+      for (unsigned ix = 0; ix < copy.n_rows; ++ix) copy(ix, iz) = solution(ix, indx);
+    }
+    solution = copy;
+  }
+
+ protected:
+  int kind;
+  unsigned Nx{0}, Nz{0};
+  arma::cx_mat solution;
+  arma::cx_vec prevSolution, currentSolution;
+  BC_t boundaryCondition{BC_t::DIRICHLET};
+  bool longitudinalFilterDisabled{false};
+  bool icPending{false};
+  bool materialPlanes{false};
+
+  /** src/solver2D.cpp:173-193 with a transverse ratio of 1 or a plain
+   * middle-sample downsampling (the VISA filter is not applied). */
+  void copyCurrentSolution(unsigned step) {
+    for (unsigned i = 0; i < currentSolution.n_elem; ++i) prevSolution(i) = currentSolution(i);
+    double delta = static_cast<double>(currentSolution.n_elem) / static_cast<double>(solution.n_rows);
+    if (step < solution.n_cols)
+      for (unsigned i = 0; i < solution.n_rows; ++i)
+        solution(i, step) = currentSolution((unsigned)(delta * i + delta / 2.0));
+  }
+
+  void initDevice() {
+    if (guide == nullptr) throw std::runtime_error("No waveguide specified!");
+    if (handle == nullptr) {
+      const ParaxialSimulation &g = *guide;
+      pxp_problem p{};
+      p.kind = kind;
+      p.precision = precision;
+      p.x = {g.transverseDiscretization().min, g.transverseDiscretization().max,
+             g.transverseDiscretization().step, 1};
+      p.y = p.x;
+      p.z = {g.longitudinalDiscretization().min, g.longitudinalDiscretization().max,
+             g.longitudinalDiscretization().step, 1};
+      p.wavenumber = g.getWavenumber();
+      p.transparent_bc = boundaryCondition == BC_t::TRANSPARENT;
+      p.save_every = 1;
+      check(pxp_solver_create(&p, &handle));
+      const MaterialFunction *m = g.material;
+      materialPlanes = m != nullptr && !m->zInvariant();
+      if (m != nullptr && !materialPlanes) {
+        std::vector<double> d(Nx), b(Nx);
+        for (unsigned i = 0; i < Nx; ++i) g.getXrayMatProp(g.getX(i), 0.0, d[i], b[i]);
+        check(pxp_set_material_table(handle, d.data(), b.data(), Nx));
+      }
+    }
+    if (icPending) {
+      check(pxp_set_initial_conditions(handle, reinterpret_cast<const double *>(currentSolution.memptr())));
+      icPending = false;
+    }
+  }
+
+  /** The planes the reference samples (FFTSolver2D: z = getZ(s) + dz/2,
+   * src/fftSolver2D.cpp:38; CrankNicholson: z and z - dz,
+   * src/crancNicholson.cpp:29-38) for steps s = first .. first+n-1, in
+   * chunks, then the steps. */
+  void runSteps(unsigned first, unsigned n) {
+    const ParaxialSimulation &g = *guide;
+    const double dz = g.longitudinalDiscretization().step;
+    const unsigned chunk = 256;
+    for (unsigned s0 = first; s0 < first + n;) {
+      unsigned cnt = std::min(chunk, first + n - s0);
+      if (materialPlanes) {
+        const unsigned per = kind == PXP_CRANK_NICHOLSON ? 2 : 1;
+        std::vector<double> d((size_t)cnt * per * Nx), b(d.size());
+        for (unsigned k = 0; k < cnt; ++k) {
+          const unsigned s = s0 + k;
+          for (unsigned pl = 0; pl < per; ++pl) {
+            double z;
+            if (kind == PXP_CRANK_NICHOLSON) {
+              z = g.longitudinalDiscretization().min + static_cast<double>(s) * dz;
+              if (pl == 1) z = z - dz;
+            } else {
+              z = g.getZ(s) + 0.5 * dz;
+            }
+            size_t off = ((size_t)k * per + pl) * Nx;
+            for (unsigned i = 0; i < Nx; ++i) g.getXrayMatProp(g.getX(i), z, d[off + i], b[off + i]);
+          }
+        }
+        check(pxp_set_material_planes(handle, d.data(), b.data(), (int)s0, (int)cnt));
+      } else if (!materialPlanes && s0 == first && n > chunk) {
+        cnt = n;  // z-invariant: one launch
+      }
+      check(pxp_step(handle, (int)cnt));
+      s0 += cnt;
+    }
+  }
+};
+
+/** include/fftSolver2D.hpp */
+class FFTSolver2D : public Solver2D {
+ public:
+  FFTSolver2D() : Solver2D("FFTSolver2D", PXP_FFT_SOLVER_2D) {}
+};
+
+/** include/crankNicholson.hpp */
+class CrankNicholson : public Solver2D {
+ public:
+  CrankNicholson() : Solver2D("CrankNicholson", PXP_CRANK_NICHOLSON) {}
+};
+
+/** Base of the 3-D (two transverse dimension) solvers, include/solver3D.hpp. */
+class Solver3D : public Solver {
+ public:
+  Solver3D(const char *name, int kind) : Solver(name, Dimension_t::THREE_D), kind(kind) {}
+
+  /** src/solver3D.cpp:19-44 (Ny is forced to Nx) */
+  void setSimulator(ParaxialSimulation &g) override {
+    Solver::setSimulator(g);
+    release();
+    Nx = g.nodeNumberTransverse();
+    Nz = g.nodeNumberLongitudinal();
+    Ny = Nx;
+    unsigned dx = Nx / g.transverseDiscretization().downsamplingRatio;
+    unsigned dzs = Nz / g.longitudinalDiscretization().downsamplingRatio;
+    prevSolution = arma::cx_mat(Ny, Nx);
+    currentSolution = arma::cx_mat(Ny, Nx);
+    solution = arma::cx_cube(dx, dx, dzs + 1);
+    currentStep = 1;
+  }
+  void updateDimensionsOfArrays() override { setSimulator(*guide); }
+  const arma::cx_cube &getSolution3D() const override { return solution; }
+  const arma::cx_mat &getLastSolution3D() const override { return prevSolution; }
+
+  /** src/solver3D.cpp:127-146 */
+  void setInitialConditions(const arma::cx_mat &values) override {
+    if (values.n_rows != currentSolution.n_rows || values.n_cols != currentSolution.n_cols)
+      throw std::runtime_error("Dimension of matrices does not match!");
+    std::memcpy(currentSolution.memptr(), values.memptr(), sizeof(cdouble) * values.n_elem);
+    copyCurrentSolution(0);
+    icPending = true;
+  }
+
+  void step() override {
+    initDevice();
+    check(pxp_step(handle, 1));
+    check(pxp_get_last_solution(handle, reinterpret_cast<double *>(currentSolution.memptr())));
+    copyCurrentSolution(currentStep++);
+  }
+
+  /** src/solver3D.cpp:168-199: all steps on the device; the saved slices
+   * (every longitudinal downsampling ratio steps) copied back at the end. */
+  void solve() override {
+    initDevice();
+    const unsigned first = currentStep, last = Nz - 1;
+    if (first > last) return;
+    check(pxp_step(handle, (int)(last - first + 1)));
+    const unsigned ratio = guide->longitudinalDiscretization().downsamplingRatio;
+    int nsaved = 0;
+    check(pxp_num_saved(handle, &nsaved));
+    for (int k = 0; k < nsaved; ++k) {
+      const unsigned s = (unsigned)(k + 1) * ratio;
+      if (s < first) continue;
+      check(pxp_get_saved(handle, k, reinterpret_cast<double *>(currentSolution.memptr())));
+      storeSlice(s / ratio);
+    }
+    check(pxp_get_last_solution(handle, reinterpret_cast<double *>(currentSolution.memptr())));
+    std::memcpy(prevSolution.memptr(), currentSolution.memptr(), sizeof(cdouble) * currentSolution.n_elem);
+    currentStep = last + 1;
+  }
+
+ protected:
+  int kind;
+  unsigned Nx{0}, Ny{0}, Nz{0};
+  arma::cx_cube solution;
+  arma::cx_mat prevSolution, currentSolution;
+  bool icPending{false};
+  double absorberWidth{0.0}, absorberDamping{0.0};
+  bool tbc{false};
+
+  /** src/solver3D.cpp:78-125: block average into the saved slice. */
+  void storeSlice(unsigned currZ) {
+    if (currZ >= solution.n_slices) return;
+    double deltaX = static_cast<double>(currentSolution.n_rows) / static_cast<double>(solution.n_rows);
+    double deltaY = static_cast<double>(currentSolution.n_cols) / static_cast<double>(solution.n_cols);
+    unsigned bx = (unsigned)deltaX, by = (unsigned)deltaY;
+    for (unsigned i = 0; i < solution.n_rows * solution.n_cols; ++i) {
+      unsigned row = i % solution.n_rows, col = i / solution.n_rows;
+      cdouble sum = 0.0;
+      for (unsigned c = 0; c < by; ++c) {
+        cdouble colsum = 0.0;
+        for (unsigned r = 0; r < bx; ++r)
+          colsum += currentSolution((unsigned)(row * deltaX) + r, (unsigned)(col * deltaY) + c);
+        sum += colsum;
+      }
+      solution(row, col, currZ) = sum / (deltaX * deltaY);
+    }
+  }
+  void copyCurrentSolution(unsigned step) {
+    std::memcpy(prevSolution.memptr(), currentSolution.memptr(), sizeof(cdouble) * currentSolution.n_elem);
+    if (step % guide->longitudinalDiscretization().downsamplingRatio == 0)
+      storeSlice(step / guide->longitudinalDiscretization().downsamplingRatio);
+  }
+
+  void initDevice() {
+    if (guide == nullptr) throw std::runtime_error("No waveguide specified!");
+    if (handle == nullptr) {
+      const ParaxialSimulation &g = *guide;
+      pxp_problem p{};
+      p.kind = kind;
+      p.precision = precision;
+      p.x = {g.transverseDiscretization().min, g.transverseDiscretization().max,
+             g.transverseDiscretization().step, 1};
+      p.y = {g.verticalDiscretization().min, g.verticalDiscretization().max,
+             g.verticalDiscretization().step, 1};
+      p.z = {g.longitudinalDiscretization().min, g.longitudinalDiscretization().max,
+             g.longitudinalDiscretization().step, 1};
+      p.wavenumber = g.getWavenumber();
+      p.transparent_bc = tbc ? 1 : 0;
+      p.absorber_width = absorberWidth;
+      p.absorber_damping = absorberDamping;
+      p.save_every = (int)g.longitudinalDiscretization().downsamplingRatio;
+      check(pxp_solver_create(&p, &handle));
+      if (g.material != nullptr) {
+        const SphereMaterial *sm = dynamic_cast<const SphereMaterial *>(g.material);
+        if (sm == nullptr)
+          throw std::runtime_error(
+              "the CUDA 3-D solvers take a SphereMaterial (or no material)");
+        std::vector<pxp_sphere> sp;
+        for (const auto &s : sm->spheres) sp.push_back({s.cx, s.cy, s.cz, s.radius, s.delta, s.beta});
+        check(pxp_set_material_spheres(handle, sp.data(), (int)sp.size()));
+      }
+    }
+    if (icPending) {
+      check(pxp_set_initial_conditions(handle, reinterpret_cast<const double *>(currentSolution.memptr())));
+      icPending = false;
+    }
+  }
+};
+
+/** include/fftSolver3D.hpp */
+class FFTSolver3D : public Solver3D {
+ public:
+  FFTSolver3D() : Solver3D("FFTSolver3D", PXP_FFT_SOLVER_3D) {}
+  /** src/fftSolver3D.cpp:327-349 */
+  void absorbingBC(double width, double dampingLength) {
+    if (guide == nullptr)
+      throw std::runtime_error("No waveguide set! The solver needs first to be passed to a waveguide object. Then call this function!");
+    if (handle != nullptr)
+      throw std::runtime_error("absorbingBC must be called before the first step");
+    absorberWidth = width;
+    absorberDamping = dampingLength;
+  }
+  void reset() override { Solver::reset(); }
+};
+
+/** include/alternatingDirectionSolver.hpp */
+class ADI : public Solver3D {
+ public:
+  ADI() : Solver3D("ADI", PXP_ADI) {}
+  /** If true transparent boundary conditions are used, otherwise Dirichlet. */
+  bool useTBC{true};
+  void step() override {
+    syncTbc();
+    Solver3D::step();
+  }
+  void solve() override {
+    syncTbc();
+    Solver3D::solve();
+  }
+
+ private:
+  void syncTbc() {
+    if (handle == nullptr)
+      tbc = useTBC;
+    else if (tbc != useTBC)
+      throw std::runtime_error("useTBC changed after the first step");
+  }
+};

@@ -6,7 +6,7 @@
  * and a SWIG module (pypaxpro/pypaxpro.i).  This header is the plain-C
  * boundary those classes sit on in this build: opaque handles, plain
  * pointers and sizes, int status codes, no exceptions and no C++ or torch
- * types.  The C++ mirror of the reference API (include/paxpro/*.hpp) and the
+ * types.  The C++ mirror of the reference API (the headers in include/paxpro) and the
  * Python package call only these functions.
  *
  * Conventions
