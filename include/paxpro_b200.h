@@ -154,6 +154,42 @@ int pxp_current_step(pxp_solver s, unsigned *step);
 /* Grid shape of the handle: Nx, Ny (1 for 2-D kinds), Nz. */
 int pxp_shape(pxp_solver s, unsigned *nx, unsigned *ny, unsigned *nz);
 
+/* ---- batching and serving (no reference counterpart: the reference runs
+ * one problem at a time on the host) ------------------------------------- */
+
+/* Device memory a solver holds (field, saves, tables). */
+int pxp_device_bytes(pxp_solver s, size_t *bytes);
+
+/* |u|^2 of the current field, Nx (or Ny*Nx column-major) doubles. */
+int pxp_get_intensity(pxp_solver s, double *intensity);
+
+typedef struct pxp_batch_s *pxp_batch;
+
+/* A set of independent solvers advanced together on one device, admitted
+ * against a device-memory budget (bytes). */
+int pxp_batch_create(int device, size_t hbm_budget_bytes, pxp_batch *out);
+int pxp_batch_destroy(pxp_batch b);
+
+/* Admit a solver (created, material and initial conditions set) that is to
+ * advance nsteps more steps.  PXP_ERR_NOT_READY (and no admission) when its
+ * device memory would exceed the budget.  The solver stays owned by the
+ * caller; it must not be stepped or destroyed while admitted. */
+int pxp_batch_admit(pxp_batch b, pxp_solver s, int nsteps);
+
+/* One round: every admitted solver with steps left advances by up to
+ * max_steps steps.  2-D solvers of equal kind, size, precision and matrix
+ * path share one launch (one CTA per solver, each with its own step count);
+ * 3-D solvers run their passes on their own streams.  Asynchronous. */
+int pxp_batch_round(pxp_batch b, int max_steps);
+
+/* Wait for the round, then hand back (and remove from the batch) the
+ * solvers that have no steps left: up to cap of them in done[], their number
+ * in *count.  Their memory leaves the batch budget. */
+int pxp_batch_collect(pxp_batch b, pxp_solver *done, int cap, int *count);
+
+/* Solvers admitted and device memory charged to the budget. */
+int pxp_batch_status(pxp_batch b, int *active, size_t *bytes);
+
 /* ADI steps (Solver3D::step with the ADI solver) on a field the caller owns
  * in device memory, without allocating any device memory.  This has no
  * counterpart in the reference: it is for callers that must not allocate

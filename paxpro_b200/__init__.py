@@ -210,6 +210,16 @@ class Solver:
     def reset(self) -> None:
         self._check(_capi.lib().pxp_reset(self._h))
 
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        self._check(_capi.lib().pxp_device_bytes(self._h, C.byref(b)))
+        return b.value
+
+    def get_intensity(self) -> np.ndarray:
+        out = np.empty(self.nx * self.ny, dtype=np.float64)
+        self._check(_capi.lib().pxp_get_intensity(self._h, _dptr(out)))
+        return self._unflatten(out)
+
     @property
     def current_step(self) -> int:
         s = C.c_uint()
@@ -217,5 +227,50 @@ class Solver:
         return s.value
 
 
-__all__ = ["Solver", "ProblemSpec", "Disc", "Sphere", "node_count", "PxpError",
+class Batch:
+    """Independent solvers advanced together on one device (pxp_batch_*),
+    admitted against a device-memory budget."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 150 * 10 ** 9):
+        self._b = C.c_void_p()
+        _capi.check(_capi.lib().pxp_batch_create(device, hbm_budget_bytes, C.byref(self._b)))
+        self._members = {}
+
+    def close(self) -> None:
+        if self._b:
+            _capi.lib().pxp_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def admit(self, solver: "Solver", nsteps: int) -> bool:
+        """True when admitted; False when the memory budget is full."""
+        rc = _capi.lib().pxp_batch_admit(self._b, solver._h, int(nsteps))
+        if rc == _capi.PXP_ERR_NOT_READY:
+            return False
+        _capi.check(rc)
+        self._members[solver._h.value] = solver
+        return True
+
+    def round(self, max_steps: int) -> None:
+        _capi.check(_capi.lib().pxp_batch_round(self._b, int(max_steps)))
+
+    def collect(self) -> list:
+        cap = max(len(self._members), 1)
+        arr = (C.c_void_p * cap)()
+        cnt = C.c_int()
+        _capi.check(_capi.lib().pxp_batch_collect(self._b, arr, cap, C.byref(cnt)))
+        return [self._members.pop(arr[i]) for i in range(cnt.value)]
+
+    def status(self):
+        a, b = C.c_int(), C.c_size_t()
+        _capi.check(_capi.lib().pxp_batch_status(self._b, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+
+__all__ = ["Batch", "Solver", "ProblemSpec", "Disc", "Sphere", "node_count", "PxpError",
            "FFT_SOLVER_2D", "CRANK_NICHOLSON", "FFT_SOLVER_3D", "ADI", "FP64", "FP32"]

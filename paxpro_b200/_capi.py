@@ -94,6 +94,14 @@ def lib():
         "pxp_shape": (C.c_int, [h, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),
         "pxp_adi_steps_noalloc": (C.c_int, [C.POINTER(Problem), C.POINTER(SphereC), C.c_int,
                                             C.c_void_p, C.c_uint, C.c_int, C.c_void_p]),
+        "pxp_device_bytes": (C.c_int, [h, C.POINTER(C.c_size_t)]),
+        "pxp_get_intensity": (C.c_int, [h, d]),
+        "pxp_batch_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(h)]),
+        "pxp_batch_destroy": (C.c_int, [h]),
+        "pxp_batch_admit": (C.c_int, [h, h, C.c_int]),
+        "pxp_batch_round": (C.c_int, [h, C.c_int]),
+        "pxp_batch_collect": (C.c_int, [h, C.POINTER(h), C.c_int, C.POINTER(C.c_int)]),
+        "pxp_batch_status": (C.c_int, [h, C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
         "pxp_last_error": (C.c_int, [h, C.c_char_p, C.c_size_t]),
         "pxp_status_string": (C.c_char_p, [C.c_int]),
         "pxp_build_info": (C.c_char_p, []),

@@ -15,6 +15,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <tuple>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -72,6 +74,10 @@ struct pxp_solver_s {
   void *d_field2 = nullptr;                  // ping-pong buffer
   void *d_lu = nullptr;                      // factor tables of step-invariant matrices
   bool cn_const = false;                     // CN matrix step-invariant
+  size_t dev_bytes = 0;                      // device memory held by the handle
+  pxp::Fft1dJob job_fft{};                   // host copies of the job descriptors
+  pxp::CnJob job_cn{};
+  int batch_remaining = 0;                   // steps left while admitted to a batch
   std::vector<pxp_sphere> spheres;           // first-hit sphere material
   pxp::Sphere *d_spheres = nullptr;
   // host copies
@@ -100,9 +106,27 @@ namespace {
     if (e_ != cudaSuccess) return (h)->cuda_fail(e_, #expr); \
   } while (0)
 
-template <typename T> void free_dev(T *&p) {
-  if (p) cudaFree((void *)p);
+// Device memory of a handle comes from the stream-ordered allocator on the
+// handle's stream (cudaMallocAsync), so creating and destroying solvers does
+// not synchronise the device (serving creates and retires many).
+template <typename T> void free_dev(T *&p, cudaStream_t s = nullptr) {
+  if (p) cudaFreeAsync((void *)p, s);
   p = nullptr;
+}
+
+// Keep freed pool memory for reuse instead of returning it at every
+// synchronisation (once per device; a process-local pool attribute).
+void retain_pool(int device) {
+  static std::mutex m;
+  static bool done[64] = {};
+  std::lock_guard<std::mutex> lk(m);
+  if (device < 0 || device >= 64 || done[device]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done[device] = true;
 }
 
 // Twiddles of the shared-memory Stockham transform in pass order (layout of
@@ -144,17 +168,25 @@ cd transmission(double k, double beta, double delta, double dz) {
   return std::exp(-k * (beta + im * delta) * dz);
 }
 
+// Host-to-device copy on the handle's stream, finished before returning (the
+// host buffers are temporaries).
+int h2d(pxp_solver_s *h, void *dst, const void *src, size_t bytes) {
+  PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  return PXP_OK;
+}
+
 // Upload complex128 host values in the solver's precision.
 int upload_complex(pxp_solver_s *h, void *dst, const cd *src, long long n) {
   if (h->prec == pxp::kFP64) {
-    PXP_TRY_CUDA(h, cudaMemcpy(dst, src, sizeof(cd) * n, cudaMemcpyHostToDevice));
+    if (int rc_ = h2d(h, dst, src, sizeof(cd) * n)) return rc_;
   } else {
     std::vector<float> tmp(2 * n);
     for (long long i = 0; i < n; ++i) {
       tmp[2 * i] = (float)src[i].real();
       tmp[2 * i + 1] = (float)src[i].imag();
     }
-    PXP_TRY_CUDA(h, cudaMemcpy(dst, tmp.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice));
+    if (int rc_ = h2d(h, dst, tmp.data(), sizeof(float) * 2 * n)) return rc_;
   }
   return PXP_OK;
 }
@@ -164,12 +196,14 @@ int upload_complex(pxp_solver_s *h, void *dst, const cd *src, long long n) {
 size_t table_entry_bytes(const pxp_solver_s *) { return 16; }
 
 int upload_table(pxp_solver_s *h, void *dst, const cd *src, long long n) {
-  PXP_TRY_CUDA(h, cudaMemcpy(dst, src, sizeof(cd) * n, cudaMemcpyHostToDevice));
+  PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, sizeof(cd) * n, cudaMemcpyHostToDevice, h->stream));
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
   return PXP_OK;
 }
 
 int alloc(pxp_solver_s *h, void **p, size_t bytes, const char *what) {
-  cudaError_t e = cudaMalloc(p, bytes);
+  cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
+  if (e == cudaSuccess) h->dev_bytes += bytes;
   if (e != cudaSuccess) {
     *p = nullptr;
     cudaGetLastError();
@@ -207,7 +241,7 @@ int fft1d_set_trans(pxp_solver_s *h, const double *delta, const double *beta, in
       if (h->prec == pxp::kFP32) v = v / (double)n;
       t[j] = v;
     }
-  free_dev(h->d_trans);
+  free_dev(h->d_trans, h->stream);
   int rc;
   if ((rc = alloc(h, &h->d_trans, table_entry_bytes(h) * t.size(), "transmission table")))
     return rc;
@@ -230,7 +264,8 @@ int fft1d_write_job(pxp_solver_s *h) {
   j.save_every = h->save_every;
   j.max_slots = h->max_slots;
   j.trans_step0 = h->trans_step0;
-  PXP_TRY_CUDA(h, cudaMemcpy(h->d_job, &j, sizeof(j), cudaMemcpyHostToDevice));
+  h->job_fft = j;
+  if (int rc_ = h2d(h, h->d_job, &j, sizeof(j))) return rc_;
   return PXP_OK;
 }
 
@@ -252,12 +287,11 @@ int cn_set_planes(pxp_solver_s *h, const double *delta, const double *beta, int 
     std::memcpy(&buf[2 * per + (size_t)s * n], delta + src1, sizeof(double) * n);
     std::memcpy(&buf[3 * per + (size_t)s * n], beta + src1, sizeof(double) * n);
   }
-  free_dev(h->d_mat);
+  free_dev(h->d_mat, h->stream);
   int rc;
   if ((rc = alloc(h, (void **)&h->d_mat, sizeof(double) * buf.size(), "material planes")))
     return rc;
-  PXP_TRY_CUDA(h, cudaMemcpy(h->d_mat, buf.data(), sizeof(double) * buf.size(),
-                             cudaMemcpyHostToDevice));
+  if (int rc_ = h2d(h, h->d_mat, buf.data(), sizeof(double) * buf.size())) return rc_;
   h->mat_block = (long long)per;
   h->mat_stride = nsteps > 1 ? n : 0;
   h->mat_step0 = first_step;
@@ -304,10 +338,10 @@ int cn_build_lu(pxp_solver_s *h, const double *delta, const double *beta) {
   const cd sub = -0.25 * IMAG_UNIT * rho * Hm * gval;
   std::vector<cd> gh;
   thomas_factor(diag, sub, gh);
-  free_dev(h->d_lu);
+  free_dev(h->d_lu, h->stream);
   int rc;
   if ((rc = alloc(h, &h->d_lu, sizeof(cd) * 2 * n, "factor tables"))) return rc;
-  PXP_TRY_CUDA(h, cudaMemcpy(h->d_lu, gh.data(), sizeof(cd) * 2 * n, cudaMemcpyHostToDevice));
+  if (int rc_ = h2d(h, h->d_lu, gh.data(), sizeof(cd) * 2 * n)) return rc_;
   return PXP_OK;
 }
 
@@ -325,10 +359,10 @@ int adi_build_lu(pxp_solver_s *h) {
   thomas_factor(dgx, -0.5 * im / (k * dx * dx), gx);
   thomas_factor(dgy, -0.5 * im / (k * dy * dy), gy);
   gx.insert(gx.end(), gy.begin(), gy.end());
-  free_dev(h->d_lu);
+  free_dev(h->d_lu, h->stream);
   int rc;
   if ((rc = alloc(h, &h->d_lu, sizeof(cd) * 4 * n, "factor tables"))) return rc;
-  PXP_TRY_CUDA(h, cudaMemcpy(h->d_lu, gx.data(), sizeof(cd) * 4 * n, cudaMemcpyHostToDevice));
+  if (int rc_ = h2d(h, h->d_lu, gx.data(), sizeof(cd) * 4 * n)) return rc_;
   return PXP_OK;
 }
 
@@ -512,7 +546,8 @@ int cn_write_job(pxp_solver_s *h) {
   j.transparent = h->prob.transparent_bc ? 1 : 0;
   j.lu_g = h->d_lu;
   j.lu_h = h->d_lu ? (const void *)((const cd *)h->d_lu + n) : nullptr;
-  PXP_TRY_CUDA(h, cudaMemcpy(h->d_job, &j, sizeof(j), cudaMemcpyHostToDevice));
+  h->job_cn = j;
+  if (int rc_ = h2d(h, h->d_job, &j, sizeof(j))) return rc_;
   return PXP_OK;
 }
 
@@ -596,6 +631,7 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
     return PXP_ERR_UNSUPPORTED;
   }
   cudaError_t e = cudaSetDevice(p.device);
+  if (e == cudaSuccess) retain_pool(p.device);
   if (e == cudaSuccess) e = cudaStreamCreate(&h->stream);
   if (e != cudaSuccess) {
     set_global_error(std::string("CUDA initialisation: ") + cudaGetErrorString(e));
@@ -649,16 +685,16 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
 int pxp_solver_destroy(pxp_solver h) {
   if (h == nullptr) return PXP_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  free_dev(h->d_field);
-  free_dev(h->d_saves);
-  free_dev(h->d_kern);
-  free_dev(h->d_trans);
-  free_dev(h->d_tw);
-  free_dev(h->d_mat);
-  free_dev(h->d_job);
-  free_dev(h->d_field2);
-  free_dev(h->d_spheres);
-  free_dev(h->d_lu);
+  free_dev(h->d_field, h->stream);
+  free_dev(h->d_saves, h->stream);
+  free_dev(h->d_kern, h->stream);
+  free_dev(h->d_trans, h->stream);
+  free_dev(h->d_tw, h->stream);
+  free_dev(h->d_mat, h->stream);
+  free_dev(h->d_job, h->stream);
+  free_dev(h->d_field2, h->stream);
+  free_dev(h->d_spheres, h->stream);
+  free_dev(h->d_lu, h->stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return PXP_OK;
@@ -723,7 +759,7 @@ int pxp_set_material_spheres(pxp_solver h, const pxp_sphere *spheres, int n) {
     return h->fail(PXP_ERR_UNSUPPORTED, "sphere materials apply to the 3-D kinds");
   PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
   h->spheres.assign(spheres, spheres + n);
-  free_dev(h->d_spheres);
+  free_dev(h->d_spheres, h->stream);
   if (n > 0) {
     std::vector<pxp::Sphere> dev(n);
     for (int i = 0; i < n; ++i)
@@ -731,8 +767,7 @@ int pxp_set_material_spheres(pxp_solver h, const pxp_sphere *spheres, int n) {
                 spheres[i].beta};
     int rc;
     if ((rc = alloc(h, (void **)&h->d_spheres, sizeof(pxp::Sphere) * n, "sphere list"))) return rc;
-    PXP_TRY_CUDA(h, cudaMemcpy(h->d_spheres, dev.data(), sizeof(pxp::Sphere) * n,
-                               cudaMemcpyHostToDevice));
+    if (int rc_ = h2d(h, h->d_spheres, dev.data(), sizeof(pxp::Sphere) * n)) return rc_;
   }
   h->material_set = true;
   return PXP_OK;
@@ -891,6 +926,232 @@ int pxp_shape(pxp_solver h, unsigned *nx, unsigned *ny, unsigned *nz) {
   if (nx) *nx = h->nx;
   if (ny) *ny = h->ny;
   if (nz) *nz = h->nz;
+  return PXP_OK;
+}
+
+int pxp_device_bytes(pxp_solver h, size_t *bytes) {
+  if (h == nullptr || bytes == nullptr) return PXP_ERR_INVALID;
+  *bytes = h->dev_bytes;
+  return PXP_OK;
+}
+
+int pxp_get_intensity(pxp_solver h, double *intensity) {
+  if (h == nullptr || intensity == nullptr) return PXP_ERR_INVALID;
+  std::vector<double> f(2 * h->npts);
+  int rc = download_field(h, f.data(), h->d_field);
+  if (rc) return rc;
+  for (long long i = 0; i < h->npts; ++i)
+    intensity[i] = f[2 * i] * f[2 * i] + f[2 * i + 1] * f[2 * i + 1];
+  return PXP_OK;
+}
+
+}  // extern "C"
+
+// ============================================================== batches ==
+struct pxp_batch_s {
+  int device = 0;
+  size_t budget = 0, used = 0;
+  cudaStream_t stream = nullptr;  // 2-D group launches
+  std::vector<pxp_solver_s *> active;
+  void *d_jobs = nullptr;
+  size_t d_jobs_cap = 0;
+  void *h_jobs = nullptr;  // pinned staging of the job descriptors
+  size_t h_jobs_cap = 0;
+  std::string err;
+  int fail(int code, const std::string &m) {
+    err = m;
+    set_global_error(m);
+    return code;
+  }
+};
+
+namespace {
+
+bool is_2d(const pxp_solver_s *h) {
+  return h->prob.kind == PXP_FFT_SOLVER_2D || h->prob.kind == PXP_CRANK_NICHOLSON;
+}
+bool cn_uses_const(const pxp_solver_s *h) {
+  return h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0;
+}
+
+int grow(pxp_batch_s *b, size_t bytes) {
+  if (bytes <= b->d_jobs_cap) return PXP_OK;
+  size_t cap = std::max(bytes, 2 * b->d_jobs_cap);
+  if (b->d_jobs) cudaFreeAsync(b->d_jobs, b->stream);
+  if (b->h_jobs) {
+    cudaStreamSynchronize(b->stream);
+    cudaFreeHost(b->h_jobs);
+  }
+  b->d_jobs = nullptr;
+  b->h_jobs = nullptr;
+  cudaError_t e = cudaMallocAsync(&b->d_jobs, cap, b->stream);
+  if (e == cudaSuccess) e = cudaMallocHost(&b->h_jobs, cap);
+  if (e != cudaSuccess) return b->fail(PXP_ERR_NOMEM, "batch job arrays");
+  b->d_jobs_cap = b->h_jobs_cap = cap;
+  return PXP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pxp_batch_create(int device, size_t budget, pxp_batch *out) {
+  if (out == nullptr) return PXP_ERR_INVALID;
+  *out = nullptr;
+  pxp_batch_s *b = new (std::nothrow) pxp_batch_s();
+  if (!b) return PXP_ERR_NOMEM;
+  b->device = device;
+  b->budget = budget;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) retain_pool(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    set_global_error(std::string("batch stream: ") + cudaGetErrorString(e));
+    delete b;
+    return PXP_ERR_CUDA;
+  }
+  *out = b;
+  return PXP_OK;
+}
+
+int pxp_batch_destroy(pxp_batch b) {
+  if (b == nullptr) return PXP_OK;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  if (b->d_jobs) cudaFreeAsync(b->d_jobs, b->stream);
+  cudaStreamSynchronize(b->stream);
+  if (b->h_jobs) cudaFreeHost(b->h_jobs);
+  cudaStreamDestroy(b->stream);
+  delete b;
+  return PXP_OK;
+}
+
+int pxp_batch_admit(pxp_batch b, pxp_solver h, int nsteps) {
+  if (b == nullptr || h == nullptr || nsteps < 0) return PXP_ERR_INVALID;
+  if (h->prob.device != b->device) return b->fail(PXP_ERR_INVALID, "solver on another device");
+  if (!h->ic_set) return b->fail(PXP_ERR_INVALID, "solver has no initial conditions");
+  for (pxp_solver_s *a : b->active)
+    if (a == h) return b->fail(PXP_ERR_INVALID, "solver already admitted");
+  if (h->plane_count > 0 &&
+      (h->current_step < (unsigned)h->plane_first ||
+       (long long)h->current_step + nsteps > (long long)h->plane_first + h->plane_count))
+    return b->fail(PXP_ERR_INVALID, "steps outside the material planes provided");
+  if (b->used + h->dev_bytes > b->budget) return PXP_ERR_NOT_READY;
+  cudaSetDevice(b->device);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return b->fail(PXP_ERR_CUDA, "solver stream");
+  h->batch_remaining = nsteps;
+  b->active.push_back(h);
+  b->used += h->dev_bytes;
+  return PXP_OK;
+}
+
+int pxp_batch_round(pxp_batch b, int max_steps) {
+  if (b == nullptr || max_steps <= 0) return PXP_ERR_INVALID;
+  cudaSetDevice(b->device);
+  // the staging buffer of the previous round must be consumed
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return b->fail(PXP_ERR_CUDA, "batch stream");
+  // ---- 2-D groups: key (kind, n, precision, CN matrix path)
+  struct Key {
+    int kind, n, prec, cpath;
+    bool operator<(const Key &o) const {
+      return std::tie(kind, n, prec, cpath) < std::tie(o.kind, o.n, o.prec, o.cpath);
+    }
+  };
+  std::map<Key, std::vector<pxp_solver_s *>> groups;
+  for (pxp_solver_s *h : b->active) {
+    if (!is_2d(h) || h->batch_remaining <= 0) continue;
+    Key k{h->prob.kind, (int)h->nx, (int)h->prec, h->prob.kind == PXP_CRANK_NICHOLSON ? (int)cn_uses_const(h) : 0};
+    groups[k].push_back(h);
+  }
+  size_t total = 0;
+  for (auto &g : groups)
+    total += g.second.size() * (g.first.kind == PXP_FFT_SOLVER_2D ? sizeof(pxp::Fft1dJob) : sizeof(pxp::CnJob));
+  if (total > 0) {
+    int rc = grow(b, total);
+    if (rc) return rc;
+  }
+  size_t off = 0;
+  std::vector<std::pair<size_t, const std::pair<const Key, std::vector<pxp_solver_s *>> *>> offs;
+  for (auto &g : groups) {
+    offs.push_back({off, &g});
+    for (pxp_solver_s *h : g.second) {
+      const int n = std::min(h->batch_remaining, max_steps);
+      if (g.first.kind == PXP_FFT_SOLVER_2D) {
+        pxp::Fft1dJob j = h->job_fft;
+        j.step0 = (int)h->current_step;
+        j.nsteps = n;
+        std::memcpy((char *)b->h_jobs + off, &j, sizeof(j));
+        off += sizeof(j);
+      } else {
+        pxp::CnJob j = h->job_cn;
+        j.step0 = (int)h->current_step;
+        j.nsteps = n;
+        std::memcpy((char *)b->h_jobs + off, &j, sizeof(j));
+        off += sizeof(j);
+      }
+    }
+  }
+  if (total > 0 &&
+      cudaMemcpyAsync(b->d_jobs, b->h_jobs, total, cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
+    return b->fail(PXP_ERR_CUDA, "job upload");
+  for (auto &o : offs) {
+    const Key &k = o.second->first;
+    const auto &list = o.second->second;
+    const void *jobs = (const char *)b->d_jobs + o.first;
+    cudaError_t e;
+    if (k.kind == PXP_FFT_SOLVER_2D)
+      e = pxp::launch_fft1d((pxp::Precision)k.prec, (const pxp::Fft1dJob *)jobs, (int)list.size(),
+                            k.n, -1, -1, b->stream);
+    else if (k.cpath)
+      e = pxp::launch_cn_const((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
+                               k.n, -1, -1, b->stream);
+    else
+      e = pxp::launch_cn((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(), k.n,
+                         -1, -1, b->stream);
+    if (e != cudaSuccess) return b->fail(PXP_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    for (pxp_solver_s *h : list) {
+      const int n = std::min(h->batch_remaining, max_steps);
+      h->current_step += (unsigned)n;
+      h->batch_remaining -= n;
+    }
+  }
+  // ---- 3-D solvers on their own streams
+  for (pxp_solver_s *h : b->active) {
+    if (is_2d(h) || h->batch_remaining <= 0) continue;
+    const int n = std::min(h->batch_remaining, max_steps);
+    int rc = pxp_step(h, n);
+    if (rc) return b->fail(rc, h->err);
+    h->batch_remaining -= n;
+  }
+  return PXP_OK;
+}
+
+int pxp_batch_collect(pxp_batch b, pxp_solver *done, int cap, int *count) {
+  if (b == nullptr || count == nullptr || (cap > 0 && done == nullptr)) return PXP_ERR_INVALID;
+  cudaSetDevice(b->device);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return b->fail(PXP_ERR_CUDA, "batch stream");
+  int c = 0;
+  std::vector<pxp_solver_s *> keep;
+  for (pxp_solver_s *h : b->active) {
+    if (!is_2d(h) && cudaStreamSynchronize(h->stream) != cudaSuccess)
+      return b->fail(PXP_ERR_CUDA, "solver stream");
+    if (h->batch_remaining <= 0 && c < cap) {
+      done[c++] = h;
+      b->used -= h->dev_bytes;
+    } else {
+      keep.push_back(h);
+    }
+  }
+  b->active.swap(keep);
+  *count = c;
+  return PXP_OK;
+}
+
+int pxp_batch_status(pxp_batch b, int *active, size_t *bytes) {
+  if (b == nullptr) return PXP_ERR_INVALID;
+  if (active) *active = (int)b->active.size();
+  if (bytes) *bytes = b->used;
   return PXP_OK;
 }
 
