@@ -13,9 +13,10 @@ configurations:
     spheres (radius U[20, 150], centre uniform in the volume, delta
     U[1e-6, 5e-5], beta = delta/50).
 
-Sizes above 8192 points are drawn as 8192 for the 1-D solvers: an FP64 FFT
-line above 8192 points and an FP32 Crank-Nicolson system above 8192 points
-do not fit one CTA's shared memory in this build.
+Sizes above 8192 points are drawn as 8192 for FFTSolver2D and above 4096 as
+4096 for CrankNicholson: an FP64 FFT line above 8192 points and an FP64
+Crank-Nicolson system above 4096 points do not fit one CTA's shared memory
+in this build.
 
 `run_batched` admits every job into one Batch (one launch per group of equal
 2-D kind/size, 3-D jobs on their own streams); `run_plain` runs the same jobs
@@ -36,7 +37,8 @@ import numpy as np
 import paxpro_b200 as pxp
 from paxpro_b200 import workloads as wl
 
-MAX_1D_N = 8192
+MAX_FFT2D_N = 8192
+MAX_CN_N = 4096
 
 
 @dataclass
@@ -57,7 +59,7 @@ class Job:
 
 
 def draw_2d(rng: np.random.Generator, kind: str, seed: int) -> Job:
-    n = min(2 ** int(rng.integers(8, 15)), MAX_1D_N)
+    n = min(2 ** int(rng.integers(8, 15)), MAX_FFT2D_N if kind == "fft2d" else MAX_CN_N)
     steps = int(rng.integers(200, 5001))
     core = float(rng.uniform(10.0, 60.0))
     delta = float(rng.uniform(2e-6, 3e-5))
