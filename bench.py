@@ -1,7 +1,7 @@
 """Benchmark of the paraxial propagation step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg1|cfg0|cfg2]
+                    [--workload cfg1|cfg0|cfg3|cfg4]
 
 Metric: grid-point * steps per second (whole job, all ranks).  A bench
 "step" is one pass of the workload over its synthetic input:
@@ -11,6 +11,10 @@ Metric: grid-point * steps per second (whole job, all ranks).  A bench
                   z = 1 mm), plain FP64; the two problems run concurrently on
                   two streams.  2.13e9 grid-point-steps per bench step.
   cfg0            FFTSolver2D Nx=2048, 4000 steps, FP64 (8.19e6 pt-steps).
+  cfg3            mixed batch (512 2-D + 32 3-D problems), FP32 served mode in
+                  one batch, against the same problems one at a time in FP64.
+  cfg4            serving: Poisson arrivals at 50..2000 jobs/s, p50/p99
+                  latency and throughput, against plain FP64 one at a time.
 
 Each rank runs its own replica (the path does not shard one field; weak
 scaling).  Timing: CUDA events on the solvers' own streams, warm-up first,
@@ -41,6 +45,26 @@ import numpy as np  # noqa: E402
 from paxpro_b200 import workloads as wl  # noqa: E402
 
 L2_FLUSH_BYTES = 256 << 20
+
+
+def profiled_traffic(name: str):
+    """DRAM bytes (read + write) per launch recorded in a profiles/ summary
+    (ncu --set full capture of the same kernel and size); None if absent."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    unit = {"B": 1, "KB": 1e3, "MB": 1e6, "GB": 1e9}
+    total = 0.0
+    found = False
+    with open(path) as f:
+        for line in f:
+            cells = [c.strip() for c in line.split("|")]
+            if len(cells) > 2 and cells[1] in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+                tok = cells[2].split()
+                v = float(tok[0])
+                total += v * unit.get(tok[1], 1) if len(tok) > 1 else v
+                found = True
+    return total if found else None
 
 
 def measured_peaks():
@@ -186,6 +210,85 @@ class Cfg0:
 WORKLOADS = {"cfg1": Cfg1, "cfg0": Cfg0}
 
 
+def run_mixed(args, rank, world, device):
+    """cfg3: the mixed batch (512 2-D + 32 3-D problems) in FP32 served mode,
+    one Batch, against the same problems run one at a time in plain FP64."""
+    import torch
+    from paxpro_b200 import serving as sv
+    torch.cuda.set_device(device)
+    jobs = sv.cfg3_jobs(seed=3 + rank)
+    keep = set(range(0, len(jobs), 37))
+    sv.run_batched(jobs[:40], precision=1)          # warm-up (kernels, pools)
+    batched = sv.run_batched(jobs, precision=1, keep=keep)
+    plain = sv.run_plain(jobs, precision=0, keep=keep)
+    errs = []
+    for i in keep:
+        a, b = batched.intensities[i], plain.intensities[i]
+        errs.append(float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+    if rank != 0:
+        return None
+    return {
+        "metric": "grid-pt*steps/s (FP32 served, batched)",
+        "value": world * batched.rate,
+        "unit": "grid-pt*steps/s",
+        "n_gpus": world,
+        "steps": 1,
+        "warmup": 1,
+        "ms_per_step": batched.seconds * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c64 storage, FP64 twiddle/factor products",
+        "data": "synthetic (seeded mixed workload)",
+        "config": {"workload": "cfg3: 512 x 2-D (80% FFT, 20% CN) + 32 x 3-D FFT, one batch",
+                   "grid_pt_steps": batched.pts_steps,
+                   "timing": "wall clock between device synchronisations"},
+        "plain_fp64": {"value": plain.rate, "seconds": plain.seconds},
+        "served_over_plain": batched.rate / plain.rate,
+        "max_rel_intensity_err_vs_fp64": max(errs),
+    }
+
+
+def run_serving(args, rank, world, device):
+    """cfg4: Poisson arrivals swept over rates; served FP32 continuous batching
+    against plain FP64 one-at-a-time on the same job stream."""
+    import torch
+    from paxpro_b200 import serving as sv
+    torch.cuda.set_device(device)
+    window = float(os.environ.get("PXP_SERVE_WINDOW", "2.0"))
+    sv.serve(sv.cfg4_jobs(200.0, 0.1, seed=99), precision=1)  # warm-up
+    rows = []
+    for rate in (50, 100, 200, 500, 1000, 2000):
+        jobs = sv.cfg4_jobs(float(rate), window, seed=4 + rate)
+        r = sv.serve(jobs, precision=1, round_steps=200)
+        rows.append({"rate_jobs_per_s": rate, "jobs": r.jobs, "p50_s": r.p50, "p99_s": r.p99,
+                     "throughput": r.throughput, "max_active": r.max_active})
+    jobs = sv.cfg4_jobs(200.0, window, seed=204)
+    plain = sv.run_plain(jobs, precision=0)
+    if rank != 0:
+        return None
+    best = max(rows, key=lambda x: x["throughput"])
+    return {
+        "metric": "grid-pt*steps/s served (FP32); p50/p99 job latency",
+        "value": world * best["throughput"],
+        "unit": "grid-pt*steps/s",
+        "n_gpus": world,
+        "steps": len(rows),
+        "warmup": 1,
+        "ms_per_step": None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c64 storage, FP64 twiddle/factor products",
+        "data": "synthetic (seeded Poisson job stream)",
+        "config": {"workload": f"cfg4: Poisson arrivals, {window} s per rate, 80% FFT2D / 15% CN / "
+                               "5% FFT3D, HBM budget 150 GB"},
+        "rates": rows,
+        "plain_fp64_one_at_a_time": {"value": plain.rate, "busy_seconds": plain.seconds,
+                                     "jobs": len(jobs)},
+    }
+
+
 # ------------------------------------------------------------- GPU arm --
 def run_ours(args, rank, world, device):
     import torch
@@ -279,7 +382,7 @@ def run_ours(args, rank, world, device):
                     "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(achieved / peak, 4),
                     "peak_kind": peak_kind,
-                    "traffic": None,
+                    "traffic": profiled_traffic("adi_const_kernel_1024.md"),
                     "note": "algorithmic bytes 2 x 16 B per point per half step; the 16 MB "
                             "field stays in the 126 MB L2 across half steps, so this is "
                             "effective bandwidth (see profiles/)"}
@@ -364,6 +467,10 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             rates.append(r)
     value = statistics.median(rates)
+    if args.workload not in ("cfg0", "cfg1"):
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement is timed on "
+                          "the cfg0/cfg1 workloads only"}))
+        return None
     W = {"cfg1": Cfg1.name, "cfg0": Cfg0.name}[args.workload]
     return {
         "impl": "reference",
@@ -395,7 +502,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfg1")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["cfg3", "cfg4"], default="cfg1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -411,8 +518,13 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    out = run_ours(args, rank, world, local)
-    if out is not None and not args.no_cpu_baseline:
+    if args.workload == "cfg3":
+        out = run_mixed(args, rank, world, local)
+    elif args.workload == "cfg4":
+        out = run_serving(args, rank, world, local)
+    else:
+        out = run_ours(args, rank, world, local)
+    if out is not None and not args.no_cpu_baseline and args.workload in ("cfg0", "cfg1"):
         rate, sample = cpu_rate(args.workload, 1, scale=1.0)
         out["cpu_baseline"] = {"value": rate, "unit": "grid-pt*steps/s", "cores": 1,
                                "kind": "port", "sample": sample + f"; {cpu_model()}"}

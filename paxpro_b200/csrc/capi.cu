@@ -213,18 +213,55 @@ int alloc(pxp_solver_s *h, void **p, size_t bytes, const char *what) {
   return PXP_OK;
 }
 
+// ---- shared read-only tables ---------------------------------------------
+// Twiddle and propagator tables depend only on the device, the length and the
+// grid steps, so solvers with the same ones share a single device copy,
+// built once and kept until the process exits (serving creates many solvers
+// with the same grids).  The handles do not own these copies.
+struct TableKey {
+  int device, kind;  // kind 0: twiddles, 1: 1-D propagator
+  unsigned n;
+  double dx, dz, k;
+  bool operator<(const TableKey &o) const {
+    return std::tie(device, kind, n, dx, dz, k) < std::tie(o.device, o.kind, o.n, o.dx, o.dz, o.k);
+  }
+};
+std::mutex g_table_mutex;
+std::map<TableKey, void *> g_tables;
+
+int shared_table(pxp_solver_s *h, int kind, void **out) {
+  const unsigned n = h->nx;
+  TableKey key{h->prob.device, kind, n, kind ? h->prob.x.step : 0.0, kind ? h->prob.z.step : 0.0,
+               kind ? h->prob.wavenumber : 0.0};
+  std::lock_guard<std::mutex> lk(g_table_mutex);
+  auto it = g_tables.find(key);
+  if (it != g_tables.end()) {
+    *out = it->second;
+    return PXP_OK;
+  }
+  std::vector<cd> t;
+  if (kind == 0) {
+    t = twiddles((int)n);
+  } else {
+    t.resize(n);
+    for (unsigned i = 0; i < n; ++i)
+      t[i] = kernel_2d(spatial_freq(i, n, h->prob.x.step), h->prob.z.step, h->prob.wavenumber);
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, sizeof(cd) * n);
+  if (e != cudaSuccess) return h->fail(PXP_ERR_NOMEM, "shared table allocation");
+  e = cudaMemcpy(p, t.data(), sizeof(cd) * n, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return h->cuda_fail(e, "shared table upload");
+  g_tables[key] = p;
+  *out = p;
+  return PXP_OK;
+}
+
 // ---- FFT 1-D -------------------------------------------------------------
 int fft1d_setup(pxp_solver_s *h) {
-  const unsigned n = h->nx;
-  std::vector<cd> ker(n);
-  for (unsigned i = 0; i < n; ++i)
-    ker[i] = kernel_2d(spatial_freq(i, n, h->prob.x.step), h->prob.z.step, h->prob.wavenumber);
   int rc;
-  if ((rc = alloc(h, &h->d_kern, table_entry_bytes(h) * n, "propagator table"))) return rc;
-  if ((rc = upload_table(h, h->d_kern, ker.data(), n))) return rc;
-  std::vector<cd> tw = twiddles((int)n);
-  if ((rc = alloc(h, &h->d_tw, sizeof(cd) * n, "twiddle table"))) return rc;
-  if ((rc = upload_table(h, h->d_tw, tw.data(), n))) return rc;
+  if ((rc = shared_table(h, 1, &h->d_kern))) return rc;
+  if ((rc = shared_table(h, 0, &h->d_tw))) return rc;
   return alloc(h, &h->d_job, sizeof(pxp::Fft1dJob), "job descriptor");
 }
 
@@ -671,12 +708,9 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
         return cleanup_fail(rc);
       if ((rc = adi_build_lu(h))) return cleanup_fail(rc);
       break;
-    case PXP_FFT_SOLVER_3D: {
-      std::vector<cd> tw = twiddles((int)h->nx);
-      if ((rc = alloc(h, &h->d_tw, sizeof(cd) * h->nx, "twiddle table"))) return cleanup_fail(rc);
-      if ((rc = upload_table(h, h->d_tw, tw.data(), h->nx))) return cleanup_fail(rc);
+    case PXP_FFT_SOLVER_3D:
+      if ((rc = shared_table(h, 0, &h->d_tw))) return cleanup_fail(rc);
       break;
-    }
   }
   *out = h;
   return PXP_OK;
@@ -687,9 +721,9 @@ int pxp_solver_destroy(pxp_solver h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_dev(h->d_field, h->stream);
   free_dev(h->d_saves, h->stream);
-  free_dev(h->d_kern, h->stream);
+  h->d_kern = nullptr;  // shared table, not owned
   free_dev(h->d_trans, h->stream);
-  free_dev(h->d_tw, h->stream);
+  h->d_tw = nullptr;  // shared table, not owned
   free_dev(h->d_mat, h->stream);
   free_dev(h->d_job, h->stream);
   free_dev(h->d_field2, h->stream);
