@@ -19,6 +19,7 @@
 #include <tuple>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -133,12 +134,12 @@ void retain_pool(int device) {
 // fft_smem.cuh): for each pass (sub-transform length ns, radix r = 8 while it
 // divides the rest, then 4 or 2), entries (q-1)*ns + k = exp(-2 pi i q k /
 // (ns r)), in extended precision.  At least n entries are allocated.
-std::vector<cd> twiddles(int n) {
+std::vector<cd> twiddles(int n, int maxr = 8) {
   std::vector<cd> w(std::max(n, 1));
   const long double pi_l = 3.141592653589793238462643383279502884L;
   int off = 0;
   for (int ns = 1; ns < n;) {
-    const int r = n / ns >= 8 ? 8 : n / ns;
+    const int r = n / ns >= maxr ? maxr : (n / ns >= 8 ? 8 : n / ns);
     for (int q = 1; q < r; ++q)
       for (int k = 0; k < ns; ++k) {
         long double a = -2.0L * pi_l * (long double)(q * k) / (long double)(ns * r);
@@ -219,7 +220,8 @@ int alloc(pxp_solver_s *h, void **p, size_t bytes, const char *what) {
 // built once and kept until the process exits (serving creates many solvers
 // with the same grids).  The handles do not own these copies.
 struct TableKey {
-  int device, kind;  // kind 0: twiddles, 1: 1-D propagator
+  int device, kind;  // kind 0: twiddles (radix 8), 1: 1-D propagator, 2: kx^2 per
+                     // column, 3: twiddles (radix 16)
   unsigned n;
   double dx, dz, k;
   bool operator<(const TableKey &o) const {
@@ -231,8 +233,8 @@ std::map<TableKey, void *> g_tables;
 
 int shared_table(pxp_solver_s *h, int kind, void **out) {
   const unsigned n = h->nx;
-  TableKey key{h->prob.device, kind, n, kind ? h->prob.x.step : 0.0, kind ? h->prob.z.step : 0.0,
-               kind ? h->prob.wavenumber : 0.0};
+  TableKey key{h->prob.device, kind, n, kind ? h->prob.x.step : 0.0,
+               kind == 1 ? h->prob.z.step : 0.0, kind == 1 ? h->prob.wavenumber : 0.0};
   std::lock_guard<std::mutex> lk(g_table_mutex);
   auto it = g_tables.find(key);
   if (it != g_tables.end()) {
@@ -240,17 +242,27 @@ int shared_table(pxp_solver_s *h, int kind, void **out) {
     return PXP_OK;
   }
   std::vector<cd> t;
-  if (kind == 0) {
-    t = twiddles((int)n);
-  } else {
+  std::vector<double> t2;
+  if (kind == 0 || kind == 3) {
+    t = twiddles((int)n, kind == 3 ? 16 : 8);
+  } else if (kind == 1) {
     t.resize(n);
     for (unsigned i = 0; i < n; ++i)
       t[i] = kernel_2d(spatial_freq(i, n, h->prob.x.step), h->prob.z.step, h->prob.wavenumber);
+  } else {
+    // fl(kx*kx) with kx = spatialFreqX (src/fftSolver3D.cpp:32-40)
+    t2.resize(n);
+    for (unsigned i = 0; i < n; ++i) {
+      const double kx = spatial_freq(i, n, h->prob.x.step);
+      t2[i] = kx * kx;
+    }
   }
+  const size_t bytes = kind == 2 ? sizeof(double) * n : sizeof(cd) * n;
   void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, sizeof(cd) * n);
+  cudaError_t e = cudaMalloc(&p, bytes);
   if (e != cudaSuccess) return h->fail(PXP_ERR_NOMEM, "shared table allocation");
-  e = cudaMemcpy(p, t.data(), sizeof(cd) * n, cudaMemcpyHostToDevice);
+  e = cudaMemcpy(p, kind == 2 ? (const void *)t2.data() : (const void *)t.data(), bytes,
+                 cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return h->cuda_fail(e, "shared table upload");
   g_tables[key] = p;
   *out = p;
@@ -506,6 +518,75 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
       out.push_back({sp.cx, sp.cy, sp.cz, sp.radius, sp.delta, sp.beta});
 }
 
+// Launch-variant autotuner of the FFTSolver3D passes.  The first solver with
+// a given (device, precision, n) times every variant on a zeroed scratch
+// field (one untimed x+y pass pair, then three timed ones; the fastest kept),
+// and every solver with that key runs the winner from its first step on, so
+// a field never depends on when tuning happened (radix 8 and radix 16 round
+// differently).  PXP_FFT3D_VARIANT=0|1|2 pins the variant instead.
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, unsigned>, int> g_fft3d_variant;
+
+int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, const void *tw16,
+                  int *out) {
+  if (const char *env = std::getenv("PXP_FFT3D_VARIANT")) {
+    const int v = std::atoi(env);
+    if (v >= 0 && v < pxp::kFft3dVariants) {
+      *out = v;
+      return PXP_OK;
+    }
+  }
+  const auto key = std::make_tuple(h->prob.device, (int)h->prec, h->nx);
+  std::lock_guard<std::mutex> lk(g_tune_mutex);
+  auto it = g_fft3d_variant.find(key);
+  if (it != g_fft3d_variant.end()) {
+    *out = it->second;
+    return PXP_OK;
+  }
+  const size_t bytes = h->csize * h->npts;
+  void *scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, bytes, h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "FFT3D tuning scratch");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  pxp::Fft3dPass q = q0;
+  q.field = scratch;
+  q.save = nullptr;
+  q.nspheres = 0;
+  q.spheres_all = nullptr;
+  int best_v = 0;
+  float best = 1e30f;
+  if ((e = cudaMemsetAsync(scratch, 0, bytes, h->stream)) == cudaSuccess) {
+    for (int v = 0; v < pxp::kFft3dVariants && e == cudaSuccess; ++v) {
+      float tmin = 1e30f;
+      for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+        cudaEventRecord(e0, h->stream);
+        q.mode = 1;
+        e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, h->stream);
+        q.mode = 2;
+        if (e == cudaSuccess) e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, h->stream);
+        cudaEventRecord(e1, h->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+          tmin = std::min(tmin, ms);
+      }
+      if (tmin < best) {
+        best = tmin;
+        best_v = v;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(scratch, h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "FFT3D tuning");
+  g_fft3d_variant[key] = best_v;
+  *out = best_v;
+  return PXP_OK;
+}
+
 int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   const pxp_problem &p = h->prob;
   const int n = (int)h->nx;
@@ -530,16 +611,22 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     q.inv_damp_x = p.x.step / p.absorber_damping;
     q.inv_damp_y = p.y.step / p.absorber_damping;
   }
+  void *kx2 = nullptr, *tw16 = nullptr;
+  if (int rc = shared_table(h, 2, &kx2)) return rc;
+  if (int rc = shared_table(h, 3, &tw16)) return rc;
+  int variant = 0;
+  if (int rc = fft3d_variant(h, q, kx2, tw16, &variant)) return rc;
   cudaError_t e;
   q.mode = 0;  // forward transform along y of the real-space field
-  if ((e = pxp::launch_fft3d_pass(h->prec, q, h->stream)) != cudaSuccess)
+  if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, h->stream)) != cudaSuccess)
     return h->cuda_fail(e, "FFT3D forward y pass");
   std::vector<pxp::Sphere> act;
   for (int i = 0; i < nsteps; ++i) {
     const unsigned step = first + (unsigned)i;
+    const int v = variant;
     q.mode = 1;
     q.save = nullptr;
-    if ((e = pxp::launch_fft3d_pass(h->prec, q, h->stream)) != cudaSuccess)
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, h->stream)) != cudaSuccess)
       return h->cuda_fail(e, "FFT3D x pass");
     q.mode = (i == nsteps - 1) ? 3 : 2;
     q.z1 = get_z(h, step);
@@ -557,7 +644,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
                       (int)(step / (unsigned)h->save_every) - 1 < h->max_slots;
     q.save = save ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
                   : nullptr;
-    if ((e = pxp::launch_fft3d_pass(h->prec, q, h->stream)) != cudaSuccess)
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, h->stream)) != cudaSuccess)
       return h->cuda_fail(e, "FFT3D y pass");
   }
   return PXP_OK;

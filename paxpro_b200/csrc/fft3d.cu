@@ -16,10 +16,12 @@
 // exp(-k (beta + i delta) dz) (:154), the refraction integral (:253-273) when
 // the material at z0 and z1 differs by more than 1e-10, and the absorber
 // bands (Absorber::apply, src/absorber.cpp:3-12: y bands, then x bands).
-// sin/cos/exp are CUDA's (<= 2 ulp); everything else is rounded as the
-// reference rounds it.
+// The propagator's sin/cos come from pxp_sincos.h (within 1 ulp of 1.0 on
+// the argument range), exp in the refraction is CUDA's; everything else is
+// rounded as the reference rounds it.
 #include "fft_smem.cuh"
 #include "pxp_kernels.h"
+#include "pxp_sincos.h"
 
 namespace pxp {
 
@@ -160,32 +162,43 @@ __device__ __forceinline__ void store_line(const C *src, C *field, int line, boo
   }
 }
 
-// Persistent CTAs walk the n lines of one pass.  Two line buffers: the copy
-// of the next line is in flight while the current one is transformed.  The
-// twiddle table (and for the x pass the kx^2 table) is loaded into shared
-// memory once per CTA.
-template <typename R, int N, int T>
-__global__ void __launch_bounds__(T) fft3d_pass_kernel(const Fft3dPass q) {
+// Persistent CTAs walk the n lines of one pass.  Variants (the same
+// arithmetic per radix; radix 16 changes the FFT's rounding pattern, within
+// the parity tolerance):
+//   DB = true : two line buffers; the copy of the next line is in flight while
+//               the current one is transformed; twiddles and kx^2 in shared
+//               memory (one CTA per SM at large n);
+//   DB = false: one line buffer, twiddles and kx^2 read through L1, registers
+//               capped so that two CTAs share an SM and overlap each other's
+//               copies;
+//   MAXR = 16 : radix-16 Stockham passes (three passes for 4096 points),
+//               N/16 threads per line, single buffer.
+// The launcher times the variants on the first steps and keeps the fastest.
+template <typename R, int N, int T, bool DB, int MAXR>
+__global__ void __launch_bounds__(T, (DB || MAXR == 16 || T >= 1024) ? 1 : 2) fft3d_pass_kernel(const Fft3dPass q,
+                                                                  const double *__restrict__ gkx2,
+                                                                  const double2 *__restrict__ gtw) {
   using C = typename Cx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *buf0 = reinterpret_cast<C *>(smem_raw);
-  C *buf1 = buf0 + N;
-  double2 *tw = reinterpret_cast<double2 *>(buf1 + N);
-  double *kx2 = reinterpret_cast<double *>(tw + N);
+  C *buf1 = DB ? buf0 + N : buf0;
+  double2 *stw = reinterpret_cast<double2 *>(buf0 + (DB ? 2 * N : N));
+  double *skx2 = reinterpret_cast<double *>(stw + N);
   C *field = reinterpret_cast<C *>(q.field);
   const bool strided = q.mode == 1;
   const int tid = threadIdx.x;
+  const double2 *tw = gtw;
+  const double *kx2 = gkx2;
 
   int line = blockIdx.x;
   if (line < N) load_line<C, N, T>(buf0, field, line, strided);
   cp_async_commit();
-  const double2 *gtw = reinterpret_cast<const double2 *>(q.twiddle);
-  for (int i = tid; i < N; i += T) tw[i] = gtw[i];
-  if (strided) {
-    for (int i = tid; i < N; i += T) {
-      const double kx = kfreq(i, N, q.two_pi, q.stepn_x);
-      kx2[i] = __dmul_rn(kx, kx);
-    }
+  if constexpr (DB) {
+    for (int i = tid; i < N; i += T) stw[i] = gtw[i];
+    if (strided)
+      for (int i = tid; i < N; i += T) skx2[i] = gkx2[i];
+    tw = stw;
+    kx2 = skx2;
   }
   const double inv_norm = 1.0 / q.norm;  // n*n is a power of two: exact
   C *save = reinterpret_cast<C *>(q.save);
@@ -194,26 +207,30 @@ __global__ void __launch_bounds__(T) fft3d_pass_kernel(const Fft3dPass q) {
     C *u = (it & 1) ? buf1 : buf0;
     C *nxt = (it & 1) ? buf0 : buf1;
     const int next = line + gridDim.x;
-    if (next < N) load_line<C, N, T>(nxt, field, next, strided);
-    cp_async_commit();
-    cp_async_wait1();
+    if constexpr (DB) {
+      if (next < N) load_line<C, N, T>(nxt, field, next, strided);
+      cp_async_commit();
+      cp_async_wait1();
+    } else {
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+    }
     __syncthreads();
 
     if (q.mode == 1) {
-      fft_smem<C, N, T, -1>(u, tw, tid);
+      fft_smem<C, N, T, -1, MAXR>(u, tw, tid);
       const double ky = kfreq(line, N, q.two_pi, q.stepn_y);
       const double ky2 = __dmul_rn(ky, ky);
       for (int j = tid; j < N; j += T) {
         const double phi = __dmul_rn(q.a, __dadd_rn(kx2[j], ky2));
         double sn, cs;
-        sincos(phi, &sn, &cs);
+        sincos_cw(phi, &sn, &cs);
         u[sw<C>(j)] = mul_k<R>(u[sw<C>(j)], mk(cs, -sn));
       }
       __syncthreads();
-      fft_smem<C, N, T, +1>(u, tw, tid);
+      fft_smem<C, N, T, +1, MAXR>(u, tw, tid);
     } else {
       if (q.mode >= 2) {
-        fft_smem<C, N, T, +1>(u, tw, tid);
+        fft_smem<C, N, T, +1, MAXR>(u, tw, tid);
         for (int j = tid; j < N; j += T) {
           const C v = refract3<R>(q, u[sw<C>(j)], line, j, inv_norm);
           u[sw<C>(j)] = v;
@@ -221,23 +238,31 @@ __global__ void __launch_bounds__(T) fft3d_pass_kernel(const Fft3dPass q) {
         }
         __syncthreads();
       }
-      if (q.mode != 3) fft_smem<C, N, T, -1>(u, tw, tid);
+      if (q.mode != 3) fft_smem<C, N, T, -1, MAXR>(u, tw, tid);
     }
     store_line<C, N, T>(u, field, line, strided);
-    __syncthreads();  // the buffer is refilled by the prefetch of iteration it+1
+    __syncthreads();  // the buffer is refilled next
+    if constexpr (!DB) {
+      if (next < N) load_line<C, N, T>(u, field, next, strided);
+      cp_async_commit();
+    }
   }
   cp_async_commit();
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-template <int N> constexpr int pass_threads() { return N / 8 < 32 ? 32 : (N / 8 > 1024 ? 1024 : N / 8); }
+template <int N, int MAXR> constexpr int pass_threads() {
+  return N / MAXR < 32 ? 32 : (N / MAXR > 1024 ? 1024 : N / MAXR);
+}
 
-template <typename R, int N>
-static cudaError_t fft3d_launch_n(const Fft3dPass &q, cudaStream_t s) {
+template <typename R, int N, bool DB, int MAXR>
+static cudaError_t fft3d_launch_v(const Fft3dPass &q, const double *kx2, const double2 *tw,
+                                  cudaStream_t s) {
   using C = typename Cx<R>::T;
-  constexpr int T = pass_threads<N>();
-  constexpr size_t smem = 2 * sizeof(C) * N + sizeof(double2) * N + sizeof(double) * N;
-  auto k = fft3d_pass_kernel<R, N, T>;
+  constexpr int T = pass_threads<N, MAXR>();
+  constexpr size_t smem = DB ? 2 * sizeof(C) * N + sizeof(double2) * N + sizeof(double) * N
+                             : sizeof(C) * N;
+  auto k = fft3d_pass_kernel<R, N, T, DB, MAXR>;
   static int grid = 0;
   if (grid == 0) {
     if (smem > 48 * 1024) {
@@ -251,8 +276,22 @@ static cudaError_t fft3d_launch_n(const Fft3dPass &q, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     grid = sms * (per > 0 ? per : 1);
   }
-  k<<<grid < N ? grid : N, T, smem, s>>>(q);
+  k<<<grid < N ? grid : N, T, smem, s>>>(q, kx2, tw);
   return cudaGetLastError();
+}
+
+template <typename R, int N>
+static cudaError_t fft3d_launch_n(const Fft3dPass &q, int variant, const double *kx2,
+                                  const double2 *tw16, cudaStream_t s) {
+  using C = typename Cx<R>::T;
+  const double2 *tw8 = reinterpret_cast<const double2 *>(q.twiddle);
+  // two line buffers plus tables exceed a CTA's shared memory above 4096
+  // points (FP64) / 8192 (FP32): the single-buffer form stands in
+  constexpr bool db_fits = (2 * sizeof(C) + sizeof(double2) + sizeof(double)) * N <= 227 * 1024;
+  if constexpr (db_fits)
+    if (variant == 0) return fft3d_launch_v<R, N, true, 8>(q, kx2, tw8, s);
+  if (variant <= 1) return fft3d_launch_v<R, N, false, 8>(q, kx2, tw8, s);
+  return fft3d_launch_v<R, N, false, 16>(q, kx2, tw16, s);
 }
 
 bool fft3d_supported(Precision p, int n) {
@@ -260,10 +299,12 @@ bool fft3d_supported(Precision p, int n) {
   return n <= 8192;
 }
 
-cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, cudaStream_t s) {
+cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, const double *kx2,
+                              const void *tw16, cudaStream_t s) {
 #define PXP_C3(NN)                                                                  \
   case NN:                                                                          \
-    return p == kFP64 ? fft3d_launch_n<double, NN>(q, s) : fft3d_launch_n<float, NN>(q, s);
+    return p == kFP64 ? fft3d_launch_n<double, NN>(q, variant, kx2, (const double2 *)tw16, s) \
+                      : fft3d_launch_n<float, NN>(q, variant, kx2, (const double2 *)tw16, s);
   switch (q.n) {
     PXP_C3(64) PXP_C3(128) PXP_C3(256) PXP_C3(512) PXP_C3(1024) PXP_C3(2048) PXP_C3(4096)
     PXP_C3(8192)

@@ -95,29 +95,78 @@ __device__ __forceinline__ void dft8(C *v) {
   v[1] = b0; v[3] = b1; v[5] = b2; v[7] = b3;
 }
 
+// v * W16^m (forward) or v * conj(W16^m) (inverse), W16 = exp(-2 pi i / 16),
+// for the internal twiddles of the 16-point DFT; products in FP64.
+template <int SIGN, int M>
+__device__ __forceinline__ double2 w16(double2 v) {
+  constexpr double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;
+  constexpr double h = 0.70710678118654752440;
+  constexpr double c = M == 1 ? c1 : M == 2 ? h : M == 3 ? s1 : M == 6 ? -h : -c1;
+  constexpr double sf = M == 1 ? -s1 : M == 2 ? -h : M == 3 ? -c1 : M == 6 ? -h : s1;
+  constexpr double sn = SIGN < 0 ? sf : -sf;
+  return make_double2(fma(v.x, c, -v.y * sn), fma(v.x, sn, v.y * c));
+}
+template <int SIGN, int M>
+__device__ __forceinline__ float2 w16(float2 v) {
+  double2 r = w16<SIGN, M>(make_double2(v.x, v.y));
+  return make_float2((float)r.x, (float)r.y);
+}
+
+// 16-point DFT as 4 x 4: DFTs over the stride-4 subsequences, internal
+// twiddles W16^(n2 k1), DFTs over n2, then the 4 x 4 transpose of the
+// output order.
+template <int SIGN, typename C>
+__device__ __forceinline__ void dft16(C *v) {
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) dft4<SIGN>(v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]);
+  // v[n2 + 4 k1] *= W16^(n2 k1)
+  v[5] = w16<SIGN, 1>(v[5]);
+  v[9] = w16<SIGN, 2>(v[9]);
+  v[13] = w16<SIGN, 3>(v[13]);
+  v[6] = w16<SIGN, 2>(v[6]);
+  v[10] = mul_i<SIGN>(v[10]);
+  v[14] = w16<SIGN, 6>(v[14]);
+  v[7] = w16<SIGN, 3>(v[7]);
+  v[11] = w16<SIGN, 6>(v[11]);
+  v[15] = w16<SIGN, 9>(v[15]);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) dft4<SIGN>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+  // X[k1 + 4 k2] sits at v[4 k1 + k2]
+  C t[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) t[i] = v[i];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[4 * k1 + k2];
+}
+
 template <int R, int SIGN, typename C>
 __device__ __forceinline__ void dft_r(C *v) {
   if constexpr (R == 2) dft2<SIGN>(v[0], v[1]);
   else if constexpr (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
-  else dft8<SIGN>(v);
+  else if constexpr (R == 8) dft8<SIGN>(v);
+  else dft16<SIGN>(v);
 }
 
 // One Stockham pass over x (length N, swizzled layout) with T threads; NS =
 // length of the sub-transforms already done.  `lane` is this thread's index
 // in [0, T).
-// Number of twiddle entries of all passes of a length-N transform, and the
-// offset of the pass with sub-transform length NS.
-__host__ __device__ constexpr int stockham_radix(int n, int ns) { return n / ns >= 8 ? 8 : n / ns; }
-__host__ __device__ constexpr int stockham_offset(int n, int ns) {
+// Radix of the pass with sub-transform length ns (largest of MAXR, 8 that
+// divides the rest, else the rest), the offset of its twiddles, and the
+// table size (n - 1 entries: the passes telescope).
+__host__ __device__ constexpr int stockham_radix(int n, int ns, int maxr) {
+  return n / ns >= maxr ? maxr : (n / ns >= 8 ? 8 : n / ns);
+}
+__host__ __device__ constexpr int stockham_offset(int n, int ns, int maxr) {
   int off = 0;
-  for (int s = 1; s < ns; s *= stockham_radix(n, s)) off += (stockham_radix(n, s) - 1) * s;
+  for (int s = 1; s < ns; s *= stockham_radix(n, s, maxr)) off += (stockham_radix(n, s, maxr) - 1) * s;
   return off;
 }
-__host__ __device__ constexpr int stockham_twiddle_count(int n) { return stockham_offset(n, n); }
 
-template <typename C, int N, int T, int SIGN, int R, int NS>
+template <typename C, int N, int T, int SIGN, int R, int NS, int MAXR>
 __device__ __forceinline__ void stockham_pass(C *x, const double2 *tw, int lane) {
-  constexpr int OFF = stockham_offset(N, NS);
+  constexpr int OFF = stockham_offset(N, NS, MAXR);
   constexpr int NB = N / R;
   constexpr int PER = (NB + T - 1) / T;
   C v[PER][R];
@@ -151,13 +200,12 @@ __device__ __forceinline__ void stockham_pass(C *x, const double2 *tw, int lane)
   __syncthreads();
 }
 
-template <typename C, int N, int T, int SIGN, int NS = 1>
+template <typename C, int N, int T, int SIGN, int MAXR = 8, int NS = 1>
 __device__ __forceinline__ void fft_smem(C *x, const double2 *tw, int lane) {
   if constexpr (NS < N) {
-    constexpr int REM = N / NS;
-    constexpr int R = REM >= 8 ? 8 : REM;
-    stockham_pass<C, N, T, SIGN, R, NS>(x, tw, lane);
-    fft_smem<C, N, T, SIGN, NS * R>(x, tw, lane);
+    constexpr int R = stockham_radix(N, NS, MAXR);
+    stockham_pass<C, N, T, SIGN, R, NS, MAXR>(x, tw, lane);
+    fft_smem<C, N, T, SIGN, MAXR, NS * R>(x, tw, lane);
   }
 }
 

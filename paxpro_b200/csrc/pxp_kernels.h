@@ -132,7 +132,13 @@ struct Fft3dPass {
   int thick_x, thick_y;
   double inv_damp_x, inv_damp_y;
 };
-cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, cudaStream_t s);
+// variant: 0 = radix 8, double-buffered, tables in shared memory; 1 = radix
+// 8, single buffer, tables through L1; 2 = radix 16, single buffer.
+// kx2: n doubles, fl(kx*kx) per column index; q.twiddle / tw16: Stockham
+// twiddles for radix 8 / radix 16 pass orders.
+cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, const double *kx2,
+                              const void *tw16, cudaStream_t s);
+constexpr int kFft3dVariants = 3;
 bool fft3d_supported(Precision p, int n);
 
 }  // namespace pxp
