@@ -68,7 +68,7 @@ def lib():
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m paxpro_b200.build`")
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python paxpro_b200/build.py`")
     L = C.CDLL(LIB_PATH)
     d = C.POINTER(C.c_double)
     h = C.c_void_p

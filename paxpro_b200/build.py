@@ -1,6 +1,8 @@
 """Build the CUDA library libpaxpro_b200.so in-tree for sm_100a.
 
-    python -m paxpro_b200.build        (or paxpro_b200.build.build())
+    python paxpro_b200/build.py
+
+(a script, not `python -m`: importing the package loads the library it builds)
 
 Each .cu under csrc/ is compiled separately (in parallel) with nvcc for
 sm_100a and linked into paxpro_b200/lib/libpaxpro_b200.so.  Host code is
