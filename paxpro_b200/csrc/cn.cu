@@ -164,9 +164,12 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
 // each step is the right-hand-side stencil plus two substitution scans
 // (scan_solve.cuh).  The field stays in registers: thread t owns points
 // t*M .. t*M+M-1 and trades its two edge values with its neighbours through
-// shared memory.  The per-point right-hand-side coefficient
-// 1 - 0.5*(beta'*r + i*delta'*r) is formed once with the reference's
-// rounding and kept in shared memory.
+// shared memory.  The right-hand side is regrouped as
+// i*q*(left + right) + d*centre, q = rho/4, with the per-point coefficient
+// d = (1 - 0.5*(beta'*r + i*delta'*r)) - i*rho/2 formed once (the first part
+// with the reference's rounding) and kept in shared memory; the regrouping
+// and the FMAs differ from the reference's operation order at rounding level.
+// Tables sit in chunk-transposed slots (cslot), free of bank conflicts.
 template <typename R, int M, int T>
 __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ jobs, int step0_ov,
                                                     int nsteps_ov) {
@@ -174,9 +177,9 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
   constexpr int N = M * T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2 *gs = reinterpret_cast<double2 *>(smem_raw);
-  constexpr int NP = N + N / 8;  // padded length (pad8)
-  double2 *hs = gs + NP;
-  double2 *xch = hs + NP;  // 2 per thread
+  double2 *hs = gs + N;
+  double2 *ds = hs + N;
+  double2 *xch = ds + N;  // 2 per thread
   Affine *scratch = reinterpret_cast<Affine *>(xch + 2 * T);
   CnJob job = jobs[blockIdx.x];
   if (nsteps_ov >= 0) {
@@ -187,29 +190,25 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
   const double rho = job.rho, r = job.r;
   const double2 *gt = reinterpret_cast<const double2 *>(job.lu_g);
   const double2 *ht = reinterpret_cast<const double2 *>(job.lu_h);
-  for (int i = t; i < N; i += T) {
-    gs[pad8(i)] = gt[i];
-    hs[pad8(i)] = ht[i];
+  const double q = __dmul_rn(0.25, rho);
+  const int s0 = t * M;
+  // each thread fills the slots of its own chunk
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int k = cslot<M, T>(t, m);
+    gs[k] = gt[s0 + m];
+    hs[k] = ht[s0 + m];
+    const double bp = job.beta_prev[s0 + m], dp = job.delta_prev[s0 + m];
+    const double2 hh = mk(__dmul_rn(0.5, __dmul_rn(bp, r)), __dmul_rn(0.5, __dmul_rn(dp, r)));
+    ds[k] = mk(__dadd_rn(-hh.x, 1.0), __dsub_rn(-hh.y, 0.5 * rho));
   }
   C *field = reinterpret_cast<C *>(job.field);
-  const int s0 = t * M;
   double2 u[M];
 #pragma unroll
   for (int m = 0; m < M; ++m) u[m] = to_d(field[s0 + m]);
-  const double q = __dmul_rn(0.25, rho);
   C *saves = reinterpret_cast<C *>(job.saves);
-  __syncthreads();
   for (int st = 0; st < job.nsteps; ++st) {
     const int step = job.step0 + st;
-    // right-hand-side coefficient 1 - 0.5*(beta'*r + i*delta'*r) of this
-    // chunk (z-invariant medium: the same cached values every step)
-    double2 coef[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const double bp = job.beta_prev[s0 + m], dp = job.delta_prev[s0 + m];
-      const double2 hh = mk(__dmul_rn(0.5, __dmul_rn(bp, r)), __dmul_rn(0.5, __dmul_rn(dp, r)));
-      coef[m] = mk(__dadd_rn(-hh.x, 1.0), -hh.y);
-    }
     xch[2 * t] = u[0];
     xch[2 * t + 1] = u[M - 1];
     __syncthreads();
@@ -220,15 +219,10 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
     for (int m = 0; m < M; ++m) {
       const double2 left = m > 0 ? u[m - 1] : lft;
       const double2 right = m < M - 1 ? u[m + 1] : rgt;
-      // cn_rhs with the coefficient precomputed (same operations)
-      double2 sum = cx_add_rn(left, right);
-      double2 v = cx_mul_rn(sum, mk(0.0, q));
-      double2 c4 = cx_scale_rn(u[m], 0.25);
-      double2 tt = cx_scale_rn(cx_scale_rn(cx_mul_rn(c4, mk(0.0, 1.0)), rho), 2.0);
-      v = cx_sub_rn(v, tt);
-      rh[m] = cx_add_rn(v, cx_mul_rn(coef[m], u[m]));
+      const double2 sum = cadd(left, right);
+      rh[m] = cfma(ds[cslot<M, T>(t, m)], u[m], mk(-q * sum.y, q * sum.x));
     }
-    const_solve<M, T>(rh, gs, hs, s0, scratch);
+    const_solve_reg<M, T>(rh, gs, hs, t, scratch);
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
@@ -250,7 +244,7 @@ template <typename R, int T>
 static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
                                      cudaStream_t s) {
   constexpr int N = kCnM * T;
-  constexpr size_t smem = sizeof(double2) * (2 * (N + N / 8) + 2 * T) + sizeof(Affine) * (T / 32 + 1);
+  constexpr size_t smem = sizeof(double2) * (3 * N + 2 * T) + sizeof(Affine) * (T / 32 + 1);
   auto k = cn_const_kernel<R, kCnM, T>;
   if (smem > 48 * 1024) {
     static const cudaError_t attr =
@@ -261,7 +255,7 @@ static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int
   return cudaGetLastError();
 }
 
-bool cn_const_supported(Precision, int n) { return n >= 2 * kCnM && !(n & (n - 1)) && n <= 4096; }
+bool cn_const_supported(Precision, int n) { return n >= 8 * kCnM && !(n & (n - 1)) && n <= 4096; }
 
 cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0, int nsteps,
                             cudaStream_t s) {
@@ -271,8 +265,7 @@ cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int
     return p == kFP64 ? cn_const_launch_t<double, TT>(d_jobs, nj, step0, nsteps, s)   \
                       : cn_const_launch_t<float, TT>(d_jobs, nj, step0, nsteps, s);
   switch (n / kCnM) {
-    PXP_CC(2) PXP_CC(4) PXP_CC(8) PXP_CC(16) PXP_CC(32) PXP_CC(64) PXP_CC(128) PXP_CC(256)
-    PXP_CC(512)
+    PXP_CC(8) PXP_CC(16) PXP_CC(32) PXP_CC(64) PXP_CC(128) PXP_CC(256) PXP_CC(512)
     default:
       return cudaErrorInvalidValue;
   }

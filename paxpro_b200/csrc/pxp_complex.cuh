@@ -39,6 +39,10 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
   return mk(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
 }
+// a * b + c with four FMAs; the chain from c is two FMAs deep
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+  return mk(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return mk(a.x * s, a.y * s); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return mk(a.x * s, a.y * s); }
 // multiply by -i (forward) or +i (inverse)
