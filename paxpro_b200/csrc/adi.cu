@@ -21,12 +21,18 @@
 // operations (the same r^2 < R^2 test as the oracle); the host culls, per
 // half step, spheres whose dz^2 alone is >= R^2, which cannot contain any
 // point of the plane.
+#include <cmath>
+
+#include "bulk_copy.cuh"
 #include "pxp_complex.cuh"
 #include "pxp_kernels.h"
 #include "scan_solve.cuh"
 #include "tridiag.cuh"
 
 namespace pxp {
+
+// kernel waits that ran out on this device (never reset), read by the host
+__device__ unsigned int g_wait_timeouts = 0;
 
 __device__ __forceinline__ void sphere_material(const AdiHalf &h, double x, double y,
                                                 double &delta, double &beta) {
@@ -307,12 +313,234 @@ static cudaError_t adi_const_launch(const AdiHalf &h, const void *g, const void 
   return cudaGetLastError();
 }
 
+// Vacuum half step, FP64, n <= 1024, one wave: G systems per CTA so that
+// ceil(n / G) CTAs cover the 148 SMs once (G = 7 at n = 1024: 147 CTAs).
+// The G + 2 staged rows (G systems and their two stencil halos) and the
+// factor tables are brought into shared memory by TMA bulk copies counted on
+// an mbarrier, and the results leave as bulk stores, so that the copy
+// engine, not per-thread requests, carries the tile in both directions.
+// Shared-memory layouts keep every copied run contiguous and the per-chunk
+// reads of the solve free of bank conflicts:
+//   XH (x half step, the G + 2 systems of a position adjacent in memory):
+//      entry (c, m, g) at c*(M*(G+2) + 1) + m*(G+2) + g, one spare entry after
+//      each chunk; one copy per position;
+//   YH (y half step, a system is a row): entry (c, m, g) at
+//      g*P*(M+1) + c*(M+1) + m, one spare entry after each chunk; one copy per
+//      chunk of a row.
+// The tables [g | h | pf | pb] (Thomas factors and the in-chunk products of
+// the multipliers, const_solve_tab) are host-built in chunk-transposed slots
+// (adi_const_staged_tables) and copied in as one block.  The same tile holds
+// the results (row g + 1 of system g) for the stores.
+template <int N, int M, int G, bool XH>
+struct AdiTmaTile {
+  static constexpr int P = N / M, RW = G + 2;
+  static constexpr int SIZE = XH ? N * RW + P : RW * P * (M + 1);
+  __device__ static __forceinline__ int at(int c, int m, int g) {
+    return XH ? c * (M * RW + 1) + m * RW + g : g * P * (M + 1) + c * (M + 1) + m;
+  }
+};
+
+template <int N, int M, int G, bool XH>
+__global__ void __launch_bounds__(G *(N / M))
+    adi_const_tma_kernel(const AdiHalf h, const double2 *__restrict__ tabs) {
+  using L = AdiTmaTile<N, M, G, XH>;
+  constexpr int P = N / M;
+  constexpr int T = G * P;
+  constexpr int RW = G + 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
+  double2 *gs = reinterpret_cast<double2 *>(smem_raw + 16);
+  double2 *hs = gs + N;
+  double2 *pf = hs + N;
+  double2 *pb = pf + N;
+  Affine *scratch = reinterpret_cast<Affine *>(pb + N);
+  double2 *tile = reinterpret_cast<double2 *>(scratch + (T / 32 + 1));
+  __shared__ int staged_ok;
+  const int tid = threadIdx.x;
+  const int s_base = blockIdx.x * G;
+  const double2 *in = reinterpret_cast<const double2 *>(h.in);
+  double2 *out = reinterpret_cast<double2 *>(h.out);
+  // staged systems s_base - 1 + g exist for g in [g_lo, g_hi)
+  const int g_lo = s_base == 0 ? 1 : 0;
+  const int g_hi = N - s_base + 1 < RW ? N - s_base + 1 : RW;
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_arrive_expect_tx(bar, (unsigned)(sizeof(double2) * (4 * N + (g_hi - g_lo) * N)));
+  }
+  __syncthreads();
+  if (tid == 0) bulk_load(gs, tabs, (unsigned)(sizeof(double2) * 4 * N), bar);
+  if constexpr (XH) {
+    for (int p = tid; p < N; p += T) {
+      const int c = p / M, m = p % M;
+      bulk_load(tile + L::at(c, m, g_lo), in + (long long)p * h.stride_pos + (s_base - 1 + g_lo),
+                (unsigned)(sizeof(double2) * (g_hi - g_lo)), bar);
+      for (int g = 0; g < g_lo; ++g) tile[L::at(c, m, g)] = mk(0.0, 0.0);
+      for (int g = g_hi; g < RW; ++g) tile[L::at(c, m, g)] = mk(0.0, 0.0);
+    }
+  } else {
+    for (int idx = tid; idx < RW * P; idx += T) {
+      const int g = idx / P, c = idx % P;
+      double2 *dst = tile + L::at(c, 0, g);
+      if (g >= g_lo && g < g_hi) {
+        bulk_load(dst, in + (long long)(s_base - 1 + g) * h.stride_sys + c * M,
+                  (unsigned)(sizeof(double2) * M), bar);
+      } else {
+#pragma unroll
+        for (int m = 0; m < M; ++m) dst[m] = mk(0.0, 0.0);
+      }
+    }
+  }
+  if (tid == 0) {
+    const bool ok = mbar_wait_bounded(bar, 0, 2000000000ull);
+    if (!ok) {
+      atomicAdd(&g_wait_timeouts, 1u);
+      mbar_wait_bounded(bar, 0, 2000000000ull);  // copies still in flight
+    }
+    staged_ok = ok;
+  }
+  __syncthreads();
+  if (!staged_ok) return;
+  (void)mbar_try_wait(bar, 0);  // phase complete: orders the copied data for this thread
+  const int g = tid / P, c = tid % P;
+  const int s = s_base + g;  // s >= N: padding system of the last CTA, all zero
+  const double inv_kd2_expl = __ddiv_rn(1.0, h.kd2_expl);
+  const double hk = 0.5 * inv_kd2_expl;
+  double2 r[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const double2 rr = cmul(mk(h.inv_dzh, -inv_kd2_expl), tile[L::at(c, m, g + 1)]);
+    double2 nb = mk(0.0, 0.0);
+    if (s > 0) nb = tile[L::at(c, m, g)];
+    if (s < N - 1) nb = cadd(nb, tile[L::at(c, m, g + 2)]);
+    r[m] = mk(fma(-hk, nb.y, rr.x), fma(hk, nb.x, rr.y));
+  }
+  const_solve_tab<M, P>(r, gs, hs, pf, pb, c, scratch);
+  __syncthreads();  // every read of the staged tile is done
+#pragma unroll
+  for (int m = 0; m < M; ++m) tile[L::at(c, m, g + 1)] = r[m];
+  fence_async_smem();
+  __syncthreads();
+  double2 *save = reinterpret_cast<double2 *>(h.save);
+  const int nsys = N - s_base < G ? N - s_base : G;  // the last CTA may hold fewer
+  if constexpr (XH) {
+    for (int p = tid; p < N; p += T) {
+      const double2 *src = tile + L::at(p / M, p % M, 1);
+      const long long off = (long long)p * h.stride_pos + s_base;
+      bulk_store(out + off, src, (unsigned)(sizeof(double2) * nsys));
+      if (save) bulk_store(save + off, src, (unsigned)(sizeof(double2) * nsys));
+    }
+  } else {
+    for (int idx = tid; idx < nsys * P; idx += T) {
+      const int gg = idx / P, cc = idx % P;
+      const double2 *src = tile + L::at(cc, 0, gg + 1);
+      const long long off = (long long)(s_base + gg) * h.stride_sys + cc * M;
+      bulk_store(out + off, src, (unsigned)(sizeof(double2) * M));
+      if (save) bulk_store(save + off, src, (unsigned)(sizeof(double2) * M));
+    }
+  }
+  bulk_commit();
+  bulk_wait_read();
+}
+
+template <int N, int M, int G, bool XH>
+static cudaError_t adi_const_tma_launch_x(const AdiHalf &h, const void *tabs, cudaStream_t s) {
+  constexpr int P = N / M, T = G * P;
+  constexpr size_t smem = 16 + sizeof(double2) * 4 * N + sizeof(Affine) * (T / 32 + 1) +
+                          sizeof(double2) * AdiTmaTile<N, M, G, XH>::SIZE;
+  static_assert(smem <= 227 * 1024, "staged ADI tile exceeds shared memory");
+  static_assert(T % 32 == 0, "whole warps per CTA");
+  auto k = adi_const_tma_kernel<N, M, G, XH>;
+  if (smem > 48 * 1024) {
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return attr;
+  }
+  k<<<(N + G - 1) / G, T, smem, s>>>(h, (const double2 *)tabs);
+  return cudaGetLastError();
+}
+
+template <int N, int M, int G>
+static cudaError_t adi_const_tma_launch(const AdiHalf &h, const void *tabs, cudaStream_t s) {
+  if (tabs == nullptr) return cudaErrorInvalidValue;
+  return h.stride_sys == 1 ? adi_const_tma_launch_x<N, M, G, true>(h, tabs, s)
+                           : adi_const_tma_launch_x<N, M, G, false>(h, tabs, s);
+}
+
+// (M, G) of the TMA-staged kernel per size: every CTA holds whole warps
+// (G*n/M a multiple of 32) and ceil(n / G) CTAs fill the SMs about once.
+static bool adi_tma_config(int n, int *m, int *g) {
+  switch (n) {
+    case 64: *m = 8; *g = 4; return true;
+    case 128: *m = 8; *g = 2; return true;
+    case 256: *m = 8; *g = 2; return true;
+    case 512: *m = 8; *g = 4; return true;
+    case 1024: *m = 16; *g = 7; return true;
+    default: return false;
+  }
+}
+
+bool adi_const_staged_tables(int n, const double *g, const double *h, double *out) {
+  int M = 0, G = 0;
+  if (!adi_tma_config(n, &M, &G)) return false;
+  const int P = n / M;
+  auto slot = [&](int c, int m) { return m * P + (c ^ (m & 7)); };
+  // the device's cmul: (fma(ax, bx, -ay*by), fma(ax, by, ay*bx))
+  auto cmul_h = [](const double *a, const double *b, double *o) {
+    const double re = std::fma(a[0], b[0], -(a[1] * b[1]));
+    const double im = std::fma(a[0], b[1], a[1] * b[0]);
+    o[0] = re;
+    o[1] = im;
+  };
+  double *gs = out, *hs = out + 2 * n, *pf = out + 4 * n, *pb = out + 6 * n;
+  for (int c = 0; c < P; ++c) {
+    double prod[2] = {1.0, 0.0};
+    for (int m = 0; m < M; ++m) {
+      const int p = c * M + m, k = slot(c, m);
+      gs[2 * k] = g[2 * p];
+      gs[2 * k + 1] = g[2 * p + 1];
+      hs[2 * k] = h[2 * p];
+      hs[2 * k + 1] = h[2 * p + 1];
+      cmul_h(h + 2 * p, prod, prod);
+      pf[2 * k] = prod[0];
+      pf[2 * k + 1] = prod[1];
+    }
+    prod[0] = 1.0;
+    prod[1] = 0.0;
+    for (int m = M - 1; m >= 0; --m) {
+      const int p = c * M + m, k = slot(c, m);
+      cmul_h(h + 2 * p, prod, prod);
+      pb[2 * k] = prod[0];
+      pb[2 * k + 1] = prod[1];
+    }
+  }
+  return true;
+}
+
+unsigned wait_timeouts(cudaStream_t s) {
+  unsigned v = 0;
+  if (cudaMemcpyFromSymbolAsync(&v, g_wait_timeouts, sizeof(v), 0, cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return 0;
+  return v;
+}
+
 cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, const void *hh,
-                                  cudaStream_t s) {
+                                  const void *staged, cudaStream_t s) {
 #define PXP_AC(NN, GG)                                                                  \
   case NN:                                                                              \
     return p == kFP64 ? adi_const_launch<double, NN, GG>(h, g, hh, s)                   \
                       : adi_const_launch<float, NN, GG>(h, g, hh, s);
+  if (p == kFP64) {
+    switch (h.n) {
+      case 64: return adi_const_tma_launch<64, 8, 4>(h, staged, s);
+      case 128: return adi_const_tma_launch<128, 8, 2>(h, staged, s);
+      case 256: return adi_const_tma_launch<256, 8, 2>(h, staged, s);
+      case 512: return adi_const_tma_launch<512, 8, 4>(h, staged, s);
+      case 1024: return adi_const_tma_launch<1024, 16, 7>(h, staged, s);
+      default: break;
+    }
+  }
   switch (h.n) {
     PXP_AC(64, 4) PXP_AC(128, 4) PXP_AC(256, 4) PXP_AC(512, 4) PXP_AC(1024, 4) PXP_AC(2048, 2)
     default:

@@ -97,8 +97,20 @@ bool adi_supported(Precision p, int n);
 // Half step whose plane holds no material and no transparent boundary: the
 // matrix is the same for every system and every step; g/h are its Thomas
 // factor tables (n complex128 each, see scan_solve.cuh).
+// `staged`: the same tables with their in-chunk products in the layout the
+// FP64 TMA-staged kernel copies into shared memory (adi_const_staged_tables;
+// not read where that returns false for n).
 cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, const void *hh,
-                                  cudaStream_t s);
+                                  const void *staged, cudaStream_t s);
+// Host: fills out[0 .. 4n) complex128 with [g | h | pf | pb] in the
+// chunk-transposed slots of the TMA-staged vacuum kernel for size n (pf, pb:
+// products of h over each chunk's rows up to / from a row) and returns true;
+// false when size n runs the other kernel (out untouched).  g, h, out:
+// interleaved (re, im).
+bool adi_const_staged_tables(int n, const double *g, const double *h, double *out);
+// Kernel waits on the current device that ran out (bounded mbarrier waits),
+// read on stream s (synchronises s).
+unsigned wait_timeouts(cudaStream_t s);
 
 // --------------------------------------------------------------- FFT 3-D --
 // FFTSolver3D (src/fftSolver3D.cpp:52-156, 327-374) on an n x n field in the

@@ -53,6 +53,15 @@ __device__ __forceinline__ Affine shfl(Affine v, int d) {
   return o;
 }
 
+__device__ __forceinline__ Affine shfl_idx(Affine v, int src) {
+  Affine o;
+  o.a.x = __shfl_sync(0xffffffffu, v.a.x, src);
+  o.a.y = __shfl_sync(0xffffffffu, v.a.y, src);
+  o.b.x = __shfl_sync(0xffffffffu, v.b.x, src);
+  o.b.y = __shfl_sync(0xffffffffu, v.b.y, src);
+  return o;
+}
+
 // Exclusive scan of chunk transfers over the P threads of each system (the
 // P threads are contiguous in the CTA, chunk c at thread offset c, P a power
 // of two).  REVERSE = false scans in increasing chunk order (forward
@@ -85,10 +94,24 @@ __device__ __forceinline__ Affine exclusive_scan(Affine v, Affine *scratch) {
     if (lane == (REVERSE ? 0 : 31)) scratch[warp] = inc;
     __syncthreads();
     Affine pre = ident;
-    if (REVERSE) {
-      for (int w = W - 1; w > chunk_warp; --w) pre = compose(pre, scratch[first_warp + w]);
+    if constexpr (W <= 2) {
+      if (REVERSE) {
+        for (int w = W - 1; w > chunk_warp; --w) pre = compose(pre, scratch[first_warp + w]);
+      } else {
+        for (int w = 0; w < chunk_warp; ++w) pre = compose(pre, scratch[first_warp + w]);
+      }
     } else {
-      for (int w = 0; w < chunk_warp; ++w) pre = compose(pre, scratch[first_warp + w]);
+      // every warp scans its system's W warp totals with shuffles (lanes < W)
+      // and takes the exclusive value at its own position
+      Affine t = lane < W ? scratch[first_warp + lane] : ident;
+#pragma unroll
+      for (int d = 1; d < W; d <<= 1) {
+        Affine o = shfl<REVERSE>(t, d);
+        const bool take = REVERSE ? (lane + d < W) : (lane >= d && lane < W);
+        if (take) t = compose(o, t);
+      }
+      const Affine x = shfl_idx(t, REVERSE ? (chunk_warp + 1) & 31 : (chunk_warp + 31) & 31);
+      if (REVERSE ? chunk_warp < W - 1 : chunk_warp > 0) pre = x;
     }
     ex = compose(pre, ex);
   }
@@ -139,6 +162,100 @@ __device__ __forceinline__ void const_solve(double2 (&r)[M], const double2 *__re
     prod = cmul(h[pad8(p0 + m)], prod);
     r[m] = cadd(r[m], cmul(prod, x_in));
   }
+}
+
+// Chunk-transposed shared-memory slot of position p (chunk c = p / M, row m =
+// p % M) in a length M*P array: slot = m*P + (c ^ (m & 7)).  Threads of a warp
+// that read row m of consecutive chunks hit consecutive 16-byte slots, and
+// eight consecutive positions (one chunk, rows m..m+7) land in eight
+// different 16-byte bank groups, so both the per-chunk reads of the solve and
+// the position-order reads and writes of staging are free of bank conflicts
+// for 16-byte elements.  P must be a multiple of 8.
+template <int M, int P>
+__host__ __device__ __forceinline__ int cslot(int c, int m) {
+  static_assert(P % 8 == 0, "cslot needs P a multiple of 8");
+  return m * P + (c ^ (m & 7));
+}
+template <int M, int P>
+__host__ __device__ __forceinline__ int cslot_pos(int p) {
+  return cslot<M, P>(p / M, p % M);
+}
+
+// const_solve with the factor tables in chunk-transposed slots (cslot) and
+// the step-invariant in-chunk products of the multipliers read from tables:
+// pf at a row holds the product of h over the chunk's rows up to and
+// including it (forward), pb over the rows from it to the chunk's end
+// (backward).  Same recurrences and scans as const_solve.
+template <int M, int P>
+__device__ __forceinline__ void const_solve_tab(double2 (&r)[M], const double2 *__restrict__ g,
+                                                const double2 *__restrict__ h,
+                                                const double2 *__restrict__ pf,
+                                                const double2 *__restrict__ pb, int c,
+                                                Affine *scratch) {
+  // forward, zero carry-in: y_i = g_i r_i + h_i y_{i-1}
+  double2 y = cmul(g[cslot<M, P>(c, 0)], r[0]);
+  r[0] = y;
+#pragma unroll
+  for (int m = 1; m < M; ++m) {
+    const int k = cslot<M, P>(c, m);
+    y = cfma(h[k], y, cmul(g[k], r[m]));
+    r[m] = y;
+  }
+  Affine ex = exclusive_scan<P, false>(Affine{pf[cslot<M, P>(c, M - 1)], y}, scratch);
+  const double2 y_in = ex.b;
+#pragma unroll
+  for (int m = 0; m < M; ++m) r[m] = cfma(pf[cslot<M, P>(c, m)], y_in, r[m]);
+  // backward, zero carry-in: x_i = y_i + h_i x_{i+1}
+  double2 x = r[M - 1];
+#pragma unroll
+  for (int m = M - 2; m >= 0; --m) {
+    x = cfma(h[cslot<M, P>(c, m)], x, r[m]);
+    r[m] = x;
+  }
+  ex = exclusive_scan<P, true>(Affine{pb[cslot<M, P>(c, 0)], x}, scratch);
+  const double2 x_in = ex.b;
+#pragma unroll
+  for (int m = 0; m < M; ++m) r[m] = cfma(pb[cslot<M, P>(c, m)], x_in, r[m]);
+}
+
+// const_solve with the factor tables in chunk-transposed slots (cslot) and
+// the in-chunk products of the multipliers formed in the sweeps and kept in
+// registers for the carry-in fix-ups.
+template <int M, int P>
+__device__ __forceinline__ void const_solve_reg(double2 (&r)[M], const double2 *__restrict__ g,
+                                                const double2 *__restrict__ h, int c,
+                                                Affine *scratch) {
+  double2 pr[M];
+  // forward, zero carry-in: y_i = g_i r_i + h_i y_{i-1}
+  double2 y = cmul(g[cslot<M, P>(c, 0)], r[0]);
+  pr[0] = h[cslot<M, P>(c, 0)];
+  r[0] = y;
+#pragma unroll
+  for (int m = 1; m < M; ++m) {
+    const int k = cslot<M, P>(c, m);
+    const double2 hm = h[k];
+    y = cfma(hm, y, cmul(g[k], r[m]));
+    pr[m] = cmul(hm, pr[m - 1]);
+    r[m] = y;
+  }
+  Affine ex = exclusive_scan<P, false>(Affine{pr[M - 1], y}, scratch);
+  const double2 y_in = ex.b;
+#pragma unroll
+  for (int m = 0; m < M; ++m) r[m] = cfma(pr[m], y_in, r[m]);
+  // backward, zero carry-in: x_i = y_i + h_i x_{i+1}
+  double2 x = r[M - 1];
+  pr[M - 1] = h[cslot<M, P>(c, M - 1)];
+#pragma unroll
+  for (int m = M - 2; m >= 0; --m) {
+    const double2 hm = h[cslot<M, P>(c, m)];
+    x = cfma(hm, x, r[m]);
+    pr[m] = cmul(hm, pr[m + 1]);
+    r[m] = x;
+  }
+  ex = exclusive_scan<P, true>(Affine{pr[0], x}, scratch);
+  const double2 x_in = ex.b;
+#pragma unroll
+  for (int m = 0; m < M; ++m) r[m] = cfma(pr[m], x_in, r[m]);
 }
 
 }  // namespace pxp
