@@ -87,6 +87,11 @@ struct pxp_solver_s {
   bool material_set = false;
   bool ic_set = false;
   unsigned current_step = 1;
+  unsigned timeouts_seen = 0;  // device count of ran-out kernel waits at creation
+  // captured block of step-invariant steps (replay_steps) and the buffers
+  // and launch choices it was captured with
+  cudaGraphExec_t graph = nullptr;
+  std::vector<const void *> graph_sig;
   std::string err;
 
   int fail(int code, const std::string &m) {
@@ -407,17 +412,78 @@ int adi_build_lu(pxp_solver_s *h) {
   std::vector<cd> gx, gy;
   thomas_factor(dgx, -0.5 * im / (k * dx * dx), gx);
   thomas_factor(dgy, -0.5 * im / (k * dy * dy), gy);
-  gx.insert(gx.end(), gy.begin(), gy.end());
+  // [gx | hx | gy | hy] in natural order, then the x and y tables staged for
+  // the TMA-staged kernel ([g | h | pf | pb] each, where its size runs it)
+  std::vector<cd> tabs(12 * (size_t)n);
+  std::copy(gx.begin(), gx.end(), tabs.begin());
+  std::copy(gy.begin(), gy.end(), tabs.begin() + 2 * n);
+  const double *t = reinterpret_cast<const double *>(tabs.data());
+  pxp::adi_const_staged_tables((int)n, t, t + 2 * n, reinterpret_cast<double *>(tabs.data() + 4 * n));
+  pxp::adi_const_staged_tables((int)n, t + 4 * n, t + 6 * n,
+                               reinterpret_cast<double *>(tabs.data() + 8 * n));
   free_dev(h->d_lu, h->stream);
   int rc;
-  if ((rc = alloc(h, &h->d_lu, sizeof(cd) * 4 * n, "factor tables"))) return rc;
-  if (int rc_ = h2d(h, h->d_lu, gx.data(), sizeof(cd) * 4 * n)) return rc_;
+  if ((rc = alloc(h, &h->d_lu, sizeof(cd) * tabs.size(), "factor tables"))) return rc;
+  if (int rc_ = h2d(h, h->d_lu, tabs.data(), sizeof(cd) * tabs.size())) return rc_;
   return PXP_OK;
 }
 
 // ---- ADI -------------------------------------------------------------------
 // getZ (src/paraxialSimulation.cpp:250-253)
 double get_z(const pxp_solver_s *h, unsigned iz) { return h->prob.z.min + iz * h->prob.z.step; }
+
+// ---- step graphs -------------------------------------------------------------
+// Steps whose launches do not depend on the step index (vacuum planes, no
+// save) are enqueued in blocks of kGraphSteps from a CUDA graph: the block's
+// launches are captured once per handle and replayed, so the host pays one
+// graph launch per block instead of two kernel launches per step, and the
+// device runs the block's kernels back to back.  The signature lists every
+// buffer and launch choice baked into the block; a change re-captures it.
+// PXP_STEP_GRAPHS=0 turns the graphs off (every step launched directly).
+constexpr int kGraphSteps = 32;
+
+bool step_graphs_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("PXP_STEP_GRAPHS");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename F>
+int replay_steps(pxp_solver_s *h, const std::vector<const void *> &sig, int blocks, F enqueue_block) {
+  if (!h->graph || h->graph_sig != sig) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return h->cuda_fail(e, "step graph capture");
+    const int rc = enqueue_block();
+    e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return h->cuda_fail(e, "step graph capture");
+    e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      h->graph = nullptr;
+      return h->cuda_fail(e, "step graph instantiation");
+    }
+    h->graph_sig = sig;
+  }
+  for (int b = 0; b < blocks; ++b) {
+    const cudaError_t e = cudaGraphLaunch(h->graph, h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "step graph launch");
+  }
+  return PXP_OK;
+}
+
+bool save_at(const pxp_solver_s *h, unsigned step) {
+  return h->save_every > 0 && step % (unsigned)h->save_every == 0 &&
+         (int)(step / (unsigned)h->save_every) - 1 < h->max_slots;
+}
 
 // Spheres that can contain a point of the plane z: the oracle's and the
 // kernel's test is ((dx^2 + dy^2) + dz^2) < R^2 with rounded operations, and
@@ -448,57 +514,93 @@ int adi_fill_spheres(pxp_solver_s *h, pxp::AdiHalf &a, double z) {
   return PXP_OK;
 }
 
-int adi_steps(pxp_solver_s *h, unsigned first, int nsteps) {
+// One ADI step (x half, then y half) launched directly.
+int adi_step(pxp_solver_s *h, unsigned step) {
   const pxp_problem &p = h->prob;
   const double dzh = p.z.step / 2.0;  // ADI::xImplicit (src/alternatingDirectionSolver.cpp:18)
   const double k = p.wavenumber;
   const double kdx2 = k * p.x.step * p.x.step, kdy2 = k * p.y.step * p.y.step;
   const long long n = h->nx;
-  for (int i = 0; i < nsteps; ++i) {
-    const unsigned step = first + (unsigned)i;
-    pxp::AdiHalf a{};
-    a.n = (int)n;
-    a.use_tbc = p.transparent_bc ? 1 : 0;
-    a.inv_dzh = 1.0 / dzh;
-    a.k = k;
-    a.xmin = p.x.min;
-    a.dx = p.x.step;
-    a.ymin = p.y.min;
-    a.dy = p.y.step;
-    // x implicit: systems are rows (y), positions run along x (stride Ny)
-    a.in = h->d_field;
-    a.out = h->d_field2;
-    a.save = nullptr;
-    a.stride_pos = n;
-    a.stride_sys = 1;
-    a.y_implicit = 0;
-    a.kd2_impl = kdx2;
-    a.kd2_expl = kdy2;
-    a.z = get_z(h, step);
-    adi_fill_spheres(h, a, a.z);
-    const cd *lu = (const cd *)h->d_lu;
-    cudaError_t e = (a.nspheres == 0 && !a.use_tbc && lu)
-                        ? pxp::launch_adi_half_const(h->prec, a, lu, lu + n, h->stream)
-                        : pxp::launch_adi_half(h->prec, a, h->stream);
-    if (e != cudaSuccess) return h->cuda_fail(e, "ADI x half step");
-    // y implicit: systems are columns (x), positions run along y (stride 1)
-    a.in = h->d_field2;
-    a.out = h->d_field;
-    const bool save = h->save_every > 0 && step % (unsigned)h->save_every == 0 &&
-                      (int)(step / (unsigned)h->save_every) - 1 < h->max_slots;
-    a.save = save ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
-                  : nullptr;
-    a.stride_pos = 1;
-    a.stride_sys = n;
-    a.y_implicit = 1;
-    a.kd2_impl = kdy2;
-    a.kd2_expl = kdx2;
-    a.z = get_z(h, step) + dzh;
-    adi_fill_spheres(h, a, a.z);
-    e = (a.nspheres == 0 && !a.use_tbc && lu)
-            ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n, h->stream)
-            : pxp::launch_adi_half(h->prec, a, h->stream);
-    if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
+  pxp::AdiHalf a{};
+  a.n = (int)n;
+  a.use_tbc = p.transparent_bc ? 1 : 0;
+  a.inv_dzh = 1.0 / dzh;
+  a.k = k;
+  a.xmin = p.x.min;
+  a.dx = p.x.step;
+  a.ymin = p.y.min;
+  a.dy = p.y.step;
+  // x implicit: systems are rows (y), positions run along x (stride Ny)
+  a.in = h->d_field;
+  a.out = h->d_field2;
+  a.save = nullptr;
+  a.stride_pos = n;
+  a.stride_sys = 1;
+  a.y_implicit = 0;
+  a.kd2_impl = kdx2;
+  a.kd2_expl = kdy2;
+  a.z = get_z(h, step);
+  adi_fill_spheres(h, a, a.z);
+  const cd *lu = (const cd *)h->d_lu;
+  cudaError_t e = (a.nspheres == 0 && !a.use_tbc && lu)
+                      ? pxp::launch_adi_half_const(h->prec, a, lu, lu + n, lu + 4 * n, h->stream)
+                      : pxp::launch_adi_half(h->prec, a, h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "ADI x half step");
+  // y implicit: systems are columns (x), positions run along y (stride 1)
+  a.in = h->d_field2;
+  a.out = h->d_field;
+  a.save = save_at(h, step)
+               ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
+               : nullptr;
+  a.stride_pos = 1;
+  a.stride_sys = n;
+  a.y_implicit = 1;
+  a.kd2_impl = kdy2;
+  a.kd2_expl = kdx2;
+  a.z = get_z(h, step) + dzh;
+  adi_fill_spheres(h, a, a.z);
+  e = (a.nspheres == 0 && !a.use_tbc && lu)
+          ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n, lu + 8 * n, h->stream)
+          : pxp::launch_adi_half(h->prec, a, h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
+  return PXP_OK;
+}
+
+// Both halves of the step on the vacuum kernel and no save: the step's
+// launches are then the same as any other such step's.
+bool adi_plain_step(const pxp_solver_s *h, unsigned step, std::vector<pxp::Sphere> &tmp) {
+  if (h->prob.transparent_bc || !h->d_lu || save_at(h, step)) return false;
+  const double z = get_z(h, step);
+  active_spheres(h, z, tmp);
+  if (!tmp.empty()) return false;
+  active_spheres(h, z + h->prob.z.step / 2.0, tmp);
+  return tmp.empty();
+}
+
+int adi_steps(pxp_solver_s *h, unsigned first, int nsteps) {
+  std::vector<pxp::Sphere> tmp;
+  const std::vector<const void *> sig = {h->d_field, h->d_field2, h->d_lu, (const void *)(size_t)1};
+  for (int i = 0; i < nsteps;) {
+    // a block is replayed only after a direct step of this call has set up
+    // every launch's one-time state
+    if (i > 0 && step_graphs_enabled() && nsteps - i >= kGraphSteps) {
+      int run = 0;
+      while (i + run < nsteps && adi_plain_step(h, first + (unsigned)(i + run), tmp)) ++run;
+      const int blocks = run / kGraphSteps;
+      if (blocks > 0) {
+        const unsigned s0 = first + (unsigned)i;
+        const int rc = replay_steps(h, sig, blocks, [&] {
+          for (int j = 0; j < kGraphSteps; ++j)
+            if (int r = adi_step(h, s0 + (unsigned)j)) return r;
+          return (int)PXP_OK;
+        });
+        if (rc) return rc;
+        i += blocks * kGraphSteps;
+        continue;
+      }
+    }
+    if (int rc = adi_step(h, first + (unsigned)i)) return rc;
+    ++i;
   }
   return PXP_OK;
 }
@@ -621,12 +723,14 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, h->stream)) != cudaSuccess)
     return h->cuda_fail(e, "FFT3D forward y pass");
   std::vector<pxp::Sphere> act;
-  for (int i = 0; i < nsteps; ++i) {
+  // step i of this call: x pass, then the y pass (mode 3 on the last step
+  // leaves the field in real space)
+  auto one_step = [&](int i) -> int {
     const unsigned step = first + (unsigned)i;
-    const int v = variant;
     q.mode = 1;
     q.save = nullptr;
-    if ((e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, h->stream)) != cudaSuccess)
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, h->stream)) !=
+        cudaSuccess)
       return h->cuda_fail(e, "FFT3D x pass");
     q.mode = (i == nsteps - 1) ? 3 : 2;
     q.z1 = get_z(h, step);
@@ -640,12 +744,44 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
       q.nspheres = (int)h->spheres.size();
       q.spheres_all = h->d_spheres;
     }
-    const bool save = h->save_every > 0 && step % (unsigned)h->save_every == 0 &&
-                      (int)(step / (unsigned)h->save_every) - 1 < h->max_slots;
-    q.save = save ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
-                  : nullptr;
-    if ((e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, h->stream)) != cudaSuccess)
+    q.save = save_at(h, step)
+                 ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
+                 : nullptr;
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, h->stream)) !=
+        cudaSuccess)
       return h->cuda_fail(e, "FFT3D y pass");
+    return PXP_OK;
+  };
+  // no sphere in the step's slab, no save, not the last step of the call:
+  // the step's launches are the same as any other such step's (the slab's z
+  // planes are read only for spheres)
+  auto plain = [&](int i) {
+    const unsigned step = first + (unsigned)i;
+    if (i == nsteps - 1 || save_at(h, step)) return false;
+    slab_spheres(h, get_z(h, step - 1), get_z(h, step), act);
+    return act.empty();
+  };
+  const std::vector<const void *> sig = {h->d_field, h->d_tw, kx2, tw16,
+                                         (const void *)(size_t)(16 + variant)};
+  for (int i = 0; i < nsteps;) {
+    if (i > 0 && step_graphs_enabled() && nsteps - i > kGraphSteps) {
+      int run = 0;
+      while (i + run < nsteps && plain(i + run)) ++run;
+      const int blocks = run / kGraphSteps;
+      if (blocks > 0) {
+        const int i0 = i;
+        const int rc = replay_steps(h, sig, blocks, [&] {
+          for (int j = 0; j < kGraphSteps; ++j)
+            if (int r = one_step(i0 + j)) return r;
+          return (int)PXP_OK;
+        });
+        if (rc) return rc;
+        i += blocks * kGraphSteps;
+        continue;
+      }
+    }
+    if (int rc = one_step(i)) return rc;
+    ++i;
   }
   return PXP_OK;
 }
@@ -762,6 +898,7 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
     delete h;
     return PXP_ERR_CUDA;
   }
+  h->timeouts_seen = pxp::wait_timeouts(h->stream);
   int rc = PXP_OK;
   auto cleanup_fail = [&](int code) {
     std::string m = h->err;
@@ -806,6 +943,8 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
 int pxp_solver_destroy(pxp_solver h) {
   if (h == nullptr) return PXP_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
   free_dev(h->d_field, h->stream);
   free_dev(h->d_saves, h->stream);
   h->d_kern = nullptr;  // shared table, not owned
@@ -906,7 +1045,16 @@ static int upload_field(pxp_solver_s *h, void *dst, const double *src) {
   return PXP_OK;
 }
 
+// A kernel of this device gave up a bounded wait since the handle was made:
+// its results are not to be trusted.
+static int check_waits(pxp_solver_s *h) {
+  if (pxp::wait_timeouts(h->stream) != h->timeouts_seen)
+    return h->fail(PXP_ERR_CUDA, "a kernel's bounded wait for its copies ran out on this device");
+  return PXP_OK;
+}
+
 static int download_field(pxp_solver_s *h, double *dst, const void *src) {
+  if (int rc = check_waits(h)) return rc;
   if (h->prec == pxp::kFP64) {
     PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, 16 * h->npts, cudaMemcpyDeviceToHost, h->stream));
     PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -990,7 +1138,7 @@ int pxp_solve(pxp_solver h) {
 int pxp_synchronize(pxp_solver h) {
   if (h == nullptr) return PXP_ERR_INVALID;
   PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
-  return PXP_OK;
+  return check_waits(h);
 }
 
 int pxp_get_last_solution(pxp_solver h, double *field) {
