@@ -315,24 +315,35 @@ static cudaError_t adi_const_launch(const AdiHalf &h, const void *g, const void 
 
 // Vacuum half step, FP64, n <= 1024, one wave: G systems per CTA so that
 // ceil(n / G) CTAs cover the 148 SMs once (G = 7 at n = 1024: 147 CTAs).
-// The G + 2 staged rows (G systems and their two stencil halos) and the
-// factor tables are brought into shared memory by TMA bulk copies counted on
-// an mbarrier, and the results leave as bulk stores, so that the copy
-// engine, not per-thread requests, carries the tile in both directions.
-// Shared-memory layouts keep every copied run contiguous and the per-chunk
-// reads of the solve free of bank conflicts:
+// The G + 2 staged rows (G systems and their two stencil halos) arrive by
+// coalesced 16-byte cp.async copies, the factor tables (one 64 KB block at
+// n = 1024) by one TMA bulk copy counted on an mbarrier; results leave by
+// coalesced stores.  (Bulk copies per position run or per chunk -- 32 to 256
+// bytes each -- measured slower than per-thread copies: the copy engine's
+// per-request cost dominates at these sizes.)
+//
+// Compute: the CTA's systems form two groups (GS0 = ceil(G/2) and G - GS0
+// systems); a thread owns one chunk of M rows of every system of its group.
+// Each staged value is read from shared memory once and serves the three
+// stencils it enters, each factor-table entry serves all systems of the
+// group, and the sweeps run the group's independent recurrences side by
+// side.  The chunk-carry scans handle the group's systems together: the
+// multiplier product is the same for all of them (one matrix), the carry
+// differs per system (multi_exclusive_scan).
+//
+// Shared-memory layouts keep the per-chunk reads of the solve and the
+// copies in memory order free of bank conflicts:
 //   XH (x half step, the G + 2 systems of a position adjacent in memory):
 //      entry (c, m, g) at c*(M*(G+2) + 1) + m*(G+2) + g, one spare entry after
-//      each chunk; one copy per position;
+//      each chunk;
 //   YH (y half step, a system is a row): entry (c, m, g) at
-//      g*P*(M+1) + c*(M+1) + m, one spare entry after each chunk; one copy per
-//      chunk of a row.
+//      g*P*(M+1) + c*(M+1) + m, one spare entry after each chunk.
 // The tables [g | h | pf | pb] (Thomas factors and the in-chunk products of
-// the multipliers, const_solve_tab) are host-built in chunk-transposed slots
+// the multipliers) are host-built in chunk-transposed slots
 // (adi_const_staged_tables) and copied in as one block.  The same tile holds
 // the results (row g + 1 of system g) for the stores.
 template <int N, int M, int G, bool XH>
-struct AdiTmaTile {
+struct AdiWaveTile {
   static constexpr int P = N / M, RW = G + 2;
   static constexpr int SIZE = XH ? N * RW + P : RW * P * (M + 1);
   __device__ static __forceinline__ int at(int c, int m, int g) {
@@ -340,21 +351,172 @@ struct AdiTmaTile {
   }
 };
 
-template <int N, int M, int G, bool XH>
-__global__ void __launch_bounds__(G *(N / M))
-    adi_const_tma_kernel(const AdiHalf h, const double2 *__restrict__ tabs) {
-  using L = AdiTmaTile<N, M, G, XH>;
+__device__ __forceinline__ void adi_cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void group_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+
+template <bool DOWN>
+__device__ __forceinline__ double2 shfl2(double2 v, int d) {
+  if (DOWN) return mk(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
+  return mk(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+
+// Exclusive scan of chunk transfers y_out = a*y_in + b[j] over the P threads
+// of a group (P a multiple of 32, the group starting at a warp boundary),
+// S systems at once with a common multiplier a.  REV scans in decreasing
+// chunk order.  On return (a, b) hold the composition of the transfers of
+// the chunks before this one in scan order (identity for the first).
+// scratch: (S + 1) * P / 32 entries for this group; bar: its named barrier.
+template <int P, int S, bool REV>
+__device__ __forceinline__ void multi_exclusive_scan(double2 &a, double2 (&b)[S], double2 *scratch,
+                                                     int gtid, int bar) {
+  const int lane = threadIdx.x & 31;
+  double2 ia = a, ib[S];
+#pragma unroll
+  for (int j = 0; j < S; ++j) ib[j] = b[j];
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const double2 oa = shfl2<REV>(ia, d);
+    double2 ob[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) ob[j] = shfl2<REV>(ib[j], d);
+    if (REV ? lane + d < 32 : lane >= d) {
+#pragma unroll
+      for (int j = 0; j < S; ++j) ib[j] = cfma(ia, ob[j], ib[j]);
+      ia = cmul(ia, oa);
+    }
+  }
+  double2 ea = shfl2<REV>(ia, 1), eb[S];
+#pragma unroll
+  for (int j = 0; j < S; ++j) eb[j] = shfl2<REV>(ib[j], 1);
+  if (REV ? lane == 31 : lane == 0) {
+    ea = mk(1.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < S; ++j) eb[j] = mk(0.0, 0.0);
+  }
+  if constexpr (P > 32) {
+    constexpr int W = P / 32;
+    const int w = gtid >> 5;
+    group_sync(bar, P);  // the previous scan's readers are done with scratch
+    if (lane == (REV ? 0 : 31)) {
+      scratch[w * (S + 1)] = ia;
+#pragma unroll
+      for (int j = 0; j < S; ++j) scratch[w * (S + 1) + 1 + j] = ib[j];
+    }
+    group_sync(bar, P);
+    double2 pa = mk(1.0, 0.0), pb[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) pb[j] = mk(0.0, 0.0);
+#pragma unroll
+    for (int k = 1; k < W; ++k) {
+      const int v = REV ? W - k : k - 1;  // warps before this one in scan order
+      if (REV ? v > w : v < w) {
+        const double2 ta = scratch[v * (S + 1)];
+#pragma unroll
+        for (int j = 0; j < S; ++j) pb[j] = cfma(ta, pb[j], scratch[v * (S + 1) + 1 + j]);
+        pa = cmul(ta, pa);
+      }
+    }
+    // compose(pre, ex): apply the preceding warps, then this warp's lanes
+#pragma unroll
+    for (int j = 0; j < S; ++j) eb[j] = cfma(ea, pb[j], eb[j]);
+    ea = cmul(ea, pa);
+  }
+  a = ea;
+#pragma unroll
+  for (int j = 0; j < S; ++j) b[j] = eb[j];
+}
+
+// Right-hand sides and solve of the S systems sys0 .. sys0+S-1 of this CTA
+// for chunk c: r[j][m] holds the solution of row c*M + m of system sys0 + j.
+template <int N, int M, int G, bool XH, int S>
+__device__ __forceinline__ void adi_group_solve(double2 (&r)[4][M], const AdiHalf &h,
+                                                const double2 *tile, const double2 *gs,
+                                                const double2 *hs, const double2 *pf,
+                                                const double2 *pb, double2 *scratch, int sys0,
+                                                int s_base, int c, int gtid, int bar) {
+  using L = AdiWaveTile<N, M, G, XH>;
   constexpr int P = N / M;
-  constexpr int T = G * P;
+  const double inv_kd2_expl = __ddiv_rn(1.0, h.kd2_expl);
+  const double hk = 0.5 * inv_kd2_expl;
+  const double2 coef = mk(h.inv_dzh, -inv_kd2_expl);
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double2 v[S + 2];
+#pragma unroll
+    for (int k = 0; k < S + 2; ++k) v[k] = tile[L::at(c, m, sys0 + k)];
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+      const int s = s_base + sys0 + j;  // s >= N: padding system, all zero
+      const double2 rr = cmul(coef, v[j + 1]);
+      double2 nb = mk(0.0, 0.0);
+      if (s > 0) nb = v[j];
+      if (s < N - 1) nb = cadd(nb, v[j + 2]);
+      r[j][m] = mk(fma(-hk, nb.y, rr.x), fma(hk, nb.x, rr.y));
+    }
+  }
+  // forward, zero carry-in: y_i = g_i r_i + h_i y_{i-1}
+  double2 y[S];
+  {
+    const double2 g0 = gs[cslot<M, P>(c, 0)];
+#pragma unroll
+    for (int j = 0; j < S; ++j) r[j][0] = y[j] = cmul(g0, r[j][0]);
+  }
+#pragma unroll
+  for (int m = 1; m < M; ++m) {
+    const int k = cslot<M, P>(c, m);
+    const double2 gm = gs[k], hm = hs[k];
+#pragma unroll
+    for (int j = 0; j < S; ++j) r[j][m] = y[j] = cfma(hm, y[j], cmul(gm, r[j][m]));
+  }
+  double2 a = pf[cslot<M, P>(c, M - 1)];
+  multi_exclusive_scan<P, S, false>(a, y, scratch, gtid, bar);
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const double2 f = pf[cslot<M, P>(c, m)];
+#pragma unroll
+    for (int j = 0; j < S; ++j) r[j][m] = cfma(f, y[j], r[j][m]);
+  }
+  // backward, zero carry-in: x_i = y_i + h_i x_{i+1}
+  double2 x[S];
+#pragma unroll
+  for (int j = 0; j < S; ++j) x[j] = r[j][M - 1];
+#pragma unroll
+  for (int m = M - 2; m >= 0; --m) {
+    const double2 hm = hs[cslot<M, P>(c, m)];
+#pragma unroll
+    for (int j = 0; j < S; ++j) r[j][m] = x[j] = cfma(hm, x[j], r[j][m]);
+  }
+  a = pb[cslot<M, P>(c, 0)];
+  multi_exclusive_scan<P, S, true>(a, x, scratch, gtid, bar);
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const double2 f = pb[cslot<M, P>(c, m)];
+#pragma unroll
+    for (int j = 0; j < S; ++j) r[j][m] = cfma(f, x[j], r[j][m]);
+  }
+}
+
+template <int N, int M, int G, bool XH>
+__global__ void __launch_bounds__(2 * (N / M), 1)
+    adi_const_wave_kernel(const AdiHalf h, const double2 *__restrict__ tabs) {
+  using L = AdiWaveTile<N, M, G, XH>;
+  constexpr int P = N / M;
+  constexpr int T = 2 * P;
   constexpr int RW = G + 2;
+  constexpr int GS0 = (G + 1) / 2, GS1 = G - GS0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
   double2 *gs = reinterpret_cast<double2 *>(smem_raw + 16);
   double2 *hs = gs + N;
   double2 *pf = hs + N;
   double2 *pb = pf + N;
-  Affine *scratch = reinterpret_cast<Affine *>(pb + N);
-  double2 *tile = reinterpret_cast<double2 *>(scratch + (T / 32 + 1));
+  double2 *scratch = pb + N;  // (GS0 + 1) * P / 32 per group
+  double2 *tile = scratch + 2 * (GS0 + 1) * (P / 32);
   __shared__ int staged_ok;
   const int tid = threadIdx.x;
   const int s_base = blockIdx.x * G;
@@ -365,31 +527,40 @@ __global__ void __launch_bounds__(G *(N / M))
   const int g_hi = N - s_base + 1 < RW ? N - s_base + 1 : RW;
   if (tid == 0) {
     mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, (unsigned)(sizeof(double2) * (4 * N + (g_hi - g_lo) * N)));
+    mbar_arrive_expect_tx(bar, (unsigned)(sizeof(double2) * 4 * N));
   }
   __syncthreads();
   if (tid == 0) bulk_load(gs, tabs, (unsigned)(sizeof(double2) * 4 * N), bar);
   if constexpr (XH) {
-    for (int p = tid; p < N; p += T) {
-      const int c = p / M, m = p % M;
-      bulk_load(tile + L::at(c, m, g_lo), in + (long long)p * h.stride_pos + (s_base - 1 + g_lo),
-                (unsigned)(sizeof(double2) * (g_hi - g_lo)), bar);
-      for (int g = 0; g < g_lo; ++g) tile[L::at(c, m, g)] = mk(0.0, 0.0);
-      for (int g = g_hi; g < RW; ++g) tile[L::at(c, m, g)] = mk(0.0, 0.0);
+    // the RW staged systems of a position are adjacent in memory:
+    // consecutive threads take consecutive systems
+    constexpr int PPI = T / RW;  // positions per pass
+    const int g = tid % RW;
+    const int sg = s_base - 1 + g;
+    if (tid < PPI * RW) {
+      for (int p = tid / RW; p < N; p += PPI) {
+        double2 *dst = tile + L::at(p / M, p % M, g);
+        if (g >= g_lo && g < g_hi)
+          adi_cp_async16(dst, in + (long long)p * h.stride_pos + sg);
+        else
+          *dst = mk(0.0, 0.0);
+      }
     }
   } else {
-    for (int idx = tid; idx < RW * P; idx += T) {
-      const int g = idx / P, c = idx % P;
-      double2 *dst = tile + L::at(c, 0, g);
-      if (g >= g_lo && g < g_hi) {
-        bulk_load(dst, in + (long long)(s_base - 1 + g) * h.stride_sys + c * M,
-                  (unsigned)(sizeof(double2) * M), bar);
-      } else {
-#pragma unroll
-        for (int m = 0; m < M; ++m) dst[m] = mk(0.0, 0.0);
+#pragma unroll 1
+    for (int g = 0; g < RW; ++g) {
+      const bool live = g >= g_lo && g < g_hi;
+      const double2 *src = in + (long long)(s_base - 1 + g) * h.stride_sys;
+      for (int p = tid; p < N; p += T) {
+        double2 *dst = tile + L::at(p / M, p % M, g);
+        if (live)
+          adi_cp_async16(dst, src + p);
+        else
+          *dst = mk(0.0, 0.0);
       }
     }
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
   if (tid == 0) {
     const bool ok = mbar_wait_bounded(bar, 0, 2000000000ull);
     if (!ok) {
@@ -398,58 +569,62 @@ __global__ void __launch_bounds__(G *(N / M))
     }
     staged_ok = ok;
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   if (!staged_ok) return;
-  (void)mbar_try_wait(bar, 0);  // phase complete: orders the copied data for this thread
-  const int g = tid / P, c = tid % P;
-  const int s = s_base + g;  // s >= N: padding system of the last CTA, all zero
-  const double inv_kd2_expl = __ddiv_rn(1.0, h.kd2_expl);
-  const double hk = 0.5 * inv_kd2_expl;
-  double2 r[M];
-#pragma unroll
-  for (int m = 0; m < M; ++m) {
-    const double2 rr = cmul(mk(h.inv_dzh, -inv_kd2_expl), tile[L::at(c, m, g + 1)]);
-    double2 nb = mk(0.0, 0.0);
-    if (s > 0) nb = tile[L::at(c, m, g)];
-    if (s < N - 1) nb = cadd(nb, tile[L::at(c, m, g + 2)]);
-    r[m] = mk(fma(-hk, nb.y, rr.x), fma(hk, nb.x, rr.y));
-  }
-  const_solve_tab<M, P>(r, gs, hs, pf, pb, c, scratch);
+  (void)mbar_try_wait(bar, 0);  // phase complete: orders the copied tables for this thread
+  const int group = tid / P, c = tid % P;
+  double2 r[4][M];
+  if (group == 0)
+    adi_group_solve<N, M, G, XH, GS0>(r, h, tile, gs, hs, pf, pb, scratch, 0, s_base, c, tid, 1);
+  else
+    adi_group_solve<N, M, G, XH, GS1>(r, h, tile, gs, hs, pf, pb, scratch + (GS0 + 1) * (P / 32),
+                                      GS0, s_base, c, tid - P, 2);
   __syncthreads();  // every read of the staged tile is done
+  const int sys0 = group == 0 ? 0 : GS0, ns = group == 0 ? GS0 : GS1;
 #pragma unroll
-  for (int m = 0; m < M; ++m) tile[L::at(c, m, g + 1)] = r[m];
-  fence_async_smem();
+  for (int j = 0; j < 4; ++j)
+    if (j < ns) {
+#pragma unroll
+      for (int m = 0; m < M; ++m) tile[L::at(c, m, sys0 + j + 1)] = r[j][m];
+    }
   __syncthreads();
   double2 *save = reinterpret_cast<double2 *>(h.save);
   const int nsys = N - s_base < G ? N - s_base : G;  // the last CTA may hold fewer
   if constexpr (XH) {
-    for (int p = tid; p < N; p += T) {
-      const double2 *src = tile + L::at(p / M, p % M, 1);
-      const long long off = (long long)p * h.stride_pos + s_base;
-      bulk_store(out + off, src, (unsigned)(sizeof(double2) * nsys));
-      if (save) bulk_store(save + off, src, (unsigned)(sizeof(double2) * nsys));
+    // consecutive threads write consecutive systems of a position
+    constexpr int PPI = T / G;
+    const int gg = tid % G;
+    if (tid < PPI * G && gg < nsys) {
+      for (int p = tid / G; p < N; p += PPI) {
+        const double2 v = tile[L::at(p / M, p % M, gg + 1)];
+        const long long off = (long long)p * h.stride_pos + s_base + gg;
+        out[off] = v;
+        if (save) save[off] = v;
+      }
     }
   } else {
-    for (int idx = tid; idx < nsys * P; idx += T) {
-      const int gg = idx / P, cc = idx % P;
-      const double2 *src = tile + L::at(cc, 0, gg + 1);
-      const long long off = (long long)(s_base + gg) * h.stride_sys + cc * M;
-      bulk_store(out + off, src, (unsigned)(sizeof(double2) * M));
-      if (save) bulk_store(save + off, src, (unsigned)(sizeof(double2) * M));
+#pragma unroll 1
+    for (int gg = 0; gg < nsys; ++gg) {
+      const long long base = (long long)(s_base + gg) * h.stride_sys;
+      for (int p = tid; p < N; p += T) {
+        const double2 v = tile[L::at(p / M, p % M, gg + 1)];
+        out[base + p] = v;
+        if (save) save[base + p] = v;
+      }
     }
   }
-  bulk_commit();
-  bulk_wait_read();
 }
 
 template <int N, int M, int G, bool XH>
-static cudaError_t adi_const_tma_launch_x(const AdiHalf &h, const void *tabs, cudaStream_t s) {
-  constexpr int P = N / M, T = G * P;
-  constexpr size_t smem = 16 + sizeof(double2) * 4 * N + sizeof(Affine) * (T / 32 + 1) +
-                          sizeof(double2) * AdiTmaTile<N, M, G, XH>::SIZE;
-  static_assert(smem <= 227 * 1024, "staged ADI tile exceeds shared memory");
-  static_assert(T % 32 == 0, "whole warps per CTA");
-  auto k = adi_const_tma_kernel<N, M, G, XH>;
+static cudaError_t adi_const_wave_launch_x(const AdiHalf &h, const void *tabs, cudaStream_t s) {
+  constexpr int P = N / M, T = 2 * P;
+  constexpr size_t smem = 16 + sizeof(double2) * (4 * N + 2 * ((G + 1) / 2 + 1) * (P / 32)) +
+                          sizeof(double2) * AdiWaveTile<N, M, G, XH>::SIZE;
+  static_assert(smem + 16 <= 227 * 1024, "staged ADI tile exceeds shared memory");
+  static_assert(P % 32 == 0, "whole warps per group");
+  static_assert((G + 1) / 2 <= 4, "at most four systems per group");
+  auto k = adi_const_wave_kernel<N, M, G, XH>;
   if (smem > 48 * 1024) {
     static const cudaError_t attr =
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -460,28 +635,28 @@ static cudaError_t adi_const_tma_launch_x(const AdiHalf &h, const void *tabs, cu
 }
 
 template <int N, int M, int G>
-static cudaError_t adi_const_tma_launch(const AdiHalf &h, const void *tabs, cudaStream_t s) {
+static cudaError_t adi_const_wave_launch(const AdiHalf &h, const void *tabs, cudaStream_t s) {
   if (tabs == nullptr) return cudaErrorInvalidValue;
-  return h.stride_sys == 1 ? adi_const_tma_launch_x<N, M, G, true>(h, tabs, s)
-                           : adi_const_tma_launch_x<N, M, G, false>(h, tabs, s);
+  return h.stride_sys == 1 ? adi_const_wave_launch_x<N, M, G, true>(h, tabs, s)
+                           : adi_const_wave_launch_x<N, M, G, false>(h, tabs, s);
 }
 
-// (M, G) of the TMA-staged kernel per size: every CTA holds whole warps
-// (G*n/M a multiple of 32) and ceil(n / G) CTAs fill the SMs about once.
-static bool adi_tma_config(int n, int *m, int *g) {
+// (M, G) of the one-wave kernel per size: each system group holds whole
+// warps (n/M a multiple of 32) and ceil(n / G) CTAs fill the SMs about once.
+static bool adi_wave_config(int n, int *m, int *g) {
   switch (n) {
-    case 64: *m = 8; *g = 4; return true;
-    case 128: *m = 8; *g = 2; return true;
+    case 64: *m = 2; *g = 4; return true;
+    case 128: *m = 4; *g = 2; return true;
     case 256: *m = 8; *g = 2; return true;
     case 512: *m = 8; *g = 4; return true;
-    case 1024: *m = 16; *g = 7; return true;
+    case 1024: *m = 8; *g = 7; return true;
     default: return false;
   }
 }
 
 bool adi_const_staged_tables(int n, const double *g, const double *h, double *out) {
   int M = 0, G = 0;
-  if (!adi_tma_config(n, &M, &G)) return false;
+  if (!adi_wave_config(n, &M, &G)) return false;
   const int P = n / M;
   auto slot = [&](int c, int m) { return m * P + (c ^ (m & 7)); };
   // the device's cmul: (fma(ax, bx, -ay*by), fma(ax, by, ay*bx))
@@ -533,11 +708,11 @@ cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, 
                       : adi_const_launch<float, NN, GG>(h, g, hh, s);
   if (p == kFP64) {
     switch (h.n) {
-      case 64: return adi_const_tma_launch<64, 8, 4>(h, staged, s);
-      case 128: return adi_const_tma_launch<128, 8, 2>(h, staged, s);
-      case 256: return adi_const_tma_launch<256, 8, 2>(h, staged, s);
-      case 512: return adi_const_tma_launch<512, 8, 4>(h, staged, s);
-      case 1024: return adi_const_tma_launch<1024, 16, 7>(h, staged, s);
+      case 64: return adi_const_wave_launch<64, 2, 4>(h, staged, s);
+      case 128: return adi_const_wave_launch<128, 4, 2>(h, staged, s);
+      case 256: return adi_const_wave_launch<256, 8, 2>(h, staged, s);
+      case 512: return adi_const_wave_launch<512, 8, 4>(h, staged, s);
+      case 1024: return adi_const_wave_launch<1024, 8, 7>(h, staged, s);
       default: break;
     }
   }

@@ -413,7 +413,7 @@ int adi_build_lu(pxp_solver_s *h) {
   thomas_factor(dgx, -0.5 * im / (k * dx * dx), gx);
   thomas_factor(dgy, -0.5 * im / (k * dy * dy), gy);
   // [gx | hx | gy | hy] in natural order, then the x and y tables staged for
-  // the TMA-staged kernel ([g | h | pf | pb] each, where its size runs it)
+  // the one-wave kernel ([g | h | pf | pb] each, where its size runs it)
   std::vector<cd> tabs(12 * (size_t)n);
   std::copy(gx.begin(), gx.end(), tabs.begin());
   std::copy(gy.begin(), gy.end(), tabs.begin() + 2 * n);

@@ -98,12 +98,12 @@ bool adi_supported(Precision p, int n);
 // matrix is the same for every system and every step; g/h are its Thomas
 // factor tables (n complex128 each, see scan_solve.cuh).
 // `staged`: the same tables with their in-chunk products in the layout the
-// FP64 TMA-staged kernel copies into shared memory (adi_const_staged_tables;
+// FP64 one-wave kernel copies into shared memory (adi_const_staged_tables;
 // not read where that returns false for n).
 cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, const void *hh,
                                   const void *staged, cudaStream_t s);
 // Host: fills out[0 .. 4n) complex128 with [g | h | pf | pb] in the
-// chunk-transposed slots of the TMA-staged vacuum kernel for size n (pf, pb:
+// chunk-transposed slots of the one-wave vacuum kernel for size n (pf, pb:
 // products of h over each chunk's rows up to / from a row) and returns true;
 // false when size n runs the other kernel (out untouched).  g, h, out:
 // interleaved (re, im).
