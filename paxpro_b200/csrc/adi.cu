@@ -355,6 +355,7 @@ __device__ __forceinline__ void adi_cp_async16(void *smem, const void *gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
 }
 
+
 __device__ __forceinline__ void group_sync(int id, int count) {
   asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
 }
@@ -433,8 +434,10 @@ __device__ __forceinline__ void multi_exclusive_scan(double2 &a, double2 (&b)[S]
 
 // Right-hand sides and solve of the S systems sys0 .. sys0+S-1 of this CTA
 // for chunk c: r[j][m] holds the solution of row c*M + m of system sys0 + j.
-template <int N, int M, int G, bool XH, int S>
-__device__ __forceinline__ void adi_group_solve(double2 (&r)[4][M], const AdiHalf &h,
+// Right-hand sides and solve of systems sys0 .. sys0+SC-1 of this CTA for
+// chunk c: r[j][m] holds the solution of row c*M + m of system sys0 + j.
+template <int N, int M, int G, bool XH, int SCAP, int S>
+__device__ __forceinline__ void adi_group_solve(double2 (&r)[SCAP][M], const AdiHalf &h,
                                                 const double2 *tile, const double2 *gs,
                                                 const double2 *hs, const double2 *pf,
                                                 const double2 *pb, double2 *scratch, int sys0,
@@ -501,24 +504,29 @@ __device__ __forceinline__ void adi_group_solve(double2 (&r)[4][M], const AdiHal
   }
 }
 
-template <int N, int M, int G, bool XH>
-__global__ void __launch_bounds__(2 * (N / M), 1)
+// Systems per group S: a thread owns one chunk of M rows of the S systems of
+// its group; NG = ceil(G / S) groups of P = n/M threads each (the last group
+// may hold fewer systems).
+template <int N, int M, int G, int S, bool XH>
+__global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
     adi_const_wave_kernel(const AdiHalf h, const double2 *__restrict__ tabs) {
   using L = AdiWaveTile<N, M, G, XH>;
   constexpr int P = N / M;
-  constexpr int T = 2 * P;
+  constexpr int NG = (G + S - 1) / S;
+  constexpr int T = NG * P;
   constexpr int RW = G + 2;
-  constexpr int GS0 = (G + 1) / 2, GS1 = G - GS0;
+  constexpr int SL = G - (NG - 1) * S;  // systems of the last group
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
   double2 *gs = reinterpret_cast<double2 *>(smem_raw + 16);
   double2 *hs = gs + N;
   double2 *pf = hs + N;
   double2 *pb = pf + N;
-  double2 *scratch = pb + N;  // (GS0 + 1) * P / 32 per group
-  double2 *tile = scratch + 2 * (GS0 + 1) * (P / 32);
+  double2 *scratch = pb + N;  // (S + 1) * P / 32 per group
+  double2 *tile = scratch + NG * (S + 1) * (P / 32);
   __shared__ int staged_ok;
   const int tid = threadIdx.x;
+  const int group = tid / P, gtid = tid % P;
   const int s_base = blockIdx.x * G;
   const double2 *in = reinterpret_cast<const double2 *>(h.in);
   double2 *out = reinterpret_cast<double2 *>(h.out);
@@ -529,6 +537,10 @@ __global__ void __launch_bounds__(2 * (N / M), 1)
     mbar_init(bar, 1);
     mbar_arrive_expect_tx(bar, (unsigned)(sizeof(double2) * 4 * N));
   }
+  // staged rows outside the grid (first and last CTA) are zero
+  for (int g = 0; g < RW; ++g)
+    if (g < g_lo || g >= g_hi)
+      for (int p = tid; p < N; p += T) tile[L::at(p / M, p % M, g)] = mk(0.0, 0.0);
   __syncthreads();
   if (tid == 0) bulk_load(gs, tabs, (unsigned)(sizeof(double2) * 4 * N), bar);
   if constexpr (XH) {
@@ -536,28 +548,16 @@ __global__ void __launch_bounds__(2 * (N / M), 1)
     // consecutive threads take consecutive systems
     constexpr int PPI = T / RW;  // positions per pass
     const int g = tid % RW;
-    const int sg = s_base - 1 + g;
-    if (tid < PPI * RW) {
-      for (int p = tid / RW; p < N; p += PPI) {
-        double2 *dst = tile + L::at(p / M, p % M, g);
-        if (g >= g_lo && g < g_hi)
-          adi_cp_async16(dst, in + (long long)p * h.stride_pos + sg);
-        else
-          *dst = mk(0.0, 0.0);
-      }
+    if (tid < PPI * RW && g >= g_lo && g < g_hi) {
+      const double2 *src = in + (s_base - 1 + g);
+      for (int p = tid / RW; p < N; p += PPI)
+        adi_cp_async16(tile + L::at(p / M, p % M, g), src + (long long)p * h.stride_pos);
     }
   } else {
 #pragma unroll 1
-    for (int g = 0; g < RW; ++g) {
-      const bool live = g >= g_lo && g < g_hi;
+    for (int g = g_lo; g < g_hi; ++g) {
       const double2 *src = in + (long long)(s_base - 1 + g) * h.stride_sys;
-      for (int p = tid; p < N; p += T) {
-        double2 *dst = tile + L::at(p / M, p % M, g);
-        if (live)
-          adi_cp_async16(dst, src + p);
-        else
-          *dst = mk(0.0, 0.0);
-      }
+      for (int p = tid; p < N; p += T) adi_cp_async16(tile + L::at(p / M, p % M, g), src + p);
     }
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -565,28 +565,29 @@ __global__ void __launch_bounds__(2 * (N / M), 1)
     const bool ok = mbar_wait_bounded(bar, 0, 2000000000ull);
     if (!ok) {
       atomicAdd(&g_wait_timeouts, 1u);
-      mbar_wait_bounded(bar, 0, 2000000000ull);  // copies still in flight
+      mbar_wait_bounded(bar, 0, 2000000000ull);  // the table copy may still be in flight
     }
     staged_ok = ok;
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   if (!staged_ok) return;
-  (void)mbar_try_wait(bar, 0);  // phase complete: orders the copied tables for this thread
-  const int group = tid / P, c = tid % P;
-  double2 r[4][M];
-  if (group == 0)
-    adi_group_solve<N, M, G, XH, GS0>(r, h, tile, gs, hs, pf, pb, scratch, 0, s_base, c, tid, 1);
+  (void)mbar_try_wait(bar, 0);  // completed phase: orders the copied tables for this thread
+  double2 r[S][M];
+  double2 *gscr = scratch + group * (S + 1) * (P / 32);
+  if (SL == S || group < NG - 1)
+    adi_group_solve<N, M, G, XH, S, S>(r, h, tile, gs, hs, pf, pb, gscr, group * S, s_base, gtid,
+                                       gtid, 1 + group);
   else
-    adi_group_solve<N, M, G, XH, GS1>(r, h, tile, gs, hs, pf, pb, scratch + (GS0 + 1) * (P / 32),
-                                      GS0, s_base, c, tid - P, 2);
+    adi_group_solve<N, M, G, XH, S, SL>(r, h, tile, gs, hs, pf, pb, gscr, group * S, s_base, gtid,
+                                        gtid, 1 + group);
   __syncthreads();  // every read of the staged tile is done
-  const int sys0 = group == 0 ? 0 : GS0, ns = group == 0 ? GS0 : GS1;
+  const int ns = group < NG - 1 ? S : SL;
 #pragma unroll
-  for (int j = 0; j < 4; ++j)
+  for (int j = 0; j < S; ++j)
     if (j < ns) {
 #pragma unroll
-      for (int m = 0; m < M; ++m) tile[L::at(c, m, sys0 + j + 1)] = r[j][m];
+      for (int m = 0; m < M; ++m) tile[L::at(gtid, m, group * S + j + 1)] = r[j][m];
     }
   __syncthreads();
   double2 *save = reinterpret_cast<double2 *>(h.save);
@@ -616,15 +617,15 @@ __global__ void __launch_bounds__(2 * (N / M), 1)
   }
 }
 
-template <int N, int M, int G, bool XH>
+template <int N, int M, int G, int S, bool XH>
 static cudaError_t adi_const_wave_launch_x(const AdiHalf &h, const void *tabs, cudaStream_t s) {
-  constexpr int P = N / M, T = 2 * P;
-  constexpr size_t smem = 16 + sizeof(double2) * (4 * N + 2 * ((G + 1) / 2 + 1) * (P / 32)) +
+  constexpr int P = N / M, NG = (G + S - 1) / S, T = NG * P;
+  constexpr size_t smem = 16 + sizeof(double2) * (4 * N + NG * (S + 1) * (P / 32)) +
                           sizeof(double2) * AdiWaveTile<N, M, G, XH>::SIZE;
   static_assert(smem + 16 <= 227 * 1024, "staged ADI tile exceeds shared memory");
   static_assert(P % 32 == 0, "whole warps per group");
-  static_assert((G + 1) / 2 <= 4, "at most four systems per group");
-  auto k = adi_const_wave_kernel<N, M, G, XH>;
+  static_assert(NG <= 15, "one named barrier per group");
+  auto k = adi_const_wave_kernel<N, M, G, S, XH>;
   if (smem > 48 * 1024) {
     static const cudaError_t attr =
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -634,11 +635,11 @@ static cudaError_t adi_const_wave_launch_x(const AdiHalf &h, const void *tabs, c
   return cudaGetLastError();
 }
 
-template <int N, int M, int G>
+template <int N, int M, int G, int S>
 static cudaError_t adi_const_wave_launch(const AdiHalf &h, const void *tabs, cudaStream_t s) {
   if (tabs == nullptr) return cudaErrorInvalidValue;
-  return h.stride_sys == 1 ? adi_const_wave_launch_x<N, M, G, true>(h, tabs, s)
-                           : adi_const_wave_launch_x<N, M, G, false>(h, tabs, s);
+  return h.stride_sys == 1 ? adi_const_wave_launch_x<N, M, G, S, true>(h, tabs, s)
+                           : adi_const_wave_launch_x<N, M, G, S, false>(h, tabs, s);
 }
 
 // (M, G) of the one-wave kernel per size: each system group holds whole
@@ -708,11 +709,11 @@ cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, 
                       : adi_const_launch<float, NN, GG>(h, g, hh, s);
   if (p == kFP64) {
     switch (h.n) {
-      case 64: return adi_const_wave_launch<64, 2, 4>(h, staged, s);
-      case 128: return adi_const_wave_launch<128, 4, 2>(h, staged, s);
-      case 256: return adi_const_wave_launch<256, 8, 2>(h, staged, s);
-      case 512: return adi_const_wave_launch<512, 8, 4>(h, staged, s);
-      case 1024: return adi_const_wave_launch<1024, 8, 7>(h, staged, s);
+      case 64: return adi_const_wave_launch<64, 2, 4, 2>(h, staged, s);
+      case 128: return adi_const_wave_launch<128, 4, 2, 1>(h, staged, s);
+      case 256: return adi_const_wave_launch<256, 8, 2, 1>(h, staged, s);
+      case 512: return adi_const_wave_launch<512, 8, 4, 2>(h, staged, s);
+      case 1024: return adi_const_wave_launch<1024, 8, 7, 2>(h, staged, s);
       default: break;
     }
   }
