@@ -378,11 +378,11 @@ def run_ours(args, rank, world, device):
         adi_ms = sum(st[1] for st in stream_times) / len(stream_times)
         per_launch_s = adi_ms / 1e3 / W.adi_launches_per_step
         achieved = W.adi_bytes_per_launch / per_launch_s / 1e9
-        roofline = {"kernel": "adi_half_kernel (FP64, 1024^2, one half step)",
+        roofline = {"kernel": "adi_const_wave_kernel (FP64 vacuum half step, 1024^2, 7 systems per CTA)",
                     "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(achieved / peak, 4),
                     "peak_kind": peak_kind,
-                    "traffic": profiled_traffic("adi_const_kernel_1024.md"),
+                    "traffic": profiled_traffic("adi_const_wave_kernel_1024.md"),
                     "note": "algorithmic bytes 2 x 16 B per point per half step; the 16 MB "
                             "field stays in the 126 MB L2 across half steps, so this is "
                             "effective bandwidth (see profiles/)"}
