@@ -251,6 +251,87 @@ __global__ void __launch_bounds__(T, (DB || MAXR == 16 || T >= 1024) ? 1 : 2) ff
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+// x pass over W adjacent lines at a time: the strided lines are columns of
+// the field, so W adjacent columns make each row's segment W elements long
+// (32 bytes: W = 2 for complex128, 4 for complex64) and every DRAM/L2 sector
+// a copy touches is used whole; the W transforms share each pass (ILP W).
+// One buffer of W lines; twiddles and kx^2 are read through L1.
+template <typename R, int N, int T, int W>
+__global__ void __launch_bounds__(T, 1) fft3d_xpass_w_kernel(const Fft3dPass q,
+                                                            const double *__restrict__ kx2,
+                                                            const double2 *__restrict__ tw) {
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *u = reinterpret_cast<C *>(smem_raw);
+  C *field = reinterpret_cast<C *>(q.field);
+  const int tid = threadIdx.x;
+  constexpr int NBLK = N / W;
+  for (int blk = blockIdx.x; blk < NBLK; blk += gridDim.x) {
+    const int line0 = blk * W;
+    // element (j, w): field[j*N + line0 + w] -> u[w*N + sw(j)]; w fastest
+    for (int idx = tid; idx < W * N; idx += T) {
+      const int w = idx % W, j = idx / W;
+      if constexpr (sizeof(C) == 16) cp_async16(u + w * N + sw<C>(j), field + (long long)j * N + line0 + w);
+      else cp_async8(u + w * N + sw<C>(j), field + (long long)j * N + line0 + w);
+    }
+    cp_async_commit();
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    fft_smem_w<C, N, T, -1, W>(u, tw, tid);
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const double ky = kfreq(line0 + w, N, q.two_pi, q.stepn_y);
+      const double ky2 = __dmul_rn(ky, ky);
+      for (int j = tid; j < N; j += T) {
+        const double phi = __dmul_rn(q.a, __dadd_rn(kx2[j], ky2));
+        double sn, cs;
+        sincos_cw(phi, &sn, &cs);
+        u[w * N + sw<C>(j)] = mul_k<R>(u[w * N + sw<C>(j)], mk(cs, -sn));
+      }
+    }
+    __syncthreads();
+    fft_smem_w<C, N, T, +1, W>(u, tw, tid);
+    for (int idx = tid; idx < W * N; idx += T) {
+      const int w = idx % W, j = idx / W;
+      field[(long long)j * N + line0 + w] = u[w * N + sw<C>(j)];
+    }
+    __syncthreads();  // the buffer is refilled next
+  }
+}
+
+template <typename R, int N>
+static cudaError_t fft3d_xpass_w_launch(const Fft3dPass &q, const double *kx2, const double2 *tw,
+                                        cudaStream_t s) {
+  using C = typename Cx<R>::T;
+  constexpr int W = 32 / (int)sizeof(C);
+  constexpr int T = N / 8 < 32 ? 32 : (N / 8 > 1024 ? 1024 : N / 8);
+  constexpr size_t smem = sizeof(C) * W * N;
+  auto k = fft3d_xpass_w_kernel<R, N, T, W>;
+  static int grid = 0;
+  if (grid == 0) {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, T, smem);
+    if (e != cudaSuccess) return e;
+    grid = sms * (per > 0 ? per : 1);
+  }
+  k<<<grid < N / W ? grid : N / W, T, smem, s>>>(q, kx2, tw);
+  return cudaGetLastError();
+}
+
+static bool fft3d_wide_x() {
+  static const bool on = [] {
+    const char *e = std::getenv("PXP_FFT3D_WIDE_X");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 template <int N, int MAXR> constexpr int pass_threads() {
   return N / MAXR < 32 ? 32 : (N / MAXR > 1024 ? 1024 : N / MAXR);
 }
@@ -285,6 +366,11 @@ static cudaError_t fft3d_launch_n(const Fft3dPass &q, int variant, const double 
                                   const double2 *tw16, cudaStream_t s) {
   using C = typename Cx<R>::T;
   const double2 *tw8 = reinterpret_cast<const double2 *>(q.twiddle);
+  // x pass: W adjacent columns per CTA where their buffer fits
+  // (measured: faster from 1024 points, slower at 512)
+  constexpr bool wide_fits = N >= 1024 && 32 * (size_t)N <= 200 * 1024;
+  if constexpr (wide_fits)
+    if (q.mode == 1 && fft3d_wide_x()) return fft3d_xpass_w_launch<R, N>(q, kx2, tw8, s);
   // two line buffers plus tables exceed a CTA's shared memory above 4096
   // points (FP64) / 8192 (FP32): the single-buffer form stands in
   constexpr bool db_fits = (2 * sizeof(C) + sizeof(double2) + sizeof(double)) * N <= 227 * 1024;

@@ -209,4 +209,58 @@ __device__ __forceinline__ void fft_smem(C *x, const double2 *tw, int lane) {
   }
 }
 
+// The same transform applied to W lines at once (line w at x + w*N): every
+// pass loads the butterflies of all W lines before one barrier, so each
+// thread carries W independent butterfly sets.
+template <typename C, int N, int T, int SIGN, int R, int NS, int W>
+__device__ __forceinline__ void stockham_pass_w(C *x, const double2 *tw, int lane) {
+  constexpr int OFF = stockham_offset(N, NS, 8);
+  constexpr int NB = N / R;
+  constexpr int PER = (NB + T - 1) / T;
+  C v[W][PER][R];
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+#pragma unroll
+    for (int b = 0; b < PER; ++b) {
+      const int j = lane + b * T;
+      if (NB % T == 0 || j < NB) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[w][b][r] = x[w * N + sw<C>(j + r * NB)];
+      }
+    }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int j = lane + b * T;
+    if (NB % T == 0 || j < NB) {
+      const int k = j & (NS - 1);
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const double2 t = tw[OFF + (r - 1) * NS + k];
+#pragma unroll
+          for (int w = 0; w < W; ++w) v[w][b][r] = SIGN < 0 ? tw_mul(v[w][b][r], t) : tw_mulc(v[w][b][r], t);
+        }
+      }
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        dft_r<R, SIGN>(v[w][b]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[w * N + sw<C>(base + r * NS)] = v[w][b][r];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <typename C, int N, int T, int SIGN, int W, int NS = 1>
+__device__ __forceinline__ void fft_smem_w(C *x, const double2 *tw, int lane) {
+  if constexpr (NS < N) {
+    constexpr int R = stockham_radix(N, NS, 8);
+    stockham_pass_w<C, N, T, SIGN, R, NS, W>(x, tw, lane);
+    fft_smem_w<C, N, T, SIGN, W, NS * R>(x, tw, lane);
+  }
+}
+
 }  // namespace pxp
