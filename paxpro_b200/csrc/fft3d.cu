@@ -255,29 +255,41 @@ __global__ void __launch_bounds__(T, (DB || MAXR == 16 || T >= 1024) ? 1 : 2) ff
 // the field, so W adjacent columns make each row's segment W elements long
 // (32 bytes: W = 2 for complex128, 4 for complex64) and every DRAM/L2 sector
 // a copy touches is used whole; the W transforms share each pass (ILP W).
-// One buffer of W lines; twiddles and kx^2 are read through L1.
+// Line w sits at w*LD, LD = N + 1 (complex128) or N + 4 (complex64)
+// elements, so that the W threads staging one row land in different banks;
+// twiddles and kx^2 are loaded into shared memory once per CTA.
+template <typename C, int N>
+constexpr int xpass_ld() { return N + (sizeof(C) == 16 ? 1 : 4); }
+
 template <typename R, int N, int T, int W>
 __global__ void __launch_bounds__(T, 1) fft3d_xpass_w_kernel(const Fft3dPass q,
-                                                            const double *__restrict__ kx2,
-                                                            const double2 *__restrict__ tw) {
+                                                            const double *__restrict__ gkx2,
+                                                            const double2 *__restrict__ gtw) {
   using C = typename Cx<R>::T;
+  constexpr int LD = xpass_ld<C, N>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *u = reinterpret_cast<C *>(smem_raw);
+  double2 *tw = reinterpret_cast<double2 *>(smem_raw);
+  double *kx2 = reinterpret_cast<double *>(tw + N);
+  C *u = reinterpret_cast<C *>(kx2 + N);
   C *field = reinterpret_cast<C *>(q.field);
   const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += T) {
+    tw[i] = gtw[i];
+    kx2[i] = gkx2[i];
+  }
   constexpr int NBLK = N / W;
   for (int blk = blockIdx.x; blk < NBLK; blk += gridDim.x) {
     const int line0 = blk * W;
-    // element (j, w): field[j*N + line0 + w] -> u[w*N + sw(j)]; w fastest
+    // element (j, w): field[j*N + line0 + w] -> u[w*LD + sw(j)]; w fastest
     for (int idx = tid; idx < W * N; idx += T) {
       const int w = idx % W, j = idx / W;
-      if constexpr (sizeof(C) == 16) cp_async16(u + w * N + sw<C>(j), field + (long long)j * N + line0 + w);
-      else cp_async8(u + w * N + sw<C>(j), field + (long long)j * N + line0 + w);
+      if constexpr (sizeof(C) == 16) cp_async16(u + w * LD + sw<C>(j), field + (long long)j * N + line0 + w);
+      else cp_async8(u + w * LD + sw<C>(j), field + (long long)j * N + line0 + w);
     }
     cp_async_commit();
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
-    fft_smem_w<C, N, T, -1, W>(u, tw, tid);
+    fft_smem_w<C, N, T, -1, W, LD>(u, tw, tid);
 #pragma unroll
     for (int w = 0; w < W; ++w) {
       const double ky = kfreq(line0 + w, N, q.two_pi, q.stepn_y);
@@ -286,14 +298,14 @@ __global__ void __launch_bounds__(T, 1) fft3d_xpass_w_kernel(const Fft3dPass q,
         const double phi = __dmul_rn(q.a, __dadd_rn(kx2[j], ky2));
         double sn, cs;
         sincos_cw(phi, &sn, &cs);
-        u[w * N + sw<C>(j)] = mul_k<R>(u[w * N + sw<C>(j)], mk(cs, -sn));
+        u[w * LD + sw<C>(j)] = mul_k<R>(u[w * LD + sw<C>(j)], mk(cs, -sn));
       }
     }
     __syncthreads();
-    fft_smem_w<C, N, T, +1, W>(u, tw, tid);
+    fft_smem_w<C, N, T, +1, W, LD>(u, tw, tid);
     for (int idx = tid; idx < W * N; idx += T) {
       const int w = idx % W, j = idx / W;
-      field[(long long)j * N + line0 + w] = u[w * N + sw<C>(j)];
+      field[(long long)j * N + line0 + w] = u[w * LD + sw<C>(j)];
     }
     __syncthreads();  // the buffer is refilled next
   }
@@ -305,7 +317,8 @@ static cudaError_t fft3d_xpass_w_launch(const Fft3dPass &q, const double *kx2, c
   using C = typename Cx<R>::T;
   constexpr int W = 32 / (int)sizeof(C);
   constexpr int T = N / 8 < 32 ? 32 : (N / 8 > 1024 ? 1024 : N / 8);
-  constexpr size_t smem = sizeof(C) * W * N;
+  constexpr size_t smem = sizeof(double2) * N + sizeof(double) * N + sizeof(C) * W * xpass_ld<C, N>();
+  static_assert(smem + 16 <= 227 * 1024, "wide x pass exceeds shared memory");
   auto k = fft3d_xpass_w_kernel<R, N, T, W>;
   static int grid = 0;
   if (grid == 0) {
@@ -368,7 +381,7 @@ static cudaError_t fft3d_launch_n(const Fft3dPass &q, int variant, const double 
   const double2 *tw8 = reinterpret_cast<const double2 *>(q.twiddle);
   // x pass: W adjacent columns per CTA where their buffer fits
   // (measured: faster from 1024 points, slower at 512)
-  constexpr bool wide_fits = N >= 1024 && 32 * (size_t)N <= 200 * 1024;
+  constexpr bool wide_fits = N >= 1024 && N <= 4096;
   if constexpr (wide_fits)
     if (q.mode == 1 && fft3d_wide_x()) return fft3d_xpass_w_launch<R, N>(q, kx2, tw8, s);
   // two line buffers plus tables exceed a CTA's shared memory above 4096

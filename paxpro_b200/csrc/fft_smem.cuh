@@ -209,10 +209,10 @@ __device__ __forceinline__ void fft_smem(C *x, const double2 *tw, int lane) {
   }
 }
 
-// The same transform applied to W lines at once (line w at x + w*N): every
-// pass loads the butterflies of all W lines before one barrier, so each
-// thread carries W independent butterfly sets.
-template <typename C, int N, int T, int SIGN, int R, int NS, int W>
+// The same transform applied to W lines at once (line w at x + w*LD, LD >=
+// N): every pass loads the butterflies of all W lines before one barrier, so
+// each thread carries W independent butterfly sets.
+template <typename C, int N, int T, int SIGN, int R, int NS, int W, int LD>
 __device__ __forceinline__ void stockham_pass_w(C *x, const double2 *tw, int lane) {
   constexpr int OFF = stockham_offset(N, NS, 8);
   constexpr int NB = N / R;
@@ -225,7 +225,7 @@ __device__ __forceinline__ void stockham_pass_w(C *x, const double2 *tw, int lan
       const int j = lane + b * T;
       if (NB % T == 0 || j < NB) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[w][b][r] = x[w * N + sw<C>(j + r * NB)];
+        for (int r = 0; r < R; ++r) v[w][b][r] = x[w * LD + sw<C>(j + r * NB)];
       }
     }
   __syncthreads();
@@ -247,19 +247,19 @@ __device__ __forceinline__ void stockham_pass_w(C *x, const double2 *tw, int lan
       for (int w = 0; w < W; ++w) {
         dft_r<R, SIGN>(v[w][b]);
 #pragma unroll
-        for (int r = 0; r < R; ++r) x[w * N + sw<C>(base + r * NS)] = v[w][b][r];
+        for (int r = 0; r < R; ++r) x[w * LD + sw<C>(base + r * NS)] = v[w][b][r];
       }
     }
   }
   __syncthreads();
 }
 
-template <typename C, int N, int T, int SIGN, int W, int NS = 1>
+template <typename C, int N, int T, int SIGN, int W, int LD, int NS = 1>
 __device__ __forceinline__ void fft_smem_w(C *x, const double2 *tw, int lane) {
   if constexpr (NS < N) {
     constexpr int R = stockham_radix(N, NS, 8);
-    stockham_pass_w<C, N, T, SIGN, R, NS, W>(x, tw, lane);
-    fft_smem_w<C, N, T, SIGN, W, NS * R>(x, tw, lane);
+    stockham_pass_w<C, N, T, SIGN, R, NS, W, LD>(x, tw, lane);
+    fft_smem_w<C, N, T, SIGN, W, LD, NS * R>(x, tw, lane);
   }
 }
 
