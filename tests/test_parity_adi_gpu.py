@@ -64,7 +64,7 @@ def test_cfg1_adi_fp64_sphere_crossing_full_size():
     assert np.std(np.abs(out)) > 1e-3
 
 
-@pytest.mark.parametrize("n", [64, 256, 2048])
+@pytest.mark.parametrize("n", [64, 256, 512, 2048])
 def test_adi_fp64_sizes(n):
     sph = [(30.0, -40.0, 3000.0, 150.0, 4.5e-5, 3.6e-6), (-100.0, 80.0, 5200.0, 90.0, 2e-5, 1e-6)]
     nsteps = 8 if n == 2048 else 12

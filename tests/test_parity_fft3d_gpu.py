@@ -127,6 +127,15 @@ def test_k1_gpu_vacuum_gaussian_closed_form():
     assert _rel(out, exact) < 1e-12
 
 
+def test_fft3d_fp32_served_intensity_four_column_x_pass():
+    # n >= 1024 runs the x pass four complex64 columns per CTA
+    sph = [(15.0, -25.0, 8000.0, 220.0, 4e-5, 8e-7)]  # centre on a sampling plane
+    out, saves, ref_out, ref_saves = _run_both(1024, 1000.0, 0.0, 1000.0, 40, sph,
+                                               save_every=10, precision=1)
+    assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
+    assert np.std(np.abs(out)) > 1e-4
+
+
 def test_fft3d_fp32_served_intensity():
     rng = np.random.default_rng(5)
     sph = wl.random_spheres(rng, 8, -500.0, 500.0, 3.0e5)
