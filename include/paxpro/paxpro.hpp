@@ -604,14 +604,15 @@ class Solver3D : public Solver {
     if (currZ >= solution.n_slices) return;
     double deltaX = static_cast<double>(currentSolution.n_rows) / static_cast<double>(solution.n_rows);
     double deltaY = static_cast<double>(currentSolution.n_cols) / static_cast<double>(solution.n_cols);
-    unsigned bx = (unsigned)deltaX, by = (unsigned)deltaY;
     for (unsigned i = 0; i < solution.n_rows * solution.n_cols; ++i) {
       unsigned row = i % solution.n_rows, col = i / solution.n_rows;
+      // submat bounds [row*deltaX, row*deltaX + deltaX - 1], truncated
+      const unsigned r0 = (unsigned)(row * deltaX), r1 = (unsigned)(row * deltaX + deltaX - 1);
+      const unsigned c0 = (unsigned)(col * deltaY), c1 = (unsigned)(col * deltaY + deltaY - 1);
       cdouble sum = 0.0;
-      for (unsigned c = 0; c < by; ++c) {
+      for (unsigned c = c0; c <= c1; ++c) {
         cdouble colsum = 0.0;
-        for (unsigned r = 0; r < bx; ++r)
-          colsum += currentSolution((unsigned)(row * deltaX) + r, (unsigned)(col * deltaY) + c);
+        for (unsigned r = r0; r <= r1; ++r) colsum += currentSolution(r, c);
         sum += colsum;
       }
       solution(row, col, currZ) = sum / (deltaX * deltaY);

@@ -141,7 +141,12 @@ int pxp_get_stream(pxp_solver s, void **stream);
 
 /* Saved fields (the columns of Solver2D::solution / slices of
  * Solver3D::solution, include/solver2D.hpp:121, include/solver3D.hpp:52):
- * number of slots filled and one slot copied to the host. */
+ * number of slots filled and one slot copied to the host.  A slot of the
+ * 3-D solvers holds m x m complex values, m = Nx / x.downsampling_ratio,
+ * the block averages Solver3D::copyCurrentSolution stores
+ * (src/solver3D.cpp:94-112); with ratio 1, the field.  The 2-D solvers
+ * accept ratio 1 only (their reference downsampling is the VISA low-pass
+ * filter): pxp_solver_create returns PXP_ERR_UNSUPPORTED otherwise. */
 int pxp_num_saved(pxp_solver s, int *count);
 int pxp_get_saved(pxp_solver s, int slot, double *field);
 

@@ -684,4 +684,25 @@ void orc_plane_wave(int n, double value_re, double value_im, double *out) {
   }
 }
 
+// Solver3D::copyCurrentSolution's block average (src/solver3D.cpp:94-112).
+void orc_block_average(const double *full, int n, int m, double *out) {
+  const cd *u = reinterpret_cast<const cd *>(full);
+  cd *o = reinterpret_cast<cd *>(out);
+  const double delta = static_cast<double>(n) / static_cast<double>(m);
+  for (int col = 0; col < m; ++col)
+    for (int row = 0; row < m; ++row) {
+      const unsigned r0 = static_cast<unsigned>(row * delta);
+      const unsigned r1 = static_cast<unsigned>(row * delta + delta - 1);
+      const unsigned c0 = static_cast<unsigned>(col * delta);
+      const unsigned c1 = static_cast<unsigned>(col * delta + delta - 1);
+      cd total(0.0, 0.0);
+      for (unsigned c = c0; c <= c1; ++c) {
+        cd colsum(0.0, 0.0);
+        for (unsigned r = r0; r <= r1; ++r) colsum += u[(size_t)c * n + r];
+        total += colsum;
+      }
+      o[(size_t)col * m + row] = total / (delta * delta);
+    }
+}
+
 }  // extern "C"

@@ -103,6 +103,16 @@ void orc_gaussian_beam_3d(const orc_grid *g, double wavelength, double waist,
                           double *out /* Ny x Nx column-major */);
 void orc_plane_wave(int n, double value_re, double value_im, double *out);
 
+/* Transverse downsampling of a saved 3-D field as Solver3D::
+ * copyCurrentSolution does it (src/solver3D.cpp:94-112): the saved slice has
+ * m = n / ratio rows and columns (src/solver3D.cpp:26, 36); with
+ * delta = n / m (a double), entry (row, col) is the sum of the n x n field's
+ * block rows [row*delta, row*delta + delta - 1] and columns [col*delta,
+ * col*delta + delta - 1] (bounds truncated to unsigned, as the submat
+ * arguments are), summed column by column, divided by delta*delta.
+ * full: n x n column-major complex; out: m x m column-major complex. */
+void orc_block_average(const double *full, int n, int m, double *out);
+
 /* Run the lines of 2-D transforms on all OpenMP threads (1) or on one
  * thread as the reference's FFTW plans do (0, default).  Results are the
  * same either way: each line's transform is computed identically. */

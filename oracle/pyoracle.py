@@ -58,6 +58,8 @@ def lib():
         _LIB.orc_node_count.argtypes = [C.c_double] * 3
         _LIB.orc_fft1d.argtypes = [d, C.c_int, C.c_int]
         _LIB.orc_thomas.argtypes = [d, d, d, C.c_int]
+        _LIB.orc_block_average.argtypes = [d, C.c_int, C.c_int, d]
+        _LIB.orc_block_average.restype = None
         for name in ("orc_fft2d_run",):
             getattr(_LIB, name).argtypes = [C.POINTER(Grid), C.POINTER(Material), d,
                                             C.c_int, C.c_int, d, d]
@@ -227,6 +229,18 @@ def gaussian_beam_3d(g, wavelength, waist, cx=0.0, cy=0.0, amplitude=1.0, z=0.0)
     out = np.zeros((ny, nx), dtype=np.complex128, order="F")
     lib().orc_gaussian_beam_3d(C.byref(g), wavelength, waist, cx, cy, amplitude, z,
                                out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def block_average(field, ratio: int):
+    """Saved-slice downsampling of Solver3D (src/solver3D.cpp:94-112): an
+    n x n field to (n // ratio) x (n // ratio)."""
+    f = np.asfortranarray(np.asarray(field, dtype=np.complex128))
+    n = f.shape[0]
+    m = n // int(ratio)
+    out = np.zeros((m, m), dtype=np.complex128, order="F")
+    lib().orc_block_average(f.ctypes.data_as(C.POINTER(C.c_double)), n, m,
+                            out.ctypes.data_as(C.POINTER(C.c_double)))
     return out
 
 

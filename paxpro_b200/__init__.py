@@ -95,6 +95,9 @@ class Solver:
         L.pxp_shape(self._h, C.byref(nx), C.byref(ny), C.byref(nz))
         self.nx, self.ny, self.nz = nx.value, ny.value, nz.value
         self.three_d = spec.kind in (FFT_SOLVER_3D, ADI)
+        # saved slices of the 3-D solvers: (nx // ratio)^2 block averages
+        ratio = max(int(spec.x.downsampling_ratio), 1)
+        self.save_n = self.nx // ratio if self.three_d else self.nx
 
     # -- lifetime
     def close(self) -> None:
@@ -203,9 +206,13 @@ class Solver:
         return c.value
 
     def get_saved(self, slot: int) -> np.ndarray:
-        out = np.empty(self.nx * self.ny, dtype=np.complex128)
+        """Saved field of a save slot; for the 3-D solvers with a transverse
+        downsampling ratio r > 1 an (n // r) x (n // r) slice of block
+        averages (Solver3D::copyCurrentSolution, src/solver3D.cpp:94-112)."""
+        m = self.save_n
+        out = np.empty(m * m if self.three_d else m, dtype=np.complex128)
         self._check(_capi.lib().pxp_get_saved(self._h, int(slot), _dptr(out.view(np.float64))))
-        return self._unflatten(out)
+        return out.reshape((m, m), order="F") if self.three_d else out
 
     def reset(self) -> None:
         self._check(_capi.lib().pxp_reset(self._h))

@@ -88,6 +88,12 @@ struct pxp_solver_s {
   bool ic_set = false;
   unsigned current_step = 1;
   unsigned timeouts_seen = 0;  // device count of ran-out kernel waits at creation
+  // saved fields: save_pts points each (3-D kinds: save_n x save_n block
+  // averages of the field when the transverse downsampling ratio is above 1,
+  // staged through d_save_stage)
+  unsigned save_n = 0;
+  long long save_pts = 0;
+  void *d_save_stage = nullptr;
   // captured block of step-invariant steps (replay_steps) and the buffers
   // and launch choices it was captured with
   cudaGraphExec_t graph = nullptr;
@@ -485,6 +491,17 @@ bool save_at(const pxp_solver_s *h, unsigned step) {
          (int)(step / (unsigned)h->save_every) - 1 < h->max_slots;
 }
 
+char *save_slot(const pxp_solver_s *h, unsigned step) {
+  return (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->save_pts;
+}
+
+// The step's full field is in the staging buffer: reduce it into its slot.
+int save_downsample(pxp_solver_s *h, char *slot) {
+  const cudaError_t e = pxp::launch_block_average(h->prec, h->d_save_stage, slot, (int)h->nx,
+                                                  (int)h->save_n, h->stream);
+  return e == cudaSuccess ? PXP_OK : h->cuda_fail(e, "saved-field downsampling");
+}
+
 // Spheres that can contain a point of the plane z: the oracle's and the
 // kernel's test is ((dx^2 + dy^2) + dz^2) < R^2 with rounded operations, and
 // the rounded sum of non-negative terms is never below dz^2, so a sphere
@@ -549,9 +566,8 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   // y implicit: systems are columns (x), positions run along y (stride 1)
   a.in = h->d_field2;
   a.out = h->d_field;
-  a.save = save_at(h, step)
-               ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
-               : nullptr;
+  char *slot = save_at(h, step) ? save_slot(h, step) : nullptr;
+  a.save = slot && h->d_save_stage ? h->d_save_stage : slot;
   a.stride_pos = 1;
   a.stride_sys = n;
   a.y_implicit = 1;
@@ -563,6 +579,7 @@ int adi_step(pxp_solver_s *h, unsigned step) {
           ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n, lu + 8 * n, h->stream)
           : pxp::launch_adi_half(h->prec, a, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
+  if (slot && h->d_save_stage) return save_downsample(h, slot);
   return PXP_OK;
 }
 
@@ -744,12 +761,12 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
       q.nspheres = (int)h->spheres.size();
       q.spheres_all = h->d_spheres;
     }
-    q.save = save_at(h, step)
-                 ? (char *)h->d_saves + (size_t)(step / h->save_every - 1) * h->csize * h->npts
-                 : nullptr;
+    char *slot = save_at(h, step) ? save_slot(h, step) : nullptr;
+    q.save = slot && h->d_save_stage ? h->d_save_stage : slot;
     if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, h->stream)) !=
         cudaSuccess)
       return h->cuda_fail(e, "FFT3D y pass");
+    if (slot && h->d_save_stage) return save_downsample(h, slot);
     return PXP_OK;
   };
   // no sphere in the step's slab, no save, not the last step of the call:
@@ -873,6 +890,22 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
   h->nz = pxp_node_count(p.z.min, p.z.max, p.z.step);
   h->ny = three_d ? h->nx : 1;  // Solver3D::setSimulator forces Ny = Nx (src/solver3D.cpp:24)
   h->npts = (long long)h->nx * h->ny;
+  {
+    // transverse downsampling of saved fields: Solver3D keeps Nx/ratio x
+    // Nx/ratio block averages (src/solver3D.cpp:26, 36, 94-112); Solver2D
+    // filters with the VISA low-pass filter (src/solver2D.cpp:34-39), which
+    // this build does not provide
+    const unsigned r = p.x.downsampling_ratio > 1 ? p.x.downsampling_ratio : 1;
+    if (r > 1 && !three_d) {
+      set_global_error("transverse downsampling_ratio > 1 of the 2-D solvers (a VISA low-pass "
+                       "filter in the reference) is not provided: use 1");
+      delete h;
+      return PXP_ERR_UNSUPPORTED;
+    }
+    h->save_n = h->nx / r;
+    if (h->save_n == 0) return bad("downsampling_ratio larger than the transverse node count");
+    h->save_pts = three_d ? (long long)h->save_n * h->save_n : h->npts;
+  }
   h->prec = p.precision == PXP_FP64 ? pxp::kFP64 : pxp::kFP32;
   h->csize = h->prec == pxp::kFP64 ? 16 : 8;
   if (h->nx < 4 || h->nz < 2) return bad("grid too small (need Nx >= 4, Nz >= 2)");
@@ -912,7 +945,10 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
   if (h->save_every) {
     h->max_slots = (int)((h->nz - 1) / (unsigned)h->save_every);
     if (h->max_slots > 0 &&
-        (rc = alloc(h, &h->d_saves, h->csize * h->npts * (size_t)h->max_slots, "save slots")))
+        (rc = alloc(h, &h->d_saves, h->csize * h->save_pts * (size_t)h->max_slots, "save slots")))
+      return cleanup_fail(rc);
+    if (h->max_slots > 0 && h->save_pts != h->npts &&
+        (rc = alloc(h, &h->d_save_stage, h->csize * h->npts, "save staging")))
       return cleanup_fail(rc);
   }
   std::vector<double> zeros(h->npts, 0.0);
@@ -947,6 +983,7 @@ int pxp_solver_destroy(pxp_solver h) {
   h->graph = nullptr;
   free_dev(h->d_field, h->stream);
   free_dev(h->d_saves, h->stream);
+  free_dev(h->d_save_stage, h->stream);
   h->d_kern = nullptr;  // shared table, not owned
   free_dev(h->d_trans, h->stream);
   h->d_tw = nullptr;  // shared table, not owned
@@ -1053,16 +1090,17 @@ static int check_waits(pxp_solver_s *h) {
   return PXP_OK;
 }
 
-static int download_field(pxp_solver_s *h, double *dst, const void *src) {
+static int download_field(pxp_solver_s *h, double *dst, const void *src, long long npts = -1) {
+  if (npts < 0) npts = h->npts;
   if (int rc = check_waits(h)) return rc;
   if (h->prec == pxp::kFP64) {
-    PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, 16 * h->npts, cudaMemcpyDeviceToHost, h->stream));
+    PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, 16 * npts, cudaMemcpyDeviceToHost, h->stream));
     PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
   } else {
-    std::vector<float> tmp(2 * h->npts);
-    PXP_TRY_CUDA(h, cudaMemcpyAsync(tmp.data(), src, 8 * h->npts, cudaMemcpyDeviceToHost, h->stream));
+    std::vector<float> tmp(2 * npts);
+    PXP_TRY_CUDA(h, cudaMemcpyAsync(tmp.data(), src, 8 * npts, cudaMemcpyDeviceToHost, h->stream));
     PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
-    for (long long i = 0; i < 2 * h->npts; ++i) dst[i] = (double)tmp[i];
+    for (long long i = 0; i < 2 * npts; ++i) dst[i] = (double)tmp[i];
   }
   return PXP_OK;
 }
@@ -1174,8 +1212,8 @@ int pxp_get_saved(pxp_solver h, int slot, double *field) {
   pxp_num_saved(h, &c);
   if (slot < 0 || slot >= c)
     return h->fail(PXP_ERR_INVALID, "save slot " + std::to_string(slot) + " not filled");
-  const char *base = (const char *)h->d_saves + (size_t)slot * h->csize * h->npts;
-  return download_field(h, field, base);
+  const char *base = (const char *)h->d_saves + (size_t)slot * h->csize * h->save_pts;
+  return download_field(h, field, base, h->save_pts);
 }
 
 int pxp_reset(pxp_solver h) {

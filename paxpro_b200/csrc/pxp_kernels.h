@@ -108,6 +108,11 @@ cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, 
 // false when size n runs the other kernel (out untouched).  g, h, out:
 // interleaved (re, im).
 bool adi_const_staged_tables(int n, const double *g, const double *h, double *out);
+// Saved-slice downsampling of the 3-D solvers (Solver3D::copyCurrentSolution,
+// src/solver3D.cpp:94-112): n x n field -> m x m block averages.
+cudaError_t launch_block_average(Precision p, const void *full, void *out, int n, int m,
+                                 cudaStream_t s);
+
 // Kernel waits on the current device that ran out (bounded mbarrier waits),
 // read on stream s (synchronises s).
 unsigned wait_timeouts(cudaStream_t s);

@@ -39,3 +39,15 @@ def test_null_arguments_are_rejected_without_a_device():
     assert lib.pxp_solver_create(None, None) == _capi.PXP_ERR_INVALID
     assert lib.pxp_step(None, 1) == _capi.PXP_ERR_INVALID
     assert lib.pxp_solver_destroy(None) == _capi.PXP_OK
+
+
+def test_transverse_downsampling_of_2d_solvers_is_rejected_before_any_device_call():
+    import ctypes as C
+    import paxpro_b200 as pxp
+    from paxpro_b200 import _capi
+    spec = pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(-250.0, 250.0, 0.5, 2),
+                           z=pxp.Disc(0.0, 1e4, 1000.0), wavenumber=62.8)
+    h = C.c_void_p()
+    rc = _capi.lib().pxp_solver_create(C.byref(spec.to_c()), C.byref(h))
+    assert rc == _capi.PXP_ERR_UNSUPPORTED
+    assert "downsampling" in _capi.last_error()
