@@ -150,6 +150,20 @@ int pxp_get_stream(pxp_solver s, void **stream);
 int pxp_num_saved(pxp_solver s, int *count);
 int pxp_get_saved(pxp_solver s, int slot, double *field);
 
+/* Post-processing quantities computed on the device (post:: modules,
+ * src/postProcessMod.cpp:7-150): out receives one double per point of a
+ * saved slot (slot >= 0; its layout and size as pxp_get_saved) or of the
+ * last solution (slot = -1; the layout of pxp_get_last_solution). */
+#define PXP_POST_ABS 0  /* |u|: post::Intensity (:7-15), IntensityUint8's scale (:17-30) */
+#define PXP_POST_ARG 1  /* arg u: post::Phase (:86-100), post::ExitPhase (:134-150) */
+#define PXP_POST_REAL 2 /* Re u: post::ExitField (:102-116) */
+#define PXP_POST_ABS2 3 /* pow(|u|, 2): post::ExitIntensity (:118-132) */
+int pxp_get_post(pxp_solver s, int quantity, int slot, double *out);
+/* Largest |u| over the filled save slots (0 when none): the scale of
+ * post::IntensityUint8 (src/postProcessMod.cpp:23, abs of the complex
+ * maximum by modulus). */
+int pxp_saved_max_abs(pxp_solver s, double *max_abs);
+
 /* Solver::reset (include/solver.hpp:30): step counter back to 1. */
 int pxp_reset(pxp_solver s);
 

@@ -86,8 +86,13 @@ def _dptr(a: np.ndarray):
 class Solver:
     """One propagation problem resident on the GPU (a C-ABI handle)."""
 
-    def __init__(self, spec: ProblemSpec):
+    def __init__(self, spec: ProblemSpec, keep_initial: bool = False):
+        """keep_initial: keep the host initial field given to
+        set_initial_conditions, as slice 0 of the post-processing modules'
+        field quantities (paxpro_b200.post)."""
         self.spec = spec
+        self.keep_initial = keep_initial
+        self._u0_host = None
         self._h = C.c_void_p()
         L = _capi.lib()
         _capi.check(L.pxp_solver_create(C.byref(spec.to_c()), C.byref(self._h)))
@@ -154,9 +159,11 @@ class Solver:
             raise ValueError(f"initial field shape {a.shape} != {self.shape}")
         flat = np.ascontiguousarray(a.reshape(-1, order="F"))
         self._check(_capi.lib().pxp_set_initial_conditions(self._h, _dptr(flat.view(np.float64))))
+        self._u0_host = a if self.keep_initial else None
 
     def set_initial_conditions_device(self, ptr: int) -> None:
         self._check(_capi.lib().pxp_set_initial_conditions_device(self._h, C.c_void_p(ptr)))
+        self._u0_host = None
 
     def step(self, nsteps: int = 1) -> None:
         self._check(_capi.lib().pxp_step(self._h, int(nsteps)))
@@ -213,6 +220,25 @@ class Solver:
         out = np.empty(m * m if self.three_d else m, dtype=np.complex128)
         self._check(_capi.lib().pxp_get_saved(self._h, int(slot), _dptr(out.view(np.float64))))
         return out.reshape((m, m), order="F") if self.three_d else out
+
+    def get_post(self, quantity: int, slot: int = -1) -> np.ndarray:
+        """A post-processing quantity (_capi.POST_ABS / POST_ARG / POST_REAL /
+        POST_ABS2) of a saved slot, or of the last solution (slot = -1),
+        computed on the device."""
+        if slot < 0:
+            n, shape = self.nx * self.ny, ((self.ny, self.nx) if self.three_d else (self.nx,))
+        else:
+            m = self.save_n
+            n, shape = (m * m, (m, m)) if self.three_d else (m, (m,))
+        out = np.empty(n, dtype=np.float64)
+        self._check(_capi.lib().pxp_get_post(self._h, int(quantity), int(slot), _dptr(out)))
+        return out.reshape(shape, order="F")
+
+    def saved_max_abs(self) -> float:
+        """Largest |u| over the filled save slots."""
+        v = C.c_double()
+        self._check(_capi.lib().pxp_saved_max_abs(self._h, C.byref(v)))
+        return v.value
 
     def reset(self) -> None:
         self._check(_capi.lib().pxp_reset(self._h))

@@ -23,6 +23,7 @@ PXP_ERR_ABORTED = -4
 PXP_ERR_BUDGET = -5
 PXP_ERR_NOT_READY = -6
 PXP_ERR_UNSUPPORTED = -7
+POST_ABS, POST_ARG, POST_REAL, POST_ABS2 = 0, 1, 2, 3
 
 FFT_SOLVER_2D, CRANK_NICHOLSON, FFT_SOLVER_3D, ADI = 1, 2, 3, 4
 FP64, FP32 = 0, 1
@@ -89,6 +90,8 @@ def lib():
         "pxp_get_stream": (C.c_int, [h, C.POINTER(C.c_void_p)]),
         "pxp_num_saved": (C.c_int, [h, C.POINTER(C.c_int)]),
         "pxp_get_saved": (C.c_int, [h, C.c_int, d]),
+        "pxp_get_post": (C.c_int, [h, C.c_int, C.c_int, d]),
+        "pxp_saved_max_abs": (C.c_int, [h, d]),
         "pxp_reset": (C.c_int, [h]),
         "pxp_current_step": (C.c_int, [h, C.POINTER(C.c_uint)]),
         "pxp_shape": (C.c_int, [h, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),

@@ -1216,6 +1216,49 @@ int pxp_get_saved(pxp_solver h, int slot, double *field) {
   return download_field(h, field, base, h->save_pts);
 }
 
+int pxp_get_post(pxp_solver h, int quantity, int slot, double *out) {
+  if (h == nullptr || out == nullptr) return PXP_ERR_INVALID;
+  if (quantity < PXP_POST_ABS || quantity > PXP_POST_ABS2)
+    return h->fail(PXP_ERR_INVALID, "unknown post-processing quantity");
+  const void *src = h->d_field;
+  long long n = h->npts;
+  if (slot >= 0) {
+    int c = 0;
+    pxp_num_saved(h, &c);
+    if (slot >= c) return h->fail(PXP_ERR_INVALID, "save slot " + std::to_string(slot) + " not filled");
+    src = (const char *)h->d_saves + (size_t)slot * h->csize * h->save_pts;
+    n = h->save_pts;
+  }
+  if (int rc = check_waits(h)) return rc;
+  double *d_out = nullptr;
+  PXP_TRY_CUDA(h, cudaMallocAsync((void **)&d_out, sizeof(double) * n, h->stream));
+  cudaError_t e = pxp::launch_post(h->prec, src, d_out, n, quantity, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream);
+  cudaFreeAsync(d_out, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? PXP_OK : h->cuda_fail(e, "post-processing reduction");
+}
+
+int pxp_saved_max_abs(pxp_solver h, double *max_abs) {
+  if (h == nullptr || max_abs == nullptr) return PXP_ERR_INVALID;
+  int c = 0;
+  pxp_num_saved(h, &c);
+  if (int rc = check_waits(h)) return rc;
+  unsigned long long *d_max = nullptr;
+  PXP_TRY_CUDA(h, cudaMallocAsync((void **)&d_max, sizeof(unsigned long long), h->stream));
+  cudaError_t e = cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), h->stream);
+  for (int k = 0; k < c && e == cudaSuccess; ++k)
+    e = pxp::launch_max_abs(h->prec, (const char *)h->d_saves + (size_t)k * h->csize * h->save_pts,
+                            h->save_pts, d_max, h->stream);
+  unsigned long long bits = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, d_max, sizeof(bits), cudaMemcpyDeviceToHost, h->stream);
+  cudaFreeAsync(d_max, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "max |u| over the saved fields");
+  std::memcpy(max_abs, &bits, sizeof(double));
+  return PXP_OK;
+}
+
 int pxp_reset(pxp_solver h) {
   if (h == nullptr) return PXP_ERR_INVALID;
   h->current_step = 1;

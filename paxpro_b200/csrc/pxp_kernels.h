@@ -113,6 +113,15 @@ bool adi_const_staged_tables(int n, const double *g, const double *h, double *ou
 cudaError_t launch_block_average(Precision p, const void *full, void *out, int n, int m,
                                  cudaStream_t s);
 
+// Post-processing quantities of n complex values into n doubles:
+// 0 = |u|, 1 = arg u, 2 = Re u, 3 = |u|^2 (post.cu).
+cudaError_t launch_post(Precision p, const void *field, double *out, long long n, int quantity,
+                        cudaStream_t s);
+// Running max of |u| over n values into *result (the bits of a double,
+// start from 0).
+cudaError_t launch_max_abs(Precision p, const void *field, long long n, unsigned long long *result,
+                           cudaStream_t s);
+
 // Kernel waits on the current device that ran out (bounded mbarrier waits),
 // read on stream s (synchronises s).
 unsigned wait_timeouts(cudaStream_t s);
