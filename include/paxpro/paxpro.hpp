@@ -17,8 +17,9 @@
 // this build does not have): HDF5 save (save() throws), post-processing
 // modules, VISA visualisation and the VISA longitudinal low-pass filter
 // (solve() requires disableLongitudinalFilter() when the longitudinal
-// downsampling ratio is above 1), CSG geometry on the 3-D solvers (they take
-// SphereMaterial or no material).
+// downsampling ratio is above 1).  The 3-D solvers take a SphereMaterial, a
+// CSGMaterial over geom::Module / Part / Shape (evaluated on the device), or
+// no material.
 #pragma once
 #include <algorithm>
 #include <cmath>
@@ -78,6 +79,219 @@ class SphereMaterial : public MaterialFunction {
     beta = 0.0;
   }
   std::vector<Sphere> spheres;
+};
+
+// ------------------------------------------------------------ geometry ----
+/** include/shapes.hpp, include/geometry.hpp, src/shape.cpp, src/geometry.cpp:
+ * shapes with a world-to-shape 4x4 transformation (row-major here), parts
+ * (shapes joined by union / difference, with a material) and modules (parts
+ * joined by union / difference). */
+namespace geom {
+enum class Axis_t { X, Y, Z };
+enum class Operation_t { UNION, DIFFERENCE };
+
+class Shape {
+ public:
+  explicit Shape(const char *name) : name(name) {
+    for (int i = 0; i < 16; ++i) transformation[i] = (i % 5 == 0) ? 1.0 : 0.0;
+  }
+  virtual ~Shape() {}
+  /** src/shape.cpp:16-26: transformation = transformation * T(-x, -y, -z) */
+  void translate(double x, double y, double z) {
+    double m[16];
+    identity(m);
+    m[3] = -x;
+    m[7] = -y;
+    m[11] = -z;
+    rightMultiply(m);
+  }
+  /** src/shape.cpp:28-57 */
+  void rotate(double angleDeg, Axis_t axis) {
+    const double PI = std::acos(-1.0);
+    const double angle = angleDeg * PI / 180.0;
+    double m[16];
+    identity(m);
+    switch (axis) {
+      case Axis_t::X: m[5] = std::cos(angle); m[6] = std::sin(angle); m[9] = -std::sin(angle); m[10] = std::cos(angle); break;
+      case Axis_t::Y: m[0] = std::cos(angle); m[2] = -std::sin(angle); m[8] = std::sin(angle); m[10] = std::cos(angle); break;
+      case Axis_t::Z: m[0] = std::cos(angle); m[1] = std::sin(angle); m[4] = -std::sin(angle); m[5] = std::cos(angle); break;
+    }
+    rightMultiply(m);
+  }
+  /** src/shape.cpp:128-144: transformation = S(1/factor) * transformation */
+  void scale(double factor, Axis_t axis) {
+    double m[16];
+    identity(m);
+    const int a = axis == Axis_t::X ? 0 : (axis == Axis_t::Y ? 1 : 2);
+    m[a * 5] = 1.0 / factor;
+    double out[16];
+    multiply(m, transformation, out);
+    std::memcpy(transformation, out, sizeof(out));
+  }
+  /** src/shape.cpp:59-70 */
+  void transform(double &x, double &y, double &z) const {
+    const double x0 = x, y0 = y, z0 = z;
+    const double *T = transformation;
+    x = T[0] * x0 + T[1] * y0 + T[2] * z0 + T[3] * 1.0;
+    y = T[4] * x0 + T[5] * y0 + T[6] * z0 + T[7] * 1.0;
+    z = T[8] * x0 + T[9] * y0 + T[10] * z0 + T[11] * 1.0;
+  }
+  virtual bool isInside(double x, double y, double z) const = 0;
+  virtual int kind() const = 0;
+  virtual void size(double out[3]) const = 0;
+  std::string name;
+  double transformation[16];
+
+ private:
+  static void identity(double *m) {
+    for (int i = 0; i < 16; ++i) m[i] = (i % 5 == 0) ? 1.0 : 0.0;
+  }
+  static void multiply(const double *a, const double *b, double *out) {
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) {
+        double acc = 0.0;
+        for (int k = 0; k < 4; ++k) acc += a[i * 4 + k] * b[k * 4 + j];
+        out[i * 4 + j] = acc;
+      }
+  }
+  void rightMultiply(const double *m) {
+    double out[16];
+    multiply(transformation, m, out);
+    std::memcpy(transformation, out, sizeof(out));
+  }
+};
+
+/** geom::Sphere (src/shape.cpp:146-151) */
+class Sphere : public Shape {
+ public:
+  explicit Sphere(double radius) : Shape("sphere"), radius(radius) {}
+  bool isInside(double x, double y, double z) const override {
+    transform(x, y, z);
+    double r = std::sqrt(x * x + y * y + z * z);
+    return r < radius;
+  }
+  int kind() const override { return PXP_SHAPE_SPHERE; }
+  void size(double out[3]) const override { out[0] = radius; out[1] = out[2] = 0.0; }
+  double radius;
+};
+
+/** geom::Box (src/shape.cpp:160-164) */
+class Box : public Shape {
+ public:
+  Box(double Lx, double Ly, double Lz) : Shape("Cube"), Lx(Lx), Ly(Ly), Lz(Lz) {}
+  bool isInside(double x, double y, double z) const override {
+    transform(x, y, z);
+    return (x > -Lx / 2.0) && (x < Lx / 2.0) && (y > -Ly / 2.0) && (y < Ly / 2.0) &&
+           (z > -Lz / 2.0) && (z < Lz / 2.0);
+  }
+  int kind() const override { return PXP_SHAPE_BOX; }
+  void size(double out[3]) const override { out[0] = Lx; out[1] = Ly; out[2] = Lz; }
+  double Lx, Ly, Lz;
+};
+
+/** geom::Cylinder (src/shape.cpp:175-187) */
+class Cylinder : public Shape {
+ public:
+  Cylinder(double radius, double height) : Shape("Cylinder"), r1(radius), r2(radius), height(height) {}
+  Cylinder(double r1, double r2, double height) : Shape("Cylinder"), r1(r1), r2(r2), height(height) {}
+  bool isInside(double x, double y, double z) const override {
+    transform(x, y, z);
+    bool zIsInside = (z < height / 2.0) && (z > -height / 2.0);
+    if (!zIsInside) return false;
+    double slope = (r2 - r1) / height;
+    double radius = slope * (z + height / 2.0) + r1;
+    double r = std::sqrt(x * x + y * y);
+    return r < radius;
+  }
+  int kind() const override { return PXP_SHAPE_CYLINDER; }
+  void size(double out[3]) const override { out[0] = height; out[1] = r1; out[2] = r2; }
+  double r1, r2, height;
+};
+
+/** geom::Part (src/geometry.cpp:53-108): non-owning shape pointers. */
+class Part {
+ public:
+  explicit Part(const char *name) : name(name) {}
+  void add(Shape &shape) {
+    shapes.push_back(&shape);
+    operations.push_back(Operation_t::UNION);
+  }
+  void difference(Shape &shape) {
+    if (shapes.empty())
+      throw std::runtime_error("There is no shape to make difference with. You have to add at least one shape before...");
+    shapes.push_back(&shape);
+    operations.push_back(Operation_t::DIFFERENCE);
+  }
+  bool isInside(double x, double y, double z) const {
+    for (size_t i = 0; i < shapes.size(); ++i)
+      if (shapes[shapes.size() - 1 - i]->isInside(x, y, z))
+        return operations[operations.size() - 1 - i] == Operation_t::UNION;
+    return false;
+  }
+  void translate(double x, double y, double z) { for (Shape *s : shapes) s->translate(x, y, z); }
+  void rotate(double deg, Axis_t axis) { for (Shape *s : shapes) s->rotate(deg, axis); }
+  void scale(double f, Axis_t axis) { for (Shape *s : shapes) s->scale(f, axis); }
+  std::string name;
+  double delta{0.0};
+  double beta{0.0};
+  std::vector<Shape *> shapes;
+  std::vector<Operation_t> operations;
+};
+
+/** geom::Module (src/geometry.cpp:195-234): non-owning part pointers. */
+class Module {
+ public:
+  explicit Module(const char *name) : name(name) {}
+  void add(Part &part) {
+    parts.push_back(&part);
+    operations.push_back(Operation_t::UNION);
+  }
+  void difference(Part &part) {
+    if (parts.size() <= 1)
+      throw std::runtime_error("There have to be at least one part present before making difference!");
+    parts.push_back(&part);
+    operations.push_back(Operation_t::DIFFERENCE);
+  }
+  bool getXrayMatProp(double x, double y, double z, double &delta, double &beta) const {
+    delta = 0.0;
+    beta = 0.0;
+    for (size_t i = 0; i < parts.size(); ++i) {
+      const Part *p = parts[parts.size() - i - 1];
+      if (p->isInside(x, y, z)) {
+        if (operations[parts.size() - i - 1] == Operation_t::UNION) {
+          delta = p->delta;
+          beta = p->beta;
+        }
+        return true;
+      }
+    }
+    return false;
+  }
+  void translate(double x, double y, double z) { for (Part *p : parts) p->translate(x, y, z); }
+  void rotate(double deg, Axis_t axis) { for (Part *p : parts) p->rotate(deg, axis); }
+  void scale(double f, Axis_t axis) { for (Part *p : parts) p->scale(f, axis); }
+  std::string name;
+  std::vector<Part *> parts;
+  std::vector<Operation_t> operations;
+};
+}  // namespace geom
+
+/** CSGMaterial (include/materialFunction.hpp, src/materialFunction.cpp:3-18):
+ * the first module that claims a point gives its material; evaluated on the
+ * device by the CUDA 3-D solvers. */
+class CSGMaterial : public MaterialFunction {
+ public:
+  void getXrayMatProp(double x, double y, double z, double &delta, double &beta) const override {
+    delta = 0.0;
+    beta = 0.0;
+    if (isReferenceRun) return;
+    for (const geom::Module *m : modules)
+      if (m->getXrayMatProp(x, y, z, delta, beta)) return;
+  }
+  void addModule(const geom::Module &module) { modules.push_back(&module); }
+  void setReferenceRun(bool ref) { isReferenceRun = ref; }
+  std::vector<const geom::Module *> modules;
+  bool isReferenceRun{false};
 };
 
 // ------------------------------------------------------------- sources ----
@@ -451,6 +665,36 @@ class Solver2D : public Solver {
         solution(i, step) = currentSolution((unsigned)(delta * i + delta / 2.0));
   }
 
+  /** Flattens a CSGMaterial for pxp_set_material_csg. */
+  void setCsg(const CSGMaterial &cm) {
+    std::vector<pxp_csg_module> mods;
+    std::vector<pxp_csg_part> parts;
+    std::vector<pxp_csg_shape> shapes;
+    for (const geom::Module *m : cm.modules) {
+      mods.push_back({(int)parts.size(), (int)m->parts.size()});
+      for (size_t i = 0; i < m->parts.size(); ++i) {
+        const geom::Part *p = m->parts[i];
+        pxp_csg_part cp{};
+        cp.operation = m->operations[i] == geom::Operation_t::UNION ? PXP_CSG_UNION : PXP_CSG_DIFFERENCE;
+        cp.first_shape = (int)shapes.size();
+        cp.num_shapes = (int)p->shapes.size();
+        cp.delta = p->delta;
+        cp.beta = p->beta;
+        parts.push_back(cp);
+        for (size_t k = 0; k < p->shapes.size(); ++k) {
+          pxp_csg_shape cs{};
+          cs.kind = p->shapes[k]->kind();
+          cs.operation = p->operations[k] == geom::Operation_t::UNION ? PXP_CSG_UNION : PXP_CSG_DIFFERENCE;
+          std::memcpy(cs.transform, p->shapes[k]->transformation, sizeof(cs.transform));
+          p->shapes[k]->size(cs.size);
+          shapes.push_back(cs);
+        }
+      }
+    }
+    check(pxp_set_material_csg(handle, mods.data(), (int)mods.size(), parts.data(), (int)parts.size(),
+                               shapes.data(), (int)shapes.size()));
+  }
+
   void initDevice() {
     if (guide == nullptr) throw std::runtime_error("No waveguide specified!");
     if (handle == nullptr) {
@@ -624,6 +868,36 @@ class Solver3D : public Solver {
       storeSlice(step / guide->longitudinalDiscretization().downsamplingRatio);
   }
 
+  /** Flattens a CSGMaterial for pxp_set_material_csg. */
+  void setCsg(const CSGMaterial &cm) {
+    std::vector<pxp_csg_module> mods;
+    std::vector<pxp_csg_part> parts;
+    std::vector<pxp_csg_shape> shapes;
+    for (const geom::Module *m : cm.modules) {
+      mods.push_back({(int)parts.size(), (int)m->parts.size()});
+      for (size_t i = 0; i < m->parts.size(); ++i) {
+        const geom::Part *p = m->parts[i];
+        pxp_csg_part cp{};
+        cp.operation = m->operations[i] == geom::Operation_t::UNION ? PXP_CSG_UNION : PXP_CSG_DIFFERENCE;
+        cp.first_shape = (int)shapes.size();
+        cp.num_shapes = (int)p->shapes.size();
+        cp.delta = p->delta;
+        cp.beta = p->beta;
+        parts.push_back(cp);
+        for (size_t k = 0; k < p->shapes.size(); ++k) {
+          pxp_csg_shape cs{};
+          cs.kind = p->shapes[k]->kind();
+          cs.operation = p->operations[k] == geom::Operation_t::UNION ? PXP_CSG_UNION : PXP_CSG_DIFFERENCE;
+          std::memcpy(cs.transform, p->shapes[k]->transformation, sizeof(cs.transform));
+          p->shapes[k]->size(cs.size);
+          shapes.push_back(cs);
+        }
+      }
+    }
+    check(pxp_set_material_csg(handle, mods.data(), (int)mods.size(), parts.data(), (int)parts.size(),
+                               shapes.data(), (int)shapes.size()));
+  }
+
   void initDevice() {
     if (guide == nullptr) throw std::runtime_error("No waveguide specified!");
     if (handle == nullptr) {
@@ -645,12 +919,17 @@ class Solver3D : public Solver {
       check(pxp_solver_create(&p, &handle));
       if (g.material != nullptr) {
         const SphereMaterial *sm = dynamic_cast<const SphereMaterial *>(g.material);
-        if (sm == nullptr)
+        const CSGMaterial *cm = dynamic_cast<const CSGMaterial *>(g.material);
+        if (sm != nullptr) {
+          std::vector<pxp_sphere> sp;
+          for (const auto &s : sm->spheres) sp.push_back({s.cx, s.cy, s.cz, s.radius, s.delta, s.beta});
+          check(pxp_set_material_spheres(handle, sp.data(), (int)sp.size()));
+        } else if (cm != nullptr) {
+          if (!cm->isReferenceRun) setCsg(*cm);
+        } else {
           throw std::runtime_error(
-              "the CUDA 3-D solvers take a SphereMaterial (or no material)");
-        std::vector<pxp_sphere> sp;
-        for (const auto &s : sm->spheres) sp.push_back({s.cx, s.cy, s.cz, s.radius, s.delta, s.beta});
-        check(pxp_set_material_spheres(handle, sp.data(), (int)sp.size()));
+              "the CUDA 3-D solvers take a SphereMaterial, a CSGMaterial or no material");
+        }
       }
     }
     if (icPending) {

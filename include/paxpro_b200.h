@@ -110,6 +110,44 @@ int pxp_set_material_planes(pxp_solver s, const double *delta, const double *bet
  * (3-D kinds; 2-D kinds take y = 0). */
 int pxp_set_material_spheres(pxp_solver s, const pxp_sphere *spheres, int n);
 
+/* Material hook, constructive solid geometry evaluated on the device
+ * (3-D kinds): the CSGMaterial of the reference (src/materialFunction.cpp:3-13)
+ * flattened.  A point's material comes from the first module (in order)
+ * that claims it; a module scans its parts from the last to the first and
+ * the first part containing the point decides: a union part gives its
+ * (delta, beta), a difference part gives vacuum (geom::Module::
+ * getXrayMatProp, src/geometry.cpp:212-234); a part contains the point when,
+ * scanning its shapes from the last to the first, the first shape containing
+ * it was added as a union (geom::Part::isInside, src/geometry.cpp:91-108).
+ * A shape tests the point after applying its 4x4 transformation
+ * (geom::Shape::transform, src/shape.cpp:59-70): sphere sqrt(x^2+y^2+z^2) <
+ * R; box |x| < Lx/2, |y| < Ly/2, |z| < Lz/2 (strict); cylinder
+ * -h/2 < z < h/2 and sqrt(x^2+y^2) < r1 + (r2-r1)/h*(z+h/2)
+ * (src/shape.cpp:146-187).  Up to 64 modules. */
+#define PXP_SHAPE_SPHERE 0
+#define PXP_SHAPE_BOX 1
+#define PXP_SHAPE_CYLINDER 2
+#define PXP_CSG_UNION 0
+#define PXP_CSG_DIFFERENCE 1
+typedef struct {
+  int kind;             /* PXP_SHAPE_* */
+  int operation;        /* joins its part as PXP_CSG_UNION (geom::Part::add) or
+                           PXP_CSG_DIFFERENCE (geom::Part::difference) */
+  double transform[16]; /* geom::Shape::transformation, row-major 4x4 */
+  double size[3];       /* sphere: radius; box: Lx, Ly, Lz; cylinder: height, r1, r2 */
+} pxp_csg_shape;
+typedef struct {
+  int operation;        /* joins its module: geom::Module::add / difference */
+  int first_shape, num_shapes;
+  double delta, beta;   /* geom::Part::delta, beta */
+} pxp_csg_part;
+typedef struct {
+  int first_part, num_parts;
+} pxp_csg_module;
+int pxp_set_material_csg(pxp_solver s, const pxp_csg_module *modules, int nmodules,
+                         const pxp_csg_part *parts, int nparts, const pxp_csg_shape *shapes,
+                         int nshapes);
+
 /* Solver::setInitialConditions (include/solver.hpp:54,57): the field at
  * z = zmin; host array.  Resets the step counter to 1 and clears saves. */
 int pxp_set_initial_conditions(pxp_solver s, const double *field);

@@ -26,6 +26,48 @@
 
 namespace {
 
+// geom::Shape::transform (src/shape.cpp:59-70): the 4x4 matrix times
+// (x, y, z, 1), each row summed left to right.
+void csg_transform(const double *T, double &x, double &y, double &z) {
+  const double x0 = x, y0 = y, z0 = z;
+  x = T[0] * x0 + T[1] * y0 + T[2] * z0 + T[3] * 1.0;
+  y = T[4] * x0 + T[5] * y0 + T[6] * z0 + T[7] * 1.0;
+  z = T[8] * x0 + T[9] * y0 + T[10] * z0 + T[11] * 1.0;
+}
+
+// Sphere / Box / Cylinder::isInside (src/shape.cpp:146-187).
+bool csg_shape_inside(const orc_csg_shape &s, double x, double y, double z) {
+  csg_transform(s.transform, x, y, z);
+  if (s.kind == 0) {
+    double r = std::sqrt(x * x + y * y + z * z);
+    return r < s.size[0];
+  }
+  if (s.kind == 1) {
+    const double Lx = s.size[0], Ly = s.size[1], Lz = s.size[2];
+    return (x > -Lx / 2.0) && (x < Lx / 2.0) && (y > -Ly / 2.0) && (y < Ly / 2.0) &&
+           (z > -Lz / 2.0) && (z < Lz / 2.0);
+  }
+  const double height = s.size[0], r1 = s.size[1], r2 = s.size[2];
+  bool zIsInside = (z < height / 2.0) && (z > -height / 2.0);
+  if (!zIsInside) return false;
+  double slope = (r2 - r1) / height;
+  double radius = slope * (z + height / 2.0) + r1;
+  double r = std::sqrt(x * x + y * y);
+  return r < radius;
+}
+
+// geom::Part::isInside (src/geometry.cpp:91-108): shapes from the last to
+// the first; the first containing the point decides by its operation.
+bool csg_part_inside(const orc_csg_shape *shapes, const orc_csg_part &p, double x,
+                            double y, double z) {
+  for (int i = p.num_shapes - 1; i >= 0; --i) {
+    const orc_csg_shape &s = shapes[p.first_shape + i];
+    if (csg_shape_inside(s, x, y, z)) return s.operation == 0;
+  }
+  return false;
+}
+
+
 using cd = std::complex<double>;
 const double PI = std::acos(-1.0);  // src/fftSolver2D.cpp:7
 
@@ -88,6 +130,25 @@ void material_eval(const orc_material *m, const orc_grid &g, double x, double y,
           delta = sp.delta;
           beta = sp.beta;
           return;
+        }
+      }
+      return;
+    }
+    case ORC_MAT_CSG: {
+      // CSGMaterial::getXrayMatProp: the first module that claims the point
+      for (int mi = 0; mi < m->n_csg_modules; ++mi) {
+        const orc_csg_module &mod = m->csg_modules[mi];
+        // geom::Module::getXrayMatProp (src/geometry.cpp:212-234): parts
+        // from the last to the first
+        for (int pi = mod.num_parts - 1; pi >= 0; --pi) {
+          const orc_csg_part &part = m->csg_parts[mod.first_part + pi];
+          if (csg_part_inside(m->csg_shapes, part, x, y, z)) {
+            if (part.operation == 0) {
+              delta = part.delta;
+              beta = part.beta;
+            }
+            return;
+          }
         }
       }
       return;

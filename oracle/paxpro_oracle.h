@@ -42,8 +42,27 @@ enum {
   ORC_MAT_VACUUM = 0,
   ORC_MAT_WAVEGUIDE = 1, /* planar core + cladding + index-based beta ramp */
   ORC_MAT_SPHERES = 2,   /* first sphere with r^2 < R^2 wins */
-  ORC_MAT_XTABLE = 3     /* z-invariant delta/beta per x index (2-D only) */
+  ORC_MAT_XTABLE = 3,    /* z-invariant delta/beta per x index (2-D only) */
+  ORC_MAT_CSG = 4        /* CSGMaterial over geom::Module / Part / Shape */
 };
+
+/* CSGMaterial (src/materialFunction.cpp:3-13) flattened: modules in order,
+ * each a range of parts, each part a range of shapes.  kind: 0 sphere, 1
+ * box, 2 cylinder; operation: 0 union (add), 1 difference; transform: the
+ * shape's 4x4 geom::Shape::transformation, row-major; size: sphere radius /
+ * box Lx, Ly, Lz / cylinder height, r1, r2. */
+typedef struct {
+  int kind, operation;
+  double transform[16];
+  double size[3];
+} orc_csg_shape;
+typedef struct {
+  int operation, first_shape, num_shapes;
+  double delta, beta;
+} orc_csg_part;
+typedef struct {
+  int first_part, num_parts;
+} orc_csg_module;
 
 typedef struct {
   int kind;
@@ -56,6 +75,11 @@ typedef struct {
   int n_spheres;
   /* x table */
   const double *delta_table, *beta_table;
+  /* constructive solid geometry */
+  const orc_csg_module *csg_modules;
+  int n_csg_modules;
+  const orc_csg_part *csg_parts;
+  const orc_csg_shape *csg_shapes;
 } orc_material;
 
 /* Node count exactly as the reference computes it (truncating cast). */

@@ -36,10 +36,26 @@ class Material(C.Structure):
         ("ramp_points", C.c_int), ("n_transverse", C.c_int),
         ("spheres", C.POINTER(Sphere)), ("n_spheres", C.c_int),
         ("delta_table", C.POINTER(C.c_double)), ("beta_table", C.POINTER(C.c_double)),
+        ("csg_modules", C.c_void_p), ("n_csg_modules", C.c_int),
+        ("csg_parts", C.c_void_p), ("csg_shapes", C.c_void_p),
     ]
 
 
-MAT_VACUUM, MAT_WAVEGUIDE, MAT_SPHERES, MAT_XTABLE = 0, 1, 2, 3
+class CsgShape(C.Structure):
+    _fields_ = [("kind", C.c_int), ("operation", C.c_int), ("transform", C.c_double * 16),
+                ("size", C.c_double * 3)]
+
+
+class CsgPart(C.Structure):
+    _fields_ = [("operation", C.c_int), ("first_shape", C.c_int), ("num_shapes", C.c_int),
+                ("delta", C.c_double), ("beta", C.c_double)]
+
+
+class CsgModule(C.Structure):
+    _fields_ = [("first_part", C.c_int), ("num_parts", C.c_int)]
+
+
+MAT_VACUUM, MAT_WAVEGUIDE, MAT_SPHERES, MAT_XTABLE, MAT_CSG = 0, 1, 2, 3, 4
 
 
 def build() -> None:
@@ -126,6 +142,19 @@ class MaterialSpec:
             self._keep.append(arr)
             self.m.spheres = C.cast(arr, C.POINTER(Sphere))
             self.m.n_spheres = len(sph)
+        csg = kw.get("csg")
+        if csg is not None:
+            mods, parts, shapes = csg
+            cm = (CsgModule * max(len(mods), 1))(*[CsgModule(*m) for m in mods])
+            cp = (CsgPart * max(len(parts), 1))(*[CsgPart(*p) for p in parts])
+            cs = (CsgShape * max(len(shapes), 1))(
+                *[CsgShape(k, op, (C.c_double * 16)(*T), (C.c_double * 3)(*sz))
+                  for k, op, T, sz in shapes])
+            self._keep += [cm, cp, cs]
+            self.m.csg_modules = C.cast(cm, C.c_void_p)
+            self.m.csg_parts = C.cast(cp, C.c_void_p)
+            self.m.csg_shapes = C.cast(cs, C.c_void_p)
+            self.m.n_csg_modules = len(mods)
         if kw.get("delta_table") is not None:
             dt = np.ascontiguousarray(kw["delta_table"], dtype=np.float64)
             bt = np.ascontiguousarray(kw["beta_table"], dtype=np.float64)

@@ -153,6 +153,23 @@ class Solver:
         self._check(_capi.lib().pxp_set_material_spheres(self._h, arr, len(spheres)))
 
     # -- field
+    def set_material_csg(self, modules) -> None:
+        """Material from constructive solid geometry (paxpro_b200.csg Modules,
+        the reference's CSGMaterial), evaluated on the device."""
+        from . import csg as _csg
+        mods, parts, shapes = _csg.flatten(modules)
+        cm = (_capi.CsgModuleC * max(len(mods), 1))()
+        for i, m in enumerate(mods):
+            cm[i] = _capi.CsgModuleC(*m)
+        cp = (_capi.CsgPartC * max(len(parts), 1))()
+        for i, p in enumerate(parts):
+            cp[i] = _capi.CsgPartC(*p)
+        cs = (_capi.CsgShapeC * max(len(shapes), 1))()
+        for i, (kind, op, T, size) in enumerate(shapes):
+            cs[i] = _capi.CsgShapeC(kind, op, (C.c_double * 16)(*T), (C.c_double * 3)(*size))
+        self._check(_capi.lib().pxp_set_material_csg(self._h, cm, len(mods), cp, len(parts), cs,
+                                                     len(shapes)))
+
     def set_initial_conditions(self, field0: np.ndarray) -> None:
         a = np.asarray(field0, dtype=np.complex128)
         if a.shape != self.shape:

@@ -48,6 +48,20 @@ class SphereC(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("cx", "cy", "cz", "radius", "delta", "beta")]
 
 
+class CsgShapeC(C.Structure):
+    _fields_ = [("kind", C.c_int), ("operation", C.c_int), ("transform", C.c_double * 16),
+                ("size", C.c_double * 3)]
+
+
+class CsgPartC(C.Structure):
+    _fields_ = [("operation", C.c_int), ("first_shape", C.c_int), ("num_shapes", C.c_int),
+                ("delta", C.c_double), ("beta", C.c_double)]
+
+
+class CsgModuleC(C.Structure):
+    _fields_ = [("first_part", C.c_int), ("num_parts", C.c_int)]
+
+
 class PxpError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{message} (status {status})")
@@ -91,6 +105,8 @@ def lib():
         "pxp_num_saved": (C.c_int, [h, C.POINTER(C.c_int)]),
         "pxp_get_saved": (C.c_int, [h, C.c_int, d]),
         "pxp_get_post": (C.c_int, [h, C.c_int, C.c_int, d]),
+        "pxp_set_material_csg": (C.c_int, [h, C.POINTER(CsgModuleC), C.c_int, C.POINTER(CsgPartC),
+                                           C.c_int, C.POINTER(CsgShapeC), C.c_int]),
         "pxp_saved_max_abs": (C.c_int, [h, d]),
         "pxp_reset": (C.c_int, [h]),
         "pxp_current_step": (C.c_int, [h, C.POINTER(C.c_uint)]),

@@ -24,6 +24,7 @@
 #include <cmath>
 
 #include "bulk_copy.cuh"
+#include "csg.cuh"
 #include "pxp_complex.cuh"
 #include "pxp_kernels.h"
 #include "scan_solve.cuh"
@@ -36,6 +37,10 @@ __device__ unsigned int g_wait_timeouts = 0;
 
 __device__ __forceinline__ void sphere_material(const AdiHalf &h, double x, double y,
                                                 double &delta, double &beta) {
+  if (h.csg.active) {
+    csg_material(h.csg, x, y, h.z, delta, beta);
+    return;
+  }
   delta = 0.0;
   beta = 0.0;
   const int n = h.nspheres;

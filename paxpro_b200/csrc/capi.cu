@@ -80,6 +80,11 @@ struct pxp_solver_s {
   pxp::CnJob job_cn{};
   int batch_remaining = 0;                   // steps left while admitted to a batch
   std::vector<pxp_sphere> spheres;           // first-hit sphere material
+  // CSG material: device copy [modules | parts | shapes] and, per module, the
+  // z range that can contain its material (lo > hi: none; -inf/+inf: any)
+  void *d_csg = nullptr;
+  int csg_nmodules = 0, csg_nparts = 0;
+  std::vector<double> csg_zlo, csg_zhi;
   pxp::Sphere *d_spheres = nullptr;
   // host copies
   std::vector<double> h_delta, h_beta;
@@ -516,7 +521,28 @@ void active_spheres(const pxp_solver_s *h, double z, std::vector<pxp::Sphere> &o
   }
 }
 
+// Modules whose z range meets [zlo, zhi]; the others contain no point of
+// those planes, so dropping them changes no material lookup.
+unsigned long long csg_active(const pxp_solver_s *h, double zlo, double zhi) {
+  unsigned long long m = 0;
+  for (int i = 0; i < h->csg_nmodules; ++i)
+    if (h->csg_zlo[i] <= zhi && h->csg_zhi[i] >= zlo) m |= 1ull << i;
+  return m;
+}
+
+pxp::Csg csg_params(const pxp_solver_s *h, double zlo, double zhi) {
+  pxp::Csg c{};
+  if (!h->d_csg) return c;
+  c.modules = (const pxp::CsgModule *)h->d_csg;
+  c.parts = (const pxp::CsgPart *)(c.modules + h->csg_nmodules);
+  c.shapes = (const pxp::CsgShape *)(c.parts + h->csg_nparts);
+  c.nmodules = h->csg_nmodules;
+  c.active = csg_active(h, std::min(zlo, zhi), std::max(zlo, zhi));
+  return c;
+}
+
 int adi_fill_spheres(pxp_solver_s *h, pxp::AdiHalf &a, double z) {
+  a.csg = csg_params(h, z, z);
   std::vector<pxp::Sphere> act;
   active_spheres(h, z, act);
   a.nspheres = (int)act.size();
@@ -559,7 +585,7 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   a.z = get_z(h, step);
   adi_fill_spheres(h, a, a.z);
   const cd *lu = (const cd *)h->d_lu;
-  cudaError_t e = (a.nspheres == 0 && !a.use_tbc && lu)
+  cudaError_t e = (a.nspheres == 0 && !a.csg.active && !a.use_tbc && lu)
                       ? pxp::launch_adi_half_const(h->prec, a, lu, lu + n, lu + 4 * n, h->stream)
                       : pxp::launch_adi_half(h->prec, a, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "ADI x half step");
@@ -575,7 +601,7 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   a.kd2_expl = kdx2;
   a.z = get_z(h, step) + dzh;
   adi_fill_spheres(h, a, a.z);
-  e = (a.nspheres == 0 && !a.use_tbc && lu)
+  e = (a.nspheres == 0 && !a.csg.active && !a.use_tbc && lu)
           ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n, lu + 8 * n, h->stream)
           : pxp::launch_adi_half(h->prec, a, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
@@ -588,6 +614,7 @@ int adi_step(pxp_solver_s *h, unsigned step) {
 bool adi_plain_step(const pxp_solver_s *h, unsigned step, std::vector<pxp::Sphere> &tmp) {
   if (h->prob.transparent_bc || !h->d_lu || save_at(h, step)) return false;
   const double z = get_z(h, step);
+  if (csg_active(h, z, z + h->prob.z.step / 2.0)) return false;
   active_spheres(h, z, tmp);
   if (!tmp.empty()) return false;
   active_spheres(h, z + h->prob.z.step / 2.0, tmp);
@@ -753,6 +780,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     q.z1 = get_z(h, step);
     q.z0 = get_z(h, step - 1);
     slab_spheres(h, q.z0, q.z1, act);
+    q.csg = csg_params(h, q.z0, q.z1);
     q.nspheres = (int)act.size();
     if (q.nspheres <= pxp::kInlineSpheres) {
       for (int j = 0; j < q.nspheres; ++j) q.spheres[j] = act[j];
@@ -776,7 +804,8 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     const unsigned step = first + (unsigned)i;
     if (i == nsteps - 1 || save_at(h, step)) return false;
     slab_spheres(h, get_z(h, step - 1), get_z(h, step), act);
-    return act.empty();
+    return act.empty() && !csg_active(h, std::min(get_z(h, step - 1), get_z(h, step)),
+                                      std::max(get_z(h, step - 1), get_z(h, step)));
   };
   const std::vector<const void *> sig = {h->d_field, h->d_tw, kx2, tw16,
                                          (const void *)(size_t)(16 + variant)};
@@ -991,6 +1020,7 @@ int pxp_solver_destroy(pxp_solver h) {
   free_dev(h->d_job, h->stream);
   free_dev(h->d_field2, h->stream);
   free_dev(h->d_spheres, h->stream);
+  free_dev(h->d_csg, h->stream);
   free_dev(h->d_lu, h->stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1057,6 +1087,10 @@ int pxp_set_material_spheres(pxp_solver h, const pxp_sphere *spheres, int n) {
   PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
   h->spheres.assign(spheres, spheres + n);
   free_dev(h->d_spheres, h->stream);
+  free_dev(h->d_csg, h->stream);
+  h->csg_nmodules = h->csg_nparts = 0;
+  h->csg_zlo.clear();
+  h->csg_zhi.clear();
   if (n > 0) {
     std::vector<pxp::Sphere> dev(n);
     for (int i = 0; i < n; ++i)
@@ -1066,6 +1100,118 @@ int pxp_set_material_spheres(pxp_solver h, const pxp_sphere *spheres, int n) {
     if ((rc = alloc(h, (void **)&h->d_spheres, sizeof(pxp::Sphere) * n, "sphere list"))) return rc;
     if (int rc_ = h2d(h, h->d_spheres, dev.data(), sizeof(pxp::Sphere) * n)) return rc_;
   }
+  h->material_set = true;
+  return PXP_OK;
+}
+
+namespace {
+
+// World-space z range of a shape's local bounding box (the shape's matrix
+// maps world to local: local = T * world, so world = T^-1 * local).  Returns
+// false when T is not an invertible affine map (no range then: always on).
+bool shape_z_range(const pxp_csg_shape &sh, double &lo, double &hi) {
+  const double *T = sh.transform;
+  if (T[12] != 0.0 || T[13] != 0.0 || T[14] != 0.0 || T[15] != 1.0) return false;
+  const double a = T[0], b = T[1], c = T[2], d = T[4], e = T[5], f = T[6], g = T[8], h = T[9], i = T[10];
+  const double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+  if (!(std::fabs(det) > 1e-300) || !std::isfinite(det)) return false;
+  // row 2 of A^-1 (gives world z): (d h - e g, b g - a h, a e - b d) / det
+  const double r0 = (d * h - e * g) / det, r1 = (b * g - a * h) / det, r2 = (a * e - b * d) / det;
+  double ex, ey, ez;
+  if (sh.kind == PXP_SHAPE_SPHERE) {
+    ex = ey = ez = sh.size[0];
+  } else if (sh.kind == PXP_SHAPE_BOX) {
+    ex = sh.size[0] / 2; ey = sh.size[1] / 2; ez = sh.size[2] / 2;
+  } else {
+    ex = ey = std::max(std::fabs(sh.size[1]), std::fabs(sh.size[2]));
+    ez = sh.size[0] / 2;
+  }
+  lo = 1e300;
+  hi = -1e300;
+  for (int k = 0; k < 8; ++k) {
+    const double lx = (k & 1 ? ex : -ex) - T[3], ly = (k & 2 ? ey : -ey) - T[7],
+                 lz = (k & 4 ? ez : -ez) - T[11];
+    const double wz = r0 * lx + r1 * ly + r2 * lz;
+    lo = std::min(lo, wz);
+    hi = std::max(hi, wz);
+  }
+  const double margin = 1e-9 * (std::fabs(lo) + std::fabs(hi) + 1.0) + 1e-6;
+  lo -= margin;
+  hi += margin;
+  return std::isfinite(lo) && std::isfinite(hi);
+}
+
+}  // namespace
+
+int pxp_set_material_csg(pxp_solver h, const pxp_csg_module *modules, int nmodules,
+                         const pxp_csg_part *parts, int nparts, const pxp_csg_shape *shapes, int nshapes) {
+  if (h == nullptr || nmodules < 0 || nparts < 0 || nshapes < 0 ||
+      (nmodules > 0 && modules == nullptr) || (nparts > 0 && parts == nullptr) ||
+      (nshapes > 0 && shapes == nullptr))
+    return PXP_ERR_INVALID;
+  if (h->prob.kind != PXP_ADI && h->prob.kind != PXP_FFT_SOLVER_3D)
+    return h->fail(PXP_ERR_UNSUPPORTED, "CSG materials apply to the 3-D kinds");
+  if (nmodules > 64) return h->fail(PXP_ERR_UNSUPPORTED, "at most 64 CSG modules");
+  for (int m = 0; m < nmodules; ++m)
+    if (modules[m].first_part < 0 || modules[m].num_parts < 0 ||
+        modules[m].first_part + modules[m].num_parts > nparts)
+      return h->fail(PXP_ERR_INVALID, "CSG module " + std::to_string(m) + ": parts out of range");
+  for (int p = 0; p < nparts; ++p)
+    if (parts[p].first_shape < 0 || parts[p].num_shapes < 0 ||
+        parts[p].first_shape + parts[p].num_shapes > nshapes ||
+        (parts[p].operation != PXP_CSG_UNION && parts[p].operation != PXP_CSG_DIFFERENCE))
+      return h->fail(PXP_ERR_INVALID, "CSG part " + std::to_string(p) + ": bad shapes or operation");
+  for (int k = 0; k < nshapes; ++k)
+    if (shapes[k].kind < PXP_SHAPE_SPHERE || shapes[k].kind > PXP_SHAPE_CYLINDER ||
+        (shapes[k].operation != PXP_CSG_UNION && shapes[k].operation != PXP_CSG_DIFFERENCE))
+      return h->fail(PXP_ERR_INVALID, "CSG shape " + std::to_string(k) + ": bad kind or operation");
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  // z range per module: the union of its parts' union shapes' ranges (a
+  // difference shape only removes; a point outside every union shape of a
+  // module's parts is claimed by none of them)
+  std::vector<double> zlo(nmodules, 1e300), zhi(nmodules, -1e300);
+  for (int m = 0; m < nmodules; ++m)
+    for (int p = modules[m].first_part; p < modules[m].first_part + modules[m].num_parts; ++p)
+      for (int k = parts[p].first_shape; k < parts[p].first_shape + parts[p].num_shapes; ++k) {
+        if (shapes[k].operation != PXP_CSG_UNION) continue;
+        double lo, hi;
+        if (!shape_z_range(shapes[k], lo, hi)) {
+          lo = -1e300;
+          hi = 1e300;
+        }
+        zlo[m] = std::min(zlo[m], lo);
+        zhi[m] = std::max(zhi[m], hi);
+      }
+  std::vector<char> buf(sizeof(pxp::CsgModule) * nmodules + sizeof(pxp::CsgPart) * nparts +
+                        sizeof(pxp::CsgShape) * nshapes);
+  pxp::CsgModule *dm = (pxp::CsgModule *)buf.data();
+  pxp::CsgPart *dp = (pxp::CsgPart *)(dm + nmodules);
+  pxp::CsgShape *ds = (pxp::CsgShape *)(dp + nparts);
+  for (int m = 0; m < nmodules; ++m) dm[m] = {modules[m].first_part, modules[m].num_parts};
+  for (int p = 0; p < nparts; ++p)
+    dp[p] = {parts[p].delta, parts[p].beta, parts[p].operation, parts[p].first_shape, parts[p].num_shapes};
+  for (int k = 0; k < nshapes; ++k) {
+    pxp::CsgShape c{};
+    for (int j = 0; j < 12; ++j) c.m[j] = shapes[k].transform[j];
+    for (int j = 0; j < 3; ++j) c.size[j] = shapes[k].size[j];
+    c.kind = shapes[k].kind;
+    c.op = shapes[k].operation;
+    ds[k] = c;
+  }
+  free_dev(h->d_csg, h->stream);
+  h->csg_nmodules = h->csg_nparts = 0;
+  if (!buf.empty()) {
+    int rc;
+    if ((rc = alloc(h, &h->d_csg, buf.size(), "CSG material"))) return rc;
+    if ((rc = h2d(h, h->d_csg, buf.data(), buf.size()))) return rc;
+  }
+  h->csg_nmodules = nmodules;
+  h->csg_nparts = nparts;
+  h->csg_zlo = zlo;
+  h->csg_zhi = zhi;
+  // a CSG material replaces a sphere list
+  h->spheres.clear();
+  free_dev(h->d_spheres, h->stream);
   h->material_set = true;
   return PXP_OK;
 }

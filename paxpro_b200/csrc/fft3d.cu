@@ -19,6 +19,7 @@
 // The propagator's sin/cos come from pxp_sincos.h (within 1 ulp of 1.0 on
 // the argument range), exp in the refraction is CUDA's; everything else is
 // rounded as the reference rounds it.
+#include "csg.cuh"
 #include "fft_smem.cuh"
 #include "pxp_kernels.h"
 #include "pxp_sincos.h"
@@ -27,6 +28,10 @@ namespace pxp {
 
 __device__ __forceinline__ void sph_eval(const Fft3dPass &q, double x, double y, double z,
                                          double &delta, double &beta) {
+  if (q.csg.active) {
+    csg_material(q.csg, x, y, z, delta, beta);
+    return;
+  }
   delta = 0.0;
   beta = 0.0;
   const int n = q.nspheres;
@@ -91,7 +96,7 @@ __device__ __forceinline__ typename Cx<R>::T refract3(const Fft3dPass &q, typena
   const double x = __dadd_rn(q.xmin, __dmul_rn((double)ix, q.dx));
   const double y = __dadd_rn(q.ymin, __dmul_rn((double)iy, q.dy));
   double delta = 0.0, beta = 0.0;
-  if (q.nspheres > 0) step_material(q, x, y, delta, beta);
+  if (q.nspheres > 0 || q.csg.active) step_material(q, x, y, delta, beta);
   double2 u = to_d(uu);
   if (delta != 0.0 || beta != 0.0) {
     // exp(-k*(beta + i*delta)*dz)

@@ -69,6 +69,31 @@ struct Sphere {
 };
 constexpr int kInlineSpheres = 16;
 
+// Constructive solid geometry on the device (the reference's CSGMaterial
+// flattened, see pxp_set_material_csg): shapes hold rows 0-2 of their 4x4
+// transformation.  `active` marks the modules that can contain a point of
+// the planes the launch samples (the others are skipped: they claim no such
+// point); modules == nullptr or active == 0 means no CSG material.
+struct CsgShape {
+  double m[12];
+  double size[3];
+  int kind, op;
+};
+struct CsgPart {
+  double delta, beta;
+  int op, first, count;
+};
+struct CsgModule {
+  int first, count;
+};
+struct Csg {
+  const CsgModule *modules;
+  const CsgPart *parts;
+  const CsgShape *shapes;
+  int nmodules;
+  unsigned long long active;
+};
+
 // One half step of ADI (ADI::xImplicit / yImplicit,
 // src/alternatingDirectionSolver.cpp:8-134) on an n x n field.  Systems run
 // along the implicit direction ("position"); the explicit stencil couples
@@ -89,6 +114,7 @@ struct AdiHalf {
   double k;
   double xmin, dx, ymin, dy;
   double z;                // material plane of this half step
+  Csg csg;                 // CSG material (instead of spheres) when csg.active
   const Sphere *spheres_all;
   Sphere spheres[kInlineSpheres];
 };
@@ -151,6 +177,7 @@ struct Fft3dPass {
   // refraction (y pass)
   double k, dz, xmin, dx, ymin, dy, z1, z0, norm;
   int nspheres;
+  Csg csg;                 // CSG material (instead of spheres) when csg.active
   const Sphere *spheres_all;
   Sphere spheres[kInlineSpheres];
   // absorber (FFTSolver3D::absorbingBC): thickness in pixels and inverse

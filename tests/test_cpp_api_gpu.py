@@ -71,3 +71,31 @@ def test_sphere3d_example(kind):
         ref_last, ref_saves = po.adi3d_run(g, spec, u0, steps, ratio, False)
     assert _rel(last, ref_last) <= TOL
     assert _rel(slice1, ref_saves[0]) <= TOL
+
+
+@pytest.mark.parametrize("kind", ["fft3d", "adi"])
+def test_csg3d_example(kind):
+    """CSGMaterial built from geom:: shapes in C++ propagates to the oracle's
+    fields for the same geometry built by the Python classes."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from csg_geometry import geometry
+    from paxpro_b200 import csg
+    exe = build("csg3d")
+    n, steps = 128, 7
+    out = os.path.join(OUT, f"csg_{kind}.bin")
+    r = subprocess.run([exe, kind, str(n), str(steps), out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    data = np.fromfile(out, dtype=np.complex128)
+    last = data[:n * n].reshape((n, n), order="F")
+    slice1 = data[n * n:2 * n * n].reshape((n, n), order="F")
+    g = po.grid(-500.0, 500.0, _dx(n, 1000.0), 0.0, steps * 1000.0, 1000.0, wl.K)
+    spec = po.MaterialSpec(po.MAT_CSG, csg=csg.flatten(geometry()))
+    u0 = np.ones((n, n), dtype=np.complex128, order="F")
+    if kind == "fft3d":
+        ref_last, ref_saves = po.fft3d_run(g, spec, u0, steps, 1)
+    else:
+        ref_last, ref_saves = po.adi3d_run(g, spec, u0, steps, 1, False)
+    assert _rel(last, ref_last) <= TOL
+    assert _rel(slice1, ref_saves[0]) <= TOL
+    assert np.std(np.abs(last)) > 1e-4

@@ -42,7 +42,9 @@ np.save(out, np.stack(res))
 
 def _run(kind, n, nsteps, graphs, tmp_path):
     out = str(tmp_path / f"{kind}_{n}_{graphs}.npy")
-    env = dict(os.environ, PXP_STEP_GRAPHS="1" if graphs else "0")
+    # the FFT3D launch variant is pinned: each process would otherwise time
+    # the variants itself, and radix 8 and radix 16 round differently
+    env = dict(os.environ, PXP_STEP_GRAPHS="1" if graphs else "0", PXP_FFT3D_VARIANT="1")
     subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT), kind, str(n), str(nsteps), out],
                    check=True, env=env, timeout=600)
     return np.load(out)
