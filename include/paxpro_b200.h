@@ -202,6 +202,50 @@ int pxp_get_post(pxp_solver s, int quantity, int slot, double *out);
  * maximum by modulus). */
 int pxp_saved_max_abs(pxp_solver s, double *max_abs);
 
+/* post::FarField (src/farFieldPost.cpp:22-62, 141-247; include/postProcessMod.hpp:68-123)
+ * of the last solution, computed on the device.
+ *   2-D kinds: the exit field centred in a line of pad_length entries filled
+ *     with pad_value (ParaxialSimulation::setFarFieldPadValue; the bare field
+ *     when pad_length is below Nx), |FFT| / sqrt(L), fftshift, the angular
+ *     window along x: rows = window length, cols = 1.  `padding` and the
+ *     export and reference fields are not used (the reference's 2-D result
+ *     does not use them).
+ *   3-D kinds: L = max(pad_length, Ny, Nx); the field minus the reference
+ *     (when subtract_reference; see pxp_set_reference); columns padded to L
+ *     (zero or constant padding), transformed, fftshifted and cut to the
+ *     window along y; then the conjugated rows of that (Armadillo's .t() of
+ *     a complex row) likewise along x; |.|^2 / L; then
+ *     PostProcessingModule::resizeMatrix (src/postProcessing.cpp:29-49) to
+ *     export_rows x export_cols when both are set and both smaller.
+ * The window of an axis is farFieldAngleToIndx(phi_min) ..
+ * farFieldAngleToIndx(phi_max) (:78-101) with that axis' step.  Output:
+ * rows x cols doubles, column-major (an arma::mat), shape from
+ * pxp_farfield_shape.  PXP_PAD_LINEAR_FIT (GSL fits, marked untested in the
+ * reference) and L above 2^22 return PXP_ERR_UNSUPPORTED; an empty window
+ * (phi_max below phi_min) PXP_ERR_INVALID. */
+#define PXP_PAD_ZERO 0
+#define PXP_PAD_LINEAR_FIT 1
+#define PXP_PAD_CONSTANT 2
+typedef struct pxp_farfield_params {
+  unsigned pad_length;       /* FarField::setPadLength (default 0) */
+  double phi_min, phi_max;   /* FarField::setAngleRange, degrees (-90, 90) */
+  int padding;               /* FarField::setPadding, 3-D (PXP_PAD_ZERO) */
+  double pad_value_re, pad_value_im; /* 2-D padded entries (0) */
+  unsigned export_rows, export_cols; /* setExportDimensions, 3-D (0, 0: none) */
+  int subtract_reference;    /* FarField::setReference, 3-D (0) */
+} pxp_farfield_params;
+/* Fills pxp_farfield_params with the reference's defaults. */
+void pxp_farfield_defaults(pxp_farfield_params *p);
+int pxp_farfield_shape(pxp_solver s, const pxp_farfield_params *p, unsigned *rows, unsigned *cols);
+int pxp_farfield(pxp_solver s, const pxp_farfield_params *p, double *out);
+/* The field FarField subtracts (GenericScattering's reference run,
+ * src/genericScattering.cpp:160-178): a host array in the layout of
+ * pxp_get_last_solution (Nx*Ny complex128), or NULL to clear. */
+int pxp_set_reference(pxp_solver s, const double *field);
+/* The same, from another handle's current field on the same device (same
+ * grid size), copied on the device. */
+int pxp_set_reference_from(pxp_solver s, pxp_solver src);
+
 /* Solver::reset (include/solver.hpp:30): step counter back to 1. */
 int pxp_reset(pxp_solver s);
 

@@ -257,6 +257,37 @@ class Solver:
         self._check(_capi.lib().pxp_saved_max_abs(self._h, C.byref(v)))
         return v.value
 
+    def farfield(self, pad_length: int = 0, phi_min: float = -90.0, phi_max: float = 90.0,
+                 padding: int = _capi.PAD_ZERO, pad_value: complex = 0.0,
+                 export_dims: tuple = (0, 0), subtract_reference: bool = False) -> np.ndarray:
+        """post::FarField of the last solution, computed on the device: a
+        vector for the 2-D kinds, a (rows, cols) matrix for the 3-D kinds
+        (see pxp_farfield in include/paxpro_b200.h)."""
+        pv = complex(pad_value)
+        p = _capi.FarFieldParams(int(pad_length), float(phi_min), float(phi_max), int(padding),
+                                 pv.real, pv.imag, int(export_dims[0]), int(export_dims[1]),
+                                 1 if subtract_reference else 0)
+        r, c = C.c_uint(), C.c_uint()
+        self._check(_capi.lib().pxp_farfield_shape(self._h, C.byref(p), C.byref(r), C.byref(c)))
+        out = np.empty(r.value * c.value, dtype=np.float64)
+        self._check(_capi.lib().pxp_farfield(self._h, C.byref(p), _dptr(out)))
+        return out.reshape((r.value, c.value), order="F") if self.three_d else out
+
+    def set_reference(self, field) -> None:
+        """The field the 3-D far field subtracts: an array of the solution's
+        shape, another Solver (its current field, copied on the device) or
+        None to clear."""
+        if field is None:
+            self._check(_capi.lib().pxp_set_reference(self._h, None))
+        elif isinstance(field, Solver):
+            self._check(_capi.lib().pxp_set_reference_from(self._h, field._h))
+        else:
+            a = np.asarray(field, dtype=np.complex128)
+            if a.shape != self.shape:
+                raise ValueError(f"reference shape {a.shape} != {self.shape}")
+            flat = np.ascontiguousarray(a.reshape(-1, order="F"))
+            self._check(_capi.lib().pxp_set_reference(self._h, _dptr(flat.view(np.float64))))
+
     def reset(self) -> None:
         self._check(_capi.lib().pxp_reset(self._h))
 

@@ -62,6 +62,16 @@ class CsgModuleC(C.Structure):
     _fields_ = [("first_part", C.c_int), ("num_parts", C.c_int)]
 
 
+PAD_ZERO, PAD_LINEAR_FIT, PAD_CONSTANT = 0, 1, 2
+
+
+class FarFieldParams(C.Structure):
+    _fields_ = [("pad_length", C.c_uint), ("phi_min", C.c_double), ("phi_max", C.c_double),
+                ("padding", C.c_int), ("pad_value_re", C.c_double), ("pad_value_im", C.c_double),
+                ("export_rows", C.c_uint), ("export_cols", C.c_uint),
+                ("subtract_reference", C.c_int)]
+
+
 class PxpError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{message} (status {status})")
@@ -108,6 +118,12 @@ def lib():
         "pxp_set_material_csg": (C.c_int, [h, C.POINTER(CsgModuleC), C.c_int, C.POINTER(CsgPartC),
                                            C.c_int, C.POINTER(CsgShapeC), C.c_int]),
         "pxp_saved_max_abs": (C.c_int, [h, d]),
+        "pxp_farfield_defaults": (None, [C.POINTER(FarFieldParams)]),
+        "pxp_farfield_shape": (C.c_int, [h, C.POINTER(FarFieldParams), C.POINTER(C.c_uint),
+                                         C.POINTER(C.c_uint)]),
+        "pxp_farfield": (C.c_int, [h, C.POINTER(FarFieldParams), d]),
+        "pxp_set_reference": (C.c_int, [h, d]),
+        "pxp_set_reference_from": (C.c_int, [h, h]),
         "pxp_reset": (C.c_int, [h]),
         "pxp_current_step": (C.c_int, [h, C.POINTER(C.c_uint)]),
         "pxp_shape": (C.c_int, [h, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),

@@ -86,6 +86,8 @@ struct pxp_solver_s {
   int csg_nmodules = 0, csg_nparts = 0;
   std::vector<double> csg_zlo, csg_zhi;
   pxp::Sphere *d_spheres = nullptr;
+  // field the far field subtracts (complex128, npts; null when not set)
+  void *d_ref = nullptr;
   // host copies
   std::vector<double> h_delta, h_beta;
   int plane_first = 1, plane_count = 0;  // per-step material planes (0 = z-invariant)
@@ -1022,6 +1024,7 @@ int pxp_solver_destroy(pxp_solver h) {
   free_dev(h->d_spheres, h->stream);
   free_dev(h->d_csg, h->stream);
   free_dev(h->d_lu, h->stream);
+  free_dev(h->d_ref, h->stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return PXP_OK;
@@ -1403,6 +1406,286 @@ int pxp_saved_max_abs(pxp_solver h, double *max_abs) {
   if (e != cudaSuccess) return h->cuda_fail(e, "max |u| over the saved fields");
   std::memcpy(max_abs, &bits, sizeof(double));
   return PXP_OK;
+}
+
+// ---- far field -------------------------------------------------------------
+namespace {
+
+// FarField::farFieldAngleToIndx (src/farFieldPost.cpp:78-101).
+unsigned ff_angle_index(double angle, unsigned size, double k, double step) {
+  const double angle_rad = angle * PI / 180.0;
+  const double v = size * k * step * std::sin(angle_rad) / (2.0 * PI);
+  // int conversion truncates; a value beyond int range is past either end
+  if (!(std::fabs(v) < 2147483647.0)) return angle > 0.0 ? size - 1 : 0;
+  const int n = (int)v;
+  if ((unsigned)std::abs(n) >= size / 2) return angle > 0.0 ? size - 1 : 0;
+  return (unsigned)(n + (int)(size / 2));
+}
+
+// Device tables of the far field, shared like the solver tables: kind 4 the
+// L-entry table exp(-2 pi i m / L), kind 5 the Stockham twiddles of length q.
+int ff_table(pxp_solver_s *h, int kind, long long len, const double2 **out) {
+  TableKey key{h->prob.device, kind, (unsigned)len, 0.0, 0.0, 0.0};
+  std::lock_guard<std::mutex> lk(g_table_mutex);
+  auto it = g_tables.find(key);
+  if (it == g_tables.end()) {
+    std::vector<cd> t;
+    if (kind == 5) {
+      t = twiddles((int)len);
+    } else {
+      t.resize((size_t)len);
+      const long double pi_l = 3.141592653589793238462643383279502884L;
+      for (long long m = 0; m < len; ++m) {
+        const long double a = -2.0L * pi_l * (long double)m / (long double)len;
+        t[(size_t)m] = cd((double)cosl(a), (double)sinl(a));
+      }
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, sizeof(cd) * t.size()) != cudaSuccess) {
+      cudaGetLastError();
+      return h->fail(PXP_ERR_NOMEM, "far-field table allocation");
+    }
+    cudaError_t e = cudaMemcpy(p, t.data(), sizeof(cd) * t.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return h->cuda_fail(e, "far-field table upload");
+    it = g_tables.emplace(key, p).first;
+  }
+  *out = (const double2 *)it->second;
+  return PXP_OK;
+}
+
+struct FfPlan {
+  bool three_d = false;
+  long long L = 0;
+  unsigned y0 = 0, y1 = 0, x0 = 0, x1 = 0;  // windows (3-D: y along columns, x along rows)
+  unsigned rows = 0, cols = 0;              // result before resizing
+  unsigned out_rows = 0, out_cols = 0;      // returned shape
+  bool resize = false;
+};
+
+int ff_plan(pxp_solver_s *h, const pxp_farfield_params *p, FfPlan &f) {
+  if (p == nullptr) return h->fail(PXP_ERR_INVALID, "far-field parameters missing");
+  f.three_d = h->prob.kind == PXP_FFT_SOLVER_3D || h->prob.kind == PXP_ADI;
+  const double k = h->prob.wavenumber;
+  const long long n = h->nx;
+  if (!f.three_d) {
+    f.L = p->pad_length < n ? n : p->pad_length;
+  } else {
+    if (p->padding == PXP_PAD_LINEAR_FIT)
+      return h->fail(PXP_ERR_UNSUPPORTED, "linear-fit padding is not provided");
+    if (p->padding != PXP_PAD_ZERO && p->padding != PXP_PAD_CONSTANT)
+      return h->fail(PXP_ERR_INVALID, "unknown far-field padding");
+    f.L = std::max<long long>({(long long)p->pad_length, (long long)h->ny, n});
+  }
+  if (f.L > (1LL << 22)) return h->fail(PXP_ERR_UNSUPPORTED, "far-field pad length above 2^22");
+  const unsigned L = (unsigned)f.L;
+  f.x0 = ff_angle_index(p->phi_min, L, k, h->prob.x.step);
+  f.x1 = ff_angle_index(p->phi_max, L, k, h->prob.x.step);
+  if (f.x1 < f.x0) return h->fail(PXP_ERR_INVALID, "empty far-field angular range");
+  if (!f.three_d) {
+    f.rows = f.out_rows = f.x1 - f.x0 + 1;
+    f.cols = f.out_cols = 1;
+    return PXP_OK;
+  }
+  f.y0 = ff_angle_index(p->phi_min, L, k, h->prob.y.step);
+  f.y1 = ff_angle_index(p->phi_max, L, k, h->prob.y.step);
+  if (f.y1 < f.y0) return h->fail(PXP_ERR_INVALID, "empty far-field angular range");
+  f.rows = f.y1 - f.y0 + 1;
+  f.cols = f.x1 - f.x0 + 1;
+  f.resize = p->export_rows != 0 && p->export_cols != 0 && p->export_rows < f.rows &&
+             p->export_cols < f.cols;
+  f.out_rows = f.resize ? p->export_rows : f.rows;
+  f.out_cols = f.resize ? p->export_cols : f.cols;
+  return PXP_OK;
+}
+
+// The pruned transform unless computing the kept outputs directly is cheaper.
+// PXP_FARFIELD_PATH=direct or =pruned pins the choice (the pruned transform
+// where the length allows it).
+int ff_choose_q(long long n, long long L, long long window) {
+  const int q = pxp::farfield_pruned_q(n, L);
+  if (q == 0) return 0;
+  if (const char *v = std::getenv("PXP_FARFIELD_PATH")) {
+    if (std::strcmp(v, "direct") == 0) return 0;
+    if (std::strcmp(v, "pruned") == 0) return q;
+  }
+  int lg = 0;
+  while ((1 << lg) < q) ++lg;
+  const long long passes = std::min(L / q, window);
+  return n * window < passes * q * lg ? 0 : q;
+}
+
+}  // namespace
+
+void pxp_farfield_defaults(pxp_farfield_params *p) {
+  if (p == nullptr) return;
+  *p = pxp_farfield_params{};
+  p->phi_min = -90.0;
+  p->phi_max = 90.0;
+  p->padding = PXP_PAD_ZERO;
+}
+
+int pxp_farfield_shape(pxp_solver h, const pxp_farfield_params *p, unsigned *rows, unsigned *cols) {
+  if (h == nullptr) return PXP_ERR_INVALID;
+  FfPlan f;
+  if (int rc = ff_plan(h, p, f)) return rc;
+  if (rows) *rows = f.out_rows;
+  if (cols) *cols = f.out_cols;
+  return PXP_OK;
+}
+
+int pxp_farfield(pxp_solver h, const pxp_farfield_params *p, double *out) {
+  if (h == nullptr || out == nullptr) return PXP_ERR_INVALID;
+  FfPlan f;
+  if (int rc = ff_plan(h, p, f)) return rc;
+  if (!h->ic_set) return h->fail(PXP_ERR_INVALID, "no field: set the initial conditions first");
+  if (f.three_d && p->subtract_reference && h->d_ref == nullptr)
+    return h->fail(PXP_ERR_INVALID, "no reference field set");
+  if (int rc = check_waits(h)) return rc;
+  const double2 *wL = nullptr;
+  if (int rc = ff_table(h, 4, f.L, &wL)) return rc;
+  cudaStream_t s = h->stream;
+  const bool c64 = h->prec != pxp::kFP64;
+  std::vector<void *> tmp;
+  auto release = [&]() {
+    for (void *t : tmp) cudaFreeAsync(t, s);
+  };
+  auto dalloc = [&](size_t bytes) -> void * {
+    void *q = nullptr;
+    if (cudaMallocAsync(&q, bytes, s) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    tmp.push_back(q);
+    return q;
+  };
+  auto lines_for = [&](long long n, long long window, int *q, const double2 **twq) -> int {
+    *q = ff_choose_q(n, f.L, window);
+    *twq = nullptr;
+    if (*q) return ff_table(h, 5, *q, twq);
+    return PXP_OK;
+  };
+  cudaError_t e = cudaSuccess;
+  double *d_res = nullptr;
+  const size_t out_elems = (size_t)f.out_rows * f.out_cols;
+  if (!f.three_d) {
+    pxp::FarFieldLines ln{};
+    ln.in = h->d_field;
+    ln.in_c64 = c64;
+    ln.line_stride = h->nx;
+    ln.n = (int)h->nx;
+    ln.nlines = 1;
+    ln.pad_value = (p->pad_length < h->nx) ? make_double2(0.0, 0.0)
+                                           : make_double2(p->pad_value_re, p->pad_value_im);
+    ln.L = f.L;
+    ln.i0 = f.x0;
+    ln.i1 = f.x1;
+    ln.mode = 2;
+    ln.divisor = std::sqrt((double)f.L);
+    ln.out_stride = 1;
+    ln.wL = wL;
+    int q;
+    if (int rc = lines_for(ln.n, f.rows, &q, &ln.twQ)) return rc;
+    d_res = (double *)dalloc(sizeof(double) * out_elems);
+    if (d_res == nullptr) return h->fail(PXP_ERR_NOMEM, "far-field buffers");
+    ln.out = d_res;
+    e = pxp::launch_farfield_lines(ln, q, s);
+  } else {
+    const unsigned rows = h->ny, cols = h->nx;
+    if (p->padding == PXP_PAD_CONSTANT && rows != cols)
+      return h->fail(PXP_ERR_UNSUPPORTED, "constant padding needs a square field");
+    double2 *d_t = (double2 *)dalloc(sizeof(double2) * (size_t)f.rows * cols);
+    d_res = (double *)dalloc(sizeof(double) * (size_t)f.rows * f.cols);
+    double *d_small = f.resize ? (double *)dalloc(sizeof(double) * out_elems) : nullptr;
+    if (d_t == nullptr || d_res == nullptr || (f.resize && d_small == nullptr)) {
+      release();
+      return h->fail(PXP_ERR_NOMEM, "far-field buffers");
+    }
+    // columns, cut along y -> d_t[(i - y0) * cols + c]
+    pxp::FarFieldLines a{};
+    a.in = h->d_field;
+    a.in_c64 = c64;
+    a.ref = p->subtract_reference ? (const double2 *)h->d_ref : nullptr;
+    a.line_stride = rows;
+    a.n = (int)rows;
+    a.nlines = cols;
+    a.pad_const = p->padding == PXP_PAD_CONSTANT;
+    a.L = f.L;
+    a.i0 = f.y0;
+    a.i1 = f.y1;
+    a.mode = 0;
+    a.out = d_t;
+    a.out_stride = cols;
+    a.wL = wL;
+    int qa;
+    if (int rc = lines_for(a.n, f.rows, &qa, &a.twQ)) {
+      release();
+      return rc;
+    }
+    e = pxp::launch_farfield_lines(a, qa, s);
+    // conjugated rows, cut along x -> d_res[r + (i - x0) * rows], |X|^2 / L
+    pxp::FarFieldLines b{};
+    b.in = d_t;
+    b.line_stride = cols;
+    b.n = (int)cols;
+    b.nlines = f.rows;
+    b.conj_in = 1;
+    b.pad_const = a.pad_const;
+    b.L = f.L;
+    b.i0 = f.x0;
+    b.i1 = f.x1;
+    b.mode = 1;
+    b.divisor = (double)f.L;
+    b.out = d_res;
+    b.out_stride = f.rows;
+    b.wL = wL;
+    int qb;
+    if (int rc = lines_for(b.n, f.cols, &qb, &b.twQ)) {
+      release();
+      return rc;
+    }
+    if (e == cudaSuccess) e = pxp::launch_farfield_lines(b, qb, s);
+    if (e == cudaSuccess && f.resize) {
+      const double dX = (double)f.cols / ((double)p->export_cols + 1.0);
+      const double dY = (double)f.rows / ((double)p->export_rows + 1.0);
+      e = pxp::launch_resize(d_res, f.rows, d_small, (int)p->export_rows, (int)p->export_cols, dY,
+                             dX, s);
+      d_res = d_small;
+    }
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, d_res, sizeof(double) * out_elems, cudaMemcpyDeviceToHost, s);
+  release();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e == cudaSuccess ? PXP_OK : h->cuda_fail(e, "far field");
+}
+
+int pxp_set_reference(pxp_solver h, const double *field) {
+  if (h == nullptr) return PXP_ERR_INVALID;
+  if (field == nullptr) {
+    free_dev(h->d_ref, h->stream);
+    return PXP_OK;
+  }
+  if (h->d_ref == nullptr)
+    if (int rc = alloc(h, &h->d_ref, sizeof(cd) * h->npts, "reference field")) return rc;
+  return h2d(h, h->d_ref, field, sizeof(cd) * h->npts);
+}
+
+int pxp_set_reference_from(pxp_solver h, pxp_solver src) {
+  if (h == nullptr || src == nullptr) return PXP_ERR_INVALID;
+  if (src->npts != h->npts || src->prob.device != h->prob.device)
+    return h->fail(PXP_ERR_INVALID, "reference handle has another grid size or device");
+  if (!src->ic_set) return h->fail(PXP_ERR_INVALID, "reference handle holds no field");
+  if (int rc = check_waits(src)) return rc;
+  if (h->d_ref == nullptr)
+    if (int rc = alloc(h, &h->d_ref, sizeof(cd) * h->npts, "reference field")) return rc;
+  // the source's pending steps finish before this handle's stream reads its field
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(src->stream));
+  cudaError_t e = src->prec == pxp::kFP64
+                      ? cudaMemcpyAsync(h->d_ref, src->d_field, sizeof(cd) * h->npts,
+                                        cudaMemcpyDeviceToDevice, h->stream)
+                      : pxp::launch_widen(src->d_field, h->d_ref, h->npts, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? PXP_OK : h->cuda_fail(e, "copying the reference field");
 }
 
 int pxp_reset(pxp_solver h) {

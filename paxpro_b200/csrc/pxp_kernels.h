@@ -148,6 +148,42 @@ cudaError_t launch_post(Precision p, const void *field, double *out, long long n
 cudaError_t launch_max_abs(Precision p, const void *field, long long n, unsigned long long *result,
                            cudaStream_t s);
 
+// Lines of a far-field transform (farfield.cu): line l, entry j at
+// in[l * line_stride + j] (complex64 when in_c64, else complex128), minus
+// ref (complex128, same layout) when ref is set, conjugated when conj_in;
+// padded to L entries with pad_value (or, when pad_const, with the line's
+// entry 0).  Kept: outputs i0..i1 of the fftshifted transform, written to
+// out[l + (i - i0) * out_stride] as complex128 (mode 0), |X|^2 / divisor
+// (mode 1) or |X| / divisor (mode 2).  wL: L entries exp(-2 pi i m / L);
+// twQ: Stockham twiddles of the sub-transform length.
+struct FarFieldLines {
+  const void *in;
+  const double2 *ref;
+  long long line_stride;
+  int in_c64, conj_in, pad_const, mode;
+  int n;
+  long long nlines;
+  double2 pad_value;
+  long long L, i0, i1;
+  void *out;
+  long long out_stride;
+  double divisor;
+  const double2 *wL;
+  const double2 *twQ;
+};
+
+// Sub-transform length of the pruned transform for lines of n entries
+// padded to L, or 0 when L is not a power of two or n needs more than 8192
+// (the direct DFT then runs).
+int farfield_pruned_q(long long n, long long L);
+// q: farfield_pruned_q's choice, or 0 for the direct DFT.
+cudaError_t launch_farfield_lines(const FarFieldLines &p, int q, cudaStream_t s);
+// resizeMatrix of a column-major rows-row matrix to er x ec.
+cudaError_t launch_resize(const double *in, long long rows, double *out, int er, int ec, double dY,
+                          double dX, cudaStream_t s);
+// complex64 -> complex128, n entries.
+cudaError_t launch_widen(const void *in, void *out, long long n, cudaStream_t s);
+
 // Kernel waits on the current device that ran out (bounded mbarrier waits),
 // read on stream s (synchronises s).
 unsigned wait_timeouts(cudaStream_t s);
