@@ -13,13 +13,19 @@
 // Errors surface as std::runtime_error, as in the reference
 // (src/solver.cpp:5-28).
 //
+// Also here: post::FarField (computed on the device), Cladding,
+// WaveGuideFDSimulation, CurvedWaveGuideFD with post::Transmittivity (its
+// per-step integrals fused into the step kernels) and GenericScattering.
+//
 // Not provided (no counterpart on the GPU path, or a third-party dependency
-// this build does not have): HDF5 save (save() throws), post-processing
-// modules, VISA visualisation and the VISA longitudinal low-pass filter
-// (solve() requires disableLongitudinalFilter() when the longitudinal
-// downsampling ratio is above 1).  The 3-D solvers take a SphereMaterial, a
-// CSGMaterial over geom::Module / Part / Shape (evaluated on the device), or
-// no material.
+// this build does not have): HDF5 save (save() throws), the other
+// post-processing modules (the Python package has them), VISA visualisation
+// and the VISA longitudinal low-pass filter (solve() requires
+// disableLongitudinalFilter() when the longitudinal downsampling ratio is
+// above 1), the waveguides' border tracker, control files and eigenmode
+// projections, the projection solver.  The 3-D solvers take a
+// SphereMaterial, a CSGMaterial over geom::Module / Part / Shape (evaluated
+// on the device), or no material.
 #pragma once
 #include <algorithm>
 #include <cmath>
@@ -437,6 +443,8 @@ class Solver {
   virtual void updateDimensionsOfArrays() {}
   /** Precision of the CUDA solver: PXP_FP64 (plain) or PXP_FP32 (served). */
   void setPrecision(int p) { precision = p; }
+  /** The C-ABI handle behind this solver (null before the first step). */
+  pxp_solver nativeHandle() const { return handle; }
 
  protected:
   Dimension_t dim;
@@ -562,6 +570,28 @@ class ParaxialSimulation {
     throw std::runtime_error("HDF5 export is not available in this build");
   }
   const Solver &getSolver() const { return *solver; }
+  Solver &getSolver() { return *solver; }
+
+  /** True when getXrayMatProp describes a medium (a material function, or
+   * a simulation that overrides getXrayMatProp). */
+  virtual bool hasMaterial() const { return material != nullptr; }
+  /** True when delta and beta do not depend on z. */
+  virtual bool materialZInvariant() const { return material == nullptr || material->zInvariant(); }
+
+  /** src/paraxialSimulation.cpp:215-219 (conversions truncate). */
+  void closestIndex(double x, double z, unsigned int &ix, unsigned int &iz) const {
+    ix = (unsigned int)((x - xDisc.min) / xDisc.step);
+    iz = (unsigned int)((z - zDisc.min) / zDisc.step);
+  }
+  /** Far-field parameters (include/farFieldParameters.hpp). */
+  void setFarFieldPadValue(double padValue) { farPadValue = padValue; }
+  void setFarFieldAngleRange(double phiMin, double phiMax) {
+    farPhiMin = phiMin;
+    farPhiMax = phiMax;
+  }
+  /** Value of the padded entries of the 2-D far field
+   * (include/paraxialSimulation.hpp:174). */
+  virtual double padExitField(double, double) const { return farPadValue; }
 
   std::string description{""};
   const MaterialFunction *material{nullptr};
@@ -572,6 +602,7 @@ class ParaxialSimulation {
   double wavenumber{1.0};
   std::string name;
   const ParaxialSource *src{nullptr};
+  double farPadValue{0.0}, farPhiMin{-90.0}, farPhiMax{90.0};
 };
 
 /** Base of the 2-D (one transverse dimension) solvers, include/solver2D.hpp. */
@@ -602,6 +633,28 @@ class Solver2D : public Solver {
   }
   void setBoundaryCondition(BC_t bc) { boundaryCondition = bc; }
   void disableLongitudinalFilter() { longitudinalFilterDisabled = true; }
+
+  /** Per-step flux windows (pxp_set_flux_windows): the step kernels sum
+   * |u|^2 with trapezoid weights over [start[k], end[k]] after step
+   * first + k. */
+  void setFluxWindows(unsigned first, const std::vector<unsigned> &start,
+                      const std::vector<unsigned> &end) {
+    initDevice();
+    if (start.size() != end.size()) throw std::invalid_argument("flux windows: sizes differ");
+    check(pxp_set_flux_windows(handle, (int)first, (int)start.size(), start.data(), end.data()));
+  }
+  std::vector<double> getFlux(unsigned first, unsigned count) const {
+    std::vector<double> out(count);
+    check(pxp_get_flux(handle, (int)first, (int)count, out.data()));
+    return out;
+  }
+  /** The same sum over the current field. */
+  double fieldFlux(unsigned start, unsigned end) {
+    initDevice();
+    double v = 0.0;
+    check(pxp_field_flux(handle, start, end, &v));
+    return v;
+  }
 
   /** Solver2D::step (src/solver2D.cpp:243-250): one step, field copied back. */
   void step() override {
@@ -711,9 +764,8 @@ class Solver2D : public Solver {
       p.transparent_bc = boundaryCondition == BC_t::TRANSPARENT;
       p.save_every = 1;
       check(pxp_solver_create(&p, &handle));
-      const MaterialFunction *m = g.material;
-      materialPlanes = m != nullptr && !m->zInvariant();
-      if (m != nullptr && !materialPlanes) {
+      materialPlanes = g.hasMaterial() && !g.materialZInvariant();
+      if (g.hasMaterial() && !materialPlanes) {
         std::vector<double> d(Nx), b(Nx);
         for (unsigned i = 0; i < Nx; ++i) g.getXrayMatProp(g.getX(i), 0.0, d[i], b[i]);
         check(pxp_set_material_table(handle, d.data(), b.data(), Nx));
@@ -977,4 +1029,367 @@ class ADI : public Solver3D {
     else if (tbc != useTBC)
       throw std::runtime_error("useTBC changed after the first step");
   }
+};
+
+// ---------------------------------------------------- post-processing ----
+namespace post {
+
+/** post::FarField (include/postProcessMod.hpp:68-123, src/farFieldPost.cpp),
+ * computed on the device by pxp_farfield. */
+class FarField {
+ public:
+  enum class Pad_t { ZERO, LINEAR_FIT, CONSTANT };
+  void setPadding(Pad_t padType) { padding = padType; }
+  void setPadLength(unsigned int pad) { signalLength = pad; }
+  void setReference(const arma::cx_mat &ref) { reference = &ref; }
+  void setAngleRange(double angMin, double angMax) {
+    phiMin = angMin;
+    phiMax = angMax;
+  }
+  void linkParaxialSim(const ParaxialSimulation &simulation) { sim = &simulation; }
+  double getMaxScatteringAngle() const { return phiMax; }
+  double getMinScatteringAngle() const { return phiMin; }
+  /** PostProcessingModule::setExportDimensions (src/postProcessing.cpp:51-56) */
+  void setExportDimensions(unsigned int nrows, unsigned int ncols) {
+    exportRows = nrows;
+    exportCols = ncols;
+    resizeMatrices = true;
+  }
+  /** src/farFieldPost.cpp:323-333 */
+  void verifyConsistentAngles(double dx, double dy, double wavenumber) const {
+    double d = dx > dy ? dy : dx;
+    double PI = std::acos(-1.0);
+    double qmax = PI / d;
+    double alphaMax = 2.0 * std::asin(qmax / wavenumber);
+    if (alphaMax * 180.0 / PI < phiMax)
+      throw std::runtime_error("The specified scattering angle is to large. Increase the spatial resolution!");
+  }
+  /** Amplitude of the far field of a 2-D solver (:22-62). */
+  void result(const Solver &solver, arma::vec &res) {
+    pxp_farfield_params p = params();
+    p.pad_value_re = sim ? sim->padExitField(0.0, 0.0) : 0.0;
+    run(solver, p, res);
+  }
+  /** Far field of a 3-D solver (:141-247). */
+  void result(const Solver &solver, arma::mat &res) {
+    pxp_farfield_params p = params();
+    pxp_solver h = solver.nativeHandle();
+    if (h == nullptr) throw std::runtime_error("FarField: the solver has not run");
+    if (reference != nullptr) {
+      if (pxp_set_reference(h, reinterpret_cast<const double *>(reference->memptr())) != PXP_OK)
+        throw std::runtime_error("FarField: the reference does not match the solver's grid");
+      p.subtract_reference = 1;
+    }
+    run(solver, p, res);
+  }
+
+ private:
+  unsigned int signalLength{0};
+  double phiMin{-90.0};
+  double phiMax{90.0};
+  const ParaxialSimulation *sim{nullptr};
+  Pad_t padding{Pad_t::ZERO};
+  const arma::cx_mat *reference{nullptr};
+  unsigned int exportRows{0}, exportCols{0};
+  bool resizeMatrices{false};
+
+  pxp_farfield_params params() const {
+    pxp_farfield_params p;
+    pxp_farfield_defaults(&p);
+    p.pad_length = signalLength;
+    p.phi_min = phiMin;
+    p.phi_max = phiMax;
+    p.padding = padding == Pad_t::ZERO ? PXP_PAD_ZERO
+                                       : (padding == Pad_t::CONSTANT ? PXP_PAD_CONSTANT : PXP_PAD_LINEAR_FIT);
+    if (resizeMatrices) {
+      p.export_rows = exportRows;
+      p.export_cols = exportCols;
+    }
+    return p;
+  }
+  void run(const Solver &solver, const pxp_farfield_params &p, arma::Mat<double> &res) const {
+    pxp_solver h = solver.nativeHandle();
+    if (h == nullptr) throw std::runtime_error("FarField: the solver has not run");
+    unsigned rows = 0, cols = 0;
+    int rc = pxp_farfield_shape(h, &p, &rows, &cols);
+    if (rc == PXP_OK) {
+      res.set_size(rows, cols);
+      rc = pxp_farfield(h, &p, res.memptr());
+    }
+    if (rc != PXP_OK) {
+      char msg[512];
+      pxp_last_error(h, msg, sizeof(msg));
+      throw std::runtime_error(std::string("FarField: ") + msg);
+    }
+  }
+};
+
+class Transmittivity;
+}  // namespace post
+
+// ------------------------------------------------------------ waveguides ----
+/** Cladding (include/cladding.hpp, src/cladding.cpp): a refractive index. */
+class Cladding {
+ public:
+  void setRefractiveIndex(double newdelta, double newbeta) {
+    delta = newdelta;
+    beta = newbeta;
+  }
+  /** src/cladding.cpp:7-16 */
+  void setElectronDensity(double eDensity) {
+    electronDensity = eDensity;
+    potential = 4.0 * std::acos(-1.0) * thomsonScatteringLength * electronDensity;
+  }
+  double getDelta() const { return delta; }
+  double getBeta() const { return beta; }
+  double getPotential() const { return potential; }
+  double delta{0.0};
+  double beta{0.0};
+  double thomsonScatteringLength{2.8179403267E-6};
+  double electronDensity{0.0};
+
+ private:
+  double potential{0.0};
+};
+
+/** WaveGuideFDSimulation (include/waveGuideFDSimulation.hpp,
+ * src/waveGuideFDSimulation.cpp:219-265): a 2-D simulation whose medium is a
+ * waveguide in a cladding, sampled per step (it depends on z).  The border
+ * tracker, the HDF5 datasets and the control-file set-up are not provided. */
+class WaveGuideFDSimulation : public ParaxialSimulation {
+ public:
+  explicit WaveGuideFDSimulation(const char *name) : ParaxialSimulation(name) {}
+  void setCladding(const Cladding &clad) { cladding = &clad; }
+  void setInsideMaterial(const Cladding &mat) { insideMaterial = &mat; }
+  void setWaveguideLength(double wgl) { wglength = wgl; }
+  virtual bool isInsideGuide(double x, double z) const = 0;
+  virtual bool waveguideEnded(double, double z) const { return z > wglength; }
+  bool hasMaterial() const override { return true; }
+  bool materialZInvariant() const override { return false; }
+  void getXrayMatProp(double x, double z, double &delta, double &beta) const override {
+    if (cladding == nullptr) throw std::runtime_error("No cladding set!");
+    const double dx = xDisc.step, dz = zDisc.step;
+    if (waveguideEnded(x, z)) {
+      beta = 0.0;
+      delta = 0.0;
+      return;
+    }
+    bool isInside = isInsideGuide(x, z);
+    bool neighboursAreInside = isInsideGuide(x + dx, z) && isInsideGuide(x - dx, z) &&
+                               isInsideGuide(x, z + dz) && isInsideGuide(x, z - dz);
+    double betaInside = 0.0, deltaInside = 0.0;
+    if (insideMaterial != nullptr) {
+      betaInside = insideMaterial->getBeta();
+      deltaInside = insideMaterial->getDelta();
+    }
+    if (isInside && neighboursAreInside) {
+      beta = betaInside;
+      delta = deltaInside;
+      return;
+    } else if (isInside && !neighboursAreInside) {
+      delta = 0.5 * (cladding->getDelta() + deltaInside);
+      beta = 0.5 * (cladding->getBeta() + betaInside);
+      return;
+    }
+    delta = cladding->getDelta();
+    beta = cladding->getBeta();
+  }
+  void getXrayMatProp(double x, double, double z, double &delta, double &beta) const override {
+    getXrayMatProp(x, z, delta, beta);
+  }
+
+ protected:
+  const Cladding *cladding{nullptr};
+  const Cladding *insideMaterial{nullptr};
+  double wglength{1E10};
+};
+
+class CurvedWaveGuideFD;
+
+namespace post {
+/** post::Transmittivity (include/transmittivity.hpp, src/transmittivity.cpp):
+ * |u|^2 integrated over the waveguide after every step, relative to the
+ * integral over [0, width] after the first step.  The step kernels compute
+ * the per-step trapezoid sums (pxp_set_flux_windows); the dx/2 factors and
+ * the ratio are applied here. */
+class Transmittivity {
+ public:
+  const std::vector<double> &get() const { return transmission; }
+  double getIntensityAtZero() const { return intensityAtZero; }
+
+ private:
+  friend class ::CurvedWaveGuideFD;
+  std::vector<double> transmission;
+  double intensityAtZero{1E80};
+};
+}  // namespace post
+
+/** CurvedWaveGuideFD (include/curvedWaveGuide2D.hpp, src/curvedWaveGuide2D.cpp):
+ * a waveguide of width `width` bent with radius R, inner wall
+ * x = -z^2/(2R).  solve() steps it on the device with the transmittivity
+ * fused into the step kernels. */
+class CurvedWaveGuideFD : public WaveGuideFDSimulation {
+ public:
+  CurvedWaveGuideFD() : CurvedWaveGuideFD("CurvedWaveGuide2D") {}
+  explicit CurvedWaveGuideFD(const char *name) : WaveGuideFDSimulation(name) {}
+  void setRadiusOfCurvature(double newR) { R = newR; }
+  void setWidth(double newWidth) { width = newWidth; }
+  double getWidth() const { return width; }
+  double getRadiusOfCurvature() const { return R; }
+  void useSmoothedWG() { useSmoothed = true; }
+  /** src/curvedWaveGuide2D.cpp:49-52 */
+  bool isInsideGuide(double x, double z) const override {
+    return (2.0 * x * R + z * z > 0.0) && (2.0 * x * R + z * z < 2.0 * width * R);
+  }
+  /** src/curvedWaveGuide2D.cpp:61-69 */
+  double waveGuideStartX(double z) const { return -0.5 * z * z / R; }
+  double waveGuideEndX(double z) const { return waveGuideStartX(z) + width; }
+  /** src/curvedWaveGuide2D.cpp:178-193 */
+  double smoothedWG(double x, double z) const {
+    double w = 0.1 * width;
+    double d = 2.0 * R * x + z * z;
+    double f1 = 1.0 / (1.0 + std::exp(-d / w));
+    double f2 = 1.0 / (1.0 + std::exp((2 * R * width - d) / w));
+    return 1.0 - (f1 - f2);
+  }
+  /** src/curvedWaveGuide2D.cpp:195-205 */
+  void getXrayMatProp(double x, double z, double &delta, double &beta) const override {
+    if (!useSmoothed) {
+      WaveGuideFDSimulation::getXrayMatProp(x, z, delta, beta);
+      return;
+    }
+    delta = cladding->getDelta() * smoothedWG(x, z);
+    beta = cladding->getBeta() * smoothedWG(x, z);
+  }
+  using WaveGuideFDSimulation::getXrayMatProp;
+  const post::Transmittivity &getTransmittivity() const { return transmittivity; }
+
+  /** src/curvedWaveGuide2D.cpp:207-219 with Transmittivity::compute
+   * (src/transmittivity.cpp:43-83) at every step. */
+  void solve() override {
+    Solver2D *s2 = dynamic_cast<Solver2D *>(solver);
+    if (s2 == nullptr) throw std::runtime_error("CurvedWaveGuideFD needs a 2-D solver");
+    const unsigned Nz = nodeNumberLongitudinal(), Nx = nodeNumberTransverse();
+    if (Nz < 2) return;
+    std::vector<unsigned> a(Nz - 1), b(Nz - 1);
+    unsigned iz;
+    for (unsigned n = 1; n < Nz; ++n) {
+      const double z = getZ(n);
+      closestIndex(waveGuideStartX(z), z, a[n - 1], iz);
+      closestIndex(waveGuideEndX(z), z, b[n - 1], iz);
+      if (waveGuideStartX(z) < xDisc.min || a[n - 1] > b[n - 1] || b[n - 1] >= Nx)
+        throw std::runtime_error("the waveguide leaves the transverse grid at z = " + std::to_string(z));
+    }
+    s2->setFluxWindows(1, a, b);
+    s2->step();
+    unsigned z0, z1;
+    closestIndex(0.0, 0.0, z0, iz);
+    closestIndex(width, 0.0, z1, iz);
+    if (z0 > z1 || z1 >= Nx) throw std::runtime_error("the waveguide's entrance is outside the grid");
+    transmittivity.intensityAtZero = integral(s2->fieldFlux(z0, z1), z0, z1);
+    s2->solve();
+    const std::vector<double> sums = s2->getFlux(1, Nz - 1);
+    transmittivity.transmission.resize(Nz - 1);
+    for (unsigned n = 1; n < Nz; ++n)
+      transmittivity.transmission[n - 1] =
+          integral(sums[n - 1], a[n - 1], b[n - 1]) / transmittivity.intensityAtZero;
+  }
+
+ private:
+  double R{1.0};
+  double width{1.0};
+  bool useSmoothed{false};
+  post::Transmittivity transmittivity;
+
+  /** trapezoidalIntegrateIntensityZ (src/transmittivity.cpp:30-41) from
+   * the weighted sum. */
+  double integral(double sum, unsigned ixStart, unsigned ixEnd) const {
+    double dx = (getX(ixEnd) - getX(ixStart)) / static_cast<double>(ixEnd - ixStart);
+    return sum * dx * 0.5;
+  }
+};
+
+// -------------------------------------------------------------- scattering ----
+/** GenericScattering (include/genericScattering.hpp, src/genericScattering.cpp):
+ * a Gaussian beam through a 3-D object, first in vacuum with three steps
+ * (the reference run whose exit field the far field subtracts), then through
+ * the material.  The material is a SphereMaterial or a CSGMaterial (evaluated
+ * on the device); real-time visualisation, image export and the projection
+ * solver are not provided. */
+class GenericScattering : public ParaxialSimulation {
+ public:
+  enum class SolverType_t { ADI, FFT, PROJ };
+  explicit GenericScattering(const char *name) : ParaxialSimulation(name) {
+    gbeam.setDim(ParaxialSource::Dim_t::THREE_D);
+  }
+  void setMaterial(const MaterialFunction &mat) { userMaterial = &mat; }
+  void setBeamWaist(double w) { gbeam.setWaist(w); }
+  void setMaxScatteringAngle(double anglemax) { ff.setAngleRange(-anglemax, anglemax); }
+  /** GenericScattering::getFarField (src/genericScattering.cpp:235-238) */
+  void getFarField(arma::mat &farF) { ff.result(*solver, farF); }
+  const arma::cx_mat &getReference() const { return reference; }
+
+  /** src/genericScattering.cpp:21-135 */
+  void init() {
+    reset();
+    ff.setPadLength(FFTPadLength);
+    ff.setExportDimensions(exportNx, exportNy);
+    setTransverseDiscretization(xmin, xmax, dx, downSampleX);
+    setVerticalDiscretization(ymin, ymax, dy);
+    setLongitudinalDiscretization(zmin, zmax, (zmax - zmin) / 3.0, 1);
+    setWaveLength(wavelength);
+    gbeam.setWavelength(wavelength);
+    switch (propagator) {
+      case SolverType_t::ADI: setSolver(adisolver); break;
+      case SolverType_t::FFT: setSolver(fft3Dsolver); break;
+      case SolverType_t::PROJ: throw std::runtime_error("the projection solver is not provided");
+    }
+    material = nullptr;  // reference run: vacuum
+    setBoundaryConditions(gbeam);
+    ff.linkParaxialSim(*this);
+    ff.verifyConsistentAngles(dx, dy, wavenumber);
+  }
+
+  /** src/genericScattering.cpp:148-213 */
+  void solve() override {
+    if (userMaterial == nullptr) throw std::runtime_error("No material set!");
+    init();
+    ParaxialSimulation::solve();
+    reference = solver->getLastSolution3D();
+    if (subtract_reference) ff.setReference(reference);
+    reset();
+    material = userMaterial;
+    setLongitudinalDiscretization(zmin, zmax, dz, downSampleZ);
+    solver->updateDimensionsOfArrays();
+    setBoundaryConditions(gbeam);
+    ParaxialSimulation::solve();
+  }
+
+  unsigned int exportNx{512};
+  unsigned int exportNy{512};
+  unsigned int FFTPadLength{1024};
+  double xmin{-1.0};
+  double xmax{1.0};
+  double ymin{-1.0};
+  double ymax{1.0};
+  double zmin{-1.0};
+  double zmax{1.0};
+  double dx{0.1};
+  double dy{0.1};
+  double dz{0.1};
+  unsigned int downSampleX{1};
+  unsigned int downSampleY{1};
+  unsigned int downSampleZ{1};
+  double wavelength{0.1569};
+  bool subtract_reference{true};
+  SolverType_t propagator{SolverType_t::FFT};
+  bool supressMessages{false};
+
+ private:
+  const MaterialFunction *userMaterial{nullptr};
+  post::FarField ff;
+  GaussianBeam gbeam;
+  FFTSolver3D fft3Dsolver;
+  ADI adisolver;
+  arma::cx_mat reference;
 };

@@ -246,6 +246,19 @@ int pxp_set_reference(pxp_solver s, const double *field);
  * grid size), copied on the device. */
 int pxp_set_reference_from(pxp_solver s, pxp_solver src);
 
+/* post::Transmittivity (src/transmittivity.cpp:30-83) for the 2-D kinds:
+ * the trapezoid sum of pow(|u|, 2) over an index window [a, b] (weights 1
+ * at a and b, 2 between: trapezoidalIntegrateIntensityZ, :30-41, without
+ * its factor dx/2), computed by the step kernels as they store each new
+ * field.  pxp_set_flux_windows gives one window per step for steps
+ * first_step .. first_step + count - 1 (count = 0 clears; a <= b < Nx);
+ * pxp_get_flux returns the sums of those steps (NaN for steps not run
+ * yet); pxp_field_flux sums the current field over one window. */
+int pxp_set_flux_windows(pxp_solver s, int first_step, int count, const unsigned *start,
+                         const unsigned *end);
+int pxp_get_flux(pxp_solver s, int first_step, int count, double *out);
+int pxp_field_flux(pxp_solver s, unsigned start, unsigned end, double *sum);
+
 /* Solver::reset (include/solver.hpp:30): step counter back to 1. */
 int pxp_reset(pxp_solver s);
 

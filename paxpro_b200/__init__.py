@@ -288,6 +288,31 @@ class Solver:
             flat = np.ascontiguousarray(a.reshape(-1, order="F"))
             self._check(_capi.lib().pxp_set_reference(self._h, _dptr(flat.view(np.float64))))
 
+    def set_flux_windows(self, first_step: int, start, end) -> None:
+        """Per-step index windows [start[k], end[k]] of steps first_step + k
+        whose trapezoid sums of |u|^2 the 2-D step kernels compute
+        (post::Transmittivity); empty arrays clear them."""
+        a = np.ascontiguousarray(np.asarray(start, dtype=np.uint32))
+        b = np.ascontiguousarray(np.asarray(end, dtype=np.uint32))
+        if a.shape != b.shape or a.ndim != 1:
+            raise ValueError("start and end must be 1-D arrays of one length")
+        pa = a.ctypes.data_as(C.POINTER(C.c_uint)) if a.size else None
+        pb = b.ctypes.data_as(C.POINTER(C.c_uint)) if b.size else None
+        self._check(_capi.lib().pxp_set_flux_windows(self._h, int(first_step), int(a.size), pa, pb))
+
+    def get_flux(self, first_step: int, count: int) -> np.ndarray:
+        """The trapezoid sums of steps first_step .. first_step + count - 1
+        (NaN for steps not run yet)."""
+        out = np.empty(count, dtype=np.float64)
+        self._check(_capi.lib().pxp_get_flux(self._h, int(first_step), int(count), _dptr(out)))
+        return out
+
+    def field_flux(self, start: int, end: int) -> float:
+        """Trapezoid sum of |u|^2 of the current field over [start, end]."""
+        v = C.c_double()
+        self._check(_capi.lib().pxp_field_flux(self._h, int(start), int(end), C.byref(v)))
+        return v.value
+
     def reset(self) -> None:
         self._check(_capi.lib().pxp_reset(self._h))
 

@@ -124,6 +124,10 @@ def lib():
         "pxp_farfield": (C.c_int, [h, C.POINTER(FarFieldParams), d]),
         "pxp_set_reference": (C.c_int, [h, d]),
         "pxp_set_reference_from": (C.c_int, [h, h]),
+        "pxp_set_flux_windows": (C.c_int, [h, C.c_int, C.c_int, C.POINTER(C.c_uint),
+                                           C.POINTER(C.c_uint)]),
+        "pxp_get_flux": (C.c_int, [h, C.c_int, C.c_int, d]),
+        "pxp_field_flux": (C.c_int, [h, C.c_uint, C.c_uint, d]),
         "pxp_reset": (C.c_int, [h]),
         "pxp_current_step": (C.c_int, [h, C.POINTER(C.c_uint)]),
         "pxp_shape": (C.c_int, [h, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),

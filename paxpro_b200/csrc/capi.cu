@@ -88,6 +88,10 @@ struct pxp_solver_s {
   pxp::Sphere *d_spheres = nullptr;
   // field the far field subtracts (complex128, npts; null when not set)
   void *d_ref = nullptr;
+  // per-step flux windows and sums of the 2-D step kernels
+  int2 *d_flux_win = nullptr;
+  double *d_flux = nullptr;
+  int flux_step0 = 0, flux_count = 0;
   // host copies
   std::vector<double> h_delta, h_beta;
   int plane_first = 1, plane_count = 0;  // per-step material planes (0 = z-invariant)
@@ -331,6 +335,7 @@ int fft1d_write_job(pxp_solver_s *h) {
   j.save_every = h->save_every;
   j.max_slots = h->max_slots;
   j.trans_step0 = h->trans_step0;
+  j.flux = pxp::FluxSpec{h->d_flux_win, h->d_flux, h->flux_step0, h->flux_count};
   h->job_fft = j;
   if (int rc_ = h2d(h, h->d_job, &j, sizeof(j))) return rc_;
   return PXP_OK;
@@ -854,6 +859,7 @@ int cn_write_job(pxp_solver_s *h) {
   j.transparent = h->prob.transparent_bc ? 1 : 0;
   j.lu_g = h->d_lu;
   j.lu_h = h->d_lu ? (const void *)((const cd *)h->d_lu + n) : nullptr;
+  j.flux = pxp::FluxSpec{h->d_flux_win, h->d_flux, h->flux_step0, h->flux_count};
   h->job_cn = j;
   if (int rc_ = h2d(h, h->d_job, &j, sizeof(j))) return rc_;
   return PXP_OK;
@@ -1025,6 +1031,8 @@ int pxp_solver_destroy(pxp_solver h) {
   free_dev(h->d_csg, h->stream);
   free_dev(h->d_lu, h->stream);
   free_dev(h->d_ref, h->stream);
+  free_dev(h->d_flux_win, h->stream);
+  free_dev(h->d_flux, h->stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return PXP_OK;
@@ -1686,6 +1694,65 @@ int pxp_set_reference_from(pxp_solver h, pxp_solver src) {
                       : pxp::launch_widen(src->d_field, h->d_ref, h->npts, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   return e == cudaSuccess ? PXP_OK : h->cuda_fail(e, "copying the reference field");
+}
+
+// ---- per-step flux (post::Transmittivity) -----------------------------------
+int pxp_set_flux_windows(pxp_solver h, int first_step, int count, const unsigned *start,
+                         const unsigned *end) {
+  if (h == nullptr || count < 0) return PXP_ERR_INVALID;
+  if (h->prob.kind != PXP_FFT_SOLVER_2D && h->prob.kind != PXP_CRANK_NICHOLSON)
+    return h->fail(PXP_ERR_UNSUPPORTED, "flux windows apply to the 2-D kinds");
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  free_dev(h->d_flux_win, h->stream);
+  free_dev(h->d_flux, h->stream);
+  h->flux_step0 = 0;
+  h->flux_count = 0;
+  if (count > 0) {
+    if (first_step < 1 || start == nullptr || end == nullptr) return PXP_ERR_INVALID;
+    std::vector<int2> w((size_t)count);
+    for (int k = 0; k < count; ++k) {
+      if (start[k] > end[k] || end[k] >= h->nx)
+        return h->fail(PXP_ERR_INVALID, "flux window " + std::to_string(k) + " is not a <= b < Nx");
+      w[(size_t)k] = make_int2((int)start[k], (int)end[k]);
+    }
+    const std::vector<double> nan((size_t)count, std::nan(""));
+    int rc;
+    if ((rc = alloc(h, (void **)&h->d_flux_win, sizeof(int2) * count, "flux windows"))) return rc;
+    if ((rc = alloc(h, (void **)&h->d_flux, sizeof(double) * count, "flux sums"))) return rc;
+    if ((rc = h2d(h, h->d_flux_win, w.data(), sizeof(int2) * count))) return rc;
+    if ((rc = h2d(h, h->d_flux, nan.data(), sizeof(double) * count))) return rc;
+    h->flux_step0 = first_step;
+    h->flux_count = count;
+  }
+  return rewrite_job(h);
+}
+
+int pxp_get_flux(pxp_solver h, int first_step, int count, double *out) {
+  if (h == nullptr || out == nullptr || count < 0) return PXP_ERR_INVALID;
+  if (first_step < h->flux_step0 || (long long)first_step + count > (long long)h->flux_step0 + h->flux_count)
+    return h->fail(PXP_ERR_INVALID, "steps outside the flux windows set");
+  if (count == 0) return PXP_OK;
+  if (int rc = check_waits(h)) return rc;
+  PXP_TRY_CUDA(h, cudaMemcpyAsync(out, h->d_flux + (first_step - h->flux_step0), sizeof(double) * count,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  return PXP_OK;
+}
+
+int pxp_field_flux(pxp_solver h, unsigned start, unsigned end, double *sum) {
+  if (h == nullptr || sum == nullptr) return PXP_ERR_INVALID;
+  if (h->prob.kind != PXP_FFT_SOLVER_2D && h->prob.kind != PXP_CRANK_NICHOLSON)
+    return h->fail(PXP_ERR_UNSUPPORTED, "flux sums apply to the 2-D kinds");
+  if (start > end || end >= h->nx) return h->fail(PXP_ERR_INVALID, "flux window is not a <= b < Nx");
+  if (!h->ic_set) return h->fail(PXP_ERR_INVALID, "no field: set the initial conditions first");
+  if (int rc = check_waits(h)) return rc;
+  double *d = nullptr;
+  PXP_TRY_CUDA(h, cudaMallocAsync((void **)&d, sizeof(double), h->stream));
+  cudaError_t e = pxp::launch_flux_sum(h->prec, h->d_field, (int)start, (int)end, d, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sum, d, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  cudaFreeAsync(d, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? PXP_OK : h->cuda_fail(e, "flux sum");
 }
 
 int pxp_reset(pxp_solver h) {

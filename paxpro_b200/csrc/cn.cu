@@ -21,6 +21,7 @@
 // serial Thomas sweep; the step matrix is well conditioned (Cayley transform,
 // condition ~ rho), so the difference stays near machine precision.
 #include "pxp_complex.cuh"
+#include "flux.cuh"
 #include "pxp_kernels.h"
 #include "scan_solve.cuh"
 #include "tridiag.cuh"
@@ -85,6 +86,7 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
                                               int nsteps_ov) {
   using C = typename Cx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double flux_red[2][flux_slots<T>()];
   CnJob job = jobs[blockIdx.x];
   if (nsteps_ov >= 0) {
     job.step0 = step0_ov;
@@ -148,13 +150,19 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * n : nullptr;
+    int2 fw;
+    const bool flux = flux_window(job.flux, step, fw);
+    FluxSum acc;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const C v = from_d<R>(chunk_value<M>(m, xf, xl, y, p, q));
       u[s0 + m] = v;
       if (save) slot[s0 + m] = v;
+      if (flux) flux_add(acc, s0 + m, fw, to_d(v));
     }
+    if (flux) flux_warp_total<T>(acc, flux_red[st & 1]);
     __syncthreads();
+    if (flux) flux_store<T>(job.flux, step, flux_red[st & 1]);
   }
   for (int i = t; i < n; i += T) field[i] = u[i];
 }
@@ -181,6 +189,7 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
   double2 *ds = hs + N;
   double2 *xch = ds + N;  // 2 per thread
   Affine *scratch = reinterpret_cast<Affine *>(xch + 2 * T);
+  __shared__ double flux_red[2][flux_slots<T>()];
   CnJob job = jobs[blockIdx.x];
   if (nsteps_ov >= 0) {
     job.step0 = step0_ov;
@@ -226,13 +235,19 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
+    int2 fw;
+    const bool flux = flux_window(job.flux, step, fw);
+    FluxSum acc;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const C v = from_d<R>(rh[m]);
       u[m] = to_d(v);
       if (save) slot[s0 + m] = v;
+      if (flux) flux_add(acc, s0 + m, fw, u[m]);
     }
+    if (flux) flux_warp_total<T>(acc, flux_red[st & 1]);
     __syncthreads();  // xch is rewritten next step
+    if (flux) flux_store<T>(job.flux, step, flux_red[st & 1]);
   }
 #pragma unroll
   for (int m = 0; m < M; ++m) field[s0 + m] = from_d<R>(u[m]);

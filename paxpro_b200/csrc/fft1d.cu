@@ -13,6 +13,7 @@
 // reference evaluates it.  FP32 mode multiplies by t/N, the product formed
 // in FP64 and rounded once.
 #include "fft_smem.cuh"
+#include "flux.cuh"
 #include "pxp_kernels.h"
 
 namespace pxp {
@@ -43,6 +44,7 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
                                                  int nsteps_ov) {
   using C = typename Cx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double flux_red[2][flux_slots<T>()];
   C *u = reinterpret_cast<C *>(smem_raw);
   Fft1dJob job = jobs[blockIdx.x];
   if (nsteps_ov >= 0) {
@@ -75,13 +77,19 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
+    int2 fw;
+    const bool flux = flux_window(job.flux, step, fw);
+    FluxSum acc;
     for (int i = lane; i < N; i += T) {
       C v = u[sw<C>(i)];
       refract<R>(v, trans[i], nreal);
       u[sw<C>(i)] = v;
       if (save) slot[i] = v;
+      if (flux) flux_add(acc, i, fw, to_d(v));
     }
+    if (flux) flux_warp_total<T>(acc, flux_red[s & 1]);
     __syncthreads();
+    if (flux) flux_store<T>(job.flux, step, flux_red[s & 1]);
   }
   for (int i = lane; i < N; i += T) field[i] = u[sw<C>(i)];
 }

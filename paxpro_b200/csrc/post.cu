@@ -8,6 +8,7 @@
 // resident fields, so a caller copies back 8 bytes per point instead of the
 // complex field; max_abs_kernel gives the largest |u| over a set of saved
 // fields (IntensityUint8's scale, src/postProcessMod.cpp:23).
+#include "flux.cuh"
 #include "pxp_complex.cuh"
 #include "pxp_kernels.h"
 
@@ -48,6 +49,22 @@ __global__ void max_abs_kernel(const typename Cx<R>::T *__restrict__ in, long lo
   if ((threadIdx.x & 31) == 0) atomicMax(result, (unsigned long long)__double_as_longlong(m));
 }
 
+// The trapezoid sum of |u|^2 over [a, b] of the current field
+// (Transmittivity's integral outside the step kernels, e.g. its intensity at
+// zero), with the step kernels' summation.
+template <typename R, int T>
+__global__ void __launch_bounds__(T) flux_sum_kernel(const typename Cx<R>::T *__restrict__ u, int a,
+                                                     int b, double *__restrict__ out) {
+  __shared__ double red[flux_slots<T>()];
+  FluxSum acc;
+  const int2 w = make_int2(a, b);
+  for (int i = a + (int)threadIdx.x; i <= b; i += T) flux_add(acc, i, w, to_d(u[i]));
+  flux_warp_total<T>(acc, red);
+  __syncthreads();
+  const FluxSpec f{nullptr, out, 0, 1};
+  flux_store<T>(f, 0, red);
+}
+
 static int post_grid(long long n) {
   const long long b = (n + 255) / 256;
   return (int)(b < 148 * 8 ? (b > 0 ? b : 1) : 148 * 8);
@@ -69,6 +86,15 @@ cudaError_t launch_max_abs(Precision p, const void *field, long long n, unsigned
     max_abs_kernel<double><<<post_grid(n), 256, 0, s>>>((const double2 *)field, n, result);
   else
     max_abs_kernel<float><<<post_grid(n), 256, 0, s>>>((const float2 *)field, n, result);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_flux_sum(Precision p, const void *field, int a, int b, double *out,
+                            cudaStream_t s) {
+  if (p == kFP64)
+    flux_sum_kernel<double, 256><<<1, 256, 0, s>>>((const double2 *)field, a, b, out);
+  else
+    flux_sum_kernel<float, 256><<<1, 256, 0, s>>>((const float2 *)field, a, b, out);
   return cudaGetLastError();
 }
 

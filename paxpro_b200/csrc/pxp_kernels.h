@@ -15,6 +15,15 @@ void set_last_error(const char *msg);
 // ---------------------------------------------------------------- FFT 1-D --
 // One split-step problem with one transverse dimension (FFTSolver2D).
 // All complex arrays are interleaved and in the solver's precision.
+// Per-step flux integrals of the 2-D step kernels (flux.cuh): for steps
+// step0 .. step0 + count - 1 the kernel stores out[step - step0] = the
+// trapezoid sum of |u|^2 over win[step - step0] = (a, b), a <= b.
+struct FluxSpec {
+  const int2 *win;
+  double *out;
+  int step0, count;
+};
+
 struct Fft1dJob {
   void *field;             // N complex: field after the previous step
   const void *kern;        // N complex128: propagator exp(-i (dz/2k) kx^2)
@@ -31,6 +40,7 @@ struct Fft1dJob {
   int save_every;          // save when step % save_every == 0 (0 = never)
   int max_slots;           // capacity of saves
   int trans_step0;         // step that per-step table 0 belongs to
+  FluxSpec flux;           // per-step flux integrals (out == null: none)
 };
 
 // Launch nj jobs that all share one transform length n (one CTA per job).
@@ -53,6 +63,7 @@ struct CnJob {
   int transparent;             // BC_t::TRANSPARENT
   int status;                  // unused (reserved)
   const void *lu_g, *lu_h;     // factor tables of the step matrix (const path)
+  FluxSpec flux;               // per-step flux integrals (out == null: none)
 };
 cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
                       int nsteps, cudaStream_t s);
@@ -181,6 +192,9 @@ cudaError_t launch_farfield_lines(const FarFieldLines &p, int q, cudaStream_t s)
 // resizeMatrix of a column-major rows-row matrix to er x ec.
 cudaError_t launch_resize(const double *in, long long rows, double *out, int er, int ec, double dY,
                           double dX, cudaStream_t s);
+// Trapezoid sum of |u|^2 over [a, b] of a field of n points (one CTA).
+cudaError_t launch_flux_sum(Precision p, const void *field, int a, int b, double *out,
+                            cudaStream_t s);
 // complex64 -> complex128, n entries.
 cudaError_t launch_widen(const void *in, void *out, long long n, cudaStream_t s);
 

@@ -14,7 +14,7 @@ from csg_geometry import geometry  # noqa: E402
 
 
 def test_cpp_examples_compile_and_link():
-    for name in ("waveguide2d", "sphere3d", "csg3d"):
+    for name in ("waveguide2d", "sphere3d", "csg3d", "scattering3d", "curved2d"):
         assert build(name)
 
 

@@ -99,3 +99,79 @@ def test_csg3d_example(kind):
     assert _rel(last, ref_last) <= TOL
     assert _rel(slice1, ref_saves[0]) <= TOL
     assert np.std(np.abs(last)) > 1e-4
+
+
+@pytest.mark.parametrize("kind", ["fft", "adi"])
+def test_generic_scattering_example(kind):
+    """GenericScattering: the vacuum reference run (three steps), the run
+    through the sphere and the far field of the difference, resized to the
+    export dimensions, against the oracle."""
+    from oracle import farfield as off
+    exe = build("scattering3d")
+    n, steps, pad, ang, exp = 128, 6, 1024, 0.05, 64
+    out = os.path.join(OUT, f"gs_{kind}.bin")
+    r = subprocess.run([exe, kind, str(n), str(steps), str(pad), str(ang), str(exp), out],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    data = np.fromfile(out, dtype=np.float64)
+    N, rows, cols = int(data[0]), int(data[1]), int(data[2])
+    c = data[3:3 + 6 * N * N].view(np.complex128)
+    u0, ref, ex = (c[k * N * N:(k + 1) * N * N].reshape((N, N), order="F") for k in range(3))
+    ff = data[3 + 6 * N * N:].reshape((rows, cols), order="F")
+    K = 2.0 * math.pi / 0.1569
+    dx = _dx(n, 1000.0)
+    g0 = po.grid(-500.0, 500.0, dx, -300.0, 300.0, 200.0, K)
+    g1 = po.grid(-500.0, 500.0, dx, -300.0, 300.0, 600.0 / steps, K)
+    assert _rel(u0, po.gaussian_beam_3d(g0, 0.1569, 300.0)) <= 1e-13
+    sphere = po.MaterialSpec(po.MAT_SPHERES, spheres=[(20.0, -10.0, 0.0, 200.0, 8.9e-6, 7e-7)])
+    if kind == "fft":
+        ref_o, _ = po.fft3d_run(g0, po.MaterialSpec(), u0, 3, 0)
+        ex_o, _ = po.fft3d_run(g1, sphere, u0, steps, 0)
+    else:
+        ref_o, _ = po.adi3d_run(g0, po.MaterialSpec(), u0, 3, 0, True)
+        ex_o, _ = po.adi3d_run(g1, sphere, u0, steps, 0, True)
+    assert _rel(ref, ref_o) <= TOL
+    assert _rel(ex, ex_o) <= TOL
+    ff_o = off.farfield_3d(ex, pad, -ang, ang, K, dx, dx, reference=ref, export_rows=exp,
+                           export_cols=exp)
+    assert ff.shape == ff_o.shape == (exp, exp)
+    assert _rel(ff, ff_o) <= TOL
+
+
+@pytest.mark.parametrize("kind,smoothed", [("cn", 0), ("fft", 0), ("cn", 1)])
+def test_curved_waveguide_transmittivity(kind, smoothed):
+    """CurvedWaveGuideFD::solve with post::Transmittivity: the transmission
+    the step kernels integrate equals Transmittivity::compute
+    (src/transmittivity.cpp:30-83) evaluated on the saved fields."""
+    exe = build("curved2d")
+    n, steps = 1024, 150
+    out = os.path.join(OUT, f"cw_{kind}_{smoothed}.bin")
+    r = subprocess.run([exe, kind, str(n), str(steps), str(smoothed), out], capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
+    data = np.fromfile(out, dtype=np.float64)
+    nx, nz, i0 = int(data[0]), int(data[1]), data[2]
+    t = data[3:3 + nz - 1]
+    sol = data[3 + nz - 1:].view(np.complex128).reshape((nx, nz), order="F")
+    xmin, xmax, R, width, dz = -400.0, 200.0, 40e6, 100.0, 500.0
+    dx = wl.step_for_nodes(xmin, xmax, n)
+
+    def closest(x):
+        return int((x - xmin) / dx)
+
+    def integral(u, a, b):
+        total = abs(u[a]) ** 2 + abs(u[b]) ** 2
+        for i in range(a + 1, b):
+            total += 2.0 * abs(u[i]) ** 2
+        step = ((xmin + b * dx) - (xmin + a * dx)) / (b - a)
+        return total * step * 0.5
+
+    I0 = integral(sol[:, 1], closest(0.0), closest(width))
+    want = []
+    for k in range(1, nz):
+        z = 0.0 + k * dz
+        start = -0.5 * z * z / R
+        want.append(integral(sol[:, k], closest(start), closest(start + width)) / I0)
+    assert i0 == pytest.approx(I0, rel=1e-12)
+    np.testing.assert_allclose(t, np.array(want), rtol=1e-12, atol=0)
+    assert 0.0 < t[-1] < 1.0
