@@ -1296,15 +1296,15 @@ int pxp_step(pxp_solver h, int nsteps) {
   switch (h->prob.kind) {
     case PXP_FFT_SOLVER_2D:
       e = pxp::launch_fft1d(h->prec, (const pxp::Fft1dJob *)h->d_job, 1, (int)h->nx,
-                            (int)first, nsteps, h->stream);
+                            (int)first, nsteps, h->stream, h->flux_count > 0);
       break;
     case PXP_CRANK_NICHOLSON:
       if (h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0)
         e = pxp::launch_cn_const(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first,
-                                 nsteps, h->stream);
+                                 nsteps, h->stream, h->flux_count > 0);
       else
         e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first,
-                           nsteps, h->stream);
+                           nsteps, h->stream, h->flux_count > 0);
       break;
     case PXP_ADI: {
       int rc = adi_steps(h, (unsigned)first, nsteps);
@@ -1945,16 +1945,18 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
     const Key &k = o.second->first;
     const auto &list = o.second->second;
     const void *jobs = (const char *)b->d_jobs + o.first;
+    bool any_flux = false;
+    for (const pxp_solver_s *h : list) any_flux = any_flux || h->flux_count > 0;
     cudaError_t e;
     if (k.kind == PXP_FFT_SOLVER_2D)
       e = pxp::launch_fft1d((pxp::Precision)k.prec, (const pxp::Fft1dJob *)jobs, (int)list.size(),
-                            k.n, -1, -1, b->stream);
+                            k.n, -1, -1, b->stream, any_flux);
     else if (k.cpath)
       e = pxp::launch_cn_const((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
-                               k.n, -1, -1, b->stream);
+                               k.n, -1, -1, b->stream, any_flux);
     else
       e = pxp::launch_cn((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(), k.n,
-                         -1, -1, b->stream);
+                         -1, -1, b->stream, any_flux);
     if (e != cudaSuccess) return b->fail(PXP_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     for (pxp_solver_s *h : list) {
       const int n = std::min(h->batch_remaining, max_steps);

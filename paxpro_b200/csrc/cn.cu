@@ -81,7 +81,7 @@ __device__ __forceinline__ void cn_tbc(double2 outer, double2 inner, double rho,
   rhs = cx_add_rn(rhs, cx_mul_rn(coef, outer));
 }
 
-template <typename R, int M, int T>
+template <typename R, int M, int T, bool FLUX>
 __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, int step0_ov,
                                               int nsteps_ov) {
   using C = typename Cx<R>::T;
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * n : nullptr;
     int2 fw;
-    const bool flux = flux_window(job.flux, step, fw);
+    const bool flux = FLUX && flux_window(job.flux, step, fw);
     FluxSum acc;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
 // with the reference's rounding) and kept in shared memory; the regrouping
 // and the FMAs differ from the reference's operation order at rounding level.
 // Tables sit in chunk-transposed slots (cslot), free of bank conflicts.
-template <typename R, int M, int T>
+template <typename R, int M, int T, bool FLUX>
 __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ jobs, int step0_ov,
                                                     int nsteps_ov) {
   using C = typename Cx<R>::T;
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
     int2 fw;
-    const bool flux = flux_window(job.flux, step, fw);
+    const bool flux = FLUX && flux_window(job.flux, step, fw);
     FluxSum acc;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
@@ -255,13 +255,13 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
 
 static constexpr int kCnM = 8;
 
-template <typename R, int M, int T>
-static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
+template <typename R, int M, int T, bool FLUX>
+static cudaError_t cn_const_launch_f(const CnJob *d_jobs, int nj, int step0, int nsteps,
                                      cudaStream_t s) {
   constexpr int N = M * T;
   constexpr size_t smem = sizeof(double2) * (3 * N + 2 * T) + sizeof(Affine) * (T / 32 + 1);
-  auto k = cn_const_kernel<R, M, T>;
-  if (smem > 48 * 1024) {
+  auto k = cn_const_kernel<R, M, T, FLUX>;
+  {  // the static flux slots count against the 48 KB default too
     static const cudaError_t attr =
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return attr;
@@ -270,24 +270,31 @@ static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int
   return cudaGetLastError();
 }
 
+template <typename R, int M, int T>
+static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
+                                     cudaStream_t s, bool flux) {
+  return flux ? cn_const_launch_f<R, M, T, true>(d_jobs, nj, step0, nsteps, s)
+              : cn_const_launch_f<R, M, T, false>(d_jobs, nj, step0, nsteps, s);
+}
+
 bool cn_const_supported(Precision, int n) { return n >= 8 * kCnM && !(n & (n - 1)) && n <= 4096; }
 
 cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0, int nsteps,
-                            cudaStream_t s) {
+                            cudaStream_t s, bool flux) {
   if (nj <= 0) return cudaSuccess;
   // n >= 2048: 16 rows per thread (half the threads of 8 rows: fewer warps
   // in each scan's barriers and shuffles; measured 4.07 -> 3.08 us per step
   // at n = 4096)
   if (n == 4096)
-    return p == kFP64 ? cn_const_launch_t<double, 16, 256>(d_jobs, nj, step0, nsteps, s)
-                      : cn_const_launch_t<float, 16, 256>(d_jobs, nj, step0, nsteps, s);
+    return p == kFP64 ? cn_const_launch_t<double, 16, 256>(d_jobs, nj, step0, nsteps, s, flux)
+                      : cn_const_launch_t<float, 16, 256>(d_jobs, nj, step0, nsteps, s, flux);
   if (n == 2048)
-    return p == kFP64 ? cn_const_launch_t<double, 16, 128>(d_jobs, nj, step0, nsteps, s)
-                      : cn_const_launch_t<float, 16, 128>(d_jobs, nj, step0, nsteps, s);
+    return p == kFP64 ? cn_const_launch_t<double, 16, 128>(d_jobs, nj, step0, nsteps, s, flux)
+                      : cn_const_launch_t<float, 16, 128>(d_jobs, nj, step0, nsteps, s, flux);
 #define PXP_CC(TT)                                                                     \
   case TT:                                                                             \
-    return p == kFP64 ? cn_const_launch_t<double, kCnM, TT>(d_jobs, nj, step0, nsteps, s) \
-                      : cn_const_launch_t<float, kCnM, TT>(d_jobs, nj, step0, nsteps, s);
+    return p == kFP64 ? cn_const_launch_t<double, kCnM, TT>(d_jobs, nj, step0, nsteps, s, flux) \
+                      : cn_const_launch_t<float, kCnM, TT>(d_jobs, nj, step0, nsteps, s, flux);
   switch (n / kCnM) {
     PXP_CC(8) PXP_CC(16) PXP_CC(32) PXP_CC(64) PXP_CC(128)
     default:
@@ -296,13 +303,13 @@ cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int
 #undef PXP_CC
 }
 
-template <typename R, int T>
-static cudaError_t cn_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
+template <typename R, int T, bool FLUX>
+static cudaError_t cn_launch_f(const CnJob *d_jobs, int nj, int step0, int nsteps,
                                cudaStream_t s) {
   using C = typename Cx<R>::T;
   size_t smem = sizeof(double2) * 4 * 2 * T + sizeof(C) * kCnM * T;
-  auto k = cn_kernel<R, kCnM, T>;
-  if (smem > 48 * 1024) {
+  auto k = cn_kernel<R, kCnM, T, FLUX>;
+  {  // the static flux slots count against the 48 KB default too
     static const cudaError_t attr =
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return attr;
@@ -311,24 +318,31 @@ static cudaError_t cn_launch_t(const CnJob *d_jobs, int nj, int step0, int nstep
   return cudaGetLastError();
 }
 
+template <typename R, int T>
+static cudaError_t cn_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps, cudaStream_t s,
+                               bool flux) {
+  return flux ? cn_launch_f<R, T, true>(d_jobs, nj, step0, nsteps, s)
+              : cn_launch_f<R, T, false>(d_jobs, nj, step0, nsteps, s);
+}
+
 bool cn_supported(Precision p, int n) {
   if (n < 2 * kCnM || (n & (n - 1))) return false;
   return p == kFP64 ? n <= 4096 : n <= 8192;
 }
 
 cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0, int nsteps,
-                      cudaStream_t s) {
+                      cudaStream_t s, bool flux) {
   if (nj <= 0) return cudaSuccess;
   const int T = n / kCnM;
 #define PXP_CN(TT)                                                                 \
   case TT:                                                                         \
-    return p == kFP64 ? cn_launch_t<double, TT>(d_jobs, nj, step0, nsteps, s)      \
-                      : cn_launch_t<float, TT>(d_jobs, nj, step0, nsteps, s);
+    return p == kFP64 ? cn_launch_t<double, TT>(d_jobs, nj, step0, nsteps, s, flux) \
+                      : cn_launch_t<float, TT>(d_jobs, nj, step0, nsteps, s, flux);
   switch (T) {
     PXP_CN(2) PXP_CN(4) PXP_CN(8) PXP_CN(16) PXP_CN(32) PXP_CN(64) PXP_CN(128) PXP_CN(256)
     PXP_CN(512)
     case 1024:
-      if (p == kFP32) return cn_launch_t<float, 1024>(d_jobs, nj, step0, nsteps, s);
+      if (p == kFP32) return cn_launch_t<float, 1024>(d_jobs, nj, step0, nsteps, s, flux);
       return cudaErrorInvalidValue;
     default:
       return cudaErrorInvalidValue;

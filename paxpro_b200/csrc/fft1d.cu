@@ -39,7 +39,7 @@ template <> __device__ __forceinline__ float2 kmul<float>(float2 u, double2 k) {
   return tw_mul(u, k);
 }
 
-template <typename R, int N, int T, bool TW_SMEM>
+template <typename R, int N, int T, bool TW_SMEM, bool FLUX>
 __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ jobs, int step0_ov,
                                                  int nsteps_ov) {
   using C = typename Cx<R>::T;
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
     int2 fw;
-    const bool flux = flux_window(job.flux, step, fw);
+    const bool flux = FLUX && flux_window(job.flux, step, fw);
     FluxSum acc;
     for (int i = lane; i < N; i += T) {
       C v = u[sw<C>(i)];
@@ -98,7 +98,7 @@ template <typename R> constexpr int fft1d_threads(int n) {
   return n >= 8192 ? 512 : (n >= 2048 ? 256 : (n >= 512 ? 64 : 32));
 }
 
-template <typename R, int N>
+template <typename R, int N, bool FLUX>
 static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nsteps,
                             cudaStream_t s) {
   using C = typename Cx<R>::T;
@@ -107,8 +107,8 @@ static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nstep
   constexpr size_t tw_bytes = sizeof(double2) * N;
   constexpr bool tw_smem = field_bytes + tw_bytes <= 200 * 1024;
   constexpr size_t smem = tw_smem ? field_bytes + tw_bytes : field_bytes;
-  auto k = fft1d_kernel<R, N, T, tw_smem>;
-  if (smem > 48 * 1024) {
+  auto k = fft1d_kernel<R, N, T, tw_smem, FLUX>;
+  {  // the static flux slots count against the 48 KB default too
     static const cudaError_t attr =
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return attr;
@@ -122,18 +122,25 @@ bool fft1d_supported(Precision p, int n) {
   return p == kFP64 ? n <= 8192 : n <= 16384;
 }
 
+template <typename R, int N>
+static cudaError_t launch_nf(const Fft1dJob *d_jobs, int nj, int step0, int nsteps, cudaStream_t s,
+                             bool flux) {
+  return flux ? launch_n<R, N, true>(d_jobs, nj, step0, nsteps, s)
+              : launch_n<R, N, false>(d_jobs, nj, step0, nsteps, s);
+}
+
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
-                         int nsteps, cudaStream_t s) {
+                         int nsteps, cudaStream_t s, bool flux) {
   if (nj <= 0) return cudaSuccess;
 #define PXP_CASE(NN)                                                              \
   case NN:                                                                        \
-    return p == kFP64 ? launch_n<double, NN>(d_jobs, nj, step0, nsteps, s)            \
-                      : launch_n<float, NN>(d_jobs, nj, step0, nsteps, s);
+    return p == kFP64 ? launch_nf<double, NN>(d_jobs, nj, step0, nsteps, s, flux)     \
+                      : launch_nf<float, NN>(d_jobs, nj, step0, nsteps, s, flux);
   switch (n) {
     PXP_CASE(8) PXP_CASE(16) PXP_CASE(32) PXP_CASE(64) PXP_CASE(128) PXP_CASE(256)
     PXP_CASE(512) PXP_CASE(1024) PXP_CASE(2048) PXP_CASE(4096) PXP_CASE(8192)
     case 16384:
-      if (p == kFP32) return launch_n<float, 16384>(d_jobs, nj, step0, nsteps, s);
+      if (p == kFP32) return launch_nf<float, 16384>(d_jobs, nj, step0, nsteps, s, flux);
       return cudaErrorInvalidValue;
     default:
       return cudaErrorInvalidValue;

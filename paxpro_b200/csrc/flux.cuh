@@ -41,7 +41,7 @@ __device__ __forceinline__ void flux_add(FluxSum &acc, int i, int2 w, double2 u)
 
 // Slots of the per-step partial sums: one per warp, or one per thread when
 // the CTA is smaller than a warp.
-template <int T> constexpr int flux_slots() { return T >= 32 ? T / 32 : T; }
+template <int T> __host__ __device__ constexpr int flux_slots() { return T >= 32 ? T / 32 : T; }
 
 // Before the step's closing barrier: each warp's total (each thread's sum
 // in a CTA of fewer than 32 threads) into row.

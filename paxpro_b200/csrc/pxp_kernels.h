@@ -45,8 +45,9 @@ struct Fft1dJob {
 
 // Launch nj jobs that all share one transform length n (one CTA per job).
 // step0/nsteps >= 0 override every job's own values (single-problem use).
+// flux: some job has flux windows (the kernel variant that sums them).
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n,
-                         int step0, int nsteps, cudaStream_t s);
+                         int step0, int nsteps, cudaStream_t s, bool flux = false);
 bool fft1d_supported(Precision p, int n);
 
 // ------------------------------------------------------------ CN 1-D ------
@@ -66,12 +67,12 @@ struct CnJob {
   FluxSpec flux;               // per-step flux integrals (out == null: none)
 };
 cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
-                      int nsteps, cudaStream_t s);
+                      int nsteps, cudaStream_t s, bool flux = false);
 bool cn_supported(Precision p, int n);
 // z-invariant medium and Dirichlet ends: the step matrix never changes; the
 // job's lu_g / lu_h hold its Thomas factor tables (n complex128 each).
 cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
-                            int nsteps, cudaStream_t s);
+                            int nsteps, cudaStream_t s, bool flux = false);
 bool cn_const_supported(Precision p, int n);
 
 // ------------------------------------------------------------- ADI ------

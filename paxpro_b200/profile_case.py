@@ -7,6 +7,14 @@ z steps per repeat.  Inputs are the benchmark workloads' synthetic fields and
 materials (planar waveguide for the 2-D kinds, the config-1 sphere for ADI,
 the config-2 sphere set for FFT3D).  Prints the mean time per step measured
 with CUDA events on the solver's stream.
+
+    python -m paxpro_b200.profile_case farfield N STEPS --pad L --angle A
+
+runs STEPS FFTSolver3D steps of the config-2 workload at size N, then times
+the 3-D far field of the exit field (pad length L, angles -A..A degrees,
+the subtraction of a reference field included) through pxp_farfield:
+CUDA-event time on the solver's stream around the call (the transforms, the
+reference subtraction and the copy of the result to the host).
 """
 from __future__ import annotations
 
@@ -47,12 +55,16 @@ def make(kind: str, n: int, steps: int, precision: int):
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("kind", choices=["fft2d", "cn", "adi", "fft3d"])
+    ap.add_argument("kind", choices=["fft2d", "cn", "adi", "fft3d", "farfield"])
     ap.add_argument("n", type=int)
     ap.add_argument("steps", type=int)
     ap.add_argument("--fp32", action="store_true")
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--pad", type=int, default=32768)
+    ap.add_argument("--angle", type=float, default=0.05)
     a = ap.parse_args(argv)
+    if a.kind == "farfield":
+        return farfield(a)
     s = make(a.kind, a.n, a.steps, 1 if a.fp32 else 0)
     import torch
     st = torch.cuda.ExternalStream(s.stream_ptr())
@@ -68,6 +80,29 @@ def main(argv=None) -> int:
     assert np.all(np.isfinite(out))
     print(f"{a.kind} n={a.n} steps={a.steps} {'fp32' if a.fp32 else 'fp64'}: "
           f"{min(times) * 1e3:.2f} us/step (min of {a.repeat})")
+    s.close()
+    return 0
+
+
+def farfield(a) -> int:
+    import torch
+    s = make("fft3d", a.n, a.steps, 1 if a.fp32 else 0)
+    s.step(a.steps)
+    s.set_reference(np.ones((a.n, a.n), dtype=np.complex128))
+    st = torch.cuda.ExternalStream(s.stream_ptr())
+    res = s.farfield(pad_length=a.pad, phi_min=-a.angle, phi_max=a.angle, subtract_reference=True)
+    times = []
+    for _ in range(max(a.repeat, 1)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        res = s.farfield(pad_length=a.pad, phi_min=-a.angle, phi_max=a.angle,
+                         subtract_reference=True)
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    assert np.all(np.isfinite(res))
+    print(f"farfield n={a.n} pad={a.pad} angle={a.angle}: result {res.shape[0]} x {res.shape[1]}, "
+          f"{min(times):.3f} ms per call (min of {len(times)})")
     s.close()
     return 0
 

@@ -95,3 +95,20 @@ def test_resize_matrix_blocks():
     assert r[1, 1] == pytest.approx(m[1:4, 2:5].mean())
     assert r[1, 0] == pytest.approx(m[1:4, 0:3].mean())
     assert ff.resize_matrix(m, 5, 2) is m                 # not smaller in both: unchanged
+
+
+def test_sources_match_the_oracle_beam():
+    """paxpro_b200.sources.GaussianBeam against the oracle's restatement of
+    GaussianBeam::get (no GPU needed)."""
+    from oracle import pyoracle as po
+    from paxpro_b200.sources import GaussianBeam
+    from paxpro_b200 import workloads as wl
+    n = 64
+    dx = wl.step_for_nodes(-500.0, 500.0, n)
+    g = po.grid(-500.0, 500.0, dx, -300.0, 300.0, 100.0, 2 * math.pi / 0.1569)
+    gb = GaussianBeam(300.0)
+    gb.set_wavelength(0.1569)
+    x = -500.0 + dx * np.arange(n)
+    got = gb.field_3d(x, x)
+    want = po.gaussian_beam_3d(g, 0.1569, 300.0)
+    assert np.max(np.abs(got - want)) <= 1e-14 * np.max(np.abs(want))

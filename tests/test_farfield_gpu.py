@@ -125,3 +125,46 @@ def test_farfield_fp32_field_and_errors():
             s.farfield(padding=_capi.PAD_LINEAR_FIT)
         with pytest.raises(pxp.PxpError):
             s.farfield(phi_min=10.0, phi_max=-10.0)
+
+
+@pytest.mark.parametrize("propagator", ["fft", "adi"])
+def test_python_generic_scattering(propagator):
+    """paxpro_b200.scattering.GenericScattering: the reference run, the sample
+    run and the far field against the oracle on the same fields."""
+    import paxpro_b200 as pxp
+    from oracle import pyoracle as po
+    from paxpro_b200.scattering import GenericScattering
+    n, steps = 128, 6
+    dx = wl.step_for_nodes(-500.0, 500.0, n)
+    with GenericScattering("sphere") as gs:
+        gs.setBeamWaist(300.0)
+        gs.setMaxScatteringAngle(0.05)
+        gs.xmin = gs.ymin = -500.0
+        gs.xmax = gs.ymax = 500.0
+        gs.zmin, gs.zmax = -300.0, 300.0
+        gs.dx = gs.dy = dx
+        gs.dz = 600.0 / steps
+        gs.FFTPadLength = 1024
+        gs.exportNx = gs.exportNy = 64
+        gs.propagator = propagator
+        gs.setMaterial([pxp.Sphere(20.0, -10.0, 0.0, 200.0, 8.9e-6, 7e-7)])
+        gs.solve()
+        ff = gs.getFarField()
+        K = 2.0 * np.pi / 0.1569
+        g0 = po.grid(-500.0, 500.0, dx, -300.0, 300.0, 200.0, K)
+        g1 = po.grid(-500.0, 500.0, dx, -300.0, 300.0, 100.0, K)
+        u0 = po.gaussian_beam_3d(g0, 0.1569, 300.0)
+        assert _rel(gs._initial(), u0) <= 1e-13
+        sph = po.MaterialSpec(po.MAT_SPHERES, spheres=[(20.0, -10.0, 0.0, 200.0, 8.9e-6, 7e-7)])
+        if propagator == "fft":
+            ref_o, _ = po.fft3d_run(g0, po.MaterialSpec(), u0, 3, 0)
+            ex_o, _ = po.fft3d_run(g1, sph, u0, steps, 0)
+        else:
+            ref_o, _ = po.adi3d_run(g0, po.MaterialSpec(), u0, 3, 0, True)
+            ex_o, _ = po.adi3d_run(g1, sph, u0, steps, 0, True)
+        assert _rel(gs.reference, ref_o) <= TOL
+        assert _rel(gs.exit_field, ex_o) <= TOL
+        want = off.farfield_3d(gs.exit_field, 1024, -0.05, 0.05, K, dx, dx,
+                               reference=gs.reference, export_rows=64, export_cols=64)
+        assert ff.shape == want.shape == (64, 64)
+        assert _rel(ff, want) <= TOL
