@@ -1431,7 +1431,9 @@ unsigned ff_angle_index(double angle, unsigned size, double k, double step) {
 }
 
 // Device tables of the far field, shared like the solver tables: kind 4 the
-// L-entry table exp(-2 pi i m / L), kind 5 the Stockham twiddles of length q.
+// L-entry table exp(-2 pi i m / L), kind 5 the Stockham twiddles of length q,
+// kind 6 the split form of kind 4: lo[r] = exp(-2 pi i r / L) for
+// r < 2^b, then hi[q] = exp(-2 pi i q 2^b / L) for q < L / 2^b.
 int ff_table(pxp_solver_s *h, int kind, long long len, const double2 **out) {
   TableKey key{h->prob.device, kind, (unsigned)len, 0.0, 0.0, 0.0};
   std::lock_guard<std::mutex> lk(g_table_mutex);
@@ -1440,6 +1442,19 @@ int ff_table(pxp_solver_s *h, int kind, long long len, const double2 **out) {
     std::vector<cd> t;
     if (kind == 5) {
       t = twiddles((int)len);
+    } else if (kind == 6) {
+      const int b = pxp::farfield_split_bits(len);
+      const long long nlo = 1LL << b, nhi = len >> b;
+      const long double pi_l = 3.141592653589793238462643383279502884L;
+      t.resize((size_t)(nlo + nhi));
+      for (long long r = 0; r < nlo; ++r) {
+        const long double a = -2.0L * pi_l * (long double)r / (long double)len;
+        t[(size_t)r] = cd((double)cosl(a), (double)sinl(a));
+      }
+      for (long long q = 0; q < nhi; ++q) {
+        const long double a = -2.0L * pi_l * (long double)(q * nlo) / (long double)len;
+        t[(size_t)(nlo + q)] = cd((double)cosl(a), (double)sinl(a));
+      }
     } else {
       t.resize((size_t)len);
       const long double pi_l = 3.141592653589793238462643383279502884L;
@@ -1566,11 +1581,15 @@ int pxp_farfield(pxp_solver h, const pxp_farfield_params *p, double *out) {
     tmp.push_back(q);
     return q;
   };
+  const double2 *wsplit = nullptr;
+  const int split_bits = pxp::farfield_split_bits(f.L);
   auto lines_for = [&](long long n, long long window, int *q, const double2 **twq) -> int {
     *q = ff_choose_q(n, f.L, window);
     *twq = nullptr;
-    if (*q) return ff_table(h, 5, *q, twq);
-    return PXP_OK;
+    if (*q == 0) return PXP_OK;
+    if (wsplit == nullptr)
+      if (int rc = ff_table(h, 6, f.L, &wsplit)) return rc;
+    return ff_table(h, 5, *q, twq);
   };
   cudaError_t e = cudaSuccess;
   double *d_res = nullptr;
@@ -1593,6 +1612,8 @@ int pxp_farfield(pxp_solver h, const pxp_farfield_params *p, double *out) {
     ln.wL = wL;
     int q;
     if (int rc = lines_for(ln.n, f.rows, &q, &ln.twQ)) return rc;
+    ln.wsplit = wsplit;
+    ln.split_bits = split_bits;
     d_res = (double *)dalloc(sizeof(double) * out_elems);
     if (d_res == nullptr) return h->fail(PXP_ERR_NOMEM, "far-field buffers");
     ln.out = d_res;
@@ -1629,6 +1650,8 @@ int pxp_farfield(pxp_solver h, const pxp_farfield_params *p, double *out) {
       release();
       return rc;
     }
+    a.wsplit = wsplit;
+    a.split_bits = split_bits;
     e = pxp::launch_farfield_lines(a, qa, s);
     // conjugated rows, cut along x -> d_res[r + (i - x0) * rows], |X|^2 / L
     pxp::FarFieldLines b{};
@@ -1651,6 +1674,8 @@ int pxp_farfield(pxp_solver h, const pxp_farfield_params *p, double *out) {
       release();
       return rc;
     }
+    b.wsplit = wsplit;
+    b.split_bits = split_bits;
     if (e == cudaSuccess) e = pxp::launch_farfield_lines(b, qb, s);
     if (e == cudaSuccess && f.resize) {
       const double dX = (double)f.cols / ((double)p->export_cols + 1.0);

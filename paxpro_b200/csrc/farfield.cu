@@ -72,7 +72,7 @@ __device__ __forceinline__ long long ff_unshift(long long i, long long L) {
 }  // namespace
 
 // G lines per CTA, T threads, sub-transform length Q (power of two, n <= Q,
-// Q | L).  With REG, each thread keeps its S = Q / T entries of (x - c) in
+// Q | L); blockIdx.y selects a share of the k1 range.  With REG, each thread keeps its S = Q / T entries of (x - c) in
 // registers for the P passes over k1; without (Q = 8192, where registers
 // would spill), it reads them again each pass (from L2 after the first).
 template <int Q, int T, int G, bool REG>
@@ -83,7 +83,14 @@ __global__ void __launch_bounds__(T) ff_pruned_kernel(FarFieldLines p) {
   static_assert(S * T == Q, "Q must be a multiple of T");
   extern __shared__ double2 ff_smem[];
   double2 *x = ff_smem;
+  // twiddle factors exp(-2 pi i m / L) as lo[m mod B] * hi[m / B], B = 2^split_bits:
+  // two tables of about sqrt(L) entries each, held in shared memory
+  const int sb = p.split_bits;
+  const int nlo = 1 << sb, nhi = (int)(p.L >> sb);
+  double2 *wlo = x + G * LD;
+  double2 *whi = wlo + nlo;
   const int tid = threadIdx.x;
+  for (int i = tid; i < nlo + nhi; i += T) wlo[i] = p.wsplit[i];
   const long long line0 = (long long)blockIdx.x * G;
   double2 c[G];
   double2 v[G][SR];
@@ -105,9 +112,13 @@ __global__ void __launch_bounds__(T) ff_pruned_kernel(FarFieldLines p) {
       for (int s = 0; s < S; ++s) v[g][s] = src(g, tid + s * T);
     }
   }
+  __syncthreads();  // the twiddle tables are in place
   const long long L = p.L, P = L / Q, h = L / 2, mask = L - 1;
   const long long win = p.i1 - p.i0 + 1;
-  for (long long k1 = 0; k1 < P; ++k1) {
+  // blockIdx.y takes one contiguous share of the P sub-transforms
+  const long long kchunk = (P + gridDim.y - 1) / gridDim.y;
+  const long long k1_end = min(P, (long long)(blockIdx.y + 1) * kchunk);
+  for (long long k1 = (long long)blockIdx.y * kchunk; k1 < k1_end; ++k1) {
     // outputs of this k1 sit at i = (k1 + P k2 + h) mod L: one residue class mod P
     if (win < P) {
       const long long r = (k1 + h) % P;
@@ -117,7 +128,8 @@ __global__ void __launch_bounds__(T) ff_pruned_kernel(FarFieldLines p) {
 #pragma unroll
     for (int s = 0; s < S; ++s) {
       const int j = tid + s * T;
-      const double2 w = p.wL[((long long)j * k1) & mask];
+      const long long m = ((long long)j * k1) & mask;
+      const double2 w = cmul(whi[m >> sb], wlo[m & (nlo - 1)]);
 #pragma unroll
       for (int g = 0; g < G; ++g) {
         double2 a;
@@ -223,16 +235,28 @@ namespace {
 template <int Q, int T, int G>
 cudaError_t ff_pruned_launch(const FarFieldLines &p, cudaStream_t s) {
   constexpr bool REG = Q <= 4096;
-  const size_t smem = sizeof(double2) * G * (Q + 1);
+  const size_t smem =
+      sizeof(double2) * (G * (Q + 1) + (1LL << p.split_bits) + (p.L >> p.split_bits));
   cudaError_t e = cudaFuncSetAttribute(ff_pruned_kernel<Q, T, G, REG>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long blocks = (p.nlines + G - 1) / G;
-  ff_pruned_kernel<Q, T, G, REG><<<(unsigned)blocks, T, smem, s>>>(p);
+  // few lines (or many sub-transforms per line): split each line's
+  // sub-transforms over blockIdx.y until about 8 CTAs per SM are in flight
+  const long long P = p.L / Q;
+  long long ky = (148LL * 8 + blocks - 1) / blocks;
+  ky = ky < 1 ? 1 : (ky > P ? P : ky);
+  ff_pruned_kernel<Q, T, G, REG><<<dim3((unsigned)blocks, (unsigned)ky), T, smem, s>>>(p);
   return cudaGetLastError();
 }
 
 }  // namespace
+
+int farfield_split_bits(long long L) {
+  int lg = 0;
+  while ((1LL << lg) < L) ++lg;
+  return (lg + 1) / 2;
+}
 
 int farfield_pruned_q(long long n, long long L) {
   long long q = 64;

@@ -167,7 +167,8 @@ cudaError_t launch_max_abs(Precision p, const void *field, long long n, unsigned
 // entry 0).  Kept: outputs i0..i1 of the fftshifted transform, written to
 // out[l + (i - i0) * out_stride] as complex128 (mode 0), |X|^2 / divisor
 // (mode 1) or |X| / divisor (mode 2).  wL: L entries exp(-2 pi i m / L);
-// twQ: Stockham twiddles of the sub-transform length.
+// twQ: Stockham twiddles of the sub-transform length; wsplit: the same
+// factors as two short tables (see below).
 struct FarFieldLines {
   const void *in;
   const double2 *ref;
@@ -182,12 +183,18 @@ struct FarFieldLines {
   double divisor;
   const double2 *wL;
   const double2 *twQ;
+  // pruned transform: exp(-2 pi i m / L) = hi[m >> split_bits] * lo[m & (2^split_bits - 1)],
+  // wsplit = lo (2^split_bits entries) followed by hi (L >> split_bits entries)
+  const double2 *wsplit;
+  int split_bits;
 };
 
 // Sub-transform length of the pruned transform for lines of n entries
 // padded to L, or 0 when L is not a power of two or n needs more than 8192
 // (the direct DFT then runs).
 int farfield_pruned_q(long long n, long long L);
+// split_bits of the pruned transform's twiddle tables for length L.
+int farfield_split_bits(long long L);
 // q: farfield_pruned_q's choice, or 0 for the direct DFT.
 cudaError_t launch_farfield_lines(const FarFieldLines &p, int q, cudaStream_t s);
 // resizeMatrix of a column-major rows-row matrix to er x ec.
