@@ -197,6 +197,13 @@ int pxp_get_saved(pxp_solver s, int slot, double *field);
 #define PXP_POST_REAL 2 /* Re u: post::ExitField (:102-116) */
 #define PXP_POST_ABS2 3 /* pow(|u|, 2): post::ExitIntensity (:118-132) */
 int pxp_get_post(pxp_solver s, int quantity, int slot, double *out);
+/* The same quantity of a 3-D field resized to rows x cols by
+ * PostProcessingModule::resizeMatrix (src/postProcessing.cpp:29-49: block
+ * means, the matrix unchanged unless both dimensions shrink), as the
+ * modules do after setExportDimensions; out holds rows x cols doubles
+ * (column-major), or the full field when it is not resized. */
+int pxp_get_post_resized(pxp_solver s, int quantity, int slot, unsigned rows, unsigned cols,
+                         double *out);
 /* Largest |u| over the filled save slots (0 when none): the scale of
  * post::IntensityUint8 (src/postProcessMod.cpp:23, abs of the complex
  * maximum by modulus). */

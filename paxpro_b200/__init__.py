@@ -251,6 +251,16 @@ class Solver:
         self._check(_capi.lib().pxp_get_post(self._h, int(quantity), int(slot), _dptr(out)))
         return out.reshape(shape, order="F")
 
+    def get_post_resized(self, quantity: int, rows: int, cols: int, slot: int = -1) -> np.ndarray:
+        """A post-processing quantity of a 3-D field resized on the device to
+        (rows, cols) by resizeMatrix (unchanged unless both shrink)."""
+        side = self.nx if slot < 0 else self.save_n
+        shape = (rows, cols) if (rows < side and cols < side) else (self.ny if slot < 0 else side, side)
+        out = np.empty(shape[0] * shape[1], dtype=np.float64)
+        self._check(_capi.lib().pxp_get_post_resized(self._h, int(quantity), int(slot), int(rows),
+                                                     int(cols), _dptr(out)))
+        return out.reshape(shape, order="F")
+
     def saved_max_abs(self) -> float:
         """Largest |u| over the filled save slots."""
         v = C.c_double()

@@ -115,6 +115,7 @@ def lib():
         "pxp_num_saved": (C.c_int, [h, C.POINTER(C.c_int)]),
         "pxp_get_saved": (C.c_int, [h, C.c_int, d]),
         "pxp_get_post": (C.c_int, [h, C.c_int, C.c_int, d]),
+        "pxp_get_post_resized": (C.c_int, [h, C.c_int, C.c_int, C.c_uint, C.c_uint, d]),
         "pxp_set_material_csg": (C.c_int, [h, C.POINTER(CsgModuleC), C.c_int, C.POINTER(CsgPartC),
                                            C.c_int, C.POINTER(CsgShapeC), C.c_int]),
         "pxp_saved_max_abs": (C.c_int, [h, d]),

@@ -1396,6 +1396,43 @@ int pxp_get_post(pxp_solver h, int quantity, int slot, double *out) {
   return e == cudaSuccess ? PXP_OK : h->cuda_fail(e, "post-processing reduction");
 }
 
+int pxp_get_post_resized(pxp_solver h, int quantity, int slot, unsigned rows, unsigned cols,
+                         double *out) {
+  if (h == nullptr || out == nullptr) return PXP_ERR_INVALID;
+  if (h->prob.kind != PXP_FFT_SOLVER_3D && h->prob.kind != PXP_ADI)
+    return h->fail(PXP_ERR_UNSUPPORTED, "resized post-processing applies to the 3-D kinds");
+  if (quantity < PXP_POST_ABS || quantity > PXP_POST_ABS2)
+    return h->fail(PXP_ERR_INVALID, "unknown post-processing quantity");
+  if (rows == 0 || cols == 0) return h->fail(PXP_ERR_INVALID, "export dimensions must be positive");
+  const void *src = h->d_field;
+  long long side = h->nx;
+  if (slot >= 0) {
+    int c = 0;
+    pxp_num_saved(h, &c);
+    if (slot >= c) return h->fail(PXP_ERR_INVALID, "save slot " + std::to_string(slot) + " not filled");
+    src = (const char *)h->d_saves + (size_t)slot * h->csize * h->save_pts;
+    side = h->save_n;
+  }
+  // resizeMatrix returns the matrix unchanged unless both dimensions shrink
+  if (rows >= side || cols >= side) return pxp_get_post(h, quantity, slot, out);
+  if (int rc = check_waits(h)) return rc;
+  const long long n = side * side;
+  double *d_full = nullptr, *d_small = nullptr;
+  PXP_TRY_CUDA(h, cudaMallocAsync((void **)&d_full, sizeof(double) * n, h->stream));
+  cudaError_t e = cudaMallocAsync((void **)&d_small, sizeof(double) * rows * cols, h->stream);
+  if (e == cudaSuccess) e = pxp::launch_post(h->prec, src, d_full, n, quantity, h->stream);
+  if (e == cudaSuccess) {
+    const double dX = (double)side / ((double)cols + 1.0), dY = (double)side / ((double)rows + 1.0);
+    e = pxp::launch_resize(d_full, side, d_small, (int)rows, (int)cols, dY, dX, h->stream);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, d_small, sizeof(double) * rows * cols, cudaMemcpyDeviceToHost, h->stream);
+  cudaFreeAsync(d_full, h->stream);
+  if (d_small) cudaFreeAsync(d_small, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? PXP_OK : h->cuda_fail(e, "resized post-processing");
+}
+
 int pxp_saved_max_abs(pxp_solver h, double *max_abs) {
   if (h == nullptr || max_abs == nullptr) return PXP_ERR_INVALID;
   int c = 0;

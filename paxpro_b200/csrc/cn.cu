@@ -110,6 +110,9 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
 
   for (int st = 0; st < job.nsteps; ++st) {
     const int step = job.step0 + st;
+    // this step's flux window, loaded early so its latency hides behind the step
+    int2 fw;
+    const bool flux = FLUX && flux_window(job.flux, step, fw);
     const long long moff = job.mat_stride * (long long)(step - job.mat_step0);
     // ---- 1. rows of this chunk
     double2 dg[M], rh[M];
@@ -150,9 +153,7 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * n : nullptr;
-    int2 fw;
-    const bool flux = FLUX && flux_window(job.flux, step, fw);
-    FluxSum acc;
+    double acc = 0.0;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const C v = from_d<R>(chunk_value<M>(m, xf, xl, y, p, q));
@@ -218,6 +219,9 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
   C *saves = reinterpret_cast<C *>(job.saves);
   for (int st = 0; st < job.nsteps; ++st) {
     const int step = job.step0 + st;
+    // this step's flux window, loaded early so its latency hides behind the step
+    int2 fw;
+    const bool flux = FLUX && flux_window(job.flux, step, fw);
     xch[2 * t] = u[0];
     xch[2 * t + 1] = u[M - 1];
     __syncthreads();
@@ -235,9 +239,7 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
-    int2 fw;
-    const bool flux = FLUX && flux_window(job.flux, step, fw);
-    FluxSum acc;
+    double acc = 0.0;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const C v = from_d<R>(rh[m]);

@@ -69,6 +69,9 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
   const R nreal = (R)N;
   for (int s = 0; s < job.nsteps; ++s) {
     const int step = job.step0 + s;
+    // this step's flux window, loaded early so its latency hides behind the step
+    int2 fw;
+    const bool flux = FLUX && flux_window(job.flux, step, fw);
     fft_smem<C, N, T, -1>(u, tw, lane);
     for (int i = lane; i < N; i += T) u[sw<C>(i)] = kmul<R>(u[sw<C>(i)], kern[i]);
     __syncthreads();
@@ -77,9 +80,7 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
-    int2 fw;
-    const bool flux = FLUX && flux_window(job.flux, step, fw);
-    FluxSum acc;
+    double acc = 0.0;
     for (int i = lane; i < N; i += T) {
       C v = u[sw<C>(i)];
       refract<R>(v, trans[i], nreal);

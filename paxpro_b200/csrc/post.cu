@@ -56,7 +56,7 @@ template <typename R, int T>
 __global__ void __launch_bounds__(T) flux_sum_kernel(const typename Cx<R>::T *__restrict__ u, int a,
                                                      int b, double *__restrict__ out) {
   __shared__ double red[flux_slots<T>()];
-  FluxSum acc;
+  double acc = 0.0;
   const int2 w = make_int2(a, b);
   for (int i = a + (int)threadIdx.x; i <= b; i += T) flux_add(acc, i, w, to_d(u[i]));
   flux_warp_total<T>(acc, red);

@@ -11,7 +11,8 @@ include/postProcessMod.hpp) turn a solver's stored fields into the datasets
     the 3-D solvers;
   * projection quantities of the exit field -- `ExitField` ("exitField",
     Re u), `ExitIntensity` ("exitIntensity", |u|^2), `ExitPhase`
-    ("exitPhase", arg u): a vector (2-D) or a matrix (3-D).
+    ("exitPhase", arg u): a vector (2-D) or a matrix (3-D), resized on the
+    device after set_export_dimensions; `FarField` ("farField").
 
 The stored slices are the initial condition (slice 0, from the host copy the
 solver keeps when it was given a host array) followed by the saved fields
@@ -60,6 +61,13 @@ def _block_average(u: np.ndarray, m: int) -> np.ndarray:
 class PostProcessingModule:
     name = ""
     is_uint8 = False
+    export_dims = None
+
+    def set_export_dimensions(self, rows: int, cols: int) -> None:
+        """PostProcessingModule::setExportDimensions (src/postProcessing.cpp:51-56):
+        3-D projection results are resized by resizeMatrix (:29-49), on the
+        device, when both dimensions are smaller."""
+        self.export_dims = (int(rows), int(cols))
 
     def result(self, solver) -> np.ndarray:
         raise NotImplementedError
@@ -149,6 +157,8 @@ class ProjectionQuantity(PostProcessingModule):
     quantity = _capi.POST_REAL
 
     def result(self, solver) -> np.ndarray:
+        if solver.three_d and self.export_dims:
+            return solver.get_post_resized(self.quantity, *self.export_dims)
         return solver.get_post(self.quantity, -1)
 
 
@@ -168,6 +178,38 @@ class ExitPhase(ProjectionQuantity):
     """arg u of the exit field (post::ExitPhase, :134-150)."""
     name = "exitPhase"
     quantity = _capi.POST_ARG
+
+
+class FarField(ProjectionQuantity):
+    """post::FarField (src/farFieldPost.cpp): |FFT| of the padded exit field
+    (2-D) or the |.|^2 / L of the two padded transforms of the exit field
+    minus a reference (3-D), over the angular window, computed on the
+    device by Solver.farfield."""
+    name = "farField"
+
+    def __init__(self, pad_length: int = 0, phi_min: float = -90.0, phi_max: float = 90.0,
+                 padding: int = _capi.PAD_ZERO, pad_value: complex = 0.0,
+                 subtract_reference: bool = False):
+        self.pad_length = pad_length
+        self.phi = (phi_min, phi_max)
+        self.padding = padding
+        self.pad_value = pad_value
+        self.subtract_reference = subtract_reference
+
+    def set_angle_range(self, phi_min: float, phi_max: float) -> None:
+        self.phi = (float(phi_min), float(phi_max))
+
+    def attributes(self, solver) -> dict:
+        """FarField::addAttrib (src/farFieldPost.cpp:131-139)."""
+        k = solver.spec.wavenumber
+        return {"phiMin": self.phi[0], "phiMax": self.phi[1],
+                "qmin": self.phi[0] * k * math.pi / 180.0, "qmax": self.phi[1] * k * math.pi / 180.0}
+
+    def result(self, solver) -> np.ndarray:
+        return solver.farfield(pad_length=self.pad_length, phi_min=self.phi[0],
+                               phi_max=self.phi[1], padding=self.padding, pad_value=self.pad_value,
+                               export_dims=self.export_dims or (0, 0),
+                               subtract_reference=self.subtract_reference)
 
 
 def group_attributes(solver, description: str = "") -> dict:
@@ -197,6 +239,11 @@ def save(solver, path: str, modules: Iterable[PostProcessingModule], description
         f = os.path.join(d, mod.name + ".npy")
         np.save(f, arr)
         written.append(f)
+    attrs = group_attributes(solver, description)
+    for mod in modules:
+        extra = getattr(mod, "attributes", None)
+        if extra is not None:
+            attrs[mod.name] = extra(solver)
     with open(os.path.join(d, "attributes.json"), "w") as fh:
-        json.dump(group_attributes(solver, description), fh, indent=1, sort_keys=True)
+        json.dump(attrs, fh, indent=1, sort_keys=True)
     return written

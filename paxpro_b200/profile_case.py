@@ -60,12 +60,17 @@ def main(argv=None) -> int:
     ap.add_argument("steps", type=int)
     ap.add_argument("--fp32", action="store_true")
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--flux", action="store_true",
+                    help="2-D kinds: per-step flux windows over the whole line (Transmittivity)")
     ap.add_argument("--pad", type=int, default=32768)
     ap.add_argument("--angle", type=float, default=0.05)
     a = ap.parse_args(argv)
     if a.kind == "farfield":
         return farfield(a)
     s = make(a.kind, a.n, a.steps, 1 if a.fp32 else 0)
+    if a.flux:
+        total = a.steps * max(a.repeat, 1)
+        s.set_flux_windows(1, np.zeros(total, np.uint32), np.full(total, a.n - 1, np.uint32))
     import torch
     st = torch.cuda.ExternalStream(s.stream_ptr())
     times = []
@@ -78,7 +83,8 @@ def main(argv=None) -> int:
         times.append(e0.elapsed_time(e1) / a.steps)
     out = s.get_last_solution()
     assert np.all(np.isfinite(out))
-    print(f"{a.kind} n={a.n} steps={a.steps} {'fp32' if a.fp32 else 'fp64'}: "
+    print(f"{a.kind} n={a.n} steps={a.steps} {'fp32' if a.fp32 else 'fp64'}"
+          f"{' flux' if a.flux else ''}: "
           f"{min(times) * 1e3:.2f} us/step (min of {a.repeat})")
     s.close()
     return 0

@@ -125,6 +125,26 @@ class GenericScattering:
                                      phi_max=self._phi[1], export_dims=(self.exportNx, self.exportNy),
                                      subtract_reference=self.subtract_reference)
 
+    def modules(self):
+        """The modules GenericScattering attaches (src/genericScattering.cpp:
+        28-33, 121): ExitField, ExitIntensity, ExitPhase and FarField, each
+        with the export dimensions."""
+        from . import post
+        mods = [post.ExitField(), post.ExitIntensity(), post.ExitPhase(),
+                post.FarField(self.FFTPadLength, self._phi[0], self._phi[1],
+                              subtract_reference=self.subtract_reference)]
+        for m in mods:
+            m.set_export_dimensions(self.exportNx, self.exportNy)
+        return mods
+
+    def save(self, path: str):
+        """The datasets ParaxialSimulation::save writes for this simulation,
+        as .npy files (see paxpro_b200.post.save)."""
+        from . import post
+        if self._solver is None:
+            raise RuntimeError("solve() first")
+        return post.save(self._solver, path, self.modules(), self.description)
+
     def close(self) -> None:
         if self._solver is not None:
             self._solver.close()

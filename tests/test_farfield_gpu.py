@@ -128,7 +128,7 @@ def test_farfield_fp32_field_and_errors():
 
 
 @pytest.mark.parametrize("propagator", ["fft", "adi"])
-def test_python_generic_scattering(propagator):
+def test_python_generic_scattering(propagator, tmp_path):
     """paxpro_b200.scattering.GenericScattering: the reference run, the sample
     run and the far field against the oracle on the same fields."""
     import paxpro_b200 as pxp
@@ -168,3 +168,32 @@ def test_python_generic_scattering(propagator):
                                reference=gs.reference, export_rows=64, export_cols=64)
         assert ff.shape == want.shape == (64, 64)
         assert _rel(ff, want) <= TOL
+        # the saved datasets: projections resized to the export dimensions on the device
+        written = gs.save(str(tmp_path))
+        names = sorted(os.path.basename(w) for w in written)
+        assert names == ["exitField.npy", "exitIntensity.npy", "exitPhase.npy", "farField.npy"]
+        d = os.path.join(str(tmp_path), "data")
+        assert _rel(np.load(os.path.join(d, "farField.npy")), want) <= TOL
+        ei = np.load(os.path.join(d, "exitIntensity.npy"))
+        want_ei = off.resize_matrix(np.abs(gs.exit_field) ** 2, 64, 64)
+        assert ei.shape == (64, 64) and _rel(ei, want_ei) <= 1e-13
+        ef = np.load(os.path.join(d, "exitField.npy"))
+        assert _rel(ef, off.resize_matrix(gs.exit_field.real, 64, 64)) <= 1e-13
+
+
+def test_resized_post_quantities_match_resize_matrix():
+    """pxp_get_post_resized: the device's |u|^2, Re u and arg u of a 3-D
+    field resized by resizeMatrix equal the restatement on the same field;
+    export dimensions not smaller in both directions return the field."""
+    from paxpro_b200 import _capi
+    s, dx = _solver3d("fft3d", 256)
+    with s:
+        u = s.get_last_solution()
+        for q, f in ((_capi.POST_ABS2, lambda a: np.abs(a) ** 2), (_capi.POST_REAL, np.real),
+                     (_capi.POST_ARG, np.angle)):
+            got = s.get_post_resized(q, 100, 60)
+            want = off.resize_matrix(f(u), 100, 60)
+            assert got.shape == (100, 60)
+            np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-15)
+        full = s.get_post_resized(_capi.POST_ABS2, 300, 60)
+        np.testing.assert_allclose(full, np.abs(u) ** 2, rtol=4e-16 * 4, atol=0)
