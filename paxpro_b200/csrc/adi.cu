@@ -548,6 +548,13 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
       for (int p = tid; p < N; p += T) tile[L::at(p / M, p % M, g)] = mk(0.0, 0.0);
   __syncthreads();
   if (tid == 0) bulk_load(gs, tabs, (unsigned)(sizeof(double2) * 4 * N), bar);
+  // Programmatic dependent launch: everything above (barrier set-up, zero
+  // rows, the table copy) does not depend on the previous kernel in the
+  // stream, so it may overlap that kernel's tail; the field is read and
+  // written only after the previous grid has completed and its writes are
+  // visible.  The next kernel may likewise start its own set-up early.
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   if constexpr (XH) {
     // the RW staged systems of a position are adjacent in memory:
     // consecutive threads take consecutive systems
@@ -636,8 +643,19 @@ static cudaError_t adi_const_wave_launch_x(const AdiHalf &h, const void *tabs, c
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (attr != cudaSuccess) return attr;
   }
-  k<<<(N + G - 1) / G, T, smem, s>>>(h, (const double2 *)tabs);
-  return cudaGetLastError();
+  // launched as a programmatic dependent of the previous kernel in the
+  // stream (the kernel waits for it with griddepcontrol.wait)
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((N + G - 1) / G);
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, h, (const double2 *)tabs);
 }
 
 template <int N, int M, int G, int S>
