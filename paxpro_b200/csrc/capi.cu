@@ -852,7 +852,8 @@ int cn_write_job(pxp_solver_s *h) {
   j.saves = h->d_saves;
   j.rho = dz / (k * dx * dx);  // CrankNicholson::solveStep (src/crancNicholson.cpp:25-26)
   j.r = k * dz;
-  j.n = (int)n;
+  j.n = pxp::cn_padded_n((int)n);
+  j.n_real = (int)n;
   j.save_every = h->save_every;
   j.max_slots = h->max_slots;
   j.mat_step0 = h->mat_step0;
@@ -949,7 +950,11 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
   bool supported = false;
   switch (p.kind) {
     case PXP_FFT_SOLVER_2D: supported = pxp::fft1d_supported(h->prec, (int)h->nx); break;
-    case PXP_CRANK_NICHOLSON: supported = pxp::cn_supported(h->prec, (int)h->nx); break;
+    case PXP_CRANK_NICHOLSON:
+      // a grid that is padded to the kernel's row count takes Dirichlet ends only
+      supported = pxp::cn_supported(h->prec, (int)h->nx) &&
+                  (!p.transparent_bc || pxp::cn_padded_n((int)h->nx) == (int)h->nx);
+      break;
     case PXP_ADI: supported = pxp::adi_supported(h->prec, (int)h->nx); break;
     case PXP_FFT_SOLVER_3D: supported = pxp::fft3d_supported(h->prec, (int)h->nx); break;
     default: supported = false;
@@ -1303,8 +1308,8 @@ int pxp_step(pxp_solver h, int nsteps) {
         e = pxp::launch_cn_const(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first,
                                  nsteps, h->stream, h->flux_count > 0);
       else
-        e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first,
-                           nsteps, h->stream, h->flux_count > 0);
+        e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, pxp::cn_padded_n((int)h->nx),
+                           (int)first, nsteps, h->stream, h->flux_count > 0);
       break;
     case PXP_ADI: {
       int rc = adi_steps(h, (unsigned)first, nsteps);
@@ -2017,7 +2022,8 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
       e = pxp::launch_cn_const((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
                                k.n, -1, -1, b->stream, any_flux);
     else
-      e = pxp::launch_cn((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(), k.n,
+      e = pxp::launch_cn((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
+                         pxp::cn_padded_n(k.n),
                          -1, -1, b->stream, any_flux);
     if (e != cudaSuccess) return b->fail(PXP_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     for (pxp_solver_s *h : list) {

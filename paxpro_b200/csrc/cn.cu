@@ -81,6 +81,9 @@ __device__ __forceinline__ void cn_tbc(double2 outer, double2 inner, double rho,
   rhs = cx_add_rn(rhs, cx_mul_rn(coef, outer));
 }
 
+// Diagonal of the padding rows of a system padded to M * T rows.
+constexpr double kCnPad = 1e30;
+
 template <typename R, int M, int T, bool FLUX>
 __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, int step0_ov,
                                               int nsteps_ov) {
@@ -93,6 +96,10 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
     job.nsteps = nsteps_ov;
   }
   const int n = job.n;  // == M * T
+  // rows at and beyond nreal pad the system to M * T: diagonal kCnPad, zero
+  // right-hand side and zero field, so they decouple from row nreal - 1 to
+  // within |sub|^2 / kCnPad (the field beyond the grid is the Dirichlet zero)
+  const int nreal = job.n_real > 0 ? job.n_real : n;
   const int nr = 2 * T;
   double2 *ra = reinterpret_cast<double2 *>(smem_raw);
   double2 *rb = ra + nr;
@@ -101,7 +108,7 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
   C *u = reinterpret_cast<C *>(rd + nr);
   const int t = threadIdx.x;
   C *field = reinterpret_cast<C *>(job.field);
-  for (int i = t; i < n; i += T) u[i] = field[i];
+  for (int i = t; i < n; i += T) u[i] = i < nreal ? field[i] : C{};
   __syncthreads();
   const double rho = job.rho, r = job.r;
   const double2 sub = mk(-0.0, __dmul_rn(-0.25, rho));  // -0.25*i*rho*H-*g
@@ -119,9 +126,14 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       int i = s0 + m;
+      if (i >= nreal) {
+        dg[m] = mk(kCnPad, 0.0);
+        rh[m] = mk(0.0, 0.0);
+        continue;
+      }
       double2 center = to_d(u[i]);
       double2 left = i > 0 ? to_d(u[i - 1]) : mk(0.0, 0.0);
-      double2 right = i < n - 1 ? to_d(u[i + 1]) : mk(0.0, 0.0);
+      double2 right = i < nreal - 1 ? to_d(u[i + 1]) : mk(0.0, 0.0);
       double de = job.delta[moff + i], be = job.beta[moff + i];
       double dp = job.delta_prev[moff + i], bp = job.beta_prev[moff + i];
       dg[m] = cn_diag(de, be, rho, r);
@@ -152,20 +164,20 @@ __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, i
     const double2 xf = rd[2 * t], xl = rd[2 * t + 1];
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
-    C *slot = save ? saves + (long long)(step / job.save_every - 1) * n : nullptr;
+    C *slot = save ? saves + (long long)(step / job.save_every - 1) * nreal : nullptr;
     double acc = 0.0;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const C v = from_d<R>(chunk_value<M>(m, xf, xl, y, p, q));
       u[s0 + m] = v;
-      if (save) slot[s0 + m] = v;
+      if (save && s0 + m < nreal) slot[s0 + m] = v;
       if (flux) flux_add(acc, s0 + m, fw, to_d(v));
     }
     if (flux) flux_warp_total<T>(acc, flux_red[st & 1]);
     __syncthreads();
     if (flux) flux_store<T>(job.flux, step, flux_red[st & 1]);
   }
-  for (int i = t; i < n; i += T) field[i] = u[i];
+  for (int i = t; i < nreal; i += T) field[i] = u[i];
 }
 
 // z-invariant medium, Dirichlet ends: the step matrix is fixed, so the
@@ -327,9 +339,16 @@ static cudaError_t cn_launch_t(const CnJob *d_jobs, int nj, int step0, int nstep
               : cn_launch_f<R, T, false>(d_jobs, nj, step0, nsteps, s);
 }
 
+int cn_padded_n(int n) {
+  int t = 2;
+  while (t * kCnM < n) t *= 2;
+  return t * kCnM;
+}
+
 bool cn_supported(Precision p, int n) {
-  if (n < 2 * kCnM || (n & (n - 1))) return false;
-  return p == kFP64 ? n <= 4096 : n <= 8192;
+  if (n < 2 * kCnM) return false;
+  const int np = cn_padded_n(n);
+  return p == kFP64 ? np <= 4096 : np <= 8192;
 }
 
 cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0, int nsteps,

@@ -59,7 +59,8 @@ struct CnJob {
   long long mat_stride;        // doubles between per-step planes (0 = z-invariant)
   void *saves;
   double rho, r;               // dz/(k dx^2), k dz
-  int n;
+  int n;                       // rows solved: Nx, or Nx padded to M*T (cn_padded_n)
+  int n_real;                  // Nx; rows n_real..n-1 are decoupled padding
   int step0, nsteps, save_every, max_slots, mat_step0;
   int transparent;             // BC_t::TRANSPARENT
   int status;                  // unused (reserved)
@@ -69,6 +70,9 @@ struct CnJob {
 cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
                       int nsteps, cudaStream_t s, bool flux = false);
 bool cn_supported(Precision p, int n);
+// Rows the general CN kernel solves for Nx = n: n itself when n/8 is a
+// power of two, else n padded up to 8 times the next power of two.
+int cn_padded_n(int n);
 // z-invariant medium and Dirichlet ends: the step matrix never changes; the
 // job's lu_g / lu_h hold its Thomas factor tables (n complex128 each).
 cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0,

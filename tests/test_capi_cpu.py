@@ -51,3 +51,18 @@ def test_transverse_downsampling_of_2d_solvers_is_rejected_before_any_device_cal
     rc = _capi.lib().pxp_solver_create(C.byref(spec.to_c()), C.byref(h))
     assert rc == _capi.PXP_ERR_UNSUPPORTED
     assert "downsampling" in _capi.last_error()
+
+
+def test_transparent_ends_on_a_padded_cn_grid_are_rejected_before_any_device_call():
+    """CrankNicholson takes any Nx with Dirichlet ends; transparent ends need
+    Nx / 8 to be a power of two (the kernel pads other sizes)."""
+    import ctypes as C
+    import paxpro_b200 as pxp
+    from paxpro_b200 import _capi
+    from paxpro_b200 import workloads as wl
+    dx = wl.step_for_nodes(-250.0, 250.0, 300)
+    spec = pxp.ProblemSpec(kind=pxp.CRANK_NICHOLSON, x=pxp.Disc(-250.0, 250.0, dx),
+                           z=pxp.Disc(0.0, 1e4, 500.0), wavenumber=62.8, transparent_bc=True)
+    h = C.c_void_p()
+    rc = _capi.lib().pxp_solver_create(C.byref(spec.to_c()), C.byref(h))
+    assert rc == _capi.PXP_ERR_UNSUPPORTED
