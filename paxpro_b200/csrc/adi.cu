@@ -70,11 +70,19 @@ __device__ __forceinline__ double2 tbc_factor(double2 num, double2 den) {
   return cx_mul_rn(mk(0.0, 0.5), mk(e * cs, e * sn));
 }
 
+// Diagonal of the padding rows of a system padded to M times a power of two.
+constexpr double kAdiPad = 1e30;
+
 template <typename R, int M, int G>
 __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
   using C = typename Cx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int n = h.n;
+  // n: rows of each solved system (h.n, or h.n padded to M times a power of
+  // two); nreal: the grid's positions per system and its number of systems.
+  // Pad rows get diagonal kAdiPad, zero right-hand side and zero field, so
+  // they decouple from the last real row to within |sub|^2 / kAdiPad.
+  const int n = h.n_pad > 0 ? h.n_pad : h.n;
+  const int nreal = h.n;
   const int P = n / M;        // chunks per system
   const int T = G * P;        // threads
   const int ld = n + n / 8 + 2;  // padded row of the staging tile (pad8)
@@ -101,7 +109,8 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
     }
     const int s = s_base - 1 + g;
     C v = from_d<R>(mk(0.0, 0.0));
-    if (s >= 0 && s < n) v = in[(long long)p * h.stride_pos + (long long)s * h.stride_sys];
+    if (s >= 0 && s < nreal && p < nreal)
+      v = in[(long long)p * h.stride_pos + (long long)s * h.stride_sys];
     tile[g * ld + pad8(p)] = v;
   }
   __syncthreads();
@@ -123,6 +132,11 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     const int p = p0 + m;
+    if (p >= nreal) {
+      dg[m] = mk(kAdiPad, 0.0);
+      rh[m] = mk(0.0, 0.0);
+      continue;
+    }
     // coordinates: position runs along x in the x half step, along y in the y half step
     double x, y;
     const double pos_c = (double)p, sys_c = (double)s;
@@ -154,18 +168,23 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
     double2 r = cmul(mk(h.inv_dzh, -inv_kd2_expl), uc);
     double2 nb = mk(0.0, 0.0);
     if (s > 0) nb = to_d(lft[pad8(p)]);
-    if (s < n - 1) nb = cadd(nb, to_d(rgt[pad8(p)]));
+    if (s < nreal - 1) nb = cadd(nb, to_d(rgt[pad8(p)]));
     const double hk = 0.5 * inv_kd2_expl;
     r = mk(fma(-hk, nb.y, r.x), fma(hk, nb.x, r.y));
     rh[m] = r;
   }
   if (h.use_tbc) {
     const double zero = 1e-6;
-    // along the system (implicit direction): diagonal at both ends
-    if (c == P - 1) {
-      double2 inner = to_d(ctr[pad8(n - 2)]);
-      if (hypot(inner.x, inner.y) > zero)
-        dg[M - 1] = cx_sub_rn(dg[M - 1], cx_div_real_rn(tbc_factor(to_d(ctr[pad8(n - 1)]), inner), h.kd2_impl));
+    // along the system (implicit direction): diagonal at both ends (the last
+    // real row: row n - 1 of an unpadded system)
+    if (p0 <= nreal - 1 && nreal - 1 < p0 + M) {
+      double2 inner = to_d(ctr[pad8(nreal - 2)]);
+      if (hypot(inner.x, inner.y) > zero) {
+        const double2 t = cx_div_real_rn(tbc_factor(to_d(ctr[pad8(nreal - 1)]), inner), h.kd2_impl);
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+          if (p0 + m == nreal - 1) dg[m] = cx_sub_rn(dg[m], t);
+      }
     }
     if (c == 0) {
       double2 inner = to_d(ctr[pad8(1)]);
@@ -173,11 +192,12 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
         dg[0] = cx_sub_rn(dg[0], cx_div_real_rn(tbc_factor(to_d(ctr[pad8(0)]), inner), h.kd2_impl));
     }
     // across systems (explicit direction): rhs of the first and last system
-    if (s == n - 1 || s == 0) {
-      const C *inner_row = (s == n - 1) ? lft : rgt;
+    if (s == nreal - 1 || s == 0) {
+      const C *inner_row = (s == nreal - 1) ? lft : rgt;
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         const int p = p0 + m;
+        if (p >= nreal) continue;
         double2 inner = to_d(inner_row[pad8(p)]);
         if (hypot(inner.x, inner.y) > zero) {
           double2 edge = to_d(ctr[pad8(p)]);
@@ -213,6 +233,7 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
       gg = idx / n;
       p = idx - gg * n;
     }
+    if (p >= nreal || s_base + gg >= nreal) continue;
     const long long off = (long long)p * h.stride_pos + (long long)(s_base + gg) * h.stride_sys;
     const C v = tile[(gg + 1) * ld + pad8(p)];
     out[off] = v;
@@ -755,7 +776,7 @@ template <int G> constexpr int adi_threads(int n) { return G * (n / kAdiM); }
 template <typename R, int G>
 static cudaError_t adi_launch_g(const AdiHalf &h, cudaStream_t s) {
   using C = typename Cx<R>::T;
-  const int n = h.n;
+  const int n = h.n_pad > 0 ? h.n_pad : h.n;  // solved system length
   const int T = adi_threads<G>(n);
   const size_t tile = (sizeof(C) * (G + 2) * (n + n / 8 + 2) + 15) & ~size_t(15);
   const size_t smem = tile + sizeof(double2) * 4 * G * 2 * (n / kAdiM);
@@ -767,7 +788,7 @@ static cudaError_t adi_launch_g(const AdiHalf &h, cudaStream_t s) {
       (int)(((sizeof(C) * (G + 2) * (G == 2 ? 2048 + 258 : 1024 + 130) + 15) & ~size_t(15)) +
             sizeof(double2) * 4 * G * 2 * ((G == 2 ? 2048 : 1024) / kAdiM)));
   if (attr != cudaSuccess) return attr;
-  k<<<n / G, T, smem, s>>>(h);
+  k<<<(h.n + G - 1) / G, T, smem, s>>>(h);  // one CTA per G of the grid's h.n systems
   return cudaGetLastError();
 }
 
@@ -776,10 +797,22 @@ bool adi_supported(Precision p, int n) {
   return p == kFP64 ? n <= 2048 : n <= 2048;
 }
 
+int adi_padded_n(int n) {
+  if (n >= 64 && !(n & (n - 1))) return n;
+  int t = 8;
+  while (t * kAdiM < n) t *= 2;
+  return t * kAdiM;
+}
+
+bool adi_padded_supported(Precision p, int n) {
+  return n >= 4 && adi_supported(p, adi_padded_n(n));
+}
+
 cudaError_t launch_adi_half(Precision p, const AdiHalf &h, cudaStream_t s) {
-  if (!adi_supported(p, h.n)) return cudaErrorInvalidValue;
+  const int np = h.n_pad > 0 ? h.n_pad : h.n;
+  if (!adi_supported(p, np) || h.n > np) return cudaErrorInvalidValue;
   // G systems per CTA so that G * n/8 <= 512 threads
-  if (h.n <= 1024) return p == kFP64 ? adi_launch_g<double, 4>(h, s) : adi_launch_g<float, 4>(h, s);
+  if (np <= 1024) return p == kFP64 ? adi_launch_g<double, 4>(h, s) : adi_launch_g<float, 4>(h, s);
   return p == kFP64 ? adi_launch_g<double, 2>(h, s) : adi_launch_g<float, 2>(h, s);
 }
 

@@ -573,6 +573,7 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   const long long n = h->nx;
   pxp::AdiHalf a{};
   a.n = (int)n;
+  a.n_pad = pxp::adi_padded_n((int)n) != (int)n ? pxp::adi_padded_n((int)n) : 0;
   a.use_tbc = p.transparent_bc ? 1 : 0;
   a.inv_dzh = 1.0 / dzh;
   a.k = k;
@@ -955,7 +956,11 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
       supported = pxp::cn_supported(h->prec, (int)h->nx) &&
                   (!p.transparent_bc || pxp::cn_padded_n((int)h->nx) == (int)h->nx);
       break;
-    case PXP_ADI: supported = pxp::adi_supported(h->prec, (int)h->nx); break;
+    case PXP_ADI:
+      // other sizes run padded on the general kernel
+      supported = pxp::adi_supported(h->prec, (int)h->nx) ||
+                  pxp::adi_padded_supported(h->prec, (int)h->nx);
+      break;
     case PXP_FFT_SOLVER_3D: supported = pxp::fft3d_supported(h->prec, (int)h->nx); break;
     default: supported = false;
   }
@@ -1008,7 +1013,9 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
     case PXP_ADI:
       if ((rc = alloc(h, &h->d_field2, h->csize * h->npts, "second field buffer")))
         return cleanup_fail(rc);
-      if ((rc = adi_build_lu(h))) return cleanup_fail(rc);
+      // vacuum factor tables for the step-invariant kernels (grids those run)
+      if (pxp::adi_supported(h->prec, (int)h->nx))
+        if ((rc = adi_build_lu(h))) return cleanup_fail(rc);
       break;
     case PXP_FFT_SOLVER_3D:
       if ((rc = shared_table(h, 0, &h->d_tw))) return cleanup_fail(rc);

@@ -120,7 +120,9 @@ struct AdiHalf {
   void *out;
   void *save;              // optional extra copy of the output (save slot)
   long long stride_pos, stride_sys;
-  int n;
+  int n;                   // Nx = Ny: positions per system and number of systems
+  int n_pad;               // 0, or the padded system length the general kernel
+                           // solves (adi_padded_n; rows n..n_pad-1 decoupled)
   int y_implicit;          // 1: y-implicit diagonal formula (reference :103)
   int use_tbc;             // ADI::useTBC
   int nspheres;            // active spheres; > kInlineSpheres: use spheres_all
@@ -136,6 +138,11 @@ struct AdiHalf {
 };
 cudaError_t launch_adi_half(Precision p, const AdiHalf &h, cudaStream_t s);
 bool adi_supported(Precision p, int n);
+// System length the general ADI kernel solves for Nx = n (n itself for the
+// powers of two adi_supported takes, else 8 times the next power of two),
+// and whether that kernel runs n.
+int adi_padded_n(int n);
+bool adi_padded_supported(Precision p, int n);
 // Half step whose plane holds no material and no transparent boundary: the
 // matrix is the same for every system and every step; g/h are its Thomas
 // factor tables (n complex128 each, see scan_solve.cuh).

@@ -101,15 +101,15 @@ def test_csg3d_example(kind):
     assert np.std(np.abs(last)) > 1e-4
 
 
-@pytest.mark.parametrize("kind", ["fft", "adi"])
-def test_generic_scattering_example(kind):
+@pytest.mark.parametrize("kind,n", [("fft", 128), ("adi", 128), ("adi", 129)])
+def test_generic_scattering_example(kind, n):
     """GenericScattering: the vacuum reference run (three steps), the run
     through the sphere and the far field of the difference, resized to the
     export dimensions, against the oracle."""
     from oracle import farfield as off
     exe = build("scattering3d")
-    n, steps, pad, ang, exp = 128, 6, 1024, 0.05, 64
-    out = os.path.join(OUT, f"gs_{kind}.bin")
+    steps, pad, ang, exp = 6, 1024, 0.05, 64
+    out = os.path.join(OUT, f"gs_{kind}_{n}.bin")
     r = subprocess.run([exe, kind, str(n), str(steps), str(pad), str(ang), str(exp), out],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

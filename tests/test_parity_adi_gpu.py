@@ -95,3 +95,24 @@ def test_adi_fp32_served_intensity():
     out, saves, ref_out, ref_saves = _run_both(256, 0.0, 200, 1000.0, sph, precision=1,
                                                save_every=50)
     assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
+
+
+@pytest.mark.parametrize("n,use_tbc,precision", [(100, False, 0), (300, False, 0), (129, True, 0),
+                                                 (200, False, 1)])
+def test_adi_any_grid_size(n, use_tbc, precision):
+    """ADI on grids whose size is not a power of two (the general kernel
+    pads every system with decoupled rows): every save against the oracle,
+    with a sphere crossing the planes, Dirichlet and transparent ends."""
+    sph = [(30.0, -20.0, 3000.0, 250.0, 4.5e-5, 3.6e-6)]
+    x = -500.0 + wl.step_for_nodes(-500.0, 500.0, n) * np.arange(n)
+    u0 = np.asfortranarray(np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / 300.0 ** 2)
+                           .astype(np.complex128))
+    out, saves, ref_out, ref_saves = _run_both(n, 0.0, 8, 1000.0, sph, u0=u0, use_tbc=use_tbc,
+                                               precision=precision)
+    assert len(saves) == len(ref_saves) == 8
+    if precision == 0:
+        assert max(_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP64_TOL
+        assert _rel(out, ref_out) <= FP64_TOL
+    else:
+        assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
+    assert np.std(np.abs(out)) > 1e-3
