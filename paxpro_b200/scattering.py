@@ -9,7 +9,8 @@ resized to exportNx x exportNy, and the exit field, intensity and phase.
 
 The object is a sphere list (paxpro_b200.Sphere) or constructive solid
 geometry (paxpro_b200.csg Modules), both evaluated by the solvers on the
-device.  The solvers need a power-of-two node count per transverse axis.
+device.  With the ADI propagator any node count runs; FFTSolver3D needs a
+power of two per transverse axis.
 """
 from __future__ import annotations
 
