@@ -11,8 +11,37 @@
 #include "paxpro/paxpro.hpp"
 
 int main(int argc, char **argv) {
-  if (argc < 6) return 2;
+  if (argc < 4) return 2;
   const std::string kind = argv[1];
+  if (kind == "material") {
+    // curved2d material <smoothed> <out>: delta, beta of the guide below on
+    // a 61 x 41 grid of (x, z), x in [-400, 200], z in [0, 2e5]
+    Cladding c;
+    c.setRefractiveIndex(4.14e-5, 3.45e-6);
+    Cladding inside;
+    inside.setRefractiveIndex(1e-6, 2e-8);
+    CurvedWaveGuideFD g;
+    g.setRadiusOfCurvature(40e6);
+    g.setWidth(100.0);
+    g.setCladding(c);
+    g.setInsideMaterial(inside);
+    g.setWaveguideLength(1.5e5);
+    if (std::atoi(argv[2])) g.useSmoothedWG();
+    g.setTransverseDiscretization(-400.0, 200.0, 10.0);
+    g.setLongitudinalDiscretization(0.0, 2e5, 5000.0);
+    FILE *f = std::fopen(argv[3], "wb");
+    if (!f) return 1;
+    for (int iz = 0; iz <= 40; ++iz)
+      for (int ix = 0; ix <= 60; ++ix) {
+        double d, b;
+        g.getXrayMatProp(-400.0 + 10.0 * ix, 5000.0 * iz, d, b);
+        std::fwrite(&d, sizeof(double), 1, f);
+        std::fwrite(&b, sizeof(double), 1, f);
+      }
+    std::fclose(f);
+    return 0;
+  }
+  if (argc < 6) return 2;
   const unsigned n = std::atoi(argv[2]);
   const unsigned steps = std::atoi(argv[3]);
   const double xmin = -400.0, xmax = 200.0;
