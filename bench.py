@@ -1,19 +1,20 @@
 """Benchmark of the paraxial propagation step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg1|cfg0|cfg3|cfg4]
+                    [--workload cn4096_adi1024|waveguide_fft2d|mixed_batch|served]
 
 Metric: grid-point * steps per second (whole job, all ranks).  A bench
 "step" is one pass of the workload over its synthetic input:
 
-  cfg1 (default)  CrankNicholson Nx=4096, 8000 steps of 0.5 um  +  ADI 1024^2,
+  cn4096_adi1024 (default)
+                  CrankNicholson Nx=4096, 8000 steps of 0.5 um  +  ADI 1024^2,
                   2000 steps of 1 um (unit plane wave, sphere R = 200 nm at
                   z = 1 mm), plain FP64; the two problems run concurrently on
                   two streams.  2.13e9 grid-point-steps per bench step.
-  cfg0            FFTSolver2D Nx=2048, 4000 steps, FP64 (8.19e6 pt-steps).
-  cfg3            mixed batch (512 2-D + 32 3-D problems), FP32 served mode in
+  waveguide_fft2d FFTSolver2D Nx=2048, 4000 steps, FP64 (8.19e6 pt-steps).
+  mixed_batch     mixed batch (512 2-D + 32 3-D problems), FP32 served mode in
                   one batch, against the same problems one at a time in FP64.
-  cfg4            serving: Poisson arrivals at 50..2000 jobs/s, p50/p99
+  served          serving: Poisson arrivals at 50..2000 jobs/s, p50/p99
                   latency and throughput, against plain FP64 one at a time.
 
 Each rank runs its own replica (the path does not shard one field; weak
@@ -128,15 +129,15 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ workloads --
-class Cfg1:
+class CnAdiWorkload:
     """CN (Nx = 4096, 8000 steps) + ADI (1024^2, 2000 steps), FP64."""
-    name = "cfg1: CrankNicholson Nx=4096 x 8000 steps + ADI 1024^2 x 2000 steps, FP64"
+    name = "CrankNicholson Nx=4096 x 8000 steps + ADI 1024^2 x 2000 steps, FP64"
 
     def __init__(self, device: int, precision: int = 0):
         import paxpro_b200 as pxp
         self.pxp = pxp
-        self.cn = wl.cfg1_cn()
-        self.adi = wl.cfg1_adi()
+        self.cn = wl.waveguide_cn()
+        self.adi = wl.sphere_adi()
         c, a = self.cn, self.adi
         self.s_cn = pxp.Solver(pxp.ProblemSpec(
             kind=pxp.CRANK_NICHOLSON, x=pxp.Disc(c.xmin, c.xmax, c.dx),
@@ -175,13 +176,13 @@ class Cfg1:
             s.close()
 
 
-class Cfg0:
-    name = "cfg0: FFTSolver2D Nx=2048 x 4000 steps, FP64"
+class WaveguideFft2dWorkload:
+    name = "FFTSolver2D Nx=2048 x 4000 steps, FP64"
 
     def __init__(self, device: int, precision: int = 0):
         import paxpro_b200 as pxp
         self.pxp = pxp
-        self.p = wl.cfg0()
+        self.p = wl.waveguide_fft2d()
         p = self.p
         self.s = pxp.Solver(pxp.ProblemSpec(
             kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(p.xmin, p.xmax, p.dx),
@@ -207,11 +208,11 @@ class Cfg0:
         self.s.close()
 
 
-WORKLOADS = {"cfg1": Cfg1, "cfg0": Cfg0}
+WORKLOADS = {"cn4096_adi1024": CnAdiWorkload, "waveguide_fft2d": WaveguideFft2dWorkload}
 
 
 def run_mixed(args, rank, world, device):
-    """cfg3: the mixed batch (512 2-D + 32 3-D problems) in FP32 served mode,
+    """The mixed batch (512 2-D + 32 3-D problems) in FP32 served mode,
     one Batch per GPU, against the same problems run one at a time in plain
     FP64.  On N GPUs the one job set is split by the least-loaded scheduler
     (paxpro_b200.sharding); rates are summed grid-point*steps over the max
@@ -223,7 +224,7 @@ def run_mixed(args, rank, world, device):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    all_jobs = sv.cfg3_jobs(seed=3)
+    all_jobs = sv.mixed_batch_jobs(seed=3)
     mine = sh.partition_jobs(all_jobs, world)[rank]
     jobs = [all_jobs[i] for i in mine]
     keep = set(range(0, len(jobs), 37))
@@ -253,7 +254,7 @@ def run_mixed(args, rank, world, device):
         "vs_baseline": None,
         "dtype": "c64 storage, FP64 twiddle/factor products",
         "data": "synthetic (seeded mixed workload)",
-        "config": {"workload": "cfg3: 512 x 2-D (80% FFT, 20% CN) + 32 x 3-D FFT, one batch per GPU",
+        "config": {"workload": "mixed batch: 512 x 2-D (80% FFT, 20% CN) + 32 x 3-D FFT, one batch per GPU",
                    "grid_pt_steps": b_pts,
                    "sharding": "jobs split across GPUs, largest first to the least-loaded GPU",
                    "timing": "wall clock between device synchronisations, max over ranks"},
@@ -264,7 +265,7 @@ def run_mixed(args, rank, world, device):
 
 
 def run_serving(args, rank, world, device):
-    """cfg4: Poisson arrivals swept over rates; served FP32 continuous batching
+    """Serving: Poisson arrivals swept over rates; served FP32 continuous batching
     against plain FP64 one-at-a-time on the same job stream.  On N GPUs each
     GPU serves its own arrival stream at the rate (weak scaling); throughput
     is summed grid-point*steps over the max makespan across ranks."""
@@ -277,17 +278,17 @@ def run_serving(args, rank, world, device):
         import torch.distributed as dist
     dev = torch.device("cuda", device) if dist is not None else None
     window = float(os.environ.get("PXP_SERVE_WINDOW", "2.0"))
-    sv.serve(sv.cfg4_jobs(200.0, 0.1, seed=99), precision=1)  # warm-up
+    sv.serve(sv.served_jobs(200.0, 0.1, seed=99), precision=1)  # warm-up
     rows = []
     for rate in (50, 100, 200, 500, 1000, 2000):
-        jobs = sv.cfg4_jobs(float(rate), window, seed=4 + rate + 1000 * rank)
+        jobs = sv.served_jobs(float(rate), window, seed=4 + rate + 1000 * rank)
         r = sv.serve(jobs, precision=1, round_steps=200)
         pts, span = sh.reduce_rate(r.pts_steps, r.makespan, dist, dev)
         _, p99 = sh.reduce_rate(0.0, r.p99, dist, dev)
         rows.append({"rate_jobs_per_s_per_gpu": rate, "jobs": r.jobs, "p50_s": r.p50,
                      "p99_s_max_over_gpus": p99, "throughput": pts / span,
                      "max_active": r.max_active})
-    jobs = sv.cfg4_jobs(200.0, window, seed=204 + 1000 * rank)
+    jobs = sv.served_jobs(200.0, window, seed=204 + 1000 * rank)
     plain = sv.run_plain(jobs, precision=0)
     p_pts, p_sec = sh.reduce_rate(plain.pts_steps, plain.seconds, dist, dev)
     if rank != 0:
@@ -306,7 +307,7 @@ def run_serving(args, rank, world, device):
         "vs_baseline": None,
         "dtype": "c64 storage, FP64 twiddle/factor products",
         "data": "synthetic (seeded Poisson job stream)",
-        "config": {"workload": f"cfg4: Poisson arrivals, {window} s per rate, 80% FFT2D / 15% CN / "
+        "config": {"workload": f"served: Poisson arrivals, {window} s per rate, 80% FFT2D / 15% CN / "
                                "5% FFT3D, HBM budget 150 GB"},
         "rates": rows,
         "plain_fp64_one_at_a_time": {"value": p_pts / p_sec, "busy_seconds": p_sec,
@@ -360,7 +361,7 @@ def run_ours(args, rank, world, device):
 
     # end-to-end through the public API: host (pinned) inputs, H2D, steps, D2H
     pinned_in = [torch.from_numpy(np.ascontiguousarray(u.reshape(-1, order="F")).view(np.float64)).pin_memory()
-                 for u in ([W.u_cn, W.u_adi] if args.workload == "cfg1" else [W.u])]
+                 for u in ([W.u_cn, W.u_adi] if args.workload == "cn4096_adi1024" else [W.u])]
     pinned_out = [torch.empty_like(t).pin_memory() for t in pinned_in]
     e2e_times = []
     for it in range(args.warmup + args.steps):
@@ -399,7 +400,7 @@ def run_ours(args, rank, world, device):
     e2e_value = world * W.pts_steps / (e2e_max / 1e3)
     peak, peak_kind = measured_peaks()
     roofline = None
-    if args.workload == "cfg1":
+    if args.workload == "cn4096_adi1024":
         adi_ms = sum(st[1] for st in stream_times) / len(stream_times)
         per_launch_s = adi_ms / 1e3 / W.adi_launches_per_step
         achieved = W.adi_bytes_per_launch / per_launch_s / 1e9
@@ -441,8 +442,8 @@ def cpu_rate(workload: str, threads: int, scale: float = 1.0):
     description of the sample)."""
     from oracle import pyoracle as po
     po.set_threads(threads)
-    if workload == "cfg1":
-        c, a = wl.cfg1_cn(), wl.cfg1_adi()
+    if workload == "cn4096_adi1024":
+        c, a = wl.waveguide_cn(), wl.sphere_adi()
         n_cn = max(20, int(800 * scale))
         n_adi = max(1, int(4 * scale))
         g = po.grid(c.xmin, c.xmax, c.dx, c.zmin, c.zmax, c.dz, wl.K)
@@ -460,7 +461,7 @@ def cpu_rate(workload: str, threads: int, scale: float = 1.0):
         pts = c.nx * c.nsteps + a.nx * a.nx * a.nsteps
         return pts / total, (f"CN {n_cn} of {c.nsteps} steps ({t_cn:.2f} s) + ADI {n_adi} of "
                              f"{a.nsteps} steps ({t_adi:.2f} s), extrapolated linearly")
-    p = wl.cfg0()
+    p = wl.waveguide_fft2d()
     n = max(50, int(1000 * scale))
     g = po.grid(p.xmin, p.xmax, p.dx, p.zmin, p.zmax, p.dz, wl.K)
     d, b = p.material()
@@ -492,11 +493,11 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             rates.append(r)
     value = statistics.median(rates)
-    if args.workload not in ("cfg0", "cfg1"):
+    if args.workload not in ("waveguide_fft2d", "cn4096_adi1024"):
         print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement is timed on "
-                          "the cfg0/cfg1 workloads only"}))
+                          "the waveguide_fft2d and cn4096_adi1024 workloads only"}))
         return None
-    W = {"cfg1": Cfg1.name, "cfg0": Cfg0.name}[args.workload]
+    W = {"cn4096_adi1024": CnAdiWorkload.name, "waveguide_fft2d": WaveguideFft2dWorkload.name}[args.workload]
     return {
         "impl": "reference",
         "metric": "grid-pt*steps/s (plain FP64)",
@@ -527,7 +528,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["cfg3", "cfg4"], default="cfg1")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["mixed_batch", "served"], default="cn4096_adi1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -543,13 +544,13 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    if args.workload == "cfg3":
+    if args.workload == "mixed_batch":
         out = run_mixed(args, rank, world, local)
-    elif args.workload == "cfg4":
+    elif args.workload == "served":
         out = run_serving(args, rank, world, local)
     else:
         out = run_ours(args, rank, world, local)
-    if out is not None and not args.no_cpu_baseline and args.workload in ("cfg0", "cfg1"):
+    if out is not None and not args.no_cpu_baseline and args.workload in ("waveguide_fft2d", "cn4096_adi1024"):
         rate, sample = cpu_rate(args.workload, 1, scale=1.0)
         out["cpu_baseline"] = {"value": rate, "unit": "grid-pt*steps/s", "cores": 1,
                                "kind": "port", "sample": sample + f"; {cpu_model()}"}

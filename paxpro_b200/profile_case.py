@@ -41,7 +41,7 @@ def make(kind: str, n: int, steps: int, precision: int):
         s.set_material_table(d, b)
         u0 = p.initial_field()
     else:
-        p = wl.cfg1_adi(n=n) if kind == "adi" else wl.cfg2(n=n)
+        p = wl.sphere_adi(n=n) if kind == "adi" else wl.spheres_fft3d(n=n)
         zmin = p.zmin if kind == "fft3d" else 1.0e6 - 2 * p.dz
         s = pxp.Solver(pxp.ProblemSpec(
             kind=pxp.ADI if kind == "adi" else pxp.FFT_SOLVER_3D,

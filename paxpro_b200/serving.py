@@ -74,7 +74,7 @@ def draw_3d(rng: np.random.Generator, seed: int, sizes=(256, 512, 1024, 2048)) -
     return Job("fft3d", n, steps, seed, spheres=sph)
 
 
-def cfg3_jobs(seed: int = 3, n2d: int = 512, n3d: int = 32) -> List[Job]:
+def mixed_batch_jobs(seed: int = 3, n2d: int = 512, n3d: int = 32) -> List[Job]:
     """512 2-D problems (80 % FFT, 20 % CN) plus 32 3-D FFT problems."""
     rng = np.random.default_rng(seed)
     jobs = []
@@ -86,7 +86,7 @@ def cfg3_jobs(seed: int = 3, n2d: int = 512, n3d: int = 32) -> List[Job]:
     return jobs
 
 
-def cfg4_jobs(rate: float, duration: float, seed: int = 4) -> List[Job]:
+def served_jobs(rate: float, duration: float, seed: int = 4) -> List[Job]:
     """Poisson arrivals at `rate` jobs/s for `duration` s: 80 % 2-D FFT,
     15 % CN, 5 % 3-D FFT (N <= 2048)."""
     rng = np.random.default_rng(seed)

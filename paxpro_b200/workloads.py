@@ -11,13 +11,13 @@ these problems, so every input here is generated.
                  absorbing boundary (the reference's 2-D solvers have none;
                  Examples/waveguide2D.cpp:9-31 shows the material-function
                  pattern).
-  cfg0           FFTSolver2D, Nx = 2048 on [-250, 250], 4000 steps of 1 um,
-                 Gaussian waist 15 nm, saves every 100 steps.
-  cfg1_cn        CrankNicholson, Nx = 4096, 8000 steps of 0.5 um, same guide.
-  cfg1_adi       ADI, 1024^2 on [-500, 500]^2, 2000 steps of 1 um, unit plane
-                 wave, sphere R = 200 at (0, 0, 1 mm).
-  cfg2           FFTSolver3D, 4096^2 on [-1000, 1000]^2, 1000 steps of 2 um,
-                 unit plane wave, 64 seeded spheres.
+  waveguide_fft2d  FFTSolver2D, Nx = 2048 on [-250, 250], 4000 steps of 1 um,
+                   Gaussian waist 15 nm, saves every 100 steps.
+  waveguide_cn     CrankNicholson, Nx = 4096, 8000 steps of 0.5 um, same guide.
+  sphere_adi       ADI, 1024^2 on [-500, 500]^2, 2000 steps of 1 um, unit plane
+                   wave, sphere R = 200 at (0, 0, 1 mm).
+  spheres_fft3d    FFTSolver3D, 4096^2 on [-1000, 1000]^2, 1000 steps of 2 um,
+                   unit plane wave, 64 seeded spheres.
 """
 from __future__ import annotations
 
@@ -133,21 +133,21 @@ class Problem3D:
         return np.ones((n, n), dtype=np.complex128, order="F")
 
 
-def cfg0(nsteps: int = 4000) -> Problem2D:
+def waveguide_fft2d(nsteps: int = 4000) -> Problem2D:
     xmin, xmax = -250.0, 250.0
-    return Problem2D("cfg0_fft2d", "fft", xmin, xmax, step_for_nodes(xmin, xmax, 2048),
+    return Problem2D("waveguide_fft2d", "fft", xmin, xmax, step_for_nodes(xmin, xmax, 2048),
                      0.0, 4.0e6, 1000.0, nsteps, 15.0, Waveguide())
 
 
-def cfg1_cn(nsteps: int = 8000) -> Problem2D:
+def waveguide_cn(nsteps: int = 8000) -> Problem2D:
     xmin, xmax = -250.0, 250.0
-    return Problem2D("cfg1_cn", "cn", xmin, xmax, step_for_nodes(xmin, xmax, 4096),
+    return Problem2D("waveguide_cn", "cn", xmin, xmax, step_for_nodes(xmin, xmax, 4096),
                      0.0, 4.0e6, 500.0, nsteps, 15.0, Waveguide())
 
 
-def cfg1_adi(nsteps: int = 2000, n: int = 1024) -> Problem3D:
+def sphere_adi(nsteps: int = 2000, n: int = 1024) -> Problem3D:
     xmin, xmax = -500.0, 500.0
-    return Problem3D("cfg1_adi", "adi", xmin, xmax, step_for_nodes(xmin, xmax, n),
+    return Problem3D("sphere_adi", "adi", xmin, xmax, step_for_nodes(xmin, xmax, n),
                      0.0, 2.0e6, 1000.0, nsteps,
                      [(0.0, 0.0, 1.0e6, 200.0, 4.5e-5, 3.6e-6)])
 
@@ -163,8 +163,8 @@ def random_spheres(rng: np.random.Generator, count: int, lo: float, hi: float, z
     return out
 
 
-def cfg2(nsteps: int = 1000, n: int = 4096, seed: int = 2) -> Problem3D:
+def spheres_fft3d(nsteps: int = 1000, n: int = 4096, seed: int = 2) -> Problem3D:
     xmin, xmax = -1000.0, 1000.0
     rng = np.random.default_rng(seed)
-    return Problem3D("cfg2_fft3d", "fft3d", xmin, xmax, step_for_nodes(xmin, xmax, n),
+    return Problem3D("spheres_fft3d", "fft3d", xmin, xmax, step_for_nodes(xmin, xmax, n),
                      0.0, 2.0e6, 2000.0, nsteps, random_spheres(rng, 64, xmin, xmax, 2.0e6))

@@ -65,7 +65,7 @@ def test_batch_budget_refuses_and_releases():
 
 def test_serving_results_equal_alone():
     from paxpro_b200 import serving as sv
-    jobs = sv.cfg4_jobs(rate=400.0, duration=0.05, seed=9)
+    jobs = sv.served_jobs(rate=400.0, duration=0.05, seed=9)
     for j in jobs:
         j.nsteps = min(j.nsteps, 150)
         if j.kind == "fft3d":

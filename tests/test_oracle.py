@@ -60,7 +60,7 @@ def test_thomas_matches_dense_solve(n):
 
 def test_cn_matrix_thomas_on_config_ratio():
     # weakly dominant CN matrix of config 1 (rho ~ 534)
-    p = wl.cfg1_cn()
+    p = wl.waveguide_cn()
     rho = p.dz / (K * p.dx * p.dx)
     assert 500 < rho < 600
     n = 512
@@ -92,7 +92,7 @@ def test_node_count_truncation_and_step_choice():
 
 
 def test_waveguide_table_equals_oracle_material():
-    p = wl.cfg0()
+    p = wl.waveguide_fft2d()
     g = po.grid(p.xmin, p.xmax, p.dx, p.zmin, p.zmax, p.dz, K)
     d, b = p.material()
     spec = po.MaterialSpec(po.MAT_WAVEGUIDE, core_half_width=25.0, delta_clad=7.5e-6,

@@ -53,8 +53,8 @@ def _run_both(n, zmin, nsteps, dz, spheres, u0=None, use_tbc=False, precision=0,
     return out, saves, ref_out, ref_saves
 
 
-def test_cfg1_adi_fp64_sphere_crossing_full_size():
-    p = wl.cfg1_adi()
+def test_sphere_adi_fp64_sphere_crossing_full_size():
+    p = wl.sphere_adi()
     sph = p.spheres
     out, saves, ref_out, ref_saves = _run_both(1024, 1.0e6 - 5 * p.dz, 10, p.dz, sph)
     assert len(saves) == len(ref_saves) == 10

@@ -61,8 +61,8 @@ def _gpu_2d(p, delta, beta, u0, nsteps, save_every, precision, transparent=False
     return out, saves
 
 
-def test_cfg0_fft2d_fp64_every_save_within_1e10():
-    p = wl.cfg0()
+def test_waveguide_fft2d_fp64_every_save_within_1e10():
+    p = wl.waveguide_fft2d()
     d, b = p.material()
     u0 = p.initial_field()
     ref_out, ref_saves = _oracle_2d(p, d, b, u0, p.nsteps, 100)
@@ -86,8 +86,8 @@ def test_fft2d_fp64_sizes(n):
     assert _rel(out, ref_out) <= FP64_TOL
 
 
-def test_cfg1_cn_fp64_every_save_within_1e10():
-    p = wl.cfg1_cn()
+def test_waveguide_cn_fp64_every_save_within_1e10():
+    p = wl.waveguide_cn()
     d, b = p.material()
     u0 = p.initial_field()
     ref_out, ref_saves = _oracle_2d(p, d, b, u0, p.nsteps, 100)
@@ -111,7 +111,7 @@ def test_cn_fp64_sizes_and_boundaries(n, transparent):
 
 
 def test_fft2d_fp32_served_intensity_within_1e4():
-    p = wl.cfg0()
+    p = wl.waveguide_fft2d()
     d, b = p.material()
     u0 = p.initial_field()
     ref_out, ref_saves = _oracle_2d(p, d, b, u0, p.nsteps, 100)
@@ -121,7 +121,7 @@ def test_fft2d_fp32_served_intensity_within_1e4():
 
 
 def test_cn_fp32_served_intensity_within_1e4():
-    p = wl.cfg1_cn(nsteps=2000)
+    p = wl.waveguide_cn(nsteps=2000)
     d, b = p.material()
     u0 = p.initial_field()
     ref_out, ref_saves = _oracle_2d(p, d, b, u0, p.nsteps, 100)
@@ -157,7 +157,7 @@ def test_z_varying_planes_fft2d_and_cn():
 
 def test_api_errors_and_counters():
     pxp = _pxp()
-    p = wl.cfg0(nsteps=10)
+    p = wl.waveguide_fft2d(nsteps=10)
     spec = pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(p.xmin, p.xmax, p.dx),
                            z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K, save_every=5)
     with pxp.Solver(spec) as s:

@@ -73,8 +73,8 @@ def test_fft3d_fp64_sizes(n):
     assert max(_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP64_TOL
 
 
-def test_cfg2_fft3d_fp64_full_size_near_a_sphere():
-    p = wl.cfg2()
+def test_spheres_fft3d_fp64_full_size_near_a_sphere():
+    p = wl.spheres_fft3d()
     # start two steps before the first sphere whose z-extent meets a sampling plane
     sph = sorted(p.spheres, key=lambda s: s[2])
     target = None

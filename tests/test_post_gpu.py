@@ -77,7 +77,7 @@ def test_modules_shapes_values_and_export(tmp_path):
 def test_2d_solver_field_quantity_is_points_by_slices():
     import paxpro_b200 as pxp
     from paxpro_b200 import post
-    p = wl.cfg0(nsteps=5)
+    p = wl.waveguide_fft2d(nsteps=5)
     spec = pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(p.xmin, p.xmax, p.dx),
                            z=pxp.Disc(p.zmin, 5 * p.dz, p.dz), wavenumber=wl.K, save_every=1)
     with pxp.Solver(spec, keep_initial=True) as s:

@@ -12,7 +12,7 @@ from paxpro_b200 import sharding as sh
 
 
 def test_partition_covers_every_job_once_and_balances_work():
-    jobs = sv.cfg3_jobs(seed=3)
+    jobs = sv.mixed_batch_jobs(seed=3)
     for world in (1, 2, 3, 8):
         parts = sh.partition_jobs(jobs, world)
         flat = sorted(i for p in parts for i in p)
@@ -24,7 +24,7 @@ def test_partition_covers_every_job_once_and_balances_work():
 
 
 def test_partition_is_deterministic_and_rejects_empty_world():
-    jobs = sv.cfg3_jobs(seed=3)
+    jobs = sv.mixed_batch_jobs(seed=3)
     assert sh.partition_jobs(jobs, 4) == sh.partition_jobs(list(jobs), 4)
     with pytest.raises(ValueError):
         sh.partition_jobs(jobs, 0)
@@ -49,7 +49,7 @@ def _rank_main(rank, world, port, out):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        jobs = sv.cfg3_jobs(seed=3)
+        jobs = sv.mixed_batch_jobs(seed=3)
         mine = sh.partition_jobs(jobs, world)[rank]
         gathered = [None] * world
         dist.all_gather_object(gathered, mine)
@@ -65,7 +65,7 @@ def test_two_gloo_ranks_agree_on_the_split_and_aggregate_rates():
     out = mgr.dict()
     mp.start_processes(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True,
                        start_method="spawn")
-    jobs = sv.cfg3_jobs(seed=3)
+    jobs = sv.mixed_batch_jobs(seed=3)
     expect = sh.partition_jobs(jobs, world)
     for rank in range(world):
         gathered, pts, secs = out[rank]
