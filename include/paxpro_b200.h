@@ -89,8 +89,10 @@ unsigned pxp_node_count(double min, double max, double step);
  * Transverse sizes: CrankNicholson any Nx >= 16 (up to 4096 in FP64, 8192
  * in FP32; transparent ends need Nx / 8 to be a power of two); ADI any
  * Nx >= 4 up to 2048 (sizes other than powers of two from 64 to 1024 run on
- * the general kernel, without the vacuum fast path); FFTSolver2D and
- * FFTSolver3D powers of two.  Other sizes return PXP_ERR_UNSUPPORTED. */
+ * the general kernel, without the vacuum fast path); FFTSolver2D any
+ * Nx >= 8 up to 8192 in FP64 and 16384 in FP32 for powers of two, and up
+ * to 4096 / 8192 for other sizes (Bluestein's transform); FFTSolver3D powers
+ * of two.  Other sizes return PXP_ERR_UNSUPPORTED. */
 int pxp_solver_create(const pxp_problem *problem, pxp_solver *out);
 
 /* Solver destructor (src/solver2D.cpp:10-19, src/solver3D.cpp:11-17). */

@@ -9,7 +9,8 @@
 // -ffp-contract=off, so that for identical inputs the oracle's coefficients
 // match the reference's bit for bit wherever the reference's arithmetic does
 // not pass through FFTW.  Each function cites the reference lines it follows.
-// The FFT itself is our own radix-2 transform (FFTW3 is not available), so
+// The FFT itself is our own radix-2 transform (a direct DFT for other
+// lengths; FFTW3 is not available), so
 // FFT-based results agree with the reference to rounding, not bit for bit.
 
 #include "paxpro_oracle.h"
@@ -223,7 +224,35 @@ void fft_strided(cd *data, int n, long stride, int sign, cd *scratch) {
   for (int i = 0; i < n; ++i) data[(long)i * stride] = scratch[i];
 }
 
+// A length that is not a power of two: the plain DFT sum_j x_j w^(j k),
+// w = exp(sign 2 pi i / n), each factor taken from an n-entry table built
+// in extended precision at the exact index (j k) mod n (O(n^2); the lengths
+// the tests use are a few thousand at most).
+void dft_direct(cd *data, int n, int sign) {
+  std::vector<cd> w(n), out(n);
+  const long double pi_l = 3.141592653589793238462643383279502884L;
+  for (int m = 0; m < n; ++m) {
+    const long double a = (long double)sign * 2.0L * pi_l * (long double)m / (long double)n;
+    w[m] = cd((double)cosl(a), (double)sinl(a));
+  }
+  for (int k = 0; k < n; ++k) {
+    cd acc(0.0, 0.0);
+    long idx = 0;
+    for (int j = 0; j < n; ++j) {
+      acc += data[j] * w[idx];
+      idx += k;
+      if (idx >= n) idx -= n;
+    }
+    out[k] = acc;
+  }
+  std::copy(out.begin(), out.end(), data);
+}
+
 void fft_1d(cd *data, int n, int sign) {
+  if (!is_pow2(n)) {
+    dft_direct(data, n, sign);
+    return;
+  }
   std::vector<cd> scratch(n);
   fft_strided(data, n, 1, sign, scratch.data());
 }
@@ -309,7 +338,7 @@ void orc_set_fft_parallel(int on) { g_fft_parallel = on; }
 int orc_get_threads(void) { return nthreads(); }
 
 int orc_fft1d(double *data, int n, int sign) {
-  if (!is_pow2(n)) return -1;
+  if (n < 1) return -1;
   fft_1d(reinterpret_cast<cd *>(data), n, sign);
   return 0;
 }
@@ -333,7 +362,7 @@ int orc_fft2d_run(const orc_grid *gp, const orc_material *m, const double *u0,
                   int nsteps, int save_every, double *saves, double *u_out) {
   const orc_grid &g = *gp;
   unsigned n = node_count(g.xmin, g.xmax, g.dx);
-  if (!is_pow2(n) || n < 2 || nsteps < 0) return -1;
+  if (n < 2 || nsteps < 0) return -1;
   const cd *in = reinterpret_cast<const cd *>(u0);
   std::vector<cd> prev(in, in + n), curr(prev), ker(n);
   const double stepX = g.dx, stepZ = g.dz, wavenumber = g.wavenumber;

@@ -85,7 +85,8 @@ typedef struct {
 /* Node count exactly as the reference computes it (truncating cast). */
 unsigned orc_node_count(double mn, double mx, double step);
 
-/* In-place complex FFT of length n (power of two); sign -1 = forward
+/* In-place complex DFT of length n (radix-2 FFT for powers of two, a direct
+ * DFT otherwise); sign -1 = forward
  * exp(-2 pi i jk/n), +1 = backward exp(+2 pi i jk/n); unnormalised. */
 int orc_fft1d(double *data, int n, int sign);
 

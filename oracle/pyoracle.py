@@ -171,7 +171,7 @@ def fft1d(x: np.ndarray, sign: int) -> np.ndarray:
     a = np.ascontiguousarray(x, dtype=np.complex128).copy()
     rc = lib().orc_fft1d(_p(a), len(a), sign)
     if rc:
-        raise ValueError("length must be a power of two")
+        raise ValueError("length must be positive")
     return a
 
 

@@ -62,6 +62,7 @@ struct pxp_solver_s {
   int save_every = 0;
   // FFT 1-D tables
   void *d_kern = nullptr, *d_trans = nullptr, *d_tw = nullptr;
+  void *d_chirp = nullptr, *d_bconv = nullptr;  // Bluestein tables (shared, not owned)
   long long trans_stride = 0;
   int trans_step0 = 1;
   // CN material planes (FP64)
@@ -292,10 +293,93 @@ int shared_table(pxp_solver_s *h, int kind, void **out) {
 }
 
 // ---- FFT 1-D -------------------------------------------------------------
+// In-place radix-2 FFT in extended precision (host tables only).
+void fft_ld(std::vector<std::complex<long double>> &a, int sign) {
+  const size_t n = a.size();
+  for (size_t i = 1, j = 0; i < n; ++i) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  const long double pi_l = 3.141592653589793238462643383279502884L;
+  for (size_t len = 2; len <= n; len <<= 1) {
+    for (size_t i = 0; i < n; i += len)
+      for (size_t k = 0; k < len / 2; ++k) {
+        const long double ang = (long double)sign * 2.0L * pi_l * (long double)k / (long double)len;
+        const std::complex<long double> w(cosl(ang), sinl(ang));
+        const std::complex<long double> x = a[i + k], y = a[i + k + len / 2] * w;
+        a[i + k] = x + y;
+        a[i + k + len / 2] = x - y;
+      }
+  }
+}
+
+// Tables of the Bluestein path for n (not a power of two), shared per
+// device and n: kind 7 the chirp exp(-i pi j^2 / n), j < n (angle from the
+// exact index j^2 mod 2n); kind 8 the transform of the filter
+// b_j = exp(+i pi j^2 / n) for |j| < n wrapped to length m, divided by m;
+// kind 9 the Stockham twiddles of length m.
+int bluestein_table(pxp_solver_s *h, int kind, void **out) {
+  const unsigned n = h->nx;
+  const int m = pxp::fft1d_bluestein_m((int)n);
+  TableKey key{h->prob.device, kind, n, 0.0, 0.0, 0.0};
+  std::lock_guard<std::mutex> lk(g_table_mutex);
+  auto it = g_tables.find(key);
+  if (it != g_tables.end()) {
+    *out = it->second;
+    return PXP_OK;
+  }
+  const long double pi_l = 3.141592653589793238462643383279502884L;
+  auto chirp = [&](unsigned long long j, int sign) {
+    const unsigned long long r = (j * j) % (2ULL * n);
+    const long double a = (long double)sign * pi_l * (long double)r / (long double)n;
+    return std::complex<long double>(cosl(a), sinl(a));
+  };
+  std::vector<cd> t;
+  if (kind == 7) {
+    t.resize(n);
+    for (unsigned j = 0; j < n; ++j) {
+      const std::complex<long double> c = chirp(j, -1);
+      t[j] = cd((double)c.real(), (double)c.imag());
+    }
+  } else if (kind == 8) {
+    std::vector<std::complex<long double>> b((size_t)m, std::complex<long double>(0.0L, 0.0L));
+    for (unsigned j = 0; j < n; ++j) {
+      b[j] = chirp(j, +1);
+      if (j > 0) b[(size_t)m - j] = b[j];
+    }
+    fft_ld(b, -1);
+    t.resize((size_t)m);
+    for (int k = 0; k < m; ++k)
+      t[(size_t)k] = cd((double)(b[(size_t)k].real() / m), (double)(b[(size_t)k].imag() / m));
+  } else {
+    t = twiddles(m);
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, sizeof(cd) * t.size()) != cudaSuccess) {
+    cudaGetLastError();
+    return h->fail(PXP_ERR_NOMEM, "Bluestein table allocation");
+  }
+  cudaError_t e = cudaMemcpy(p, t.data(), sizeof(cd) * t.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return h->cuda_fail(e, "Bluestein table upload");
+  g_tables[key] = p;
+  *out = p;
+  return PXP_OK;
+}
+
 int fft1d_setup(pxp_solver_s *h) {
   int rc;
   if ((rc = shared_table(h, 1, &h->d_kern))) return rc;
-  if ((rc = shared_table(h, 0, &h->d_tw))) return rc;
+  if (h->nx & (h->nx - 1)) {
+    // not a power of two: the Bluestein path's tables (the Stockham twiddles
+    // are those of its power-of-two length)
+    if ((rc = bluestein_table(h, 7, &h->d_chirp))) return rc;
+    if ((rc = bluestein_table(h, 8, &h->d_bconv))) return rc;
+    if ((rc = bluestein_table(h, 9, &h->d_tw))) return rc;
+  } else if ((rc = shared_table(h, 0, &h->d_tw))) {
+    return rc;
+  }
   return alloc(h, &h->d_job, sizeof(pxp::Fft1dJob), "job descriptor");
 }
 
@@ -336,6 +420,9 @@ int fft1d_write_job(pxp_solver_s *h) {
   j.max_slots = h->max_slots;
   j.trans_step0 = h->trans_step0;
   j.flux = pxp::FluxSpec{h->d_flux_win, h->d_flux, h->flux_step0, h->flux_count};
+  j.chirp = h->d_chirp;
+  j.bconv = h->d_bconv;
+  j.m = pxp::fft1d_bluestein_m((int)h->nx);
   h->job_fft = j;
   if (int rc_ = h2d(h, h->d_job, &j, sizeof(j))) return rc_;
   return PXP_OK;

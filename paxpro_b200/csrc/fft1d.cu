@@ -95,6 +95,93 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
   for (int i = lane; i < N; i += T) field[i] = u[sw<C>(i)];
 }
 
+// Lengths that are not powers of two: Bluestein's chirp-z identity
+// jk = (j^2 + k^2 - (k - j)^2) / 2 turns the n-point DFT into
+//   X_k = w_k sum_j (x_j w_j) conj(w)_{k-j},   w_j = exp(-i pi j^2 / n),
+// a circular convolution of length m >= 2n - 1 (a power of two): two
+// shared-memory FFTs of length m and a pointwise product with the
+// precomputed transform of the filter (1/m folded in).  The inverse
+// transform is conj(DFT(conj(X))).  The field stays resident in shared
+// memory beside the m-point work buffer, as in the power-of-two kernel.
+template <typename R, int M, int T>
+__device__ __forceinline__ void bluestein_dft(typename Cx<R>::T *x, typename Cx<R>::T *u, int n,
+                                              const double2 *w, const double2 *bf,
+                                              const double2 *tw, int lane, bool inverse) {
+  using C = typename Cx<R>::T;
+  for (int j = lane; j < M; j += T) {
+    C a{};
+    if (j < n) {
+      C v = u[j];
+      if (inverse) v.y = -v.y;
+      a = tw_mul(v, w[j]);
+    }
+    x[sw<C>(j)] = a;
+  }
+  __syncthreads();
+  fft_smem<C, M, T, -1>(x, tw, lane);
+  for (int k = lane; k < M; k += T) x[sw<C>(k)] = tw_mul(x[sw<C>(k)], bf[k]);
+  __syncthreads();
+  fft_smem<C, M, T, +1>(x, tw, lane);
+  for (int k = lane; k < n; k += T) {
+    C v = tw_mul(x[sw<C>(k)], w[k]);
+    if (inverse) v.y = -v.y;
+    u[k] = v;
+  }
+  __syncthreads();
+}
+
+template <typename R, int M, int T, bool FLUX>
+__global__ void __launch_bounds__(T) fft1d_bluestein_kernel(const Fft1dJob *__restrict__ jobs,
+                                                           int step0_ov, int nsteps_ov) {
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double flux_red[2][flux_slots<T>()];
+  C *x = reinterpret_cast<C *>(smem_raw);  // m-point work buffer (swizzled)
+  C *u = x + M;                            // the field, n points
+  Fft1dJob job = jobs[blockIdx.x];
+  if (nsteps_ov >= 0) {
+    job.step0 = step0_ov;
+    job.nsteps = nsteps_ov;
+  }
+  const int n = job.n;
+  const int lane = threadIdx.x;
+  const double2 *tw = reinterpret_cast<const double2 *>(job.twiddle);
+  const double2 *w = reinterpret_cast<const double2 *>(job.chirp);
+  const double2 *bf = reinterpret_cast<const double2 *>(job.bconv);
+  C *field = reinterpret_cast<C *>(job.field);
+  for (int i = lane; i < n; i += T) u[i] = field[i];
+  __syncthreads();
+  const double2 *kern = reinterpret_cast<const double2 *>(job.kern);
+  const double2 *trans0 = reinterpret_cast<const double2 *>(job.trans);
+  C *saves = reinterpret_cast<C *>(job.saves);
+  const R nreal = (R)n;
+  for (int s = 0; s < job.nsteps; ++s) {
+    const int step = job.step0 + s;
+    int2 fw;
+    const bool flux = FLUX && flux_window(job.flux, step, fw);
+    bluestein_dft<R, M, T>(x, u, n, w, bf, tw, lane, false);
+    for (int i = lane; i < n; i += T) u[i] = kmul<R>(u[i], kern[i]);
+    __syncthreads();
+    bluestein_dft<R, M, T>(x, u, n, w, bf, tw, lane, true);
+    const double2 *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
+    const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
+                      (step / job.save_every - 1) < job.max_slots;
+    C *slot = save ? saves + (long long)(step / job.save_every - 1) * n : nullptr;
+    double acc = 0.0;
+    for (int i = lane; i < n; i += T) {
+      C v = u[i];
+      refract<R>(v, trans[i], nreal);
+      u[i] = v;
+      if (save) slot[i] = v;
+      if (flux) flux_add(acc, i, fw, to_d(v));
+    }
+    if (flux) flux_warp_total<T>(acc, flux_red[s & 1]);
+    __syncthreads();
+    if (flux) flux_store<T>(job.flux, step, flux_red[s & 1]);
+  }
+  for (int i = lane; i < n; i += T) field[i] = u[i];
+}
+
 template <typename R> constexpr int fft1d_threads(int n) {
   return n >= 8192 ? 512 : (n >= 2048 ? 256 : (n >= 512 ? 64 : 32));
 }
@@ -118,9 +205,56 @@ static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nstep
   return cudaGetLastError();
 }
 
+int fft1d_bluestein_m(int n) {
+  if (n >= 1 && !(n & (n - 1))) return n;
+  int m = 1;
+  while (m < 2 * n - 1) m *= 2;
+  return m;
+}
+
 bool fft1d_supported(Precision p, int n) {
-  if (n < 8 || (n & (n - 1))) return false;
+  if (n < 8) return false;
+  if (n & (n - 1)) return fft1d_bluestein_m(n) <= (p == kFP64 ? 8192 : 16384);
   return p == kFP64 ? n <= 8192 : n <= 16384;
+}
+
+template <typename R, int M, bool FLUX>
+static cudaError_t launch_blu(const Fft1dJob *d_jobs, int nj, int step0, int nsteps,
+                              cudaStream_t s, int n) {
+  using C = typename Cx<R>::T;
+  constexpr int T = M >= 8192 ? 512 : (M >= 2048 ? 256 : (M >= 512 ? 64 : 32));
+  auto k = fft1d_bluestein_kernel<R, M, T, FLUX>;
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(C) * (M + M / 2)));
+  if (attr != cudaSuccess) return attr;
+  k<<<nj, T, sizeof(C) * (M + n), s>>>(d_jobs, step0, nsteps);
+  return cudaGetLastError();
+}
+
+template <typename R, int M>
+static cudaError_t launch_bluf(const Fft1dJob *d_jobs, int nj, int step0, int nsteps,
+                               cudaStream_t s, int n, bool flux) {
+  return flux ? launch_blu<R, M, true>(d_jobs, nj, step0, nsteps, s, n)
+              : launch_blu<R, M, false>(d_jobs, nj, step0, nsteps, s, n);
+}
+
+static cudaError_t launch_bluestein(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
+                                    int nsteps, cudaStream_t s, bool flux) {
+  const int m = fft1d_bluestein_m(n);
+#define PXP_BL(MM)                                                                        \
+  case MM:                                                                                \
+    return p == kFP64 ? launch_bluf<double, MM>(d_jobs, nj, step0, nsteps, s, n, flux)    \
+                      : launch_bluf<float, MM>(d_jobs, nj, step0, nsteps, s, n, flux);
+  switch (m) {
+    PXP_BL(32) PXP_BL(64) PXP_BL(128) PXP_BL(256) PXP_BL(512) PXP_BL(1024) PXP_BL(2048)
+    PXP_BL(4096) PXP_BL(8192)
+    case 16384:
+      if (p == kFP32) return launch_bluf<float, 16384>(d_jobs, nj, step0, nsteps, s, n, flux);
+      return cudaErrorInvalidValue;
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef PXP_BL
 }
 
 template <typename R, int N>
@@ -133,6 +267,7 @@ static cudaError_t launch_nf(const Fft1dJob *d_jobs, int nj, int step0, int nste
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
                          int nsteps, cudaStream_t s, bool flux) {
   if (nj <= 0) return cudaSuccess;
+  if (n & (n - 1)) return launch_bluestein(p, d_jobs, nj, n, step0, nsteps, s, flux);
 #define PXP_CASE(NN)                                                              \
   case NN:                                                                        \
     return p == kFP64 ? launch_nf<double, NN>(d_jobs, nj, step0, nsteps, s, flux)     \

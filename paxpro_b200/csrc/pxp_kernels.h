@@ -41,6 +41,13 @@ struct Fft1dJob {
   int max_slots;           // capacity of saves
   int trans_step0;         // step that per-step table 0 belongs to
   FluxSpec flux;           // per-step flux integrals (out == null: none)
+  // n not a power of two (Bluestein): twiddle holds the Stockham twiddles of
+  // the power-of-two length m >= 2n - 1; chirp: n complex128
+  // exp(-i pi j^2 / n); bconv: m complex128, the transform of the
+  // conjugate chirp filter divided by m
+  const void *chirp;
+  const void *bconv;
+  int m;
 };
 
 // Launch nj jobs that all share one transform length n (one CTA per job).
@@ -49,6 +56,9 @@ struct Fft1dJob {
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n,
                          int step0, int nsteps, cudaStream_t s, bool flux = false);
 bool fft1d_supported(Precision p, int n);
+// Length of the power-of-two transforms of the Bluestein path for n (the
+// smallest power of two >= 2n - 1); n itself for powers of two.
+int fft1d_bluestein_m(int n);
 
 // ------------------------------------------------------------ CN 1-D ------
 // Crank-Nicolson problem (CrankNicholson with default F=G=H=1, J=0).

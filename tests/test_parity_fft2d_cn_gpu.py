@@ -172,8 +172,12 @@ def test_api_errors_and_counters():
         s.reset()
         assert s.current_step == 1
     with pytest.raises(pxp.PxpError):
-        pxp.Solver(pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(0, 10, 1.0),
-                                   z=pxp.Disc(0, 10, 1.0), wavenumber=wl.K))  # Nx = 11
+        # Nx = 5000 in FP64: its Bluestein length 16384 is beyond the FP64 limit
+        pxp.Solver(pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(0, 4999, 1.0),
+                                   z=pxp.Disc(0, 10, 1.0), wavenumber=wl.K))
+    with pytest.raises(pxp.PxpError):
+        pxp.Solver(pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(0, 4, 1.0),
+                                   z=pxp.Disc(0, 10, 1.0), wavenumber=wl.K))  # Nx = 5
 
 
 @pytest.mark.parametrize("n,precision", [(300, 0), (1000, 0), (2500, 0), (17, 0), (1000, 1)])
@@ -201,6 +205,41 @@ def test_cn_any_grid_size(n, precision):
                            z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K)
     with pxp.Solver(spec) as s:
         s.set_material_planes(np.tile(d, nsteps * 2), np.tile(b, nsteps * 2), 1, nsteps)
+        s.set_initial_conditions(u0)
+        s.set_flux_windows(1, np.zeros(nsteps, np.uint32), np.full(nsteps, n - 1, np.uint32))
+        s.step(nsteps)
+        out2 = s.get_last_solution()
+        flux = s.get_flux(nsteps, 1)[0]
+    assert _rel(out2, ref_out) <= FP64_TOL
+    w = np.full(n, 2.0)
+    w[0] = w[-1] = 1.0
+    assert flux == pytest.approx(float(np.sum(w * np.abs(out2) ** 2)), rel=1e-13)
+
+
+@pytest.mark.parametrize("n,precision", [(300, 0), (1000, 0), (3000, 0), (9, 0), (1000, 1)])
+def test_fft2d_any_grid_size(n, precision):
+    """FFTSolver2D on grids whose size is not a power of two (Bluestein's
+    chirp-z transform in the kernel) against the oracle (a direct DFT for
+    such lengths): FP64 within 1e-10 at every save, FP32 served within the
+    intensity tolerance; per-step flux sums on the same run."""
+    nsteps = 40
+    p = wl.Problem2D("t", "fft", -250.0, 250.0, wl.step_for_nodes(-250.0, 250.0, n),
+                     0.0, 1e6, 1000.0, nsteps, 15.0, wl.Waveguide())
+    d, b = p.material()
+    u0 = p.initial_field()
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, nsteps, 10)
+    out, saves = _gpu_2d(p, d, b, u0, nsteps, 10, precision)
+    assert len(saves) == len(ref_saves) == 4
+    if precision == 1:
+        assert max(_int_rel(g, r) for g, r in zip(saves, ref_saves)) <= FP32_INT_TOL
+        return
+    assert max(_rel(g, r) for g, r in zip(saves, ref_saves)) <= FP64_TOL
+    assert _rel(out, ref_out) <= FP64_TOL
+    pxp = _pxp()
+    spec = pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(p.xmin, p.xmax, p.dx),
+                           z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K)
+    with pxp.Solver(spec) as s:
+        s.set_material_table(d, b)
         s.set_initial_conditions(u0)
         s.set_flux_windows(1, np.zeros(nsteps, np.uint32), np.full(nsteps, n - 1, np.uint32))
         s.step(nsteps)
