@@ -718,36 +718,6 @@ class Solver2D : public Solver {
         solution(i, step) = currentSolution((unsigned)(delta * i + delta / 2.0));
   }
 
-  /** Flattens a CSGMaterial for pxp_set_material_csg. */
-  void setCsg(const CSGMaterial &cm) {
-    std::vector<pxp_csg_module> mods;
-    std::vector<pxp_csg_part> parts;
-    std::vector<pxp_csg_shape> shapes;
-    for (const geom::Module *m : cm.modules) {
-      mods.push_back({(int)parts.size(), (int)m->parts.size()});
-      for (size_t i = 0; i < m->parts.size(); ++i) {
-        const geom::Part *p = m->parts[i];
-        pxp_csg_part cp{};
-        cp.operation = m->operations[i] == geom::Operation_t::UNION ? PXP_CSG_UNION : PXP_CSG_DIFFERENCE;
-        cp.first_shape = (int)shapes.size();
-        cp.num_shapes = (int)p->shapes.size();
-        cp.delta = p->delta;
-        cp.beta = p->beta;
-        parts.push_back(cp);
-        for (size_t k = 0; k < p->shapes.size(); ++k) {
-          pxp_csg_shape cs{};
-          cs.kind = p->shapes[k]->kind();
-          cs.operation = p->operations[k] == geom::Operation_t::UNION ? PXP_CSG_UNION : PXP_CSG_DIFFERENCE;
-          std::memcpy(cs.transform, p->shapes[k]->transformation, sizeof(cs.transform));
-          p->shapes[k]->size(cs.size);
-          shapes.push_back(cs);
-        }
-      }
-    }
-    check(pxp_set_material_csg(handle, mods.data(), (int)mods.size(), parts.data(), (int)parts.size(),
-                               shapes.data(), (int)shapes.size()));
-  }
-
   void initDevice() {
     if (guide == nullptr) throw std::runtime_error("No waveguide specified!");
     if (handle == nullptr) {
