@@ -66,3 +66,28 @@ def test_transparent_ends_on_a_padded_cn_grid_are_rejected_before_any_device_cal
     h = C.c_void_p()
     rc = _capi.lib().pxp_solver_create(C.byref(spec.to_c()), C.byref(h))
     assert rc == _capi.PXP_ERR_UNSUPPORTED
+
+
+def test_new_entry_points_reject_null_handles_and_fill_defaults():
+    """The far-field, reference, flux and resized-post entry points reject a
+    null handle without touching a device; pxp_farfield_defaults fills the
+    reference's FarField defaults (angles -90..90, zero padding)."""
+    import ctypes as C
+    from paxpro_b200 import _capi
+    lib = _capi.lib()
+    p = _capi.FarFieldParams()
+    p.phi_min = 3.0
+    p.pad_length = 7
+    lib.pxp_farfield_defaults(C.byref(p))
+    assert (p.pad_length, p.phi_min, p.phi_max, p.padding) == (0, -90.0, 90.0, _capi.PAD_ZERO)
+    assert (p.export_rows, p.export_cols, p.subtract_reference) == (0, 0, 0)
+    out = (C.c_double * 4)()
+    r, c = C.c_uint(), C.c_uint()
+    assert lib.pxp_farfield(None, C.byref(p), out) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_farfield_shape(None, C.byref(p), C.byref(r), C.byref(c)) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_set_reference(None, None) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_set_reference_from(None, None) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_set_flux_windows(None, 1, 0, None, None) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_get_flux(None, 1, 1, out) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_field_flux(None, 0, 1, out) == _capi.PXP_ERR_INVALID
+    assert lib.pxp_get_post_resized(None, 0, -1, 2, 2, out) == _capi.PXP_ERR_INVALID
