@@ -457,7 +457,7 @@ int cn_set_planes(pxp_solver_s *h, const double *delta, const double *beta, int 
   h->material_set = true;
   // step-invariant matrix when the same plane serves every step
   h->cn_const = false;
-  if (nsteps == 1 && pxp::cn_const_supported(h->prec, (int)n)) {
+  if (nsteps == 1 && pxp::cn_const_supported(h->prec, pxp::cn_padded_n((int)n))) {
     int rc2 = cn_build_lu(h, delta, beta);
     if (rc2) return rc2;
     h->cn_const = true;
@@ -486,11 +486,13 @@ void thomas_factor(const std::vector<cd> &diag, cd sub, std::vector<cd> &out_gh)
 // std::complex expressions.
 int cn_build_lu(pxp_solver_s *h, const double *delta, const double *beta) {
   const unsigned n = h->nx;
+  // the kernels solve np rows: rows n..np-1 pad the system (diagonal kCnPad)
+  const unsigned np = (unsigned)pxp::cn_padded_n((int)n);
   const cd IMAG_UNIT(0.0, 1.0);
   const double dx = h->prob.x.step, dz = h->prob.z.step, k = h->prob.wavenumber;
   const double rho = dz / (k * dx * dx), r = k * dz;
   const double Hp = 1.0, Hm = 1.0, gval = 1.0, fval = 1.0;
-  std::vector<cd> diag(n);
+  std::vector<cd> diag(np, cd(pxp::kCnPad, 0.0));
   for (unsigned i = 0; i < n; ++i)
     diag[i] = fval * 1.0 + 0.25 * (Hp + Hm) * gval * IMAG_UNIT * rho +
               0.5 * (beta[i] * r + IMAG_UNIT * delta[i] * r);
@@ -499,8 +501,8 @@ int cn_build_lu(pxp_solver_s *h, const double *delta, const double *beta) {
   thomas_factor(diag, sub, gh);
   free_dev(h->d_lu, h->stream);
   int rc;
-  if ((rc = alloc(h, &h->d_lu, sizeof(cd) * 2 * n, "factor tables"))) return rc;
-  if (int rc_ = h2d(h, h->d_lu, gh.data(), sizeof(cd) * 2 * n)) return rc_;
+  if ((rc = alloc(h, &h->d_lu, sizeof(cd) * 2 * np, "factor tables"))) return rc;
+  if (int rc_ = h2d(h, h->d_lu, gh.data(), sizeof(cd) * 2 * np)) return rc_;
   return PXP_OK;
 }
 
@@ -947,7 +949,7 @@ int cn_write_job(pxp_solver_s *h) {
   j.mat_step0 = h->mat_step0;
   j.transparent = h->prob.transparent_bc ? 1 : 0;
   j.lu_g = h->d_lu;
-  j.lu_h = h->d_lu ? (const void *)((const cd *)h->d_lu + n) : nullptr;
+  j.lu_h = h->d_lu ? (const void *)((const cd *)h->d_lu + pxp::cn_padded_n((int)n)) : nullptr;
   j.flux = pxp::FluxSpec{h->d_flux_win, h->d_flux, h->flux_step0, h->flux_count};
   h->job_cn = j;
   if (int rc_ = h2d(h, h->d_job, &j, sizeof(j))) return rc_;
@@ -1399,8 +1401,9 @@ int pxp_step(pxp_solver h, int nsteps) {
       break;
     case PXP_CRANK_NICHOLSON:
       if (h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0)
-        e = pxp::launch_cn_const(h->prec, (const pxp::CnJob *)h->d_job, 1, (int)h->nx, (int)first,
-                                 nsteps, h->stream, h->flux_count > 0);
+        e = pxp::launch_cn_const(h->prec, (const pxp::CnJob *)h->d_job, 1,
+                                 pxp::cn_padded_n((int)h->nx), (int)first, nsteps, h->stream,
+                                 h->flux_count > 0);
       else
         e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, pxp::cn_padded_n((int)h->nx),
                            (int)first, nsteps, h->stream, h->flux_count > 0);
@@ -2114,7 +2117,7 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
                             k.n, -1, -1, b->stream, any_flux);
     else if (k.cpath)
       e = pxp::launch_cn_const((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
-                               k.n, -1, -1, b->stream, any_flux);
+                               pxp::cn_padded_n(k.n), -1, -1, b->stream, any_flux);
     else
       e = pxp::launch_cn((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
                          pxp::cn_padded_n(k.n),

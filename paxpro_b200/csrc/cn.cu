@@ -81,9 +81,6 @@ __device__ __forceinline__ void cn_tbc(double2 outer, double2 inner, double rho,
   rhs = cx_add_rn(rhs, cx_mul_rn(coef, outer));
 }
 
-// Diagonal of the padding rows of a system padded to M * T rows.
-constexpr double kCnPad = 1e30;
-
 template <typename R, int M, int T, bool FLUX>
 __global__ void __launch_bounds__(T) cn_kernel(const CnJob *__restrict__ jobs, int step0_ov,
                                               int nsteps_ov) {
@@ -214,20 +211,27 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
   const double2 *ht = reinterpret_cast<const double2 *>(job.lu_h);
   const double q = __dmul_rn(0.25, rho);
   const int s0 = t * M;
+  // rows nreal..N-1 pad the system (their factor-table rows were built with
+  // diagonal kCnPad on the host; their right-hand side is zero)
+  const int nreal = job.n_real > 0 ? job.n_real : N;
   // each thread fills the slots of its own chunk
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     const int k = cslot<M, T>(t, m);
     gs[k] = gt[s0 + m];
     hs[k] = ht[s0 + m];
-    const double bp = job.beta_prev[s0 + m], dp = job.delta_prev[s0 + m];
-    const double2 hh = mk(__dmul_rn(0.5, __dmul_rn(bp, r)), __dmul_rn(0.5, __dmul_rn(dp, r)));
-    ds[k] = mk(__dadd_rn(-hh.x, 1.0), __dsub_rn(-hh.y, 0.5 * rho));
+    if (s0 + m < nreal) {
+      const double bp = job.beta_prev[s0 + m], dp = job.delta_prev[s0 + m];
+      const double2 hh = mk(__dmul_rn(0.5, __dmul_rn(bp, r)), __dmul_rn(0.5, __dmul_rn(dp, r)));
+      ds[k] = mk(__dadd_rn(-hh.x, 1.0), __dsub_rn(-hh.y, 0.5 * rho));
+    } else {
+      ds[k] = mk(0.0, 0.0);
+    }
   }
   C *field = reinterpret_cast<C *>(job.field);
   double2 u[M];
 #pragma unroll
-  for (int m = 0; m < M; ++m) u[m] = to_d(field[s0 + m]);
+  for (int m = 0; m < M; ++m) u[m] = s0 + m < nreal ? to_d(field[s0 + m]) : mk(0.0, 0.0);
   C *saves = reinterpret_cast<C *>(job.saves);
   for (int st = 0; st < job.nsteps; ++st) {
     const int step = job.step0 + st;
@@ -243,20 +247,22 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const double2 left = m > 0 ? u[m - 1] : lft;
-      const double2 right = m < M - 1 ? u[m + 1] : rgt;
+      // the Dirichlet zero beyond the last real row
+      const double2 right = s0 + m + 1 >= nreal ? mk(0.0, 0.0) : (m < M - 1 ? u[m + 1] : rgt);
       const double2 sum = cadd(left, right);
-      rh[m] = cfma(ds[cslot<M, T>(t, m)], u[m], mk(-q * sum.y, q * sum.x));
+      rh[m] = s0 + m < nreal ? cfma(ds[cslot<M, T>(t, m)], u[m], mk(-q * sum.y, q * sum.x))
+                             : mk(0.0, 0.0);
     }
     const_solve_reg<M, T>(rh, gs, hs, t, scratch);
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
-    C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
+    C *slot = save ? saves + (long long)(step / job.save_every - 1) * nreal : nullptr;
     double acc = 0.0;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const C v = from_d<R>(rh[m]);
       u[m] = to_d(v);
-      if (save) slot[s0 + m] = v;
+      if (save && s0 + m < nreal) slot[s0 + m] = v;
       if (flux) flux_add(acc, s0 + m, fw, u[m]);
     }
     if (flux) flux_warp_total<T>(acc, flux_red[st & 1]);
@@ -264,7 +270,8 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
     if (flux) flux_store<T>(job.flux, step, flux_red[st & 1]);
   }
 #pragma unroll
-  for (int m = 0; m < M; ++m) field[s0 + m] = from_d<R>(u[m]);
+  for (int m = 0; m < M; ++m)
+    if (s0 + m < nreal) field[s0 + m] = from_d<R>(u[m]);
 }
 
 static constexpr int kCnM = 8;

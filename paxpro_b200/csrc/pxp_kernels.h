@@ -80,9 +80,12 @@ struct CnJob {
 cudaError_t launch_cn(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
                       int nsteps, cudaStream_t s, bool flux = false);
 bool cn_supported(Precision p, int n);
-// Rows the general CN kernel solves for Nx = n: n itself when n/8 is a
-// power of two, else n padded up to 8 times the next power of two.
+// Rows the CN kernels solve for Nx = n: n itself when n/8 is a power of
+// two, else n padded up to 8 times the next power of two.
 int cn_padded_n(int n);
+// Diagonal of the padding rows (zero right-hand side and field), in the
+// kernels' rows and in the host's factor tables of the step-invariant path.
+constexpr double kCnPad = 1e30;
 // z-invariant medium and Dirichlet ends: the step matrix never changes; the
 // job's lu_g / lu_h hold its Thomas factor tables (n complex128 each).
 cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
