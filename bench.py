@@ -22,9 +22,24 @@ scaling).  Timing: CUDA events on the solvers' own streams, warm-up first,
 L2 flushed (256 MB write) before every timed step, barrier +
 synchronize around the timed region, max over ranks.
 
+The default line also carries the served half of the metric: the mixed
+batch's FP32-served rate over plain FP64 one job at a time (with the largest
+relative intensity error against FP64) and the serving loop's p50/p99 job
+latency at two arrival rates (`served`; --no-served skips it).
+
 --impl reference times the CPU restatement of the reference (oracle/, the
 reference cannot be built here: Armadillo/FFTW3/HDF5 are absent) on all host
-cores, on a bounded sample of the same workload per step.
+cores, on a bounded sample of the same workload per step.  That arm imports
+nothing from the CUDA package, so the CUDA library is never loaded in it.
+
+    python bench.py --case KIND N STEPS [--fp32] [--repeat R] [--flux]
+
+runs one solver case (KIND fft2d, cn, adi or fft3d at transverse size N,
+STEPS z steps per repeat; the workloads' synthetic fields and materials) and
+prints the mean time per step (CUDA events on the solver's stream): the
+small cases the ncu summaries under profiles/ were captured on.
+`--case farfield N STEPS --pad L --angle A` times the 3-D far field of the
+exit field after STEPS FFTSolver3D steps.
 """
 from __future__ import annotations
 
@@ -43,7 +58,21 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-from paxpro_b200 import workloads as wl  # noqa: E402
+
+def _load_workloads():
+    """paxpro_b200/workloads.py loaded by path: importing it through the
+    package would load the CUDA library, which the CPU reference arm must
+    not do (workloads.py itself needs only numpy)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "pxp_bench_workloads", os.path.join(ROOT, "paxpro_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses look their module up while defining
+    spec.loader.exec_module(mod)
+    return mod
+
+
+wl = _load_workloads()
 
 L2_FLUSH_BYTES = 256 << 20
 
@@ -211,12 +240,31 @@ class WaveguideFft2dWorkload:
 WORKLOADS = {"cn4096_adi1024": CnAdiWorkload, "waveguide_fft2d": WaveguideFft2dWorkload}
 
 
-def run_mixed(args, rank, world, device):
+def workload_pts_steps(workload: str) -> int:
+    """Grid-point*steps of one pass of a timed workload."""
+    if workload == "cn4096_adi1024":
+        c, a = wl.waveguide_cn(), wl.sphere_adi()
+        return c.nx * c.nsteps + a.nx * a.nx * a.nsteps
+    p = wl.waveguide_fft2d()
+    return p.nx * p.nsteps
+
+
+def workload_config(workload: str, world: int) -> dict:
+    """The `config` object of a timed workload; both arms print this same
+    dict."""
+    return {"workload": WORKLOADS[workload].name,
+            "grid_pt_steps_per_step": workload_pts_steps(workload),
+            "parallelism": f"replicas x{world} (one independent replica per GPU)",
+            "l2": "GPU arm: flushed (256 MB write) before every timed step"}
+
+
+def mixed_core(rank, world, device):
     """The mixed batch (512 2-D + 32 3-D problems) in FP32 served mode,
     one Batch per GPU, against the same problems run one at a time in plain
     FP64.  On N GPUs the one job set is split by the least-loaded scheduler
     (paxpro_b200.sharding); rates are summed grid-point*steps over the max
-    elapsed time across ranks."""
+    elapsed time across ranks.  Every rank takes the same collective steps;
+    rank 0 gets the summary, the others None."""
     import torch
     from paxpro_b200 import serving as sv
     from paxpro_b200 import sharding as sh
@@ -241,6 +289,18 @@ def run_mixed(args, rank, world, device):
     _, err = sh.reduce_rate(0.0, max(errs), dist, dev)
     if rank != 0:
         return None
+    return {"served_fp32": b_pts / b_sec, "served_seconds": b_sec, "grid_pt_steps": b_pts,
+            "plain_fp64": p_pts / p_sec, "plain_seconds": p_sec,
+            "served_over_plain": (b_pts / b_sec) / (p_pts / p_sec),
+            "max_rel_intensity_err_vs_fp64": err,
+            "intensity_error_checked_on": f"{len(keep)} of {len(jobs)} jobs per GPU"}
+
+
+def run_mixed(args, rank, world, device):
+    r = mixed_core(rank, world, device)
+    if r is None:
+        return None
+    b_pts, b_sec = r["grid_pt_steps"], r["served_seconds"]
     return {
         "metric": "grid-pt*steps/s (FP32 served, batched)",
         "value": b_pts / b_sec,
@@ -258,17 +318,18 @@ def run_mixed(args, rank, world, device):
                    "grid_pt_steps": b_pts,
                    "sharding": "jobs split across GPUs, largest first to the least-loaded GPU",
                    "timing": "wall clock between device synchronisations, max over ranks"},
-        "plain_fp64": {"value": p_pts / p_sec, "seconds": p_sec},
-        "served_over_plain": (b_pts / b_sec) / (p_pts / p_sec),
-        "max_rel_intensity_err_vs_fp64": err,
+        "plain_fp64": {"value": r["plain_fp64"], "seconds": r["plain_seconds"]},
+        "served_over_plain": r["served_over_plain"],
+        "max_rel_intensity_err_vs_fp64": r["max_rel_intensity_err_vs_fp64"],
     }
 
 
-def run_serving(args, rank, world, device):
+def serving_core(rank, world, device, rates=(50, 100, 200, 500, 1000, 2000), window=None):
     """Serving: Poisson arrivals swept over rates; served FP32 continuous batching
     against plain FP64 one-at-a-time on the same job stream.  On N GPUs each
     GPU serves its own arrival stream at the rate (weak scaling); throughput
-    is summed grid-point*steps over the max makespan across ranks."""
+    is summed grid-point*steps over the max makespan across ranks.  Rank 0
+    gets (rows, plain summary, window), the others None."""
     import torch
     from paxpro_b200 import serving as sv
     from paxpro_b200 import sharding as sh
@@ -277,10 +338,11 @@ def run_serving(args, rank, world, device):
     if world > 1:
         import torch.distributed as dist
     dev = torch.device("cuda", device) if dist is not None else None
-    window = float(os.environ.get("PXP_SERVE_WINDOW", "2.0"))
+    if window is None:
+        window = float(os.environ.get("PXP_SERVE_WINDOW", "2.0"))
     sv.serve(sv.served_jobs(200.0, 0.1, seed=99), precision=1)  # warm-up
     rows = []
-    for rate in (50, 100, 200, 500, 1000, 2000):
+    for rate in rates:
         jobs = sv.served_jobs(float(rate), window, seed=4 + rate + 1000 * rank)
         r = sv.serve(jobs, precision=1, round_steps=200)
         pts, span = sh.reduce_rate(r.pts_steps, r.makespan, dist, dev)
@@ -293,6 +355,14 @@ def run_serving(args, rank, world, device):
     p_pts, p_sec = sh.reduce_rate(plain.pts_steps, plain.seconds, dist, dev)
     if rank != 0:
         return None
+    return rows, {"value": p_pts / p_sec, "busy_seconds": p_sec, "jobs": len(jobs)}, window
+
+
+def run_serving(args, rank, world, device):
+    r = serving_core(rank, world, device)
+    if r is None:
+        return None
+    rows, plain, window = r
     best = max(rows, key=lambda x: x["throughput"])
     return {
         "metric": "grid-pt*steps/s served (FP32); p50/p99 job latency",
@@ -310,12 +380,44 @@ def run_serving(args, rank, world, device):
         "config": {"workload": f"served: Poisson arrivals, {window} s per rate, 80% FFT2D / 15% CN / "
                                "5% FFT3D, HBM budget 150 GB"},
         "rates": rows,
-        "plain_fp64_one_at_a_time": {"value": p_pts / p_sec, "busy_seconds": p_sec,
-                                     "jobs": len(jobs)},
+        "plain_fp64_one_at_a_time": plain,
     }
 
 
+def served_half(rank, world, device):
+    """The served half of the metric for the default line: the mixed batch
+    (FP32 served over plain FP64, intensity error) and the serving loop's
+    p50/p99 at two arrival rates, 2 s of arrivals each."""
+    mixed = mixed_core(rank, world, device)
+    srv = serving_core(rank, world, device, rates=(200, 1000), window=2.0)
+    if rank != 0:
+        return None
+    rows, plain, window = srv
+    return {"mixed_batch": mixed,
+            "serving": {"window_s_per_rate": window, "rates": rows,
+                        "plain_fp64_one_at_a_time_rate": plain["value"]}}
+
+
 # ------------------------------------------------------------- GPU arm --
+def l2_resident_copy_gbs(device: int, nbytes: int, reps: int = 200) -> float:
+    """Read + write bytes per second of a device-to-device copy whose source
+    and destination (nbytes each) stay in L2: the memory system's rate for a
+    working set the size of the ADI field and its half-step copy."""
+    import torch
+    src = torch.ones(nbytes // 8, dtype=torch.float64, device=device)
+    dst = torch.empty_like(src)
+    for _ in range(10):
+        dst.copy_(src)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    e0.record()
+    for _ in range(reps):
+        dst.copy_(src)
+    e1.record()
+    torch.cuda.synchronize(device)
+    return 2.0 * nbytes * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
+
+
 def run_ours(args, rank, world, device):
     import torch
     torch.cuda.set_device(device)
@@ -404,14 +506,20 @@ def run_ours(args, rank, world, device):
         adi_ms = sum(st[1] for st in stream_times) / len(stream_times)
         per_launch_s = adi_ms / 1e3 / W.adi_launches_per_step
         achieved = W.adi_bytes_per_launch / per_launch_s / 1e9
+        l2_copy = l2_resident_copy_gbs(device, W.adi_bytes_per_launch // 2)
         roofline = {"kernel": "adi_const_wave_kernel (FP64 vacuum half step, 1024^2, 7 systems per CTA)",
                     "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(achieved / peak, 4),
                     "peak_kind": peak_kind,
                     "traffic": profiled_traffic("adi_const_wave_kernel_1024.md"),
-                    "note": "algorithmic bytes 2 x 16 B per point per half step; the 16 MB "
-                            "field stays in the 126 MB L2 across half steps, so this is "
-                            "effective bandwidth (see profiles/)"}
+                    "residency": "L2: the 16 MB field and its 16 MB half-step copy stay in the "
+                                 "126 MB L2 across half steps, so `achieved` is effective "
+                                 "bandwidth against the HBM copy peak, not an HBM-bound figure",
+                    "l2_copy_gbs": round(l2_copy, 1),
+                    "frac_of_l2_copy": round(achieved / l2_copy, 4),
+                    "note": "algorithmic bytes 2 x 16 B per point per half step; l2_copy_gbs "
+                            "= a 16 MB -> 16 MB device copy between L2-resident buffers, "
+                            "timed in this run (read + write bytes per second)"}
     return {
         "metric": "grid-pt*steps/s (plain FP64)",
         "value": value,
@@ -425,8 +533,7 @@ def run_ours(args, rank, world, device):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded inputs with the benchmark configuration's shapes)",
-        "config": {"workload": W.name, "grid_pt_steps_per_step": W.pts_steps,
-                   "parallelism": f"replicas x{world}", "l2": "flushed before every step"},
+        "config": workload_config(args.workload, world),
         "e2e": {"value": e2e_value, "unit": "grid-pt*steps/s",
                 "h2d_bytes_per_step": W.h2d_bytes, "d2h_bytes_per_step": W.d2h_bytes},
         "gpu_launches": W.gpu_launches_per_step * args.steps,
@@ -444,8 +551,8 @@ def cpu_rate(workload: str, threads: int, scale: float = 1.0):
     po.set_threads(threads)
     if workload == "cn4096_adi1024":
         c, a = wl.waveguide_cn(), wl.sphere_adi()
-        n_cn = max(20, int(800 * scale))
-        n_adi = max(1, int(4 * scale))
+        n_cn = min(c.nsteps, max(20, int(800 * scale)))
+        n_adi = min(a.nsteps, max(1, int(4 * scale)))
         g = po.grid(c.xmin, c.xmax, c.dx, c.zmin, c.zmax, c.dz, wl.K)
         d, b = c.material()
         spec = po.MaterialSpec(po.MAT_XTABLE, delta_table=d, beta_table=b)
@@ -462,7 +569,7 @@ def cpu_rate(workload: str, threads: int, scale: float = 1.0):
         return pts / total, (f"CN {n_cn} of {c.nsteps} steps ({t_cn:.2f} s) + ADI {n_adi} of "
                              f"{a.nsteps} steps ({t_adi:.2f} s), extrapolated linearly")
     p = wl.waveguide_fft2d()
-    n = max(50, int(1000 * scale))
+    n = min(p.nsteps, max(50, int(1000 * scale)))
     g = po.grid(p.xmin, p.xmax, p.dx, p.zmin, p.zmax, p.dz, wl.K)
     d, b = p.material()
     spec = po.MaterialSpec(po.MAT_XTABLE, delta_table=d, beta_table=b)
@@ -486,18 +593,18 @@ def cpu_model():
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    threads = os.cpu_count() or 1
-    rates, sample = [], ""
-    for i in range(args.warmup + args.steps):
-        r, sample = cpu_rate(args.workload, threads, scale=0.5)
-        if i >= args.warmup:
-            rates.append(r)
-    value = statistics.median(rates)
-    if args.workload not in ("waveguide_fft2d", "cn4096_adi1024"):
+    if args.workload not in WORKLOADS:
         print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement is timed on "
                           "the waveguide_fft2d and cn4096_adi1024 workloads only"}))
         return None
-    W = {"cn4096_adi1024": CnAdiWorkload.name, "waveguide_fft2d": WaveguideFft2dWorkload.name}[args.workload]
+    threads = os.cpu_count() or 1
+    rates, sample = [], ""
+    for i in range(args.warmup + args.steps):
+        # about 4 s of host work per step (CN 4800 + ADI 24 steps)
+        r, sample = cpu_rate(args.workload, threads, scale=6.0)
+        if i >= args.warmup:
+            rates.append(r)
+    value = statistics.median(rates)
     return {
         "impl": "reference",
         "metric": "grid-pt*steps/s (plain FP64)",
@@ -512,7 +619,9 @@ def run_reference(args, rank, world):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": W, "parallelism": "host cores"},
+        "config": workload_config(args.workload, world),
+        "timing": f"wall clock of a bounded sample per step on {threads} host threads, "
+                  "extrapolated to the whole workload",
         "cpu_baseline": {"value": value, "unit": "grid-pt*steps/s", "cores": threads,
                          "kind": "port", "sample": sample + f"; {cpu_model()}"},
         "e2e": {"value": value, "unit": "grid-pt*steps/s", "h2d_bytes_per_step": 0,
@@ -520,6 +629,91 @@ def run_reference(args, rank, world):
         "note": "the reference cannot be built here (Armadillo, FFTW3, HDF5, jsoncpp, VISA "
                 "absent); this is the oracle's C++ restatement of the reference path",
     }
+
+
+# -------------------------------------------------- single cases (ncu) --
+def case_solver(kind: str, n: int, steps: int, precision: int):
+    """One solver with the workloads' synthetic inputs: the planar waveguide
+    for the 2-D kinds, the sphere of the ADI workload (z starting two steps
+    before it) and the 64-sphere set of the FFTSolver3D workload."""
+    import paxpro_b200 as pxp
+    if kind in ("fft2d", "cn"):
+        p = wl.Problem2D("case", "fft" if kind == "fft2d" else "cn", -250.0, 250.0,
+                         wl.step_for_nodes(-250.0, 250.0, n), 0.0, 1.0e9, 500.0, steps, 15.0,
+                         wl.Waveguide())
+        s = pxp.Solver(pxp.ProblemSpec(
+            kind=pxp.FFT_SOLVER_2D if kind == "fft2d" else pxp.CRANK_NICHOLSON,
+            x=pxp.Disc(p.xmin, p.xmax, p.dx), z=pxp.Disc(p.zmin, p.zmax, p.dz),
+            wavenumber=wl.K, precision=precision))
+        d, b = p.material()
+        s.set_material_table(d, b)
+    else:
+        p = wl.sphere_adi(n=n) if kind == "adi" else wl.spheres_fft3d(n=n)
+        zmin = p.zmin if kind == "fft3d" else 1.0e6 - 2 * p.dz
+        s = pxp.Solver(pxp.ProblemSpec(
+            kind=pxp.ADI if kind == "adi" else pxp.FFT_SOLVER_3D,
+            x=pxp.Disc(p.xmin, p.xmax, p.dx), y=pxp.Disc(p.xmin, p.xmax, p.dx),
+            z=pxp.Disc(zmin, 1.0e9, p.dz), wavenumber=wl.K, precision=precision))
+        s.set_material_spheres([pxp.Sphere(*sp) for sp in p.spheres])
+    s.set_initial_conditions(p.initial_field())
+    return s
+
+
+def run_case(args) -> int:
+    """--case KIND N STEPS: mean time per step of one solver, CUDA events on
+    its stream, min over --repeat repeats."""
+    import torch
+    kind, n, steps = args.case[0], int(args.case[1]), int(args.case[2])
+    if kind == "farfield":
+        return run_case_farfield(args, n, steps)
+    if kind not in ("fft2d", "cn", "adi", "fft3d"):
+        raise SystemExit(f"unknown case kind {kind}")
+    s = case_solver(kind, n, steps, 1 if args.fp32 else 0)
+    if args.flux:
+        total = steps * max(args.repeat, 1)
+        s.set_flux_windows(1, np.zeros(total, np.uint32), np.full(total, n - 1, np.uint32))
+    st = torch.cuda.ExternalStream(s.stream_ptr())
+    times = []
+    for _ in range(max(args.repeat, 1)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.step(steps)
+        e1.record(st)
+        s.synchronize()
+        times.append(e0.elapsed_time(e1) / steps)
+    out = s.get_last_solution()
+    assert np.all(np.isfinite(out))
+    print(f"{kind} n={n} steps={steps} {'fp32' if args.fp32 else 'fp64'}"
+          f"{' flux' if args.flux else ''}: "
+          f"{min(times) * 1e3:.2f} us/step (min of {len(times)})", flush=True)
+    s.close()
+    return 0
+
+
+def run_case_farfield(args, n: int, steps: int) -> int:
+    """--case farfield N STEPS: FFTSolver3D steps, then the far field of the
+    exit field minus a unit reference (pad --pad, angles -A..A) through
+    pxp_farfield, CUDA-event time per call on the solver's stream."""
+    import torch
+    s = case_solver("fft3d", n, steps, 1 if args.fp32 else 0)
+    s.step(steps)
+    s.set_reference(np.ones((n, n), dtype=np.complex128))
+    st = torch.cuda.ExternalStream(s.stream_ptr())
+    kw = dict(pad_length=args.pad, phi_min=-args.angle, phi_max=args.angle, subtract_reference=True)
+    res = s.farfield(**kw)
+    times = []
+    for _ in range(max(args.repeat, 1)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        res = s.farfield(**kw)
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    assert np.all(np.isfinite(res))
+    print(f"farfield n={n} pad={args.pad} angle={args.angle}: result {res.shape[0]} x "
+          f"{res.shape[1]}, {min(times):.3f} ms per call (min of {len(times)})", flush=True)
+    s.close()
+    return 0
 
 
 def main():
@@ -530,7 +724,18 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["mixed_batch", "served"], default="cn4096_adi1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served", action="store_true",
+                    help="leave the served half (mixed batch, serving p50/p99) out of the line")
+    ap.add_argument("--case", nargs=3, metavar=("KIND", "N", "STEPS"),
+                    help="time one solver case (fft2d, cn, adi, fft3d, farfield) and exit")
+    ap.add_argument("--fp32", action="store_true", help="--case: FP32 served mode")
+    ap.add_argument("--repeat", type=int, default=1, help="--case: repeats (min reported)")
+    ap.add_argument("--flux", action="store_true", help="--case: per-step flux windows")
+    ap.add_argument("--pad", type=int, default=32768, help="--case farfield: pad length")
+    ap.add_argument("--angle", type=float, default=0.05, help="--case farfield: max angle (deg)")
     args = ap.parse_args()
+    if args.case:
+        sys.exit(run_case(args))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -550,8 +755,13 @@ def main():
         out = run_serving(args, rank, world, local)
     else:
         out = run_ours(args, rank, world, local)
+    if args.workload == "cn4096_adi1024" and not args.no_served:
+        served = served_half(rank, world, local)
+        if out is not None:
+            out["served"] = served
     if out is not None and not args.no_cpu_baseline and args.workload in ("waveguide_fft2d", "cn4096_adi1024"):
-        rate, sample = cpu_rate(args.workload, 1, scale=1.0)
+        # about 10 s of single-thread work (CN 8000 + ADI 60 steps)
+        rate, sample = cpu_rate(args.workload, 1, scale=15.0)
         out["cpu_baseline"] = {"value": rate, "unit": "grid-pt*steps/s", "cores": 1,
                                "kind": "port", "sample": sample + f"; {cpu_model()}"}
     if world > 1:

@@ -339,8 +339,11 @@ int pxp_batch_status(pxp_batch b, int *active, size_t *bytes);
  * PXP_ERR_UNSUPPORTED and a message.  All calls on a device share that
  * array, so calls that overlap on the GPU race and must be serialised by the
  * caller.  The first call on each device looks up the array's device
- * address; make that first call before any stream capture.  Errors are
- * reported through pxp_last_error(NULL, ...). */
+ * address; make that first call before any stream capture.  The call makes
+ * problem->device current for its launches and restores the caller's
+ * current device before returning.  Every sampled plane is checked before
+ * the first launch, so a refused call leaves the field untouched.  Errors
+ * are reported through pxp_last_error(NULL, ...). */
 int pxp_adi_steps_noalloc(const pxp_problem *problem, const pxp_sphere *spheres, int nspheres,
                           void *dfield, unsigned first_step, int nsteps, void *stream);
 

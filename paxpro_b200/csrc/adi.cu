@@ -330,9 +330,8 @@ static cudaError_t adi_const_launch(const AdiHalf &h, const void *g, const void 
   constexpr size_t smem = ((sizeof(C) * (G + 2) * (N + N / 8 + 2) + 15) & ~size_t(15)) +
                           2 * sizeof(double2) * (N + N / 8) + sizeof(Affine) * (T / 32 + 1);
   auto k = adi_const_kernel<R, N, M, G>;
-  if (smem > 48 * 1024) {
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  {
+    const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)smem);
     if (attr != cudaSuccess) return attr;
   }
   k<<<N / G, T, smem, s>>>(h, (const double2 *)g, (const double2 *)hh);
@@ -659,9 +658,8 @@ static cudaError_t adi_const_wave_launch_x(const AdiHalf &h, const void *tabs, c
   static_assert(P % 32 == 0, "whole warps per group");
   static_assert(NG <= 15, "one named barrier per group");
   auto k = adi_const_wave_kernel<N, M, G, S, XH>;
-  if (smem > 48 * 1024) {
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  {
+    const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)smem);
     if (attr != cudaSuccess) return attr;
   }
   // launched as a programmatic dependent of the previous kernel in the
@@ -781,10 +779,10 @@ static cudaError_t adi_launch_g(const AdiHalf &h, cudaStream_t s) {
   const size_t tile = (sizeof(C) * (G + 2) * (n + n / 8 + 2) + 15) & ~size_t(15);
   const size_t smem = tile + sizeof(double2) * 4 * G * 2 * (n / kAdiM);
   auto k = adi_half_kernel<R, kAdiM, G>;
-  // raise the dynamic shared-memory limit once per instantiation to the largest
-  // size it can need (n = 2048 for G = 2, n = 1024 for G = 4)
-  static const cudaError_t attr = cudaFuncSetAttribute(
-      k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  // raise the dynamic shared-memory limit on this device to the largest size
+  // the instantiation can need (n = 2048 for G = 2, n = 1024 for G = 4)
+  const cudaError_t attr = raise_dynamic_smem(
+      (const void *)k,
       (int)(((sizeof(C) * (G + 2) * (G == 2 ? 2048 + 258 : 1024 + 130) + 15) & ~size_t(15)) +
             sizeof(double2) * 4 * G * 2 * ((G == 2 ? 2048 : 1024) / kAdiM)));
   if (attr != cudaSuccess) return attr;

@@ -26,7 +26,10 @@
 // The array's device address is looked up once per device with
 // cudaGetSymbolAddress, with that device current, on the first call that
 // uses the device; that first call should therefore come before any stream
-// capture.
+// capture.  The call makes problem->device current for its launches and
+// gives the caller's current device back before it returns.  Every plane the
+// steps sample is checked before the first launch: a refused call (more
+// than 16 spheres meeting one plane) leaves the field untouched.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -75,6 +78,79 @@ int scratch_for_current_device(void **out) {
   return PXP_OK;
 }
 
+// Spheres that can contain a point of plane z, the handle path's test
+// (fl(dz^2) < fl(R^2)), copied in list order into out (when not null) up to
+// kInlineSpheres; returns how many there are.
+int spheres_meeting(const pxp_sphere *spheres, int nspheres, double z, pxp::Sphere *out) {
+  int c = 0;
+  for (int i = 0; i < nspheres; ++i) {
+    volatile double dz = z - spheres[i].cz;
+    volatile double dz2 = dz * dz;
+    volatile double r2 = spheres[i].radius * spheres[i].radius;
+    if (!(dz2 < r2)) continue;
+    if (out && c < pxp::kInlineSpheres)
+      out[c] = {spheres[i].cx, spheres[i].cy, spheres[i].cz, spheres[i].radius, spheres[i].delta,
+                spheres[i].beta};
+    ++c;
+  }
+  return c;
+}
+
+// The launches of pxp_adi_steps_noalloc, on the current device; the planes
+// were checked by the caller.
+int run_steps(const pxp_problem *p, pxp::Precision prec, unsigned n, const pxp_sphere *spheres,
+              int nspheres, void *dfield, unsigned first_step, int nsteps, cudaStream_t st) {
+  void *scratch = nullptr;
+  int rc = scratch_for_current_device(&scratch);
+  if (rc) return rc;
+  const double dzh = p->z.step / 2.0;  // ADI::xImplicit (src/alternatingDirectionSolver.cpp:18)
+  const double k = p->wavenumber;
+  const double kdx2 = k * p->x.step * p->x.step, kdy2 = k * p->y.step * p->y.step;
+  pxp::AdiHalf a{};
+  a.n = (int)n;
+  // sizes other than powers of two: systems padded with decoupled rows, as
+  // the solver handle runs them
+  a.n_pad = pxp::adi_padded_n((int)n) != (int)n ? pxp::adi_padded_n((int)n) : 0;
+  a.use_tbc = p->transparent_bc ? 1 : 0;
+  a.inv_dzh = 1.0 / dzh;
+  a.k = k;
+  a.xmin = p->x.min;
+  a.dx = p->x.step;
+  a.ymin = p->y.min;
+  a.dy = p->y.step;
+  a.spheres_all = nullptr;
+  a.save = nullptr;
+  for (int i = 0; i < nsteps; ++i) {
+    const unsigned step = first_step + (unsigned)i;
+    const double z = p->z.min + step * p->z.step;  // getZ
+    // x half step: field -> scratch (ADI::xImplicit, :8-76)
+    a.in = dfield;
+    a.out = scratch;
+    a.stride_pos = n;
+    a.stride_sys = 1;
+    a.y_implicit = 0;
+    a.kd2_impl = kdx2;
+    a.kd2_expl = kdy2;
+    a.z = z;
+    a.nspheres = spheres_meeting(spheres, nspheres, a.z, a.spheres);
+    cudaError_t e = pxp::launch_adi_half(prec, a, st);
+    if (e != cudaSuccess) return fail(PXP_ERR_CUDA, cudaGetErrorString(e));
+    // y half step: scratch -> field (ADI::yImplicit, :78-134)
+    a.in = scratch;
+    a.out = dfield;
+    a.stride_pos = 1;
+    a.stride_sys = n;
+    a.y_implicit = 1;
+    a.kd2_impl = kdy2;
+    a.kd2_expl = kdx2;
+    a.z = z + dzh;
+    a.nspheres = spheres_meeting(spheres, nspheres, a.z, a.spheres);
+    e = pxp::launch_adi_half(prec, a, st);
+    if (e != cudaSuccess) return fail(PXP_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return PXP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -101,74 +177,30 @@ int pxp_adi_steps_noalloc(const pxp_problem *p, const pxp_sphere *spheres, int n
                   n, n, bytes, kNoAllocScratchBytes);
     return fail(PXP_ERR_UNSUPPORTED, m);
   }
-  if (!pxp::adi_supported(prec, (int)n))
+  if (!pxp::adi_padded_supported(prec, (int)n))
     return fail(PXP_ERR_UNSUPPORTED, "pxp_adi_steps_noalloc: grid size not supported");
-  if (cudaSetDevice(p->device) != cudaSuccess) return fail(PXP_ERR_CUDA, "cudaSetDevice failed");
-  void *scratch = nullptr;
-  int rc = scratch_for_current_device(&scratch);
-  if (rc) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
 
   const double dzh = p->z.step / 2.0;  // ADI::xImplicit (src/alternatingDirectionSolver.cpp:18)
-  const double k = p->wavenumber;
-  const double kdx2 = k * p->x.step * p->x.step, kdy2 = k * p->y.step * p->y.step;
-  pxp::AdiHalf a{};
-  a.n = (int)n;
-  a.use_tbc = p->transparent_bc ? 1 : 0;
-  a.inv_dzh = 1.0 / dzh;
-  a.k = k;
-  a.xmin = p->x.min;
-  a.dx = p->x.step;
-  a.ymin = p->y.min;
-  a.dy = p->y.step;
-  // spheres that can contain a point of plane z (same test as the handle path)
-  auto fill = [&](double z) -> int {
-    int c = 0;
-    for (int i = 0; i < nspheres; ++i) {
-      volatile double dz = z - spheres[i].cz;
-      volatile double dz2 = dz * dz;
-      volatile double r2 = spheres[i].radius * spheres[i].radius;
-      if (!(dz2 < r2)) continue;
-      if (c == pxp::kInlineSpheres) return -1;
-      a.spheres[c++] = {spheres[i].cx, spheres[i].cy, spheres[i].cz, spheres[i].radius,
-                        spheres[i].delta, spheres[i].beta};
-    }
-    a.nspheres = c;
-    a.spheres_all = nullptr;
-    return 0;
-  };
+  // Every plane the call samples (getZ(step) for the x half step, getZ(step) +
+  // dz/2 for the y half step) is checked before the first launch, so a call
+  // that is refused leaves the caller's field untouched.
   for (int i = 0; i < nsteps; ++i) {
-    const unsigned step = first_step + (unsigned)i;
-    const double z = p->z.min + step * p->z.step;  // getZ
-    a.in = dfield;
-    a.out = scratch;
-    a.save = nullptr;
-    a.stride_pos = n;
-    a.stride_sys = 1;
-    a.y_implicit = 0;
-    a.kd2_impl = kdx2;
-    a.kd2_expl = kdy2;
-    a.z = z;
-    if (fill(a.z))
+    const double z = p->z.min + (first_step + (unsigned)i) * p->z.step;  // getZ
+    if (spheres_meeting(spheres, nspheres, z, nullptr) > pxp::kInlineSpheres ||
+        spheres_meeting(spheres, nspheres, z + dzh, nullptr) > pxp::kInlineSpheres)
       return fail(PXP_ERR_UNSUPPORTED,
-                  "pxp_adi_steps_noalloc: more than 16 spheres meet one plane");
-    cudaError_t e = pxp::launch_adi_half(prec, a, st);
-    if (e != cudaSuccess) return fail(PXP_ERR_CUDA, cudaGetErrorString(e));
-    a.in = scratch;
-    a.out = dfield;
-    a.stride_pos = 1;
-    a.stride_sys = n;
-    a.y_implicit = 1;
-    a.kd2_impl = kdy2;
-    a.kd2_expl = kdx2;
-    a.z = z + dzh;
-    if (fill(a.z))
-      return fail(PXP_ERR_UNSUPPORTED,
-                  "pxp_adi_steps_noalloc: more than 16 spheres meet one plane");
-    e = pxp::launch_adi_half(prec, a, st);
-    if (e != cudaSuccess) return fail(PXP_ERR_CUDA, cudaGetErrorString(e));
+                  "pxp_adi_steps_noalloc: more than 16 spheres meet one plane; nothing was run");
   }
-  return PXP_OK;
+
+  // Run on the problem's device and give the caller's current device back.
+  int caller_dev = 0;
+  if (cudaGetDevice(&caller_dev) != cudaSuccess) return fail(PXP_ERR_CUDA, "cudaGetDevice failed");
+  if (caller_dev != p->device && cudaSetDevice(p->device) != cudaSuccess)
+    return fail(PXP_ERR_CUDA, "cudaSetDevice failed");
+  const int rc = run_steps(p, prec, n, spheres, nspheres, dfield, first_step, nsteps,
+                           (cudaStream_t)stream);
+  if (caller_dev != p->device) cudaSetDevice(caller_dev);
+  return rc;
 }
 
 }  // extern "C"

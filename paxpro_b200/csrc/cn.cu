@@ -283,8 +283,7 @@ static cudaError_t cn_const_launch_f(const CnJob *d_jobs, int nj, int step0, int
   constexpr size_t smem = sizeof(double2) * (3 * N + 2 * T) + sizeof(Affine) * (T / 32 + 1);
   auto k = cn_const_kernel<R, M, T, FLUX>;
   {  // the static flux slots count against the 48 KB default too
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)smem);
     if (attr != cudaSuccess) return attr;
   }
   k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);
@@ -331,8 +330,7 @@ static cudaError_t cn_launch_f(const CnJob *d_jobs, int nj, int step0, int nstep
   size_t smem = sizeof(double2) * 4 * 2 * T + sizeof(C) * kCnM * T;
   auto k = cn_kernel<R, kCnM, T, FLUX>;
   {  // the static flux slots count against the 48 KB default too
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)smem);
     if (attr != cudaSuccess) return attr;
   }
   k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);

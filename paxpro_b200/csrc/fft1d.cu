@@ -197,8 +197,7 @@ static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nstep
   constexpr size_t smem = tw_smem ? field_bytes + tw_bytes : field_bytes;
   auto k = fft1d_kernel<R, N, T, tw_smem, FLUX>;
   {  // the static flux slots count against the 48 KB default too
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)smem);
     if (attr != cudaSuccess) return attr;
   }
   k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);
@@ -224,8 +223,7 @@ static cudaError_t launch_blu(const Fft1dJob *d_jobs, int nj, int step0, int nst
   using C = typename Cx<R>::T;
   constexpr int T = M >= 8192 ? 512 : (M >= 2048 ? 256 : (M >= 512 ? 64 : 32));
   auto k = fft1d_bluestein_kernel<R, M, T, FLUX>;
-  static const cudaError_t attr = cudaFuncSetAttribute(
-      k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(C) * (M + M / 2)));
+  const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)(sizeof(C) * (M + M / 2)));
   if (attr != cudaSuccess) return attr;
   k<<<nj, T, sizeof(C) * (M + n), s>>>(d_jobs, step0, nsteps);
   return cudaGetLastError();

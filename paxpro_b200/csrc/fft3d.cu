@@ -325,12 +325,12 @@ static cudaError_t fft3d_xpass_w_launch(const Fft3dPass &q, const double *kx2, c
   constexpr size_t smem = sizeof(double2) * N + sizeof(double) * N + sizeof(C) * W * xpass_ld<C, N>();
   static_assert(smem + 16 <= 227 * 1024, "wide x pass exceeds shared memory");
   auto k = fft3d_xpass_w_kernel<R, N, T, W>;
-  static int grid = 0;
+  {
+    const cudaError_t e = raise_dynamic_smem((const void *)k, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  static int grid = 0;  // CTAs per wave (same SM count on every B200)
   if (grid == 0) {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -362,12 +362,12 @@ static cudaError_t fft3d_launch_v(const Fft3dPass &q, const double *kx2, const d
   constexpr size_t smem = DB ? 2 * sizeof(C) * N + sizeof(double2) * N + sizeof(double) * N
                              : sizeof(C) * N;
   auto k = fft3d_pass_kernel<R, N, T, DB, MAXR>;
-  static int grid = 0;
+  {
+    const cudaError_t e = raise_dynamic_smem((const void *)k, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  static int grid = 0;  // CTAs per wave (same SM count on every B200)
   if (grid == 0) {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -12,6 +12,12 @@ enum Precision { kFP64 = 0, kFP32 = 1 };
 // Record the message pxp_last_error(NULL, ...) returns (capi.cu).
 void set_last_error(const char *msg);
 
+// Raise the dynamic shared-memory limit of `kernel` to at least `bytes` on the
+// current device (smem_attr.cu).  The attribute is per device context, so a
+// process driving several GPUs needs it set on each; this records what was
+// set per (kernel, device) and calls cudaFuncSetAttribute only when needed.
+cudaError_t raise_dynamic_smem(const void *kernel, int bytes);
+
 // ---------------------------------------------------------------- FFT 1-D --
 // One split-step problem with one transverse dimension (FFTSolver2D).
 // All complex arrays are interleaved and in the solver's precision.

@@ -1,0 +1,36 @@
+// smem_attr.cu -- per-device bookkeeping of the dynamic shared-memory limit
+// of each kernel.
+//
+// cudaFuncAttributeMaxDynamicSharedMemorySize belongs to a kernel in one
+// device's context: raising it while device 0 is current leaves the default
+// 48 KB on device 1 (and a kernel with static shared memory gets less than
+// 48 KB of dynamic memory by default).  The launchers call
+// pxp::raise_dynamic_smem before every launch; the attribute is set on the
+// current device the first time a (kernel, device) pair asks for at least
+// that many bytes, and the lookup is a short locked map search afterwards.
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "pxp_kernels.h"
+
+namespace {
+std::mutex g_mutex;
+std::map<std::pair<const void *, int>, int> g_set;  // (kernel, device) -> bytes set
+}  // namespace
+
+cudaError_t pxp::raise_dynamic_smem(const void *kernel, int bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_mutex);
+  auto key = std::make_pair(kernel, dev);
+  auto it = g_set.find(key);
+  if (it != g_set.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  g_set[key] = bytes;
+  return cudaSuccess;
+}

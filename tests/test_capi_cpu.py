@@ -91,3 +91,30 @@ def test_new_entry_points_reject_null_handles_and_fill_defaults():
     assert lib.pxp_get_flux(None, 1, 1, out) == _capi.PXP_ERR_INVALID
     assert lib.pxp_field_flux(None, 0, 1, out) == _capi.PXP_ERR_INVALID
     assert lib.pxp_get_post_resized(None, 0, -1, 2, 2, out) == _capi.PXP_ERR_INVALID
+
+
+def test_noalloc_refuses_too_many_spheres_on_a_plane_before_running_anything():
+    """pxp_adi_steps_noalloc checks every plane its steps sample before the
+    first launch: with 17 spheres meeting the plane of a later step the call
+    is refused, having made no device call (none is possible here) and left
+    the field buffer as it was."""
+    import ctypes as C
+    import numpy as np
+    import paxpro_b200 as pxp
+    from paxpro_b200 import _capi
+    from paxpro_b200 import workloads as wl
+    n = 64
+    dx = wl.step_for_nodes(-500.0, 500.0, n)
+    spec = pxp.ProblemSpec(kind=pxp.ADI, x=pxp.Disc(-500.0, 500.0, dx),
+                           y=pxp.Disc(-500.0, 500.0, dx), z=pxp.Disc(0.0, 1e4, 1000.0),
+                           wavenumber=wl.K)
+    # 17 spheres around z = 5000 (step 5); steps 1-4 meet none
+    sph = (_capi.SphereC * 17)(*[_capi.SphereC(10.0 * i, 0.0, 5000.0, 100.0, 1e-5, 1e-7)
+                                 for i in range(17)])
+    field = np.arange(2 * n * n, dtype=np.float64)
+    before = field.copy()
+    rc = _capi.lib().pxp_adi_steps_noalloc(C.byref(spec.to_c()), sph, 17,
+                                          C.c_void_p(field.ctypes.data), 1, 6, None)
+    assert rc == _capi.PXP_ERR_UNSUPPORTED
+    assert "nothing was run" in _capi.last_error()
+    assert np.array_equal(field, before)
