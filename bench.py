@@ -27,10 +27,12 @@ batch's FP32-served rate over plain FP64 one job at a time (with the largest
 relative intensity error against FP64) and the serving loop's p50/p99 job
 latency at two arrival rates (`served`; --no-served skips it).
 
---impl reference times the CPU restatement of the reference (oracle/, the
-reference cannot be built here: Armadillo/FFTW3/HDF5 are absent) on all host
-cores, on a bounded sample of the same workload per step.  That arm imports
-nothing from the CUDA package, so the CUDA library is never loaded in it.
+--impl reference times the reference's own solvers on all host cores, on a
+bounded sample of the same workload per step: its sources compiled in place
+(oracle/_ref, against stand-ins for the absent Armadillo/FFTW3/HDF5 headers),
+or the oracle's restatement when that library was not built.  That arm
+imports nothing from the CUDA package, so the CUDA library is never loaded
+in it.
 
     python bench.py --case KIND N STEPS [--fp32] [--repeat R] [--flux]
 
@@ -543,26 +545,46 @@ def run_ours(args, rank, world, device):
 
 
 # ------------------------------------------------------------- CPU arms --
-def cpu_rate(workload: str, threads: int, scale: float = 1.0):
-    """Oracle (CPU restatement of the reference) on a bounded sample of the
-    workload; returns (pt-steps/s extrapolated to the whole workload,
-    description of the sample)."""
+def cpu_kind() -> str:
+    """"reference" when the reference's own code is built (oracle/_ref, the
+    reference's solver sources compiled in place), else "port" (the
+    oracle's C++ restatement)."""
+    from oracle import pyoracle as po
+    return "reference" if po.refpin() is not None else "port"
+
+
+def cpu_rate(workload: str, threads: int, scale: float = 1.0, kind: str = "port"):
+    """A bounded sample of the workload on the host cores; returns
+    (pt-steps/s extrapolated to the whole workload, description of the
+    sample).  kind "reference" runs the reference's own solvers
+    (ParaxialSimulation + CrankNicholson / ADI / FFTSolver2D compiled from
+    its sources, oracle/_ref), "port" the oracle's restatement.  The z range
+    of each sample run covers only the sampled steps (the reference's 2-D
+    solvers keep every step's field)."""
     from oracle import pyoracle as po
     po.set_threads(threads)
+    ref = kind == "reference"
     if workload == "cn4096_adi1024":
         c, a = wl.waveguide_cn(), wl.sphere_adi()
         n_cn = min(c.nsteps, max(20, int(800 * scale)))
         n_adi = min(a.nsteps, max(1, int(4 * scale)))
-        g = po.grid(c.xmin, c.xmax, c.dx, c.zmin, c.zmax, c.dz, wl.K)
+        g = po.grid(c.xmin, c.xmax, c.dx, c.zmin, c.zmin + (n_cn + 1) * c.dz, c.dz, wl.K)
         d, b = c.material()
         spec = po.MaterialSpec(po.MAT_XTABLE, delta_table=d, beta_table=b)
         t0 = time.perf_counter()
-        po.cn2d_run(g, spec, c.initial_field(), n_cn, 0)
+        if ref:
+            po.ref_run2d(po.REF_CRANK_NICHOLSON, g, spec, c.initial_field(), n_cn, 0,
+                         threads=threads)
+        else:
+            po.cn2d_run(g, spec, c.initial_field(), n_cn, 0)
         t_cn = time.perf_counter() - t0
-        ga = po.grid(a.xmin, a.xmax, a.dx, a.zmin, a.zmax, a.dz, wl.K)
+        ga = po.grid(a.xmin, a.xmax, a.dx, a.zmin, a.zmin + (n_adi + 1) * a.dz, a.dz, wl.K)
         sph = po.MaterialSpec(po.MAT_SPHERES, spheres=a.spheres)
         t0 = time.perf_counter()
-        po.adi3d_run(ga, sph, a.initial_field(), n_adi, 0)
+        if ref:
+            po.ref_run3d(po.REF_ADI, ga, sph, a.initial_field(), n_adi, 0, threads=threads)
+        else:
+            po.adi3d_run(ga, sph, a.initial_field(), n_adi, 0)
         t_adi = time.perf_counter() - t0
         total = t_cn * c.nsteps / n_cn + t_adi * a.nsteps / n_adi
         pts = c.nx * c.nsteps + a.nx * a.nx * a.nsteps
@@ -570,11 +592,14 @@ def cpu_rate(workload: str, threads: int, scale: float = 1.0):
                              f"{a.nsteps} steps ({t_adi:.2f} s), extrapolated linearly")
     p = wl.waveguide_fft2d()
     n = min(p.nsteps, max(50, int(1000 * scale)))
-    g = po.grid(p.xmin, p.xmax, p.dx, p.zmin, p.zmax, p.dz, wl.K)
+    g = po.grid(p.xmin, p.xmax, p.dx, p.zmin, p.zmin + (n + 1) * p.dz, p.dz, wl.K)
     d, b = p.material()
     spec = po.MaterialSpec(po.MAT_XTABLE, delta_table=d, beta_table=b)
     t0 = time.perf_counter()
-    po.fft2d_run(g, spec, p.initial_field(), n, 0)
+    if ref:
+        po.ref_run2d(po.REF_FFT_SOLVER_2D, g, spec, p.initial_field(), n, 0, threads=threads)
+    else:
+        po.fft2d_run(g, spec, p.initial_field(), n, 0)
     t = time.perf_counter() - t0
     return p.nx * p.nsteps / (t * p.nsteps / n), f"FFTSolver2D {n} of {p.nsteps} steps ({t:.2f} s)"
 
@@ -598,10 +623,11 @@ def run_reference(args, rank, world):
                           "the waveguide_fft2d and cn4096_adi1024 workloads only"}))
         return None
     threads = os.cpu_count() or 1
+    kind = cpu_kind()
     rates, sample = [], ""
     for i in range(args.warmup + args.steps):
-        # about 4 s of host work per step (CN 4800 + ADI 24 steps)
-        r, sample = cpu_rate(args.workload, threads, scale=6.0)
+        # a few seconds of host work per step (CN 2400 + ADI 12 steps)
+        r, sample = cpu_rate(args.workload, threads, scale=3.0, kind=kind)
         if i >= args.warmup:
             rates.append(r)
     value = statistics.median(rates)
@@ -623,11 +649,13 @@ def run_reference(args, rank, world):
         "timing": f"wall clock of a bounded sample per step on {threads} host threads, "
                   "extrapolated to the whole workload",
         "cpu_baseline": {"value": value, "unit": "grid-pt*steps/s", "cores": threads,
-                         "kind": "port", "sample": sample + f"; {cpu_model()}"},
+                         "kind": kind, "sample": sample + f"; {cpu_model()}"},
         "e2e": {"value": value, "unit": "grid-pt*steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "note": "the reference cannot be built here (Armadillo, FFTW3, HDF5, jsoncpp, VISA "
-                "absent); this is the oracle's C++ restatement of the reference path",
+        "note": ("the reference's own solver sources compiled in place (oracle/_ref) against "
+                 "stand-ins for its absent third-party headers; FFTs by the oracle's FFT "
+                 "where FFTW would run" if kind == "reference" else
+                 "the oracle's C++ restatement of the reference path (oracle/_ref not built)"),
     }
 
 
@@ -760,10 +788,12 @@ def main():
         if out is not None:
             out["served"] = served
     if out is not None and not args.no_cpu_baseline and args.workload in ("waveguide_fft2d", "cn4096_adi1024"):
-        # about 10 s of single-thread work (CN 8000 + ADI 60 steps)
-        rate, sample = cpu_rate(args.workload, 1, scale=15.0)
+        # about 10 s of single-thread work (CN 8000 + ADI 32 steps)
+        kind = cpu_kind()
+        rate, sample = cpu_rate(args.workload, 1, scale=8.0 if kind == "reference" else 15.0,
+                                kind=kind)
         out["cpu_baseline"] = {"value": rate, "unit": "grid-pt*steps/s", "cores": 1,
-                               "kind": "port", "sample": sample + f"; {cpu_model()}"}
+                               "kind": kind, "sample": sample + f"; {cpu_model()}"}
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

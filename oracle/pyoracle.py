@@ -105,6 +105,18 @@ def refpin():
         d = C.POINTER(C.c_double)
         _REFPIN.ref_thomas_solve.argtypes = [d, d, d, C.c_int]
         _REFPIN.ref_paraxial_equation.argtypes = [C.c_double] * 3 + [d]
+        _REFPIN.ref_node_count.restype = C.c_uint
+        _REFPIN.ref_node_count.argtypes = [C.c_double] * 3
+        _REFPIN.ref_run2d.argtypes = [C.c_int, C.POINTER(Grid), C.POINTER(Material), C.c_int,
+                                      d, C.c_int, C.c_int, d, d, C.c_int]
+        _REFPIN.ref_run3d.argtypes = [C.c_int, C.POINTER(Grid), C.POINTER(Material), C.c_int,
+                                      C.c_double, C.c_double, d, C.c_int, C.c_int, d, d,
+                                      C.c_int]
+        _REFPIN.ref_run3d_saved.argtypes = [C.c_int, C.POINTER(Grid), C.POINTER(Material),
+                                            C.c_uint, C.c_uint, d, C.c_int, d,
+                                            C.POINTER(C.c_uint), C.c_int]
+        _REFPIN.ref_source_field.argtypes = [C.c_int, C.POINTER(Grid), C.c_int] + \
+            [C.c_double] * 7 + [d]
     return _REFPIN
 
 
@@ -234,6 +246,92 @@ def _run3d(fn, g, spec, u0, nsteps, save_every, *extra):
     if rc:
         raise ValueError(f"oracle rejected the problem (rc={rc})")
     return out, [s.reshape((ny, nx), order="F") for s in saves[:nsave]]
+
+
+# ---- the reference's own solvers (oracle/_ref, compiled from its sources) --
+REF_FFT_SOLVER_2D, REF_CRANK_NICHOLSON, REF_FFT_SOLVER_3D, REF_ADI = 1, 2, 3, 4
+
+
+def ref_run2d(kind, g, spec, u0, nsteps, save_every=0, transparent=False, threads=1):
+    """FFTSolver2D (kind 1) / CrankNicholson (kind 2) of the reference itself,
+    driven through ParaxialSimulation and Solver::step(); (last field, saves).
+    The grid's z range must hold more than nsteps steps."""
+    rp = refpin()
+    if rp is None:
+        raise RuntimeError("reference pin library not built")
+    u0 = np.ascontiguousarray(u0, dtype=np.complex128)
+    n = len(u0)
+    nsave = nsteps // save_every if save_every > 0 else 0
+    saves = np.zeros((max(nsave, 1), n), dtype=np.complex128)
+    out = np.zeros(n, dtype=np.complex128)
+    rc = rp.ref_run2d(int(kind), C.byref(g), C.byref(spec.m), int(transparent), _p(u0),
+                      int(nsteps), int(save_every), _p(saves), _p(out), int(threads))
+    if rc:
+        raise ValueError(f"reference run failed (rc={rc})")
+    return out, saves[:nsave]
+
+
+def ref_run3d(kind, g, spec, u0, nsteps, save_every=0, use_tbc=False, absorber_width=0.0,
+              absorber_damping=0.0, threads=1):
+    """FFTSolver3D (kind 3) / ADI (kind 4) of the reference itself; fields
+    (Ny, Nx) Fortran-order as the oracle's 3-D runs."""
+    rp = refpin()
+    if rp is None:
+        raise RuntimeError("reference pin library not built")
+    u0 = np.asfortranarray(u0, dtype=np.complex128)
+    ny, nx = u0.shape
+    nsave = nsteps // save_every if save_every > 0 else 0
+    saves = np.zeros((max(nsave, 1), nx * ny), dtype=np.complex128)
+    out = np.zeros((ny, nx), dtype=np.complex128, order="F")
+    flat_in = u0.reshape(-1, order="F")
+    rc = rp.ref_run3d(int(kind), C.byref(g), C.byref(spec.m), int(use_tbc),
+                      float(absorber_width), float(absorber_damping), _p(flat_in), int(nsteps),
+                      int(save_every), _p(saves), out.ctypes.data_as(C.POINTER(C.c_double)),
+                      int(threads))
+    if rc:
+        raise ValueError(f"reference run failed (rc={rc})")
+    return out, [s.reshape((ny, nx), order="F") for s in saves[:nsave]]
+
+
+def ref_saved_cube(kind, g, spec, u0, nsteps, ratio_x, ratio_z, threads=1):
+    """The reference's saved-slice cube (Solver3D::getSolution3D) after
+    nsteps steps with transverse / longitudinal downsampling ratios: a list
+    of (m, m) Fortran-order slices."""
+    rp = refpin()
+    if rp is None:
+        raise RuntimeError("reference pin library not built")
+    u0 = np.asfortranarray(u0, dtype=np.complex128)
+    dims = (C.c_uint * 3)()
+    flat_in = u0.reshape(-1, order="F")
+    rc = rp.ref_run3d_saved(int(kind), C.byref(g), C.byref(spec.m), int(ratio_x), int(ratio_z),
+                            _p(flat_in), int(nsteps), None, dims, int(threads))
+    if rc:
+        raise ValueError(f"reference run failed (rc={rc})")
+    m, _, ns = dims[0], dims[1], dims[2]
+    out = np.zeros(m * m * ns, dtype=np.complex128)
+    rc = rp.ref_run3d_saved(int(kind), C.byref(g), C.byref(spec.m), int(ratio_x), int(ratio_z),
+                            _p(flat_in), int(nsteps), _p(out), dims, int(threads))
+    if rc:
+        raise ValueError(f"reference run failed (rc={rc})")
+    return [out[s * m * m:(s + 1) * m * m].reshape((m, m), order="F") for s in range(ns)]
+
+
+def ref_source_field(dim, g, source, wavelength, waist=1.0, cx=0.0, cy=0.0, amplitude=1.0,
+                     angle_deg=0.0, z0=0.0):
+    """The initial field ParaxialSimulation::setBoundaryConditions gives a
+    solver: source 0 = GaussianBeam, 1 = PlaneWave; dim 2 (Nx values) or 3
+    ((Ny, Nx) Fortran order)."""
+    rp = refpin()
+    if rp is None:
+        raise RuntimeError("reference pin library not built")
+    n = node_count(g.xmin, g.xmax, g.dx)
+    out = np.zeros(n if dim == 2 else n * n, dtype=np.complex128)
+    rc = rp.ref_source_field(int(dim), C.byref(g), int(source), float(wavelength), float(waist),
+                             float(cx), float(cy), float(amplitude), float(angle_deg), float(z0),
+                             _p(out))
+    if rc:
+        raise ValueError(f"reference source failed (rc={rc})")
+    return out if dim == 2 else out.reshape((n, n), order="F")
 
 
 def fft3d_run(g, spec, u0, nsteps, save_every=0, absorber_width=0.0, absorber_damping=0.0):
