@@ -259,6 +259,89 @@ int ref_run3d_saved(int kind, const orc_grid *g, const orc_material *m, unsigned
   }
 }
 
+// A CSGMaterial (src/materialFunction.cpp:3-13) built from the reference's
+// own geometry classes (geom::Sphere / Box / Cylinder, Part, Module:
+// src/shape.cpp, src/geometry.cpp) and evaluated at npts points xyz[3*i..];
+// delta and beta of point i go to out[2*i], out[2*i + 1].  A shape is built
+// from its kind and sizes (sphere: radius; box: Lx, Ly, Lz; cylinder: r1,
+// r2, height), then its ops replayed in order: type 0 translate(a, b, c),
+// 1 rotate(a degrees, axis b), 2 scale(a, axis b) (axis 0/1/2 = X/Y/Z).
+// Shapes join their part by add (operation 0) or difference (1), parts
+// their module likewise; modules are added in order.  Returns 0, or -2 when
+// the reference threw (e.g. a difference before any add).
+typedef struct {
+  int kind, operation, first_op, num_ops;
+  double size[3];
+} ref_csg_shape;
+typedef struct {
+  int type;
+  double a, b, c;
+} ref_csg_op;
+typedef struct {
+  int operation, first_shape, num_shapes;
+  double delta, beta;
+} ref_csg_part;
+typedef struct {
+  int first_part, num_parts;
+} ref_csg_module;
+
+int ref_csg_eval(const ref_csg_module *modules, int nmodules, const ref_csg_part *parts,
+                 const ref_csg_shape *shapes, const ref_csg_op *ops, const double *xyz, int npts,
+                 double *out) {
+  try {
+    std::vector<std::unique_ptr<geom::Shape>> keep_shapes;
+    std::vector<std::unique_ptr<geom::Part>> keep_parts;
+    std::vector<std::unique_ptr<geom::Module>> keep_modules;
+    CSGMaterial mat;
+    const geom::Axis_t axes[3] = {geom::Axis_t::X, geom::Axis_t::Y, geom::Axis_t::Z};
+    for (int mi = 0; mi < nmodules; ++mi) {
+      keep_modules.emplace_back(new geom::Module("module"));
+      geom::Module &mod = *keep_modules.back();
+      for (int pi = 0; pi < modules[mi].num_parts; ++pi) {
+        const ref_csg_part &pd = parts[modules[mi].first_part + pi];
+        keep_parts.emplace_back(new geom::Part("part"));
+        geom::Part &part = *keep_parts.back();
+        part.delta = pd.delta;
+        part.beta = pd.beta;
+        for (int si = 0; si < pd.num_shapes; ++si) {
+          const ref_csg_shape &sd = shapes[pd.first_shape + si];
+          geom::Shape *sh = nullptr;
+          if (sd.kind == 0)
+            sh = new geom::Sphere(sd.size[0]);
+          else if (sd.kind == 1)
+            sh = new geom::Box(sd.size[0], sd.size[1], sd.size[2]);
+          else
+            sh = new geom::Cylinder(sd.size[0], sd.size[1], sd.size[2]);
+          keep_shapes.emplace_back(sh);
+          for (int oi = 0; oi < sd.num_ops; ++oi) {
+            const ref_csg_op &op = ops[sd.first_op + oi];
+            if (op.type == 0)
+              sh->translate(op.a, op.b, op.c);
+            else if (op.type == 1)
+              sh->rotate(op.a, axes[(int)op.b]);
+            else
+              sh->scale(op.a, axes[(int)op.b]);
+          }
+          if (sd.operation == 0)
+            part.add(*sh);
+          else
+            part.difference(*sh);
+        }
+        if (pd.operation == 0)
+          mod.add(part);
+        else
+          mod.difference(part);
+      }
+      mat.addModule(mod);
+    }
+    for (int i = 0; i < npts; ++i)
+      mat.getXrayMatProp(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], out[2 * i], out[2 * i + 1]);
+    return 0;
+  } catch (...) {
+    return -2;
+  }
+}
+
 // The initial field ParaxialSimulation::setBoundaryConditions(const
 // ParaxialSource&) hands a solver (src/paraxialSimulation.cpp:356-399) on the
 // grid g: a GaussianBeam (source 0: wavelength, waist, centre (cx, cy),

@@ -174,3 +174,40 @@ def test_node_count_matches_reference_build():
         want = po.refpin().ref_node_count(mn, mx, st)
         assert po.node_count(mn, mx, st) == want
         assert lib.pxp_node_count(mn, mx, st) == want
+
+
+def test_csg_material_matches_reference_geometry_classes():
+    """CSGMaterial::getXrayMatProp of a scene built from the reference's own
+    geom:: classes (src/shape.cpp, src/geometry.cpp, src/materialFunction.cpp)
+    against the oracle's evaluation of the flattened scene (the form the
+    device takes, pxp_set_material_csg) and the Python classes, at random
+    points around every object: equal values at every point."""
+    import ctypes as C
+
+    from paxpro_b200 import csg
+
+    from csg_geometry import geometry, reference_arrays
+
+    mods = geometry()
+    spec = po.MaterialSpec(po.MAT_CSG, csg=csg.flatten(mods))
+    g = po.grid(-500.0, 500.0, 1.0, 0.0, 8000.0, 1000.0, 62.83)
+    rng = np.random.default_rng(11)
+    centres = np.array([(0.0, 0.0, 3000.0), (100.0, -100.0, 4000.0), (-150.0, 50.0, 5000.0),
+                        (-300.0, 300.0, 6000.0), (20.0, 0.0, 3000.0)])
+    npts = 6000
+    xyz = centres[np.arange(npts) % len(centres)] + rng.uniform(-200.0, 200.0, (npts, 3))
+    xyz = np.ascontiguousarray(xyz)
+    out = np.zeros(2 * npts)
+    m, p, s, o = reference_arrays()
+    rp = po.refpin()
+    rc = rp.ref_csg_eval(m, len(m), p, s, o, xyz.ctypes.data_as(C.POINTER(C.c_double)), npts,
+                         out.ctypes.data_as(C.POINTER(C.c_double)))
+    assert rc == 0
+    hits = 0
+    for i in range(npts):
+        x, y, z = xyz[i]
+        want = (out[2 * i], out[2 * i + 1])
+        assert po.material_eval(spec, g, x, y, z) == want, (x, y, z)
+        assert csg.material(mods, x, y, z) == want, (x, y, z)
+        hits += want[0] != 0.0
+    assert 300 < hits < npts - 300  # inside and outside points of several parts
