@@ -281,21 +281,25 @@ def mixed_core(rank, world, device):
     sv.run_batched(jobs[:40], precision=1)          # warm-up (kernels, pools)
     batched = sv.run_batched(jobs, precision=1, keep=keep)
     plain = sv.run_plain(jobs, precision=0, keep=keep)
-    errs = [0.0]
+    from paxpro_b200 import accuracy
+    errs, perrs = [0.0], [0.0]
     for i in keep:
-        a, b = batched.intensities[i], plain.intensities[i]
-        errs.append(float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+        e = accuracy.field_errors(batched.fields[i], plain.fields[i])
+        errs.append(e["intensity_rel_l2"])
+        perrs.append(e["phase_rms_rad"])
     dev = torch.device("cuda", device) if dist is not None else None
     b_pts, b_sec = sh.reduce_rate(batched.pts_steps, batched.seconds, dist, dev)
     p_pts, p_sec = sh.reduce_rate(plain.pts_steps, plain.seconds, dist, dev)
     _, err = sh.reduce_rate(0.0, max(errs), dist, dev)
+    _, perr = sh.reduce_rate(0.0, max(perrs), dist, dev)
     if rank != 0:
         return None
     return {"served_fp32": b_pts / b_sec, "served_seconds": b_sec, "grid_pt_steps": b_pts,
             "plain_fp64": p_pts / p_sec, "plain_seconds": p_sec,
             "served_over_plain": (b_pts / b_sec) / (p_pts / p_sec),
             "max_rel_intensity_err_vs_fp64": err,
-            "intensity_error_checked_on": f"{len(keep)} of {len(jobs)} jobs per GPU"}
+            "max_phase_rms_rad_vs_fp64": perr,
+            "errors_checked_on": f"{len(keep)} of {len(jobs)} jobs per GPU"}
 
 
 def run_mixed(args, rank, world, device):
@@ -386,10 +390,52 @@ def run_serving(args, rank, world, device):
     }
 
 
+def precision_sweep(device, kind: str = "fft3d", every: int = 100):
+    """The FP32 served mode against FP64 on the GPU over a whole workload:
+    FFTSolver3D 4096^2 with 64 spheres, 1000 steps (kind "fft3d"), or ADI
+    1024^2, 2000 steps (kind "adi"); the relative L2 intensity error and the
+    intensity-weighted phase error (paxpro_b200.accuracy) of every
+    `every`-th field, plus each precision's time per step (CUDA events on
+    the solver's stream)."""
+    import torch
+
+    import paxpro_b200 as pxp
+    from paxpro_b200 import accuracy
+    p = wl.spheres_fft3d() if kind == "fft3d" else wl.sphere_adi()
+    k = pxp.FFT_SOLVER_3D if kind == "fft3d" else pxp.ADI
+    solvers, us = [], []
+    for prec in (0, 1):
+        s = pxp.Solver(pxp.ProblemSpec(
+            kind=k, x=pxp.Disc(p.xmin, p.xmax, p.dx), y=pxp.Disc(p.xmin, p.xmax, p.dx),
+            z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K, precision=prec,
+            save_every=every, device=device))
+        s.set_material_spheres([pxp.Sphere(*sp) for sp in p.spheres])
+        s.set_initial_conditions(p.initial_field())
+        st = torch.cuda.ExternalStream(s.stream_ptr(), device=device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.step(p.nsteps)
+        e1.record(st)
+        s.synchronize()
+        us.append(e0.elapsed_time(e1) * 1e3 / p.nsteps)
+        solvers.append(s)
+    rows = []
+    for i in range(solvers[0].num_saved()):
+        r = accuracy.field_errors(solvers[1].get_saved(i), solvers[0].get_saved(i))
+        rows.append({"step": (i + 1) * every, **{key: float(f"{v:.3e}") for key, v in r.items()}})
+    for s in solvers:
+        s.close()
+    return {"workload": f"{p.name}: {p.nx}^2, {p.nsteps} steps, {len(p.spheres)} spheres",
+            "us_per_step_fp64": round(us[0], 2), "us_per_step_fp32": round(us[1], 2),
+            "max_intensity_rel_l2": max(r["intensity_rel_l2"] for r in rows),
+            "max_phase_rms_rad": max(r["phase_rms_rad"] for r in rows), "every": rows}
+
+
 def served_half(rank, world, device):
     """The served half of the metric for the default line: the mixed batch
-    (FP32 served over plain FP64, intensity error) and the serving loop's
-    p50/p99 at two arrival rates, 2 s of arrivals each."""
+    (FP32 served over plain FP64, intensity error), the serving loop's
+    p50/p99 at two arrival rates (2 s of arrivals each) and the FFTSolver3D
+    precision sweep (rank 0 only; it needs no other rank)."""
     mixed = mixed_core(rank, world, device)
     srv = serving_core(rank, world, device, rates=(200, 1000), window=2.0)
     if rank != 0:
@@ -397,7 +443,8 @@ def served_half(rank, world, device):
     rows, plain, window = srv
     return {"mixed_batch": mixed,
             "serving": {"window_s_per_rate": window, "rates": rows,
-                        "plain_fp64_one_at_a_time_rate": plain["value"]}}
+                        "plain_fp64_one_at_a_time_rate": plain["value"]},
+            "precision_sweep": precision_sweep(device)}
 
 
 # ------------------------------------------------------------- GPU arm --

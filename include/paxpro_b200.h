@@ -347,6 +347,17 @@ int pxp_batch_status(pxp_batch b, int *active, size_t *bytes);
 int pxp_adi_steps_noalloc(const pxp_problem *problem, const pxp_sphere *spheres, int nspheres,
                           void *dfield, unsigned first_step, int nsteps, void *stream);
 
+/* Failure-path self-test, no reference counterpart.  The propagation
+ * kernels wait for their asynchronous copies with a bounded wait; when one
+ * runs out the kernel counts it and returns instead of hanging, and the next
+ * pxp_synchronize (or result copy) of every handle on that device reports
+ * PXP_ERR_CUDA.  This launches, on the handle's stream, a one-thread kernel
+ * whose wait (limit_ns of GPU time, at most 10 s) can never be satisfied,
+ * so that a test can check that path without a fault; the handle's later
+ * calls then report the error, and handles created afterwards are not
+ * affected. */
+int pxp_selftest_bounded_wait(pxp_solver s, unsigned long long limit_ns);
+
 /* Last error message of the handle (NULL handle: last global error). */
 int pxp_last_error(pxp_solver s, char *buf, size_t len);
 

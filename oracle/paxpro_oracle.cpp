@@ -293,6 +293,21 @@ void thomas(cd *diag, const cd *subdiag, cd *rhs, unsigned n) {
   for (int i = (int)n - 2; i >= 0; --i) diag[i] = rhs[i] - sup[i] * diag[i + 1];
 }
 
+// The ADI half step's Thomas solve (src/alternatingDirectionSolver.cpp:60,
+// 124): the reference runs include/thomasAlgorithm.tpp over one chain of
+// nsys*len unknowns whose sub-diagonal is exactly zero between systems.  At a
+// system's first row the chain's terms sub*sup and sub*rhs are then complex
+// zeros, so its divisions equal a fresh solve's; at a system's last row sup
+// is 0/den and the back substitution leaves rhs as it is.  Solving each
+// system on its own therefore gives the chain's values (pinned bit for bit
+// against the reference's own ADI in the tests), and the systems run in
+// parallel.
+void thomas_systems(cd *diag, const cd *subdiag, cd *rhs, unsigned nsys, unsigned len, int th) {
+#pragma omp parallel for num_threads(th)
+  for (long s = 0; s < (long)nsys; ++s)
+    thomas(diag + s * len, subdiag + s * len, rhs + s * len, len);
+}
+
 // --------------------------------------------------------- FFTSolver2D --
 // src/fftSolver2D.cpp:15-19 (kernel), :52-59 (spatialFreq)
 double spatial_freq(unsigned indx, unsigned size, double step) {
@@ -569,9 +584,9 @@ int orc_fft3d_run(const orc_grid *gp, const orc_material *m,
 
 // ADI::solveStep (src/alternatingDirectionSolver.cpp:136-155): xImplicit
 // (:8-76), prev = curr, yImplicit (:78-134, including the reference's
-// parenthesisation of the y-implicit diagonal at :103).  Thomas runs over one
-// chain of Nx*Ny unknowns whose sub-diagonal is zero at every system start,
-// so the systems decouple exactly as in the reference.  The reference's
+// parenthesisation of the y-implicit diagonal at :103).  The reference's
+// Thomas chain of Nx*Ny unknowns has a zero sub-diagonal at every system
+// start, so it is solved system by system (thomas_systems).  The reference's
 // OpenMP build loop shares delta/beta between threads (:22, :92); the oracle
 // uses per-point values, i.e. the single-thread result.  TBC: ADI::applyTBC
 // (:157-234).
@@ -659,7 +674,7 @@ int orc_adi3d_run(const orc_grid *gp, const orc_material *m, int use_tbc,
         if (i < Ny - 1) rhs[indx] += 0.5 * im * P(i + 1, j) / (k * dy * dy);
       }
       if (use_tbc) tbc(true);
-      thomas(diag.data(), subdiag.data(), rhs.data(), (unsigned)npts);
+      thomas_systems(diag.data(), subdiag.data(), rhs.data(), Ny, Nx, th);
 #pragma omp parallel for num_threads(th)
       for (long indx = 0; indx < npts; ++indx) {
         unsigned i = indx / Nx, j = indx % Nx;
@@ -685,7 +700,7 @@ int orc_adi3d_run(const orc_grid *gp, const orc_material *m, int use_tbc,
         if (i < Ny - 1) rhs[indx] += 0.5 * im * P(j, i + 1) / (k * dx * dx);
       }
       if (use_tbc) tbc(false);
-      thomas(diag.data(), subdiag.data(), rhs.data(), (unsigned)npts);
+      thomas_systems(diag.data(), subdiag.data(), rhs.data(), Nx, Ny, th);
 #pragma omp parallel for num_threads(th)
       for (long indx = 0; indx < npts; ++indx) {
         unsigned i = indx / Ny, j = indx % Ny;

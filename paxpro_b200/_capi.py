@@ -132,6 +132,7 @@ def lib():
         "pxp_reset": (C.c_int, [h]),
         "pxp_current_step": (C.c_int, [h, C.POINTER(C.c_uint)]),
         "pxp_shape": (C.c_int, [h, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),
+        "pxp_selftest_bounded_wait": (C.c_int, [h, C.c_ulonglong]),
         "pxp_adi_steps_noalloc": (C.c_int, [C.POINTER(Problem), C.POINTER(SphereC), C.c_int,
                                             C.c_void_p, C.c_uint, C.c_int, C.c_void_p]),
         "pxp_device_bytes": (C.c_int, [h, C.POINTER(C.c_size_t)]),

@@ -734,6 +734,23 @@ bool adi_const_staged_tables(int n, const double *g, const double *h, double *ou
   return true;
 }
 
+// Self-test of the bounded-wait failure path: one thread arms an mbarrier
+// for a 16-byte transaction that no copy ever delivers and waits on it with
+// the kernels' bounded wait (mbar_wait_bounded) and the given limit.  The
+// wait runs out, the kernel records it in the same counter the propagation
+// kernels use, and returns; nothing faults and the context stays usable.
+__global__ void wait_selftest_kernel(unsigned long long limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  mbar_init(&bar, 1);
+  mbar_arrive_expect_tx(&bar, 16u);
+  if (!mbar_wait_bounded(&bar, 0, limit_ns)) atomicAdd(&g_wait_timeouts, 1u);
+}
+
+cudaError_t launch_wait_selftest(unsigned long long limit_ns, cudaStream_t s) {
+  wait_selftest_kernel<<<1, 1, 0, s>>>(limit_ns);
+  return cudaGetLastError();
+}
+
 unsigned wait_timeouts(cudaStream_t s) {
   unsigned v = 0;
   if (cudaMemcpyFromSymbolAsync(&v, g_wait_timeouts, sizeof(v), 0, cudaMemcpyDeviceToHost, s) !=

@@ -1438,6 +1438,13 @@ int pxp_synchronize(pxp_solver h) {
   return check_waits(h);
 }
 
+int pxp_selftest_bounded_wait(pxp_solver h, unsigned long long limit_ns) {
+  if (h == nullptr || limit_ns == 0 || limit_ns > 10000000000ull) return PXP_ERR_INVALID;
+  cudaError_t e = pxp::launch_wait_selftest(limit_ns, h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "bounded-wait self-test launch");
+  return PXP_OK;
+}
+
 int pxp_get_last_solution(pxp_solver h, double *field) {
   if (h == nullptr || field == nullptr) return PXP_ERR_INVALID;
   return download_field(h, field, h->d_field);

@@ -239,6 +239,9 @@ cudaError_t launch_widen(const void *in, void *out, long long n, cudaStream_t s)
 // Kernel waits on the current device that ran out (bounded mbarrier waits),
 // read on stream s (synchronises s).
 unsigned wait_timeouts(cudaStream_t s);
+// One-thread kernel whose bounded wait (limit_ns of global time) runs out on
+// purpose and is counted like the propagation kernels' (adi.cu).
+cudaError_t launch_wait_selftest(unsigned long long limit_ns, cudaStream_t s);
 
 // --------------------------------------------------------------- FFT 3-D --
 // FFTSolver3D (src/fftSolver3D.cpp:52-156, 327-374) on an n x n field in the

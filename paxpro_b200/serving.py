@@ -140,6 +140,7 @@ class RunResult:
     seconds: float
     pts_steps: float
     intensities: dict
+    fields: dict = field(default_factory=dict)  # exit fields of the kept jobs
 
     @property
     def rate(self) -> float:
@@ -154,7 +155,8 @@ def _sync_all():
 def run_batched(jobs: List[Job], precision: int = pxp.FP32, max_steps: int = 100000,
                 device: int = 0, keep: Optional[set] = None) -> RunResult:
     """All jobs in one Batch; returns wall time of the rounds (inputs already
-    on the device) and the exit intensities of the jobs listed in `keep`."""
+    on the device) and the exit intensities and fields of the jobs listed in
+    `keep`."""
     solvers = [make_solver(j, precision, device) for j in jobs]
     batch = pxp.Batch(device)
     for j, s in zip(jobs, solvers):
@@ -167,20 +169,21 @@ def run_batched(jobs: List[Job], precision: int = pxp.FP32, max_steps: int = 100
         batch.round(max_steps)
         done += batch.collect()
     secs = time.perf_counter() - t0
-    out = {}
+    out, fields = {}, {}
     for i, s in enumerate(solvers):
         if keep is None or i in keep:
             out[i] = s.get_intensity()
+            fields[i] = s.get_last_solution()
         s.close()
     batch.close()
-    return RunResult(secs, sum(j.pts_steps for j in jobs), out)
+    return RunResult(secs, sum(j.pts_steps for j in jobs), out, fields)
 
 
 def run_plain(jobs: List[Job], precision: int = pxp.FP64, device: int = 0,
               keep: Optional[set] = None) -> RunResult:
     """Each job alone, one after the other, through its own solver handle."""
     total = 0.0
-    out = {}
+    out, fields = {}, {}
     for i, j in enumerate(jobs):
         s = make_solver(j, precision, device)
         s.synchronize()
@@ -190,8 +193,9 @@ def run_plain(jobs: List[Job], precision: int = pxp.FP64, device: int = 0,
         total += time.perf_counter() - t0
         if keep is None or i in keep:
             out[i] = s.get_intensity()
+            fields[i] = s.get_last_solution()
         s.close()
-    return RunResult(total, sum(j.pts_steps for j in jobs), out)
+    return RunResult(total, sum(j.pts_steps for j in jobs), out, fields)
 
 
 @dataclass
