@@ -244,7 +244,7 @@ int alloc(pxp_solver_s *h, void **p, size_t bytes, const char *what) {
 // with the same grids).  The handles do not own these copies.
 struct TableKey {
   int device, kind;  // kind 0: twiddles (radix 8), 1: 1-D propagator, 2: kx^2 per
-                     // column, 3: twiddles (radix 16)
+                     // column, 3: twiddles (radix 16), 4: exp(-2 pi i m / n), m < n
   unsigned n;
   double dx, dz, k;
   bool operator<(const TableKey &o) const {
@@ -256,7 +256,7 @@ std::map<TableKey, void *> g_tables;
 
 int shared_table(pxp_solver_s *h, int kind, void **out) {
   const unsigned n = h->nx;
-  TableKey key{h->prob.device, kind, n, kind ? h->prob.x.step : 0.0,
+  TableKey key{h->prob.device, kind, n, (kind == 1 || kind == 2) ? h->prob.x.step : 0.0,
                kind == 1 ? h->prob.z.step : 0.0, kind == 1 ? h->prob.wavenumber : 0.0};
   std::lock_guard<std::mutex> lk(g_table_mutex);
   auto it = g_tables.find(key);
@@ -268,6 +268,14 @@ int shared_table(pxp_solver_s *h, int kind, void **out) {
   std::vector<double> t2;
   if (kind == 0 || kind == 3) {
     t = twiddles((int)n, kind == 3 ? 16 : 8);
+  } else if (kind == 4) {
+    // exp(-2 pi i m / n), m < n, in extended precision
+    t.resize(n);
+    const long double pi_l = 3.141592653589793238462643383279502884L;
+    for (unsigned m = 0; m < n; ++m) {
+      const long double a = -2.0L * pi_l * (long double)m / (long double)n;
+      t[m] = cd((double)cosl(a), (double)sinl(a));
+    }
   } else if (kind == 1) {
     t.resize(n);
     for (unsigned i = 0; i < n; ++i)
@@ -766,12 +774,12 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
 // field (one untimed x+y pass pair, then three timed ones; the fastest kept),
 // and every solver with that key runs the winner from its first step on, so
 // a field never depends on when tuning happened (radix 8 and radix 16 round
-// differently).  PXP_FFT3D_VARIANT=0|1|2 pins the variant instead.
+// differently).  PXP_FFT3D_VARIANT=0|1|2|3 pins the variant instead.
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, int, unsigned>, int> g_fft3d_variant;
 
 int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, const void *tw16,
-                  int *out) {
+                  const void *wn, int *out) {
   if (const char *env = std::getenv("PXP_FFT3D_VARIANT")) {
     const int v = std::atoi(env);
     if (v >= 0 && v < pxp::kFft3dVariants) {
@@ -806,9 +814,10 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
       for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
         cudaEventRecord(e0, h->stream);
         q.mode = 1;
-        e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, h->stream);
+        e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
         q.mode = 2;
-        if (e == cudaSuccess) e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, h->stream);
+        if (e == cudaSuccess)
+          e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
         cudaEventRecord(e1, h->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -854,14 +863,15 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     q.inv_damp_x = p.x.step / p.absorber_damping;
     q.inv_damp_y = p.y.step / p.absorber_damping;
   }
-  void *kx2 = nullptr, *tw16 = nullptr;
+  void *kx2 = nullptr, *tw16 = nullptr, *wn = nullptr;
   if (int rc = shared_table(h, 2, &kx2)) return rc;
   if (int rc = shared_table(h, 3, &tw16)) return rc;
+  if (int rc = shared_table(h, 4, &wn)) return rc;
   int variant = 0;
-  if (int rc = fft3d_variant(h, q, kx2, tw16, &variant)) return rc;
+  if (int rc = fft3d_variant(h, q, kx2, tw16, wn, &variant)) return rc;
   cudaError_t e;
   q.mode = 0;  // forward transform along y of the real-space field
-  if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, h->stream)) != cudaSuccess)
+  if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, wn, h->stream)) != cudaSuccess)
     return h->cuda_fail(e, "FFT3D forward y pass");
   std::vector<pxp::Sphere> act;
   // step i of this call: x pass, then the y pass (mode 3 on the last step
@@ -870,7 +880,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     const unsigned step = first + (unsigned)i;
     q.mode = 1;
     q.save = nullptr;
-    if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, h->stream)) !=
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, wn, h->stream)) !=
         cudaSuccess)
       return h->cuda_fail(e, "FFT3D x pass");
     q.mode = (i == nsteps - 1) ? 3 : 2;
@@ -888,7 +898,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     }
     char *slot = save_at(h, step) ? save_slot(h, step) : nullptr;
     q.save = slot && h->d_save_stage ? h->d_save_stage : slot;
-    if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, h->stream)) !=
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, wn, h->stream)) !=
         cudaSuccess)
       return h->cuda_fail(e, "FFT3D y pass");
     if (slot && h->d_save_stage) return save_downsample(h, slot);
@@ -904,7 +914,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     return act.empty() && !csg_active(h, std::min(get_z(h, step - 1), get_z(h, step)),
                                       std::max(get_z(h, step - 1), get_z(h, step)));
   };
-  const std::vector<const void *> sig = {h->d_field, h->d_tw, kx2, tw16,
+  const std::vector<const void *> sig = {h->d_field, h->d_tw, kx2, tw16, wn,
                                          (const void *)(size_t)(16 + variant)};
   for (int i = 0; i < nsteps;) {
     if (i > 0 && step_graphs_enabled() && nsteps - i > kGraphSteps) {

@@ -1,0 +1,117 @@
+// fft3d_point.cuh -- per-point arithmetic of the FFTSolver3D line passes:
+// the material at a point (spheres or CSG), FFTSolver3D::refraction with its
+// refraction integral (src/fftSolver3D.cpp:122-156, 253-273), the absorber
+// bands (src/absorber.cpp:3-12), the spatial frequencies (:32-50) and the
+// propagator product.  Shared by the line-pass kernels of fft3d.cu and
+// fft3d_lines.cu so that both round every point identically.
+#pragma once
+#include "csg.cuh"
+#include "fft_smem.cuh"
+#include "pxp_kernels.h"
+#include "pxp_sincos.h"
+
+namespace pxp {
+
+__device__ __forceinline__ void sph_eval(const Fft3dPass &q, double x, double y, double z,
+                                         double &delta, double &beta) {
+  if (q.csg.active) {
+    csg_material(q.csg, x, y, z, delta, beta);
+    return;
+  }
+  delta = 0.0;
+  beta = 0.0;
+  const int n = q.nspheres;
+  const Sphere *list = n > kInlineSpheres ? q.spheres_all : q.spheres;
+  for (int i = 0; i < n; ++i) {
+    const Sphere sp = list[i];
+    double ddx = __dsub_rn(x, sp.cx), ddy = __dsub_rn(y, sp.cy), ddz = __dsub_rn(z, sp.cz);
+    double rsq = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
+    if (rsq < __dmul_rn(sp.r, sp.r)) {
+      delta = sp.delta;
+      beta = sp.beta;
+      return;
+    }
+  }
+}
+
+// FFTSolver3D::refraction for one point: delta, beta used for the step.
+__device__ __forceinline__ void step_material(const Fft3dPass &q, double x, double y,
+                                              double &delta, double &beta) {
+  double dp, bp;
+  sph_eval(q, x, y, q.z1, delta, beta);
+  sph_eval(q, x, y, q.z0, dp, bp);
+  if (fabs(__dsub_rn(delta, dp)) > 1e-10 || fabs(__dsub_rn(beta, bp)) > 1e-10) {
+    // refractionIntegral(x, y, z0, z1): endpoints once, 8 interior samples
+    // twice (the 9th is skipped), divided by 2*10
+    double dt, bt;
+    sph_eval(q, x, y, q.z0, delta, beta);
+    sph_eval(q, x, y, q.z1, dt, bt);
+    delta = __dadd_rn(delta, dt);
+    beta = __dadd_rn(beta, bt);
+    const double dzz = __ddiv_rn(__dsub_rn(q.z1, q.z0), 10.0);
+    for (int i = 1; i < 9; ++i) {
+      const double z = __dadd_rn(q.z0, __dmul_rn((double)i, dzz));
+      sph_eval(q, x, y, z, dt, bt);
+      delta = __dadd_rn(delta, __dmul_rn(2.0, dt));
+      beta = __dadd_rn(beta, __dmul_rn(2.0, bt));
+    }
+    delta = __ddiv_rn(delta, 20.0);
+    beta = __ddiv_rn(beta, 20.0);
+  }
+}
+
+// spatialFreq: fold, then 2*PI*indx / (step*size)
+__device__ __forceinline__ double kfreq(int idx, int n, double two_pi, double stepn) {
+  if (idx > n / 2) idx = n - idx;
+  return __ddiv_rn(__dmul_rn(two_pi, (double)idx), stepn);
+}
+
+template <typename R> __device__ __forceinline__ typename Cx<R>::T mul_k(typename Cx<R>::T u,
+                                                                        double2 k);
+template <> __device__ __forceinline__ double2 mul_k<double>(double2 u, double2 k) {
+  return cx_mul_rn(u, k);
+}
+template <> __device__ __forceinline__ float2 mul_k<float>(float2 u, double2 k) {
+  return tw_mul(u, k);
+}
+
+// Refraction, absorber: u = (u * t) / (n*n), then absorber factors.
+template <typename R>
+__device__ __forceinline__ typename Cx<R>::T refract3(const Fft3dPass &q, typename Cx<R>::T uu,
+                                                      int ix, int iy, double inv_norm) {
+  const double x = __dadd_rn(q.xmin, __dmul_rn((double)ix, q.dx));
+  const double y = __dadd_rn(q.ymin, __dmul_rn((double)iy, q.dy));
+  double delta = 0.0, beta = 0.0;
+  if (q.nspheres > 0 || q.csg.active) step_material(q, x, y, delta, beta);
+  double2 u = to_d(uu);
+  if (delta != 0.0 || beta != 0.0) {
+    // exp(-k*(beta + i*delta)*dz)
+    const double re = __dmul_rn(__dmul_rn(-q.k, beta), q.dz);
+    const double im = __dmul_rn(__dmul_rn(-q.k, delta), q.dz);
+    const double e = exp(re);
+    double sn, cs;
+    sincos(im, &sn, &cs);
+    const double2 t = mk(__dmul_rn(e, cs), __dmul_rn(e, sn));
+    if constexpr (sizeof(R) == 8) {
+      u = cx_mul_rn(u, t);
+    } else {
+      u = cmul(u, t);
+    }
+  }
+  // (u * t) / (n*n): n*n is a power of two, so multiplying by its exact
+  // reciprocal rounds identically to the division
+  u = cx_scale_rn(u, inv_norm);
+  if (q.thick_y > 0) {
+    if (iy < q.thick_y) u = cx_scale_rn(u, exp(-(double)(q.thick_y - iy - 1) * q.inv_damp_y));
+    if (q.n - 1 - iy < q.thick_y)
+      u = cx_scale_rn(u, exp(-(double)(q.thick_y - (q.n - 1 - iy) - 1) * q.inv_damp_y));
+  }
+  if (q.thick_x > 0) {
+    if (ix < q.thick_x) u = cx_scale_rn(u, exp(-(double)(q.thick_x - ix - 1) * q.inv_damp_x));
+    if (q.n - 1 - ix < q.thick_x)
+      u = cx_scale_rn(u, exp(-(double)(q.thick_x - (q.n - 1 - ix) - 1) * q.inv_damp_x));
+  }
+  return from_d<R>(u);
+}
+
+}  // namespace pxp

@@ -277,12 +277,20 @@ struct Fft3dPass {
   double inv_damp_x, inv_damp_y;
 };
 // variant: 0 = radix 8, double-buffered, tables in shared memory; 1 = radix
-// 8, single buffer, tables through L1; 2 = radix 16, single buffer.
+// 8, single buffer, tables through L1; 2 = radix 16, single buffer; 3 =
+// register-resident transforms with TMA-staged lines (fft3d_lines.cu; n up
+// to 4096, other sizes fall back to variant 0).
 // kx2: n doubles, fl(kx*kx) per column index; q.twiddle / tw16: Stockham
-// twiddles for radix 8 / radix 16 pass orders.
+// twiddles for radix 8 / radix 16 pass orders; wn: n complex128
+// exp(-2 pi i m / n), m < n.
 cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, const double *kx2,
-                              const void *tw16, cudaStream_t s);
-constexpr int kFft3dVariants = 3;
+                              const void *tw16, const void *wn, cudaStream_t s);
+constexpr int kFft3dVariants = 4;
 bool fft3d_supported(Precision p, int n);
+bool fft3d_lines_supported(Precision p, int n);
+cudaError_t launch_fft3d_lines(Precision p, const Fft3dPass &q, const double *kx2, const void *wn,
+                               cudaStream_t s);
+// Bounded waits of the line-pass kernels that ran out on the current device.
+unsigned fft3d_lines_wait_timeouts(cudaStream_t s);
 
 }  // namespace pxp

@@ -142,3 +142,47 @@ def test_fft3d_fp32_served_intensity():
     out, saves, ref_out, ref_saves = _run_both(512, 1000.0, 0.0, 1000.0, 300, sph,
                                                save_every=50, precision=1)
     assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
+
+
+@pytest.fixture
+def _variant(monkeypatch):
+    """Pin the FFTSolver3D launch variant for one test."""
+    def pin(v):
+        monkeypatch.setenv("PXP_FFT3D_VARIANT", str(v))
+    return pin
+
+
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024, 2048])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fft3d_register_line_kernel_every_size(n, precision, _variant):
+    """Variant 3 (register-resident transforms, TMA-staged lines) at every
+    size it takes, FP64 and FP32: spheres crossing the sampling planes (the
+    refraction integral at their rims), the absorber, saves, and calls split
+    in chunks (the forward-only and inverse-only passes at call ends)."""
+    _variant(3)
+    sph = [(20.0, 10.0, 2500.0, 200.0, 3e-5, 6e-7), (-150.0, 120.0, 4100.0, 90.0, 2e-5, 4e-7)]
+    out, saves, ref_out, ref_saves = _run_both(n, 1000.0, 0.0, 1000.0, 6, sph, save_every=2,
+                                               chunks=2, precision=precision,
+                                               absorber=(40.0, 30.0))
+    assert len(saves) == 3
+    if precision == 0:
+        assert max(_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP64_TOL
+        assert _rel(out, ref_out) <= FP64_TOL
+    else:
+        assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
+    assert np.std(np.abs(out)) > 1e-5
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fft3d_register_line_kernel_4096(precision, _variant):
+    _variant(3)
+    p = wl.spheres_fft3d()
+    near = [s for s in p.spheres if s[2] + s[3] >= 86000.0 and s[2] - s[3] <= 92000.0]
+    assert near  # step 44 of the workload samples a sphere
+    out, saves, ref_out, ref_saves = _run_both(4096, 2000.0, 84000.0, p.dz, 4, near,
+                                               save_every=2, precision=precision)
+    if precision == 0:
+        assert max(_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP64_TOL
+    else:
+        assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
+    assert np.std(np.abs(out)) > 0
