@@ -23,9 +23,11 @@
 // and the VISA longitudinal low-pass filter (solve() requires
 // disableLongitudinalFilter() when the longitudinal downsampling ratio is
 // above 1), the waveguides' border tracker, control files and eigenmode
-// projections, the projection solver.  The 3-D solvers take a
-// SphereMaterial, a CSGMaterial over geom::Module / Part / Shape (evaluated
-// on the device), or no material.
+// projections, the projection solver.  The 3-D solvers take any
+// MaterialFunction: a SphereMaterial or a CSGMaterial over geom::Module /
+// Part / Shape is evaluated on the device; any other material (a user
+// subclass, as in the reference's examples) is sampled on the host at the
+// planes the reference's solvers sample and handed over per block of steps.
 #pragma once
 #include <algorithm>
 #include <cmath>
@@ -56,7 +58,7 @@ class MaterialFunction {
   virtual void getXrayMatProp(double x, double y, double z, double &delta,
                               double &beta) const = 0;
   /** Extension without a reference counterpart: return true when delta and
-   * beta do not depend on z, so the 2-D CUDA solvers sample the medium once
+   * beta do not depend on z, so the CUDA solvers sample the medium once
    * instead of once per step.  The default (false) is always correct. */
   virtual bool zInvariant() const { return false; }
 };
@@ -830,7 +832,7 @@ class Solver3D : public Solver {
 
   void step() override {
     initDevice();
-    check(pxp_step(handle, 1));
+    runSteps(currentStep, 1);
     check(pxp_get_last_solution(handle, reinterpret_cast<double *>(currentSolution.memptr())));
     copyCurrentSolution(currentStep++);
   }
@@ -841,7 +843,7 @@ class Solver3D : public Solver {
     initDevice();
     const unsigned first = currentStep, last = Nz - 1;
     if (first > last) return;
-    check(pxp_step(handle, (int)(last - first + 1)));
+    runSteps(first, last - first + 1);
     const unsigned ratio = guide->longitudinalDiscretization().downsamplingRatio;
     int nsaved = 0;
     check(pxp_num_saved(handle, &nsaved));
@@ -864,6 +866,81 @@ class Solver3D : public Solver {
   bool icPending{false};
   double absorberWidth{0.0}, absorberDamping{0.0};
   bool tbc{false};
+  bool materialPlanes{false};  // a user MaterialFunction, sampled per step
+
+  /** FFTSolver3D::refraction's material at (x, y) for the step from z0 to
+   * z1 (src/fftSolver3D.cpp:138-149): the value at z1, or, where it differs
+   * from the value at z0 by more than 1e-10, refractionIntegral (:253-273,
+   * the endpoints once, interior samples 1..8 of 10 twice, over 2*10). */
+  static void refractionMaterial(const ParaxialSimulation &g, double x, double y, double z0,
+                                 double z1, double &delta, double &beta) {
+    const double ZERO = 1E-10;
+    const unsigned nSteps = 10;
+    double deltaPrev, betaPrev;
+    g.getXrayMatProp(x, y, z1, delta, beta);
+    g.getXrayMatProp(x, y, z0, deltaPrev, betaPrev);
+    if ((std::abs(delta - deltaPrev) > ZERO) || (std::abs(beta - betaPrev) > ZERO)) {
+      double deltaTemp = 0.0, betaTemp = 0.0;
+      g.getXrayMatProp(x, y, z0, delta, beta);
+      g.getXrayMatProp(x, y, z1, deltaTemp, betaTemp);
+      delta += deltaTemp;
+      beta += betaTemp;
+      const double dz = (z1 - z0) / nSteps;
+      for (unsigned i = 1; i < nSteps - 1; ++i) {
+        g.getXrayMatProp(x, y, z0 + i * dz, deltaTemp, betaTemp);
+        delta += 2.0 * deltaTemp;
+        beta += 2.0 * betaTemp;
+      }
+      delta /= (2.0 * nSteps);
+      beta /= (2.0 * nSteps);
+    }
+  }
+
+  /** Steps first .. first+n-1 on the device.  With a user MaterialFunction
+   * the medium is sampled on the host, per block of steps, at the planes
+   * the reference samples -- FFTSolver3D: the refraction material of each
+   * step (refractionMaterial); ADI: getZ(s) for the x half step and
+   * getZ(s) + dz/2 for the y half step (src/alternatingDirectionSolver.cpp:
+   * 21, 91) -- and handed over with pxp_set_material_planes.  Like the
+   * reference's OpenMP loops, this calls the material from several threads
+   * when OpenMP is enabled, so getXrayMatProp must be thread-safe. */
+  void runSteps(unsigned first, unsigned n) {
+    if (!materialPlanes) {
+      check(pxp_step(handle, (int)n));
+      return;
+    }
+    const ParaxialSimulation &g = *guide;
+    const long long npts = (long long)Nx * Ny;
+    const unsigned per = kind == PXP_ADI ? 2 : 1;
+    const double dz = g.longitudinalDiscretization().step;
+    // blocks of up to about 256 MB of planes
+    const unsigned cap = (unsigned)std::max<long long>(1, (256ll << 20) / (16 * per * npts));
+    for (unsigned s0 = first; s0 < first + n;) {
+      const unsigned cnt = std::min(cap, first + n - s0);
+      std::vector<double> d((size_t)cnt * per * npts), b(d.size());
+      for (unsigned k = 0; k < cnt; ++k) {
+        const unsigned s = s0 + k;
+        for (unsigned pl = 0; pl < per; ++pl) {
+          double *dp = d.data() + ((size_t)k * per + pl) * npts;
+          double *bp = b.data() + ((size_t)k * per + pl) * npts;
+#ifdef _OPENMP
+#pragma omp parallel for
+#endif
+          for (long long i = 0; i < npts; ++i) {
+            const unsigned col = (unsigned)(i / Ny), row = (unsigned)(i % Ny);
+            const double x = g.getX((int)col), y = g.getY((int)row);
+            if (kind == PXP_FFT_SOLVER_3D)
+              refractionMaterial(g, x, y, g.getZ(s - 1), g.getZ(s), dp[i], bp[i]);
+            else
+              g.getXrayMatProp(x, y, pl == 0 ? g.getZ(s) : g.getZ(s) + dz / 2.0, dp[i], bp[i]);
+          }
+        }
+      }
+      check(pxp_set_material_planes(handle, d.data(), b.data(), (int)s0, (int)cnt));
+      check(pxp_step(handle, (int)cnt));
+      s0 += cnt;
+    }
+  }
 
   /** src/solver3D.cpp:78-125: block average into the saved slice. */
   void storeSlice(unsigned currZ) {
@@ -939,6 +1016,7 @@ class Solver3D : public Solver {
       p.absorber_damping = absorberDamping;
       p.save_every = (int)g.longitudinalDiscretization().downsamplingRatio;
       check(pxp_solver_create(&p, &handle));
+      materialPlanes = false;
       if (g.material != nullptr) {
         const SphereMaterial *sm = dynamic_cast<const SphereMaterial *>(g.material);
         const CSGMaterial *cm = dynamic_cast<const CSGMaterial *>(g.material);
@@ -948,9 +1026,16 @@ class Solver3D : public Solver {
           check(pxp_set_material_spheres(handle, sp.data(), (int)sp.size()));
         } else if (cm != nullptr) {
           if (!cm->isReferenceRun) setCsg(*cm);
+        } else if (g.material->zInvariant()) {
+          // any z: the table serves every step and both half steps
+          std::vector<double> d((size_t)Nx * Ny), b(d.size());
+          for (unsigned col = 0; col < Nx; ++col)
+            for (unsigned row = 0; row < Ny; ++row)
+              g.getXrayMatProp(g.getX((int)col), g.getY((int)row), g.getZ(1),
+                               d[(size_t)col * Ny + row], b[(size_t)col * Ny + row]);
+          check(pxp_set_material_table(handle, d.data(), b.data(), d.size()));
         } else {
-          throw std::runtime_error(
-              "the CUDA 3-D solvers take a SphereMaterial, a CSGMaterial or no material");
+          materialPlanes = true;  // sampled per step (runSteps)
         }
       }
     }
@@ -1283,9 +1368,11 @@ class CurvedWaveGuideFD : public WaveGuideFDSimulation {
 /** GenericScattering (include/genericScattering.hpp, src/genericScattering.cpp):
  * a Gaussian beam through a 3-D object, first in vacuum with three steps
  * (the reference run whose exit field the far field subtracts), then through
- * the material.  The material is a SphereMaterial or a CSGMaterial (evaluated
- * on the device); real-time visualisation, image export and the projection
- * solver are not provided. */
+ * the material.  Any MaterialFunction works: a SphereMaterial or a
+ * CSGMaterial is evaluated on the device, other materials are sampled on the
+ * host at the planes the reference samples (Solver3D::runSteps);
+ * real-time visualisation, image export and the projection solver are not
+ * provided. */
 class GenericScattering : public ParaxialSimulation {
  public:
   enum class SolverType_t { ADI, FFT, PROJ };

@@ -104,12 +104,22 @@ int pxp_solver_destroy(pxp_solver s);
  * column-major for the 3-D kinds (n = Nx*Ny). */
 int pxp_set_material_table(pxp_solver s, const double *delta, const double *beta, size_t n);
 
-/* Material hook, sampled per step for z-varying 2-D media: for each step
- * s = first_step .. first_step+nsteps-1, plane (s - first_step) holds
- * delta/beta at the step's sampling plane(s): FFTSolver2D uses
- * z = getZ(s) + dz/2 (src/fftSolver2D.cpp:38); CrankNicholson uses z and
- * z - dz (src/crancNicholson.cpp:37-38), passed as two planes per step
- * (z first).  Layout [plane][x]. */
+/* Material hook, sampled per step for z-varying media (any MaterialFunction
+ * the host evaluates): for each step s = first_step .. first_step+nsteps-1
+ * the planes of that step, in step order:
+ *   FFTSolver2D: delta/beta at z = getZ(s) + dz/2 (src/fftSolver2D.cpp:38);
+ *   CrankNicholson: at z and z - dz (src/crancNicholson.cpp:37-38), two
+ *     planes per step (z first);
+ *   FFTSolver3D: the delta/beta FFTSolver3D::refraction applies at each
+ *     point (src/fftSolver3D.cpp:122-156): the values at z1 = getZ(s), or,
+ *     where they differ from those at z0 = getZ(s-1) by more than 1e-10, the
+ *     refractionIntegral of the two (:253-273); one plane per step;
+ *   ADI: at getZ(s) (x half step, src/alternatingDirectionSolver.cpp:21) and
+ *     getZ(s) + dz/2 (y half step, :91), two planes per step.
+ * Layout [plane][point]: x for the 2-D kinds; x index * Ny + y index (the
+ * field's column-major layout) for the 3-D kinds.  The planes replace a
+ * table, sphere or CSG material; stepping outside first_step ..
+ * first_step+nsteps-1 then fails with PXP_ERR_INVALID. */
 int pxp_set_material_planes(pxp_solver s, const double *delta, const double *beta,
                             int first_step, int nsteps);
 

@@ -341,6 +341,36 @@ void save_field(const cd *field, long n, int step, int save_every,
 
 }  // namespace
 
+// The (delta, beta) FFTSolver3D::refraction applies at (x, y) for the step
+// from z0 to z1 (src/fftSolver3D.cpp:122-156): the material at z1, or, where
+// it differs from the material at z0 by more than 1e-10, refractionIntegral
+// (:253-273): endpoints once, the interior samples i = 1..8 of 10 twice (the
+// ninth is skipped), divided by 2*10.
+void fft3d_point_material(const orc_material *m, const orc_grid &g, double x, double y, double z0,
+                          double z1, double &delta, double &beta) {
+  const double ZERO = 1E-10;
+  const unsigned nStepsInRefrIntegral = 10;
+  double deltaPrev, betaPrev;
+  material_eval(m, g, x, y, z1, delta, beta);
+  material_eval(m, g, x, y, z0, deltaPrev, betaPrev);
+  if ((std::abs(delta - deltaPrev) > ZERO) || (std::abs(beta - betaPrev) > ZERO)) {
+    double deltaTemp = 0.0, betaTemp = 0.0;
+    material_eval(m, g, x, y, z0, delta, beta);
+    material_eval(m, g, x, y, z1, deltaTemp, betaTemp);
+    delta += deltaTemp;
+    beta += betaTemp;
+    double dzz = (z1 - z0) / nStepsInRefrIntegral;
+    for (unsigned i = 1; i < nStepsInRefrIntegral - 1; ++i) {
+      double zz = z0 + i * dzz;
+      material_eval(m, g, x, y, zz, deltaTemp, betaTemp);
+      delta += 2.0 * deltaTemp;
+      beta += 2.0 * betaTemp;
+    }
+    delta /= (2.0 * nStepsInRefrIntegral);
+    beta /= (2.0 * nStepsInRefrIntegral);
+  }
+}
+
 // ================================================================= API ==
 extern "C" {
 
@@ -351,6 +381,32 @@ unsigned orc_node_count(double mn, double mx, double step) {
 void orc_set_threads(int n) { g_threads = n; }
 void orc_set_fft_parallel(int on) { g_fft_parallel = on; }
 int orc_get_threads(void) { return nthreads(); }
+
+int orc_material_planes(const orc_grid *gp, const orc_material *m, int kind, int first_step,
+                        int nsteps, double *delta, double *beta) {
+  const orc_grid &g = *gp;
+  const unsigned n = node_count(g.xmin, g.xmax, g.dx);
+  const long npts = (long)n * n;
+  const int per = kind == 4 ? 2 : 1;
+  if ((kind != 3 && kind != 4) || nsteps < 0 || first_step < 1) return -1;
+  const int th = nthreads();
+  for (int k = 0; k < nsteps; ++k) {
+    const unsigned step = (unsigned)(first_step + k);
+    for (int pl = 0; pl < per; ++pl) {
+      double *d = delta + ((long)k * per + pl) * npts, *b = beta + ((long)k * per + pl) * npts;
+#pragma omp parallel for num_threads(th)
+      for (long i = 0; i < npts; ++i) {
+        const unsigned col = (unsigned)(i / n), row = (unsigned)(i % n);
+        const double x = get_x(g, (int)col), y = get_y(g, (int)row);
+        if (kind == 3)
+          fft3d_point_material(m, g, x, y, get_z(g, step - 1), get_z(g, step), d[i], b[i]);
+        else
+          material_eval(m, g, x, y, get_z(g, step) + (pl ? g.dz / 2.0 : 0.0), d[i], b[i]);
+      }
+    }
+  }
+  return 0;
+}
 
 int orc_fft1d(double *data, int n, int sign) {
   if (n < 1) return -1;
@@ -502,8 +558,6 @@ int orc_fft3d_run(const orc_grid *gp, const orc_material *m,
   const unsigned n_rows = Ny, n_cols = Nx;
   const double stepX = g.dx, stepY = g.dy, dz = g.dz, k = g.wavenumber;
   const cd im(0.0, 1.0);
-  const double ZERO = 1E-10;
-  const unsigned nStepsInRefrIntegral = 10;
   // Absorber set-up (FFTSolver3D::absorbingBC, src/fftSolver3D.cpp:327-349)
   unsigned thickX = 0, thickY = 0;
   double invDampX = 0.0, invDampY = 0.0;
@@ -518,25 +572,6 @@ int orc_fft3d_run(const orc_grid *gp, const orc_material *m,
   for (unsigned c = 0; c < n_cols; ++c) kxs[c] = spatial_freq(c, n_cols, stepX);
   for (unsigned r = 0; r < n_rows; ++r) kys[r] = spatial_freq(r, n_rows, stepY);
   const int th = nthreads();
-
-  auto refr_integral = [&](double x, double y, double z1, double z2,
-                           double &delta, double &beta) {
-    double deltaTemp = 0.0, betaTemp = 0.0;
-    material_eval(m, g, x, y, z1, delta, beta);
-    material_eval(m, g, x, y, z2, deltaTemp, betaTemp);
-    delta += deltaTemp;
-    beta += betaTemp;
-    double zz = z1;
-    double dzz = (z2 - z1) / nStepsInRefrIntegral;
-    for (unsigned i = 1; i < nStepsInRefrIntegral - 1; ++i) {
-      zz = z1 + i * dzz;
-      material_eval(m, g, x, y, zz, deltaTemp, betaTemp);
-      delta += 2.0 * deltaTemp;
-      beta += 2.0 * betaTemp;
-    }
-    delta /= (2.0 * nStepsInRefrIntegral);
-    beta /= (2.0 * nStepsInRefrIntegral);
-  };
 
   for (int step = 1; step <= nsteps; ++step) {
     curr = prev;
@@ -554,11 +589,8 @@ int orc_fft3d_run(const orc_grid *gp, const orc_material *m,
     for (long i = 0; i < npts; ++i) {
       unsigned row = i % n_rows, col = i / n_rows;
       double x = get_x(g, (int)col), y = get_y(g, (int)row);
-      double delta, beta, deltaPrev, betaPrev;
-      material_eval(m, g, x, y, z1, delta, beta);
-      material_eval(m, g, x, y, z0, deltaPrev, betaPrev);
-      if ((std::abs(delta - deltaPrev) > ZERO) || (std::abs(beta - betaPrev) > ZERO))
-        refr_integral(x, y, z0, z1, delta, beta);
+      double delta, beta;
+      fft3d_point_material(m, g, x, y, z0, z1, delta, beta);
       curr[i] = prev[i] * std::exp(-k * (beta + im * delta) * dz) / normalization;
     }
     // absorbY on every column (rows 0..t-1 and their mirrors), then absorbX on

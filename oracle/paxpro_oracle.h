@@ -110,6 +110,15 @@ int orc_cn2d_run(const orc_grid *g, const orc_material *m, int transparent_bc,
                  const double *u0, int nsteps, int save_every, double *saves,
                  double *u_out);
 
+/* The per-step material planes the reference samples, as the C ABI's
+ * pxp_set_material_planes takes them for the 3-D kinds: kind 3
+ * (FFTSolver3D): one plane per step, the (delta, beta) refraction applies
+ * (refraction integral included); kind 4 (ADI): two planes per step, at
+ * getZ(step) and getZ(step) + dz/2.  Steps first_step .. +nsteps-1; each
+ * plane Nx*Ny doubles in the field's column-major layout. */
+int orc_material_planes(const orc_grid *g, const orc_material *m, int kind, int first_step,
+                        int nsteps, double *delta, double *beta);
+
 int orc_fft3d_run(const orc_grid *g, const orc_material *m,
                   double absorber_width, double absorber_damping,
                   const double *u0, int nsteps, int save_every, double *saves,

@@ -89,6 +89,8 @@ def lib():
         _LIB.orc_material_eval.argtypes = [C.POINTER(Material), C.POINTER(Grid)] + \
             [C.c_double] * 3 + [d, d]
         _LIB.orc_set_threads.argtypes = [C.c_int]
+        _LIB.orc_material_planes.argtypes = [C.POINTER(Grid), C.POINTER(Material), C.c_int,
+                                             C.c_int, C.c_int, d, d]
         _LIB.orc_set_fft_parallel.argtypes = [C.c_int]
     return _LIB
 
@@ -369,6 +371,22 @@ def block_average(field, ratio: int):
     lib().orc_block_average(f.ctypes.data_as(C.POINTER(C.c_double)), n, m,
                             out.ctypes.data_as(C.POINTER(C.c_double)))
     return out
+
+
+def material_planes(g, spec, kind, first_step, nsteps):
+    """The per-step planes the reference samples for a 3-D kind (3 =
+    FFTSolver3D: the refraction material of each step; 4 = ADI: the x and y
+    half-step planes), as pxp_set_material_planes takes them: (delta, beta),
+    each of shape (nplanes, Nx*Ny) in the field's column-major layout."""
+    n = node_count(g.xmin, g.xmax, g.dx)
+    per = 2 if kind == 4 else 1
+    d = np.zeros((nsteps * per, n * n))
+    b = np.zeros_like(d)
+    rc = lib().orc_material_planes(C.byref(g), C.byref(spec.m), int(kind), int(first_step),
+                                   int(nsteps), _p(d), _p(b))
+    if rc:
+        raise ValueError(f"oracle rejected the planes (rc={rc})")
+    return d, b
 
 
 def set_threads(n: int) -> None:

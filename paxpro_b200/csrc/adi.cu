@@ -35,8 +35,15 @@ namespace pxp {
 // kernel waits that ran out on this device (never reset), read by the host
 __device__ unsigned int g_wait_timeouts = 0;
 
+// The material of the half step's plane at (x, y); idx: the point's index in
+// the field's layout, for a sampled plane.
 __device__ __forceinline__ void sphere_material(const AdiHalf &h, double x, double y,
-                                                double &delta, double &beta) {
+                                                long long idx, double &delta, double &beta) {
+  if (h.plane_delta) {
+    delta = h.plane_delta[idx];
+    beta = h.plane_beta[idx];
+    return;
+  }
   if (h.csg.active) {
     csg_material(h.csg, x, y, h.z, delta, beta);
     return;
@@ -148,7 +155,8 @@ __global__ void __launch_bounds__(512) adi_half_kernel(const AdiHalf h) {
       y = __dadd_rn(h.ymin, __dmul_rn(pos_c, h.dy));
     }
     double delta, beta;
-    sphere_material(h, x, y, delta, beta);
+    sphere_material(h, x, y,
+                    h.y_implicit ? (long long)s * h.n + p : (long long)p * h.n + s, delta, beta);
     if (!h.y_implicit) {
       // 1.0/dz + i/(k dx dx) + beta*k + i*delta*k   (reference :38)
       dg[m] = mk(__dadd_rn(h.inv_dzh, __dmul_rn(beta, h.k)),

@@ -96,6 +96,12 @@ struct pxp_solver_s {
   // host copies
   std::vector<double> h_delta, h_beta;
   int plane_first = 1, plane_count = 0;  // per-step material planes (0 = z-invariant)
+  // 3-D kinds: sampled material planes for steps plane_first .. +plane_count-1,
+  // planes3_per a step (FFTSolver3D 1, ADI 2): [delta planes | beta planes]
+  double *d_planes3 = nullptr;
+  size_t planes3_cap = 0;  // doubles allocated
+  int planes3_per = 0;
+  bool planes3_invariant = false;  // one plane (a z-invariant table) for every step
   bool material_set = false;
   bool ic_set = false;
   unsigned current_step = 1;
@@ -645,6 +651,24 @@ pxp::Csg csg_params(const pxp_solver_s *h, double zlo, double zhi) {
   return c;
 }
 
+// Device planes of a 3-D kind for step `step`, plane `which` (ADI: 0 = x half
+// step, 1 = y half step): delta and beta, or null when no planes are set.
+void planes3_at(const pxp_solver_s *h, unsigned step, int which, const double **delta,
+                const double **beta) {
+  *delta = *beta = nullptr;
+  if (h->d_planes3 == nullptr) return;
+  if (h->planes3_invariant) {
+    *delta = h->d_planes3;
+    *beta = h->d_planes3 + h->npts;
+    return;
+  }
+  if (h->plane_count <= 0) return;
+  const long long nplanes = (long long)h->plane_count * h->planes3_per;
+  const long long p = ((long long)step - h->plane_first) * h->planes3_per + which;
+  *delta = h->d_planes3 + p * h->npts;
+  *beta = h->d_planes3 + (nplanes + p) * h->npts;
+}
+
 int adi_fill_spheres(pxp_solver_s *h, pxp::AdiHalf &a, double z) {
   a.csg = csg_params(h, z, z);
   std::vector<pxp::Sphere> act;
@@ -689,8 +713,9 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   a.kd2_expl = kdy2;
   a.z = get_z(h, step);
   adi_fill_spheres(h, a, a.z);
+  planes3_at(h, step, 0, &a.plane_delta, &a.plane_beta);
   const cd *lu = (const cd *)h->d_lu;
-  cudaError_t e = (a.nspheres == 0 && !a.csg.active && !a.use_tbc && lu)
+  cudaError_t e = (a.nspheres == 0 && !a.csg.active && !a.plane_delta && !a.use_tbc && lu)
                       ? pxp::launch_adi_half_const(h->prec, a, lu, lu + n, lu + 4 * n, h->stream)
                       : pxp::launch_adi_half(h->prec, a, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "ADI x half step");
@@ -706,7 +731,8 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   a.kd2_expl = kdx2;
   a.z = get_z(h, step) + dzh;
   adi_fill_spheres(h, a, a.z);
-  e = (a.nspheres == 0 && !a.csg.active && !a.use_tbc && lu)
+  planes3_at(h, step, 1, &a.plane_delta, &a.plane_beta);
+  e = (a.nspheres == 0 && !a.csg.active && !a.plane_delta && !a.use_tbc && lu)
           ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n, lu + 8 * n, h->stream)
           : pxp::launch_adi_half(h->prec, a, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
@@ -717,7 +743,9 @@ int adi_step(pxp_solver_s *h, unsigned step) {
 // Both halves of the step on the vacuum kernel and no save: the step's
 // launches are then the same as any other such step's.
 bool adi_plain_step(const pxp_solver_s *h, unsigned step, std::vector<pxp::Sphere> &tmp) {
-  if (h->prob.transparent_bc || !h->d_lu || save_at(h, step)) return false;
+  if (h->prob.transparent_bc || !h->d_lu || save_at(h, step) || h->plane_count > 0 ||
+      h->planes3_invariant)
+    return false;
   const double z = get_z(h, step);
   if (csg_active(h, z, z + h->prob.z.step / 2.0)) return false;
   active_spheres(h, z, tmp);
@@ -888,6 +916,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     q.z0 = get_z(h, step - 1);
     slab_spheres(h, q.z0, q.z1, act);
     q.csg = csg_params(h, q.z0, q.z1);
+    planes3_at(h, step, 0, &q.plane_delta, &q.plane_beta);
     q.nspheres = (int)act.size();
     if (q.nspheres <= pxp::kInlineSpheres) {
       for (int j = 0; j < q.nspheres; ++j) q.spheres[j] = act[j];
@@ -909,7 +938,8 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   // planes are read only for spheres)
   auto plain = [&](int i) {
     const unsigned step = first + (unsigned)i;
-    if (i == nsteps - 1 || save_at(h, step)) return false;
+    if (i == nsteps - 1 || save_at(h, step) || h->plane_count > 0 || h->planes3_invariant)
+      return false;
     slab_spheres(h, get_z(h, step - 1), get_z(h, step), act);
     return act.empty() && !csg_active(h, std::min(get_z(h, step - 1), get_z(h, step)),
                                       std::max(get_z(h, step - 1), get_z(h, step)));
@@ -1136,6 +1166,7 @@ int pxp_solver_destroy(pxp_solver h) {
   free_dev(h->d_trans, h->stream);
   h->d_tw = nullptr;  // shared table, not owned
   free_dev(h->d_mat, h->stream);
+  free_dev(h->d_planes3, h->stream);
   free_dev(h->d_job, h->stream);
   free_dev(h->d_field2, h->stream);
   free_dev(h->d_spheres, h->stream);
@@ -1157,6 +1188,34 @@ static int rewrite_job(pxp_solver_s *h) {
   }
 }
 
+// Copy nplanes sampled planes of a 3-D kind to the device ([delta planes |
+// beta planes]); the planes replace a sphere or CSG material.
+static int store_planes3(pxp_solver_s *h, const double *delta, const double *beta, size_t nplanes) {
+  const size_t need = 2 * nplanes * (size_t)h->npts;
+  if (need > h->planes3_cap) {
+    free_dev(h->d_planes3, h->stream);
+    h->dev_bytes -= sizeof(double) * h->planes3_cap;
+    h->planes3_cap = 0;
+    if (int rc = alloc(h, (void **)&h->d_planes3, sizeof(double) * need, "3-D material planes"))
+      return rc;
+    h->planes3_cap = need;
+  }
+  const size_t half = nplanes * (size_t)h->npts;
+  PXP_TRY_CUDA(h, cudaMemcpyAsync(h->d_planes3, delta, sizeof(double) * half,
+                                  cudaMemcpyHostToDevice, h->stream));
+  PXP_TRY_CUDA(h, cudaMemcpyAsync(h->d_planes3 + half, beta, sizeof(double) * half,
+                                  cudaMemcpyHostToDevice, h->stream));
+  PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->spheres.clear();
+  free_dev(h->d_spheres, h->stream);
+  free_dev(h->d_csg, h->stream);
+  h->csg_nmodules = h->csg_nparts = 0;
+  h->csg_zlo.clear();
+  h->csg_zhi.clear();
+  h->material_set = true;
+  return PXP_OK;
+}
+
 int pxp_set_material_table(pxp_solver h, const double *delta, const double *beta, size_t n) {
   if (h == nullptr || delta == nullptr || beta == nullptr) return PXP_ERR_INVALID;
   if (n != (size_t)h->npts)
@@ -1171,6 +1230,15 @@ int pxp_set_material_table(pxp_solver h, const double *delta, const double *beta
     case PXP_CRANK_NICHOLSON:
       if ((rc = cn_set_planes(h, delta, beta, 1, 1, false))) return rc;
       break;
+    case PXP_FFT_SOLVER_3D:
+    case PXP_ADI:
+      // z-invariant: the sampled plane serves every step and half step
+      // (FFTSolver3D's z0 and z1 values agree, so no refraction integral)
+      if ((rc = store_planes3(h, delta, beta, 1))) return rc;
+      h->planes3_invariant = true;
+      h->planes3_per = 1;
+      h->plane_count = 0;
+      return PXP_OK;
     default:
       return h->fail(PXP_ERR_UNSUPPORTED, "material tables not supported for this kind");
   }
@@ -1194,8 +1262,18 @@ int pxp_set_material_planes(pxp_solver h, const double *delta, const double *bet
     case PXP_CRANK_NICHOLSON:
       if ((rc = cn_set_planes(h, delta, beta, nsteps, first_step, true))) return rc;
       break;
+    case PXP_FFT_SOLVER_3D:
+    case PXP_ADI: {
+      const int per = h->prob.kind == PXP_ADI ? 2 : 1;
+      if ((rc = store_planes3(h, delta, beta, (size_t)nsteps * per))) return rc;
+      h->planes3_per = per;
+      h->planes3_invariant = false;
+      h->plane_first = first_step;
+      h->plane_count = nsteps;
+      return PXP_OK;
+    }
     default:
-      return h->fail(PXP_ERR_UNSUPPORTED, "material planes apply to the 2-D kinds");
+      return h->fail(PXP_ERR_UNSUPPORTED, "material planes not supported for this kind");
   }
   h->plane_first = first_step;
   h->plane_count = nsteps;
@@ -1207,6 +1285,8 @@ int pxp_set_material_spheres(pxp_solver h, const pxp_sphere *spheres, int n) {
   if (h->prob.kind != PXP_ADI && h->prob.kind != PXP_FFT_SOLVER_3D)
     return h->fail(PXP_ERR_UNSUPPORTED, "sphere materials apply to the 3-D kinds");
   PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->plane_count = 0;  // a sphere list replaces sampled planes
+  h->planes3_invariant = false;
   h->spheres.assign(spheres, spheres + n);
   free_dev(h->d_spheres, h->stream);
   free_dev(h->d_csg, h->stream);
@@ -1288,6 +1368,8 @@ int pxp_set_material_csg(pxp_solver h, const pxp_csg_module *modules, int nmodul
         (shapes[k].operation != PXP_CSG_UNION && shapes[k].operation != PXP_CSG_DIFFERENCE))
       return h->fail(PXP_ERR_INVALID, "CSG shape " + std::to_string(k) + ": bad kind or operation");
   PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->plane_count = 0;  // a CSG material replaces sampled planes
+  h->planes3_invariant = false;
   // z range per module: the union of its parts' union shapes' ranges (a
   // difference shape only removes; a point outside every union shape of a
   // module's parts is claimed by none of them)

@@ -82,7 +82,13 @@ __device__ __forceinline__ typename Cx<R>::T refract3(const Fft3dPass &q, typena
   const double x = __dadd_rn(q.xmin, __dmul_rn((double)ix, q.dx));
   const double y = __dadd_rn(q.ymin, __dmul_rn((double)iy, q.dy));
   double delta = 0.0, beta = 0.0;
-  if (q.nspheres > 0 || q.csg.active) step_material(q, x, y, delta, beta);
+  if (q.plane_delta) {
+    const long long idx = (long long)ix * q.n + iy;
+    delta = q.plane_delta[idx];
+    beta = q.plane_beta[idx];
+  } else if (q.nspheres > 0 || q.csg.active) {
+    step_material(q, x, y, delta, beta);
+  }
   double2 u = to_d(uu);
   if (delta != 0.0 || beta != 0.0) {
     // exp(-k*(beta + i*delta)*dz)

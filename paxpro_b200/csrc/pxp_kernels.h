@@ -152,6 +152,10 @@ struct AdiHalf {
   double xmin, dx, ymin, dy;
   double z;                // material plane of this half step
   Csg csg;                 // CSG material (instead of spheres) when csg.active
+  // sampled material of this half step's plane (instead of spheres or CSG)
+  // when plane_delta is set: n*n doubles each, the field's layout (x index *
+  // n + y index)
+  const double *plane_delta, *plane_beta;
   const Sphere *spheres_all;
   Sphere spheres[kInlineSpheres];
 };
@@ -269,6 +273,10 @@ struct Fft3dPass {
   double k, dz, xmin, dx, ymin, dy, z1, z0, norm;
   int nspheres;
   Csg csg;                 // CSG material (instead of spheres) when csg.active
+  // sampled material of this step (instead of spheres or CSG) when
+  // plane_delta is set: the (delta, beta) FFTSolver3D::refraction applies at
+  // each point, n*n doubles each in the field's layout
+  const double *plane_delta, *plane_beta;
   const Sphere *spheres_all;
   Sphere spheres[kInlineSpheres];
   // absorber (FFTSolver3D::absorbingBC): thickness in pixels and inverse

@@ -175,3 +175,38 @@ def test_curved_waveguide_transmittivity(kind, smoothed):
     assert i0 == pytest.approx(I0, rel=1e-12)
     np.testing.assert_allclose(t, np.array(want), rtol=1e-12, atol=0)
     assert 0.0 < t[-1] < 1.0
+
+
+def test_reference_sphere_example_with_a_user_material_function():
+    """The reference's Examples/sphere.cpp through the B200 API: a user
+    MaterialFunction subclass (not a type the device evaluates), sampled on
+    the host at the planes ADI samples, 513 transverse nodes (the padded
+    general kernel), 256 steps, GenericScattering's vacuum reference run and
+    far field.  Exit fields against the oracle with the same sphere (1e-10),
+    the far field against the numpy far field of those fields."""
+    from oracle import farfield as off
+    exe = build("example_sphere")
+    out = os.path.join(OUT, "example_sphere.bin")
+    r = subprocess.run([exe, out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    data = np.fromfile(out, dtype=np.float64)
+    N, rows, cols = int(data[0]), int(data[1]), int(data[2])
+    assert N == 513
+    c = data[3:3 + 4 * N * N].view(np.complex128)
+    ref, ex = (c[k * N * N:(k + 1) * N * N].reshape((N, N), order="F") for k in range(2))
+    ff = data[3 + 4 * N * N:].reshape((rows, cols), order="F")
+    K = 2.0 * math.pi / 0.1569
+    dx = 1500.0 / 512
+    g0 = po.grid(-750.0, 750.0, dx, -525.0, 525.0, 1050.0 / 3.0, K)
+    g1 = po.grid(-750.0, 750.0, dx, -525.0, 525.0, 1050.0 / 256, K)
+    u0 = po.gaussian_beam_3d(g0, 0.1569, 200000.0)
+    ref_o, _ = po.adi3d_run(g0, po.MaterialSpec(), u0, 3, 0, True)
+    sphere = po.MaterialSpec(po.MAT_SPHERES, spheres=[(0.0, 0.0, 0.0, 500.0, 8.9e-6, 7e-7)])
+    ex_o, _ = po.adi3d_run(g1, sphere, u0, 256, 0, True)
+    assert _rel(ref, ref_o) <= TOL
+    assert _rel(ex, ex_o) <= TOL
+    assert np.std(np.abs(ex)) > 1e-3  # the sphere left its mark
+    ff_o = off.farfield_3d(ex, 1024, -0.05, 0.05, K, dx, dx, reference=ref, export_rows=512,
+                           export_cols=512)
+    assert ff.shape == ff_o.shape
+    assert _rel(ff, ff_o) <= TOL
