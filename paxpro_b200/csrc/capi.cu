@@ -260,8 +260,13 @@ struct TableKey {
 std::mutex g_table_mutex;
 std::map<TableKey, void *> g_tables;
 
-int shared_table(pxp_solver_s *h, int kind, void **out) {
-  const unsigned n = h->nx;
+int shared_table_n(pxp_solver_s *h, int kind, unsigned n, void **out);
+
+int shared_table(pxp_solver_s *h, int kind, void **out) { return shared_table_n(h, kind, h->nx, out); }
+
+// The table of the given kind for length n (the grid's own length for the
+// propagator and kx^2 tables).
+int shared_table_n(pxp_solver_s *h, int kind, unsigned n, void **out) {
   TableKey key{h->prob.device, kind, n, (kind == 1 || kind == 2) ? h->prob.x.step : 0.0,
                kind == 1 ? h->prob.z.step : 0.0, kind == 1 ? h->prob.wavenumber : 0.0};
   std::lock_guard<std::mutex> lk(g_table_mutex);
@@ -391,6 +396,11 @@ int fft1d_setup(pxp_solver_s *h) {
     if ((rc = bluestein_table(h, 7, &h->d_chirp))) return rc;
     if ((rc = bluestein_table(h, 8, &h->d_bconv))) return rc;
     if ((rc = bluestein_table(h, 9, &h->d_tw))) return rc;
+  } else if (pxp::fft1d_pair_size(h->prec, (int)h->nx)) {
+    // two CTAs of n/2 points: the n/2-point Stockham twiddles and
+    // exp(-2 pi i k / n) for the split between the halves
+    if ((rc = shared_table_n(h, 0, h->nx / 2, &h->d_tw))) return rc;
+    if ((rc = shared_table_n(h, 4, h->nx, &h->d_chirp))) return rc;
   } else if ((rc = shared_table(h, 0, &h->d_tw))) {
     return rc;
   }
@@ -1081,8 +1091,13 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
   switch (p.kind) {
     case PXP_FFT_SOLVER_2D: supported = pxp::fft1d_supported(h->prec, (int)h->nx); break;
     case PXP_CRANK_NICHOLSON:
-      // a grid that is padded to the kernel's row count takes Dirichlet ends only
-      supported = pxp::cn_supported(h->prec, (int)h->nx) &&
+      // a grid that is padded to the kernel's row count takes Dirichlet ends
+      // only; 8192 and 16384 rows beyond the general kernel's size run the
+      // step-invariant path on a cluster (z-invariant medium, Dirichlet ends:
+      // checked when stepping)
+      supported = (pxp::cn_supported(h->prec, (int)h->nx) ||
+                   (!p.transparent_bc &&
+                    pxp::cn_const_supported(h->prec, pxp::cn_padded_n((int)h->nx)))) &&
                   (!p.transparent_bc || pxp::cn_padded_n((int)h->nx) == (int)h->nx);
       break;
     case PXP_ADI:
@@ -1492,6 +1507,11 @@ int pxp_step(pxp_solver h, int nsteps) {
                             (int)first, nsteps, h->stream, h->flux_count > 0);
       break;
     case PXP_CRANK_NICHOLSON:
+      if (!(h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0) &&
+          !pxp::cn_supported(h->prec, (int)h->nx))
+        return h->fail(PXP_ERR_UNSUPPORTED,
+                       "CrankNicholson at " + std::to_string(h->nx) +
+                           " points runs with a z-invariant medium and Dirichlet ends only");
       if (h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0)
         e = pxp::launch_cn_const(h->prec, (const pxp::CnJob *)h->d_job, 1,
                                  pxp::cn_padded_n((int)h->nx), (int)first, nsteps, h->stream,
@@ -2145,6 +2165,10 @@ int pxp_batch_admit(pxp_batch b, pxp_solver h, int nsteps) {
       (h->current_step < (unsigned)h->plane_first ||
        (long long)h->current_step + nsteps > (long long)h->plane_first + h->plane_count))
     return b->fail(PXP_ERR_INVALID, "steps outside the material planes provided");
+  if (h->prob.kind == PXP_CRANK_NICHOLSON && !cn_uses_const(h) &&
+      !pxp::cn_supported(h->prec, (int)h->nx))
+    return b->fail(PXP_ERR_UNSUPPORTED, "CrankNicholson at this size needs a z-invariant medium "
+                                        "and Dirichlet ends");
   if (b->used + h->dev_bytes > b->budget) return PXP_ERR_NOT_READY;
   cudaSetDevice(b->device);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess)

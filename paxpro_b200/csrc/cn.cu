@@ -23,8 +23,12 @@
 #include "pxp_complex.cuh"
 #include "flux.cuh"
 #include "pxp_kernels.h"
+#include <cooperative_groups.h>
+
 #include "scan_solve.cuh"
 #include "tridiag.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace pxp {
 
@@ -274,6 +278,175 @@ __global__ void __launch_bounds__(T) cn_const_kernel(const CnJob *__restrict__ j
     if (s0 + m < nreal) field[s0 + m] = from_d<R>(u[m]);
 }
 
+// The same step for systems of K * M * T rows (8192 and 16384) on a cluster
+// of K CTAs, one per SM, CTA k holding rows [k*M*T, (k+1)*M*T) with its
+// slice of the factor tables in shared memory.  What crosses CTAs goes
+// through distributed shared memory, each behind one cluster barrier:
+//   * the stencil halo: the first and last rows of the neighbouring CTAs;
+//   * the forward recurrence's carry: each CTA scans its chunks as in the
+//     single-CTA kernel, publishes its total transfer (y_end = a y_start +
+//     b), and folds the totals of the CTAs before it to get its y_start;
+//   * the backward recurrence's carry, likewise from the CTAs after it.
+// Every chunk's carry-in is then ex.a * start + ex.b (ex: the in-CTA
+// exclusive scan), the single-CTA fix-up with a nonzero CTA start.
+template <int M, int P>
+__device__ __forceinline__ void const_solve_cluster(double2 (&r)[M], const double2 *__restrict__ g,
+                                                    const double2 *__restrict__ h, int c,
+                                                    Affine *scratch, Affine *tot_fwd,
+                                                    Affine *tot_bwd, cg::cluster_group &cluster,
+                                                    int rank, int K) {
+  double2 pr[M];
+  double2 y = cmul(g[cslot<M, P>(c, 0)], r[0]);
+  pr[0] = h[cslot<M, P>(c, 0)];
+  r[0] = y;
+#pragma unroll
+  for (int m = 1; m < M; ++m) {
+    const int k = cslot<M, P>(c, m);
+    const double2 hm = h[k];
+    y = cfma(hm, y, cmul(g[k], r[m]));
+    pr[m] = cmul(hm, pr[m - 1]);
+    r[m] = y;
+  }
+  const Affine own_f{pr[M - 1], y};
+  Affine ex = exclusive_scan<P, false>(own_f, scratch);
+  if (c == P - 1) *tot_fwd = compose(ex, own_f);  // this CTA's total transfer
+  cluster.sync();
+  double2 start = mk(0.0, 0.0);  // y at the end of the previous CTA's rows
+  for (int j = 0; j < rank; ++j) {
+    const Affine t = *cluster.map_shared_rank(tot_fwd, j);
+    start = cfma(t.a, start, t.b);
+  }
+  const double2 y_in = cfma(ex.a, start, ex.b);
+#pragma unroll
+  for (int m = 0; m < M; ++m) r[m] = cfma(pr[m], y_in, r[m]);
+  double2 x = r[M - 1];
+  pr[M - 1] = h[cslot<M, P>(c, M - 1)];
+#pragma unroll
+  for (int m = M - 2; m >= 0; --m) {
+    const double2 hm = h[cslot<M, P>(c, m)];
+    x = cfma(hm, x, r[m]);
+    pr[m] = cmul(hm, pr[m + 1]);
+    r[m] = x;
+  }
+  const Affine own_b{pr[0], x};
+  ex = exclusive_scan<P, true>(own_b, scratch);
+  if (c == 0) *tot_bwd = compose(ex, own_b);
+  cluster.sync();
+  start = mk(0.0, 0.0);  // x at the first row of the next CTA
+  for (int j = K - 1; j > rank; --j) {
+    const Affine t = *cluster.map_shared_rank(tot_bwd, j);
+    start = cfma(t.a, start, t.b);
+  }
+  const double2 x_in = cfma(ex.a, start, ex.b);
+#pragma unroll
+  for (int m = 0; m < M; ++m) r[m] = cfma(pr[m], x_in, r[m]);
+}
+
+template <typename R, int M, int T, int K, bool FLUX>
+__global__ void __launch_bounds__(T) cn_const_cluster_kernel(const CnJob *__restrict__ jobs,
+                                                            int step0_ov, int nsteps_ov) {
+  using C = typename Cx<R>::T;
+  constexpr int NC = M * T;  // rows of this CTA
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *gs = reinterpret_cast<double2 *>(smem_raw);
+  double2 *hs = gs + NC;
+  double2 *ds = hs + NC;
+  double2 *xch = ds + NC;  // 2 per thread
+  Affine *scratch = reinterpret_cast<Affine *>(xch + 2 * T);
+  __shared__ Affine tot_fwd, tot_bwd;
+  __shared__ double flux_red[2][flux_slots<T>()];
+  __shared__ double flux_part[K];
+  CnJob job = jobs[blockIdx.x / K];
+  if (nsteps_ov >= 0) {
+    job.step0 = step0_ov;
+    job.nsteps = nsteps_ov;
+  }
+  const int t = threadIdx.x;
+  const double rho = job.rho, r = job.r;
+  const double2 *gt = reinterpret_cast<const double2 *>(job.lu_g);
+  const double2 *ht = reinterpret_cast<const double2 *>(job.lu_h);
+  const double q = __dmul_rn(0.25, rho);
+  const int base = rank * NC;     // first row of this CTA
+  const int s0 = base + t * M;    // first row of this thread
+  const int nreal = job.n_real > 0 ? job.n_real : K * NC;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int k = cslot<M, T>(t, m);
+    gs[k] = gt[s0 + m];
+    hs[k] = ht[s0 + m];
+    if (s0 + m < nreal) {
+      const double bp = job.beta_prev[s0 + m], dp = job.delta_prev[s0 + m];
+      const double2 hh = mk(__dmul_rn(0.5, __dmul_rn(bp, r)), __dmul_rn(0.5, __dmul_rn(dp, r)));
+      ds[k] = mk(__dadd_rn(-hh.x, 1.0), __dsub_rn(-hh.y, 0.5 * rho));
+    } else {
+      ds[k] = mk(0.0, 0.0);
+    }
+  }
+  C *field = reinterpret_cast<C *>(job.field);
+  double2 u[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) u[m] = s0 + m < nreal ? to_d(field[s0 + m]) : mk(0.0, 0.0);
+  C *saves = reinterpret_cast<C *>(job.saves);
+  const double2 *xch_prev = rank > 0 ? cluster.map_shared_rank(xch, rank - 1) : nullptr;
+  const double2 *xch_next = rank < K - 1 ? cluster.map_shared_rank(xch, rank + 1) : nullptr;
+  for (int st = 0; st < job.nsteps; ++st) {
+    const int step = job.step0 + st;
+    int2 fw;
+    const bool flux = FLUX && flux_window(job.flux, step, fw);
+    xch[2 * t] = u[0];
+    xch[2 * t + 1] = u[M - 1];
+    cluster.sync();  // every CTA's edge rows are published
+    double2 lft = mk(0.0, 0.0), rgt = mk(0.0, 0.0);
+    if (t > 0) lft = xch[2 * t - 1];
+    else if (rank > 0) lft = xch_prev[2 * T - 1];
+    if (t < T - 1) rgt = xch[2 * t + 2];
+    else if (rank < K - 1) rgt = xch_next[0];
+    double2 rh[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const double2 left = m > 0 ? u[m - 1] : lft;
+      const double2 right = s0 + m + 1 >= nreal ? mk(0.0, 0.0) : (m < M - 1 ? u[m + 1] : rgt);
+      const double2 sum = cadd(left, right);
+      rh[m] = s0 + m < nreal ? cfma(ds[cslot<M, T>(t, m)], u[m], mk(-q * sum.y, q * sum.x))
+                             : mk(0.0, 0.0);
+    }
+    const_solve_cluster<M, T>(rh, gs, hs, t, scratch, &tot_fwd, &tot_bwd, cluster, rank, K);
+    const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
+                      (step / job.save_every - 1) < job.max_slots;
+    C *slot = save ? saves + (long long)(step / job.save_every - 1) * nreal : nullptr;
+    double acc = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const C v = from_d<R>(rh[m]);
+      u[m] = to_d(v);
+      if (save && s0 + m < nreal) slot[s0 + m] = v;
+      if (flux) flux_add(acc, s0 + m, fw, u[m]);
+    }
+    if constexpr (FLUX) {
+      if (flux) flux_warp_total<T>(acc, flux_red[st & 1]);
+      __syncthreads();
+      if (flux && t < 32) {
+        double v = t < flux_slots<T>() ? flux_red[st & 1][t] : 0.0;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+        if (t == 0) *cluster.map_shared_rank(&flux_part[rank], 0) = v;
+      }
+      cluster.sync();  // every CTA's total is in CTA 0's flux_part
+      if (flux && rank == 0 && t == 0) {
+        double v = 0.0;
+        for (int j = 0; j < K; ++j) v += flux_part[j];
+        job.flux.out[step - job.flux.step0] = v;
+      }
+    }
+  }
+  cluster.sync();  // no CTA leaves while a peer may still address its shared memory
+#pragma unroll
+  for (int m = 0; m < M; ++m)
+    if (s0 + m < nreal) field[s0 + m] = from_d<R>(u[m]);
+}
+
 static constexpr int kCnM = 8;
 
 template <typename R, int M, int T, bool FLUX>
@@ -297,11 +470,51 @@ static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int
               : cn_const_launch_f<R, M, T, false>(d_jobs, nj, step0, nsteps, s);
 }
 
-bool cn_const_supported(Precision, int n) { return n >= 8 * kCnM && !(n & (n - 1)) && n <= 4096; }
+template <typename R, int K, bool FLUX>
+static cudaError_t cn_cluster_launch_f(const CnJob *d_jobs, int nj, int step0, int nsteps,
+                                       cudaStream_t s) {
+  constexpr int M = 16, T = 256, NC = M * T;
+  constexpr size_t smem = sizeof(double2) * (3 * NC + 2 * T) + sizeof(Affine) * (T / 32 + 1);
+  auto k = cn_const_cluster_kernel<R, M, T, K, FLUX>;
+  {
+    const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)smem);
+    if (attr != cudaSuccess) return attr;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(K * nj);
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = K;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, d_jobs, step0, nsteps);
+}
+
+template <typename R, int K>
+static cudaError_t cn_cluster_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
+                                       cudaStream_t s, bool flux) {
+  return flux ? cn_cluster_launch_f<R, K, true>(d_jobs, nj, step0, nsteps, s)
+              : cn_cluster_launch_f<R, K, false>(d_jobs, nj, step0, nsteps, s);
+}
+
+bool cn_const_supported(Precision, int n) {
+  return n >= 8 * kCnM && !(n & (n - 1)) && n <= 16384;  // 8192, 16384: clusters of 2, 4
+}
 
 cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0, int nsteps,
                             cudaStream_t s, bool flux) {
   if (nj <= 0) return cudaSuccess;
+  if (n == 8192)
+    return p == kFP64 ? cn_cluster_launch_t<double, 2>(d_jobs, nj, step0, nsteps, s, flux)
+                      : cn_cluster_launch_t<float, 2>(d_jobs, nj, step0, nsteps, s, flux);
+  if (n == 16384)
+    return p == kFP64 ? cn_cluster_launch_t<double, 4>(d_jobs, nj, step0, nsteps, s, flux)
+                      : cn_cluster_launch_t<float, 4>(d_jobs, nj, step0, nsteps, s, flux);
   // n >= 2048: 16 rows per thread (half the threads of 8 rows: fewer warps
   // in each scan's barriers and shuffles; measured 4.07 -> 3.08 us per step
   // at n = 4096)

@@ -214,7 +214,7 @@ int fft1d_bluestein_m(int n) {
 bool fft1d_supported(Precision p, int n) {
   if (n < 8) return false;
   if (n & (n - 1)) return fft1d_bluestein_m(n) <= (p == kFP64 ? 8192 : 16384);
-  return p == kFP64 ? n <= 8192 : n <= 16384;
+  return n <= 16384;  // FP64 16384: the two-CTA kernel (fft1d_pair.cu)
 }
 
 template <typename R, int M, bool FLUX>
@@ -266,6 +266,7 @@ cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n, int
                          int nsteps, cudaStream_t s, bool flux) {
   if (nj <= 0) return cudaSuccess;
   if (n & (n - 1)) return launch_bluestein(p, d_jobs, nj, n, step0, nsteps, s, flux);
+  if (fft1d_pair_size(p, n)) return launch_fft1d_pair(p, d_jobs, nj, n, step0, nsteps, s, flux);
 #define PXP_CASE(NN)                                                              \
   case NN:                                                                        \
     return p == kFP64 ? launch_nf<double, NN>(d_jobs, nj, step0, nsteps, s, flux)     \

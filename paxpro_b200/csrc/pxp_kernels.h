@@ -62,6 +62,12 @@ struct Fft1dJob {
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n,
                          int step0, int nsteps, cudaStream_t s, bool flux = false);
 bool fft1d_supported(Precision p, int n);
+// complex128 lines of 16384 points (fft1d_pair.cu): a cluster of two CTAs per
+// job, each holding the points of one parity; the job's twiddle is the
+// 8192-point Stockham table and its chirp the table exp(-2 pi i k / 16384).
+cudaError_t launch_fft1d_pair(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
+                              int nsteps, cudaStream_t s, bool flux);
+inline bool fft1d_pair_size(Precision p, int n) { return p == kFP64 && n == 16384; }
 // Length of the power-of-two transforms of the Bluestein path for n (the
 // smallest power of two >= 2n - 1); n itself for powers of two.
 int fft1d_bluestein_m(int n);

@@ -13,10 +13,10 @@ configurations:
     spheres (radius U[20, 150], centre uniform in the volume, delta
     U[1e-6, 5e-5], beta = delta/50).
 
-Sizes above 8192 points are drawn as 8192 for FFTSolver2D and above 4096 as
-4096 for CrankNicholson: an FP64 FFT line above 8192 points and an FP64
-Crank-Nicolson system above 4096 points do not fit one CTA's shared memory
-in this build.
+Every size is drawn as stated: FFTSolver2D lines of 16384 complex128 points
+run on a cluster of two CTAs, CrankNicholson systems of 8192 and 16384 rows
+on clusters of two and four CTAs (the step-invariant path of the
+waveguides' z-invariant media).
 
 `run_batched` admits every job into one Batch (one launch per group of equal
 2-D kind/size, 3-D jobs on their own streams); `run_plain` runs the same jobs
@@ -37,8 +37,8 @@ import numpy as np
 import paxpro_b200 as pxp
 from paxpro_b200 import workloads as wl
 
-MAX_FFT2D_N = 8192
-MAX_CN_N = 4096
+MAX_FFT2D_N = 16384
+MAX_CN_N = 16384
 
 
 @dataclass

@@ -49,6 +49,7 @@ def _run(kind, n, precision, steps, planes, transparent=False):
 
 @pytest.mark.parametrize("kind,n,precision,planes", [
     ("fft", 1024, 0, False), ("fft", 256, 1, True), ("fft", 8192, 0, False),
+    ("fft", 16384, 0, False),
     ("cn", 1024, 0, False), ("cn", 512, 0, True), ("cn", 16, 0, False), ("cn", 4096, 1, False)])
 def test_fused_flux_matches_saved_fields(kind, n, precision, planes):
     steps = 24

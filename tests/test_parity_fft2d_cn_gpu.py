@@ -249,3 +249,82 @@ def test_fft2d_any_grid_size(n, precision):
     w = np.full(n, 2.0)
     w[0] = w[-1] = 1.0
     assert flux == pytest.approx(float(np.sum(w * np.abs(out2) ** 2)), rel=1e-13)
+
+
+@pytest.mark.parametrize("planes", [False, True])
+def test_fft2d_fp64_16384_two_cta_cluster(planes):
+    """FFTSolver2D at 16384 points in FP64: the line (256 KB) is split by
+    parity over a cluster of two CTAs that exchange halves through
+    distributed shared memory; every save within 1e-10 of the oracle, with a
+    z-invariant table and with per-step planes."""
+    n, nsteps = 16384, 60
+    p = wl.Problem2D("n16k", "fft", -500.0, 500.0, wl.step_for_nodes(-500.0, 500.0, n), 0.0,
+                     1e6, 1000.0, nsteps, 20.0, wl.Waveguide())
+    d, b = p.material()
+    u0 = p.initial_field()
+    if not planes:
+        out, saves = _gpu_2d(p, d, b, u0, nsteps, 10, 0, chunks=2)
+        ref_out, ref_saves = _oracle_2d(p, d, b, u0, nsteps, 10)
+    else:
+        pxp = _pxp()
+        x = p.x
+        zs = p.zmin + (np.arange(1, nsteps + 1) + 0.5) * p.dz
+        dp = np.stack([np.where(np.abs(x - 1e-5 * z) <= 25.0, 0.0, 7.5e-6) for z in zs])
+        bp = np.full_like(dp, 1e-7)
+        spec = pxp.ProblemSpec(kind=pxp.FFT_SOLVER_2D, x=pxp.Disc(p.xmin, p.xmax, p.dx),
+                               z=pxp.Disc(p.zmin, p.zmax, p.dz), wavenumber=wl.K, save_every=10)
+        with pxp.Solver(spec) as s:
+            s.set_material_planes(dp, bp, 1, nsteps)
+            s.set_initial_conditions(u0)
+            s.step(nsteps)
+            out = s.get_last_solution()
+            saves = [s.get_saved(i) for i in range(s.num_saved())]
+        # the oracle takes the same planes one step at a time
+        g = po.grid(p.xmin, p.xmax, p.dx, p.zmin, p.zmax, p.dz, wl.K)
+        ref_out, ref_saves = u0, []
+        for k in range(nsteps):
+            gk = po.grid(p.xmin, p.xmax, p.dx, p.zmin + k * p.dz, p.zmax, p.dz, wl.K)
+            spec_k = po.MaterialSpec(po.MAT_XTABLE, delta_table=dp[k], beta_table=bp[k])
+            ref_out, _ = po.fft2d_run(gk, spec_k, ref_out, 1, 0)
+            if (k + 1) % 10 == 0:
+                ref_saves.append(ref_out)
+    assert len(saves) == len(ref_saves) == nsteps // 10
+    errs = [_rel(a, r) for a, r in zip(saves, ref_saves)]
+    assert max(errs) <= FP64_TOL, errs
+    assert _rel(out, ref_out) <= FP64_TOL
+
+
+@pytest.mark.parametrize("n,precision", [(8192, 0), (16384, 0), (16384, 1), (6000, 0)])
+def test_cn_cluster_sizes(n, precision):
+    """CrankNicholson beyond one SM's shared memory (8192 and 16384 rows,
+    and 6000 padded to 8192): the step-invariant path on a cluster of 2 or 4
+    CTAs, the stencil halo and the recurrences' carries crossing CTAs
+    through distributed shared memory.  FP64 within 1e-10 of the oracle at
+    every save, FP32 intensity within 1e-4."""
+    nsteps = 40
+    p = wl.Problem2D("cn_big", "cn", -500.0, 500.0, wl.step_for_nodes(-500.0, 500.0, n), 0.0,
+                     1e6, 500.0, nsteps, 20.0, wl.Waveguide())
+    d, b = p.material()
+    u0 = p.initial_field()
+    out, saves = _gpu_2d(p, d, b, u0, nsteps, 10, precision, chunks=2)
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, nsteps, 10)
+    assert len(saves) == len(ref_saves) == nsteps // 10
+    if precision == 0:
+        errs = [_rel(a, r) for a, r in zip(saves, ref_saves)]
+        assert max(errs) <= FP64_TOL, errs
+    else:
+        assert max(_int_rel(a, r) for a, r in zip(saves, ref_saves)) <= FP32_INT_TOL
+
+
+def test_cn_cluster_size_rejects_planes_and_transparent_ends():
+    import paxpro_b200 as pxp
+    from paxpro_b200 import _capi
+    n = 8192
+    dx = wl.step_for_nodes(-500.0, 500.0, n)
+    spec = pxp.ProblemSpec(kind=pxp.CRANK_NICHOLSON, x=pxp.Disc(-500.0, 500.0, dx),
+                           z=pxp.Disc(0.0, 1e4, 500.0), wavenumber=wl.K)
+    with pxp.Solver(spec) as s:
+        d = np.zeros((2 * 3, n))
+        s.set_material_planes(d, d, 1, 3)  # z-varying: the general kernel would be needed
+        s.set_initial_conditions(np.ones(n, dtype=np.complex128))
+        assert _capi.lib().pxp_step(s._h, 1) == _capi.PXP_ERR_UNSUPPORTED
