@@ -22,6 +22,7 @@
 // half step, spheres whose dz^2 alone is >= R^2, which cannot contain any
 // point of the plane.
 #include <cmath>
+#include <cstdlib>
 
 #include "bulk_copy.cuh"
 #include "csg.cuh"
@@ -657,15 +658,154 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
   }
 }
 
+// cp.async completion counted on an mbarrier: when every cp.async this
+// thread issued before the instruction has landed, the barrier sees one
+// arrival (noinc: the arrival is one of the count the barrier was set up
+// with).
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// Bytes before the factor tables in the one-wave kernels' shared memory: the
+// mbarriers (one for the tables and, in the pipelined kernel, one per
+// system group), rounded up to 16 bytes.
+template <int NG> constexpr size_t adi_wave_bar_bytes() { return 16 * ((NG + 2) / 2 + 1); }
+
+// The one-wave vacuum half step with its staging pipelined against the
+// solves.  The staged rows are copied in stages, one per system group in
+// group order (stage 0: the rows group 0 reads; stage k: the rows group k
+// needs that no earlier stage brought); every thread issues its share of a
+// stage's copies and then an asynchronous arrival on that stage's mbarrier,
+// so a stage completes when all of its copies (and every earlier stage's)
+// have landed.  Each group waits for its own stage and the factor tables
+// (its leader with the bounded wait, then the group's named barrier),
+// solves, and stores its systems straight from registers: group 0 computes
+// while later rows are still arriving, and one group's stores overlap the
+// others' solves.  Same arithmetic as adi_const_wave_kernel.
+template <int N, int M, int G, int S, bool XH>
+__global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
+    adi_pipe_wave_kernel(const AdiHalf h, const double2 *__restrict__ tabs) {
+  using L = AdiWaveTile<N, M, G, XH>;
+  constexpr int P = N / M;
+  constexpr int NG = (G + S - 1) / S;
+  constexpr int T = NG * P;
+  constexpr int RW = G + 2;
+  constexpr int SL = G - (NG - 1) * S;  // systems of the last group
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);  // [0]: tables, [1 + k]: stage k
+  double2 *gs = reinterpret_cast<double2 *>(smem_raw + adi_wave_bar_bytes<NG>());
+  double2 *hs = gs + N;
+  double2 *pf = hs + N;
+  double2 *pb = pf + N;
+  double2 *scratch = pb + N;  // (S + 1) * P / 32 per group
+  double2 *tile = scratch + NG * (S + 1) * (P / 32);
+  __shared__ int group_ok[NG];
+  const int tid = threadIdx.x;
+  const int group = tid / P, gtid = tid % P;
+  const int s_base = blockIdx.x * G;
+  const double2 *in = reinterpret_cast<const double2 *>(h.in);
+  double2 *out = reinterpret_cast<double2 *>(h.out);
+  double2 *save = reinterpret_cast<double2 *>(h.save);
+  const int g_lo = s_base == 0 ? 1 : 0;
+  const int g_hi = N - s_base + 1 < RW ? N - s_base + 1 : RW;
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    for (int k = 0; k < NG; ++k) mbar_init(bar + 1 + k, T);
+    mbar_arrive_expect_tx(bar, (unsigned)(sizeof(double2) * 4 * N));
+  }
+  for (int g = 0; g < RW; ++g)
+    if (g < g_lo || g >= g_hi)
+      for (int p = tid; p < N; p += T) tile[L::at(p / M, p % M, g)] = mk(0.0, 0.0);
+  __syncthreads();
+  if (tid == 0) bulk_load(gs, tabs, (unsigned)(sizeof(double2) * 4 * N), bar);
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  // stage k brings staged rows [lo_k, hi_k); group k reads rows k*S .. k*S + S + 1
+#pragma unroll 1
+  for (int k = 0; k < NG; ++k) {
+    const int lo = k == 0 ? 0 : k * S + 2;
+    const int hi = k == NG - 1 ? RW : (k + 1) * S + 2;
+    const int rows = hi - lo;
+    if constexpr (XH) {
+      // the rows of a position are adjacent in memory: consecutive threads
+      // take consecutive rows, then the next position
+      for (int i = tid; i < N * rows; i += T) {
+        const int p = i / rows, g = lo + i % rows;
+        if (g >= g_lo && g < g_hi)
+          adi_cp_async16(tile + L::at(p / M, p % M, g),
+                         in + (long long)p * h.stride_pos + (s_base - 1 + g));
+      }
+    } else {
+      for (int g = lo; g < hi; ++g) {
+        if (g < g_lo || g >= g_hi) continue;
+        const double2 *src = in + (long long)(s_base - 1 + g) * h.stride_sys;
+        for (int p = tid; p < N; p += T) adi_cp_async16(tile + L::at(p / M, p % M, g), src + p);
+      }
+    }
+    cp_async_mbar_arrive(bar + 1 + k);
+  }
+  // this group's rows and the tables
+  if (gtid == 0) {
+    bool ok = mbar_wait_bounded(bar + 1 + group, 0, 2000000000ull);
+    ok = mbar_wait_bounded(bar, 0, 2000000000ull) && ok;
+    if (!ok) atomicAdd(&g_wait_timeouts, 1u);
+    group_ok[group] = ok;
+  }
+  group_sync(1 + group, P);
+  if (!group_ok[group]) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    return;
+  }
+  (void)mbar_try_wait(bar + 1 + group, 0);  // completed phases: order the rows and tables
+  (void)mbar_try_wait(bar, 0);
+  double2 r[S][M];
+  double2 *gscr = scratch + group * (S + 1) * (P / 32);
+  if (SL == S || group < NG - 1)
+    adi_group_solve<N, M, G, XH, S, S>(r, h, tile, gs, hs, pf, pb, gscr, group * S, s_base, gtid,
+                                       gtid, 1 + group);
+  else
+    adi_group_solve<N, M, G, XH, S, SL>(r, h, tile, gs, hs, pf, pb, gscr, group * S, s_base, gtid,
+                                        gtid, 1 + group);
+  // results straight to global memory: position gtid*M + m of system
+  // s_base + group*S + j
+  const int ns = group < NG - 1 ? S : SL;
+#pragma unroll
+  for (int j = 0; j < S; ++j) {
+    const int sys = s_base + group * S + j;
+    if (j < ns && sys < N) {
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const long long off =
+            (long long)(gtid * M + m) * h.stride_pos + (long long)sys * h.stride_sys;
+        out[off] = r[j][m];
+        if (save) save[off] = r[j][m];
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");  // copies this thread issued for later groups
+}
+
+// The pipelined one-wave kernel (PXP_ADI_PIPE=0 selects the unpipelined one).
+static bool adi_pipe_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("PXP_ADI_PIPE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 template <int N, int M, int G, int S, bool XH>
 static cudaError_t adi_const_wave_launch_x(const AdiHalf &h, const void *tabs, cudaStream_t s) {
   constexpr int P = N / M, NG = (G + S - 1) / S, T = NG * P;
-  constexpr size_t smem = 16 + sizeof(double2) * (4 * N + NG * (S + 1) * (P / 32)) +
+  constexpr size_t smem = adi_wave_bar_bytes<NG>() +
+                          sizeof(double2) * (4 * N + NG * (S + 1) * (P / 32)) +
                           sizeof(double2) * AdiWaveTile<N, M, G, XH>::SIZE;
   static_assert(smem + 16 <= 227 * 1024, "staged ADI tile exceeds shared memory");
   static_assert(P % 32 == 0, "whole warps per group");
   static_assert(NG <= 15, "one named barrier per group");
-  auto k = adi_const_wave_kernel<N, M, G, S, XH>;
+  auto k = adi_pipe_enabled() ? adi_pipe_wave_kernel<N, M, G, S, XH>
+                              : adi_const_wave_kernel<N, M, G, S, XH>;
   {
     const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)smem);
     if (attr != cudaSuccess) return attr;
