@@ -265,6 +265,23 @@ int g_fft_parallel = 0;
 
 void fft_2d(cd *data, int nrows, int ncols, int sign) {
   int th = g_fft_parallel ? nthreads() : 1;
+  if (!is_pow2(nrows) || !is_pow2(ncols)) {
+    // other lengths: the direct DFT per line, contiguous lines first, then
+    // each strided line gathered, transformed and scattered back
+#pragma omp parallel num_threads(th)
+    {
+      std::vector<cd> line(nrows > ncols ? nrows : ncols);
+#pragma omp for
+      for (int c = 0; c < ncols; ++c) fft_1d(data + (long)c * nrows, nrows, sign);
+#pragma omp for
+      for (int r = 0; r < nrows; ++r) {
+        for (int c = 0; c < ncols; ++c) line[c] = data[(long)c * nrows + r];
+        fft_1d(line.data(), ncols, sign);
+        for (int c = 0; c < ncols; ++c) data[(long)c * nrows + r] = line[c];
+      }
+    }
+    return;
+  }
 #pragma omp parallel num_threads(th)
   {
     std::vector<cd> scratch(nrows > ncols ? nrows : ncols);
@@ -551,7 +568,7 @@ int orc_fft3d_run(const orc_grid *gp, const orc_material *m,
   const orc_grid &g = *gp;
   unsigned Nx = node_count(g.xmin, g.xmax, g.dx);
   unsigned Ny = Nx;  // Solver3D::setSimulator forces Ny = Nx (solver3D.cpp:24)
-  if (!is_pow2(Nx) || Nx < 2 || nsteps < 0) return -1;
+  if (Nx < 2 || nsteps < 0) return -1;
   const long npts = (long)Nx * Ny;
   const cd *in = reinterpret_cast<const cd *>(u0);
   std::vector<cd> prev(in, in + npts), curr(prev);

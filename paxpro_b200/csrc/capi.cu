@@ -825,6 +825,10 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
       return PXP_OK;
     }
   }
+  if (h->nx & (h->nx - 1)) {  // one kernel (Bluestein) for other sizes: nothing to tune
+    *out = 0;
+    return PXP_OK;
+  }
   const auto key = std::make_tuple(h->prob.device, (int)h->prec, h->nx);
   std::lock_guard<std::mutex> lk(g_tune_mutex);
   auto it = g_fft3d_variant.find(key);
@@ -883,6 +887,9 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   pxp::Fft3dPass q{};
   q.field = h->d_field;
   q.twiddle = h->d_tw;
+  q.chirp = h->d_chirp;
+  q.bconv = h->d_bconv;
+  q.m = pxp::fft1d_bluestein_m(n);
   q.n = n;
   q.a = 0.5 * p.z.step / p.wavenumber;  // FFTSolver3D::kernel (src/fftSolver3D.cpp:24-30)
   q.two_pi = 2.0 * PI;
@@ -1162,7 +1169,14 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
         if ((rc = adi_build_lu(h))) return cleanup_fail(rc);
       break;
     case PXP_FFT_SOLVER_3D:
-      if ((rc = shared_table(h, 0, &h->d_tw))) return cleanup_fail(rc);
+      if (h->nx & (h->nx - 1)) {
+        // not a power of two: the Bluestein tables of the line transforms
+        if ((rc = bluestein_table(h, 7, &h->d_chirp))) return cleanup_fail(rc);
+        if ((rc = bluestein_table(h, 8, &h->d_bconv))) return cleanup_fail(rc);
+        if ((rc = bluestein_table(h, 9, &h->d_tw))) return cleanup_fail(rc);
+      } else if ((rc = shared_table(h, 0, &h->d_tw))) {
+        return cleanup_fail(rc);
+      }
       break;
   }
   *out = h;

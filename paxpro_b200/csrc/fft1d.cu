@@ -12,6 +12,7 @@
 // (prev * t) / N with t taken from a host table built with std::exp, as the
 // reference evaluates it.  FP32 mode multiplies by t/N, the product formed
 // in FP64 and rounded once.
+#include "bluestein.cuh"
 #include "fft_smem.cuh"
 #include "flux.cuh"
 #include "pxp_kernels.h"
@@ -93,41 +94,6 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     if (flux) flux_store<T>(job.flux, step, flux_red[s & 1]);
   }
   for (int i = lane; i < N; i += T) field[i] = u[sw<C>(i)];
-}
-
-// Lengths that are not powers of two: Bluestein's chirp-z identity
-// jk = (j^2 + k^2 - (k - j)^2) / 2 turns the n-point DFT into
-//   X_k = w_k sum_j (x_j w_j) conj(w)_{k-j},   w_j = exp(-i pi j^2 / n),
-// a circular convolution of length m >= 2n - 1 (a power of two): two
-// shared-memory FFTs of length m and a pointwise product with the
-// precomputed transform of the filter (1/m folded in).  The inverse
-// transform is conj(DFT(conj(X))).  The field stays resident in shared
-// memory beside the m-point work buffer, as in the power-of-two kernel.
-template <typename R, int M, int T>
-__device__ __forceinline__ void bluestein_dft(typename Cx<R>::T *x, typename Cx<R>::T *u, int n,
-                                              const double2 *w, const double2 *bf,
-                                              const double2 *tw, int lane, bool inverse) {
-  using C = typename Cx<R>::T;
-  for (int j = lane; j < M; j += T) {
-    C a{};
-    if (j < n) {
-      C v = u[j];
-      if (inverse) v.y = -v.y;
-      a = tw_mul(v, w[j]);
-    }
-    x[sw<C>(j)] = a;
-  }
-  __syncthreads();
-  fft_smem<C, M, T, -1>(x, tw, lane);
-  for (int k = lane; k < M; k += T) x[sw<C>(k)] = tw_mul(x[sw<C>(k)], bf[k]);
-  __syncthreads();
-  fft_smem<C, M, T, +1>(x, tw, lane);
-  for (int k = lane; k < n; k += T) {
-    C v = tw_mul(x[sw<C>(k)], w[k]);
-    if (inverse) v.y = -v.y;
-    u[k] = v;
-  }
-  __syncthreads();
 }
 
 template <typename R, int M, int T, bool FLUX>

@@ -293,13 +293,17 @@ static cudaError_t fft3d_launch_n(const Fft3dPass &q, int variant, const double 
   return fft3d_launch_v<R, N, false, 16>(q, kx2, tw16, s);
 }
 
+int fft1d_bluestein_m(int n);
+
 bool fft3d_supported(Precision p, int n) {
-  if (n < 64 || (n & (n - 1))) return false;
-  return n <= 8192;
+  if (n & (n - 1))  // Bluestein line transforms (fft3d_blu.cu)
+    return n >= 8 && fft1d_bluestein_m(n) <= (p == kFP64 ? 8192 : 16384);
+  return n >= 64 && n <= 8192;
 }
 
 cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, const double *kx2,
                               const void *tw16, const void *wn, cudaStream_t s) {
+  if (q.n & (q.n - 1)) return launch_fft3d_bluestein(p, q, kx2, s);
   if (variant == 3) {
     if (fft3d_lines_supported(p, q.n) && wn != nullptr) return launch_fft3d_lines(p, q, kx2, wn, s);
     variant = 0;

@@ -104,9 +104,10 @@ __device__ __forceinline__ typename Cx<R>::T refract3(const Fft3dPass &q, typena
       u = cmul(u, t);
     }
   }
-  // (u * t) / (n*n): n*n is a power of two, so multiplying by its exact
-  // reciprocal rounds identically to the division
-  u = cx_scale_rn(u, inv_norm);
+  // (u * t) / (n*n): when n*n is a power of two, multiplying by its exact
+  // reciprocal rounds identically to the division; other sizes pass
+  // inv_norm = 0 and divide
+  u = inv_norm != 0.0 ? cx_scale_rn(u, inv_norm) : cx_div_real_rn(u, q.norm);
   if (q.thick_y > 0) {
     if (iy < q.thick_y) u = cx_scale_rn(u, exp(-(double)(q.thick_y - iy - 1) * q.inv_damp_y));
     if (q.n - 1 - iy < q.thick_y)

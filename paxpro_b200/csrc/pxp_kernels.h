@@ -285,6 +285,11 @@ struct Fft3dPass {
   const double *plane_delta, *plane_beta;
   const Sphere *spheres_all;
   Sphere spheres[kInlineSpheres];
+  // n not a power of two (fft3d_blu.cu): twiddle holds the Stockham
+  // twiddles of the Bluestein length m >= 2n - 1; chirp: n complex128
+  // exp(-i pi j^2 / n); bconv: m complex128, the filter's transform over m
+  const void *chirp, *bconv;
+  int m;
   // absorber (FFTSolver3D::absorbingBC): thickness in pixels and inverse
   // damping length per axis (0 thickness = off)
   int thick_x, thick_y;
@@ -302,6 +307,10 @@ cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, cons
 constexpr int kFft3dVariants = 4;
 bool fft3d_supported(Precision p, int n);
 bool fft3d_lines_supported(Precision p, int n);
+// Line passes of a size that is not a power of two (Bluestein transforms,
+// fft3d_blu.cu); q.chirp, q.bconv, q.m and q.twiddle as described above.
+cudaError_t launch_fft3d_bluestein(Precision p, const Fft3dPass &q, const double *kx2,
+                                   cudaStream_t s);
 cudaError_t launch_fft3d_lines(Precision p, const Fft3dPass &q, const double *kx2, const void *wn,
                                cudaStream_t s);
 // Bounded waits of the line-pass kernels that ran out on the current device.

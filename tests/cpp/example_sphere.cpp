@@ -1,14 +1,16 @@
 // The reference's 3-D example (Examples/sphere.cpp) through the B200 solver
 // API: a user MaterialFunction subclass (a sphere of radius 500 nm at the
 // origin), GenericScattering with the example's domain, steps, beam waist
-// and wavelength (513 transverse nodes, 257 longitudinal), the ADI
-// propagator, the far field of the exit field minus the vacuum reference.
-// Real-time visualisation and the HDF5 save are left out.  Arguments:
-// output file (N, rows, cols as doubles; the reference run's exit field, the
-// exit field (complex128, column-major); the far field (rows x cols doubles,
-// column-major)).
+// and wavelength (513 transverse nodes, 257 longitudinal), the far field of
+// the exit field minus the vacuum reference.  Real-time visualisation and
+// the HDF5 save are left out.  Arguments: output file (N, rows, cols as
+// doubles; the reference run's exit field, the exit field (complex128,
+// column-major); the far field (rows x cols doubles, column-major)), then
+// optionally the propagator: fft (GenericScattering's default, as in the
+// example) or adi.
 #include <cstdio>
 #include <iostream>
+#include <string>
 
 #include "paxpro/paxpro.hpp"
 
@@ -53,7 +55,8 @@ int main(int argc, char **argv) {
   simulation.dy = dx;
   simulation.dz = dz;
   simulation.wavelength = 0.1569;
-  simulation.propagator = GenericScattering::SolverType_t::ADI;
+  if (argc > 2 && std::string(argv[2]) == "adi")
+    simulation.propagator = GenericScattering::SolverType_t::ADI;
   Sphere sphere(r);
   simulation.setMaterial(sphere);
   arma::mat ff;

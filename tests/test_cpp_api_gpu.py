@@ -177,17 +177,20 @@ def test_curved_waveguide_transmittivity(kind, smoothed):
     assert 0.0 < t[-1] < 1.0
 
 
-def test_reference_sphere_example_with_a_user_material_function():
+@pytest.mark.parametrize("prop", ["fft", "adi"])
+def test_reference_sphere_example_with_a_user_material_function(prop):
     """The reference's Examples/sphere.cpp through the B200 API: a user
     MaterialFunction subclass (not a type the device evaluates), sampled on
-    the host at the planes ADI samples, 513 transverse nodes (the padded
-    general kernel), 256 steps, GenericScattering's vacuum reference run and
-    far field.  Exit fields against the oracle with the same sphere (1e-10),
-    the far field against the numpy far field of those fields."""
+    the host at the planes the solver samples, 513 transverse nodes
+    (FFTSolver3D: Bluestein line transforms, the example's default
+    propagator; ADI: the padded general kernel), 256 steps,
+    GenericScattering's vacuum reference run and far field.  Exit fields
+    against the oracle with the same sphere (1e-10), the far field against
+    the numpy far field of those fields."""
     from oracle import farfield as off
     exe = build("example_sphere")
-    out = os.path.join(OUT, "example_sphere.bin")
-    r = subprocess.run([exe, out], capture_output=True, text=True)
+    out = os.path.join(OUT, f"example_sphere_{prop}.bin")
+    r = subprocess.run([exe, out, prop], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     data = np.fromfile(out, dtype=np.float64)
     N, rows, cols = int(data[0]), int(data[1]), int(data[2])
@@ -200,9 +203,15 @@ def test_reference_sphere_example_with_a_user_material_function():
     g0 = po.grid(-750.0, 750.0, dx, -525.0, 525.0, 1050.0 / 3.0, K)
     g1 = po.grid(-750.0, 750.0, dx, -525.0, 525.0, 1050.0 / 256, K)
     u0 = po.gaussian_beam_3d(g0, 0.1569, 200000.0)
-    ref_o, _ = po.adi3d_run(g0, po.MaterialSpec(), u0, 3, 0, True)
     sphere = po.MaterialSpec(po.MAT_SPHERES, spheres=[(0.0, 0.0, 0.0, 500.0, 8.9e-6, 7e-7)])
-    ex_o, _ = po.adi3d_run(g1, sphere, u0, 256, 0, True)
+    if prop == "adi":
+        ref_o, _ = po.adi3d_run(g0, po.MaterialSpec(), u0, 3, 0, True)
+        ex_o, _ = po.adi3d_run(g1, sphere, u0, 256, 0, True)
+    else:
+        po.set_fft_parallel(True)
+        po.set_threads(os.cpu_count() or 1)
+        ref_o, _ = po.fft3d_run(g0, po.MaterialSpec(), u0, 3, 0)
+        ex_o, _ = po.fft3d_run(g1, sphere, u0, 256, 0)
     assert _rel(ref, ref_o) <= TOL
     assert _rel(ex, ex_o) <= TOL
     assert np.std(np.abs(ex)) > 1e-3  # the sphere left its mark

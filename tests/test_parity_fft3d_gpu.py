@@ -2,6 +2,7 @@
 through the C ABI.  FP64: <= 1e-10 relative L2 at every saved step; FP32
 served mode: <= 1e-4 relative L2 of the intensity."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -186,3 +187,23 @@ def test_fft3d_register_line_kernel_4096(precision, _variant):
     else:
         assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
     assert np.std(np.abs(out)) > 0
+
+
+@pytest.mark.parametrize("n,precision", [(100, 0), (513, 0), (300, 1), (33, 0)])
+def test_fft3d_sizes_other_than_powers_of_two(n, precision):
+    """FFTSolver3D on any grid size (the reference plans FFTW for any n):
+    Bluestein line transforms, spheres crossing the planes (refraction
+    integral), the absorber, saves, chunked calls; FP64 within 1e-10 of the
+    oracle, FP32 intensity within 1e-4."""
+    po.set_threads(os.cpu_count() or 1)
+    sph = [(20.0, 10.0, 2500.0, 200.0, 3e-5, 6e-7), (-150.0, 120.0, 4100.0, 90.0, 2e-5, 4e-7)]
+    out, saves, ref_out, ref_saves = _run_both(n, 1000.0, 0.0, 1000.0, 6, sph, save_every=2,
+                                               chunks=2, precision=precision,
+                                               absorber=(40.0, 30.0))
+    assert len(saves) == 3
+    if precision == 0:
+        assert max(_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP64_TOL
+        assert _rel(out, ref_out) <= FP64_TOL
+    else:
+        assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
+    assert np.std(np.abs(out)) > 1e-5

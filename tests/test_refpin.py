@@ -111,7 +111,7 @@ def test_adi_matches_reference_build(n, tbc):
 
 
 @pytest.mark.parametrize("n,absorber", [(64, (0.0, 0.0)), (64, (100.0, 50.0)),
-                                        (128, (0.0, 0.0))])
+                                        (128, (0.0, 0.0)), (33, (0.0, 0.0)), (50, (80.0, 40.0))])
 def test_fft_solver_3d_matches_reference_build(n, absorber):
     """FFTSolver3D through sphere rims, where the refraction integral between
     the step's planes runs (src/fftSolver3D.cpp:122-156, 253-273), with and
