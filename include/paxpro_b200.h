@@ -86,13 +86,16 @@ unsigned pxp_node_count(double min, double max, double step);
 /* Solver::setSimulator + ParaxialSimulation::setSolver
  * (src/paraxialSimulation.cpp:122-131, src/solver2D.cpp:21-42,
  * src/solver3D.cpp:19-44): allocate device state for the problem.
- * Transverse sizes: CrankNicholson any Nx >= 16 (up to 4096 in FP64, 8192
- * in FP32; transparent ends need Nx / 8 to be a power of two); ADI any
- * Nx >= 4 up to 2048 (sizes other than powers of two from 64 to 1024 run on
- * the general kernel, without the vacuum fast path); FFTSolver2D any
- * Nx >= 8 up to 8192 in FP64 and 16384 in FP32 for powers of two, and up
- * to 4096 / 8192 for other sizes (Bluestein's transform); FFTSolver3D powers
- * of two.  Other sizes return PXP_ERR_UNSUPPORTED. */
+ * Transverse sizes: CrankNicholson any Nx >= 16 up to 16384 (above 4096 in
+ * FP64 and 8192 in FP32 for z-invariant media with Dirichlet ends only, on
+ * clusters of CTAs; transparent ends need Nx / 8 to be a power of two); ADI
+ * any Nx >= 4 up to 2048 (sizes other than powers of two from 64 to 1024
+ * run on the general kernel, without the vacuum fast path); FFTSolver2D any
+ * Nx >= 8 up to 16384 for powers of two (FP64 16384 on a cluster of two
+ * CTAs), and up to 4096 (FP64) / 8192 (FP32) for other sizes (Bluestein's
+ * transform); FFTSolver3D powers of two from 64 to 8192 and other sizes up
+ * to 4096 (FP64) / 8192 (FP32) (Bluestein line transforms).  Other sizes
+ * return PXP_ERR_UNSUPPORTED. */
 int pxp_solver_create(const pxp_problem *problem, pxp_solver *out);
 
 /* Solver destructor (src/solver2D.cpp:10-19, src/solver3D.cpp:11-17). */
