@@ -319,8 +319,10 @@ int pxp_batch_admit(pxp_batch b, pxp_solver s, int nsteps);
 
 /* One round: every admitted solver with steps left advances by up to
  * max_steps steps.  2-D solvers of equal kind, size, precision and matrix
- * path share one launch (one CTA per solver, each with its own step count);
- * 3-D solvers run their passes on their own streams.  Asynchronous. */
+ * path share one launch (one CTA, or a cluster of CTAs, per solver, each
+ * with its own step count); the groups run concurrently on streams of
+ * their own, and 3-D solvers run their passes on their solvers' streams.
+ * Asynchronous. */
 int pxp_batch_round(pxp_batch b, int max_steps);
 
 /* Wait for the round, then hand back (and remove from the batch) the

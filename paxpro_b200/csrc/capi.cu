@@ -2094,7 +2094,12 @@ int pxp_get_intensity(pxp_solver h, double *intensity) {
 struct pxp_batch_s {
   int device = 0;
   size_t budget = 0, used = 0;
-  cudaStream_t stream = nullptr;  // 2-D group launches
+  cudaStream_t stream = nullptr;  // job uploads; joins the group streams
+  // 2-D groups of different (kind, size) run concurrently, one stream each,
+  // started after the round's upload and joined back into `stream`
+  std::vector<cudaStream_t> gstreams;
+  std::vector<cudaEvent_t> gdone;
+  cudaEvent_t uploaded = nullptr;
   std::vector<pxp_solver_s *> active;
   void *d_jobs = nullptr;
   size_t d_jobs_cap = 0;
@@ -2164,6 +2169,9 @@ int pxp_batch_destroy(pxp_batch b) {
   if (b->d_jobs) cudaFreeAsync(b->d_jobs, b->stream);
   cudaStreamSynchronize(b->stream);
   if (b->h_jobs) cudaFreeHost(b->h_jobs);
+  for (cudaStream_t g : b->gstreams) cudaStreamDestroy(g);
+  for (cudaEvent_t e : b->gdone) cudaEventDestroy(e);
+  if (b->uploaded) cudaEventDestroy(b->uploaded);
   cudaStreamDestroy(b->stream);
   delete b;
   return PXP_OK;
@@ -2242,7 +2250,31 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
   if (total > 0 &&
       cudaMemcpyAsync(b->d_jobs, b->h_jobs, total, cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
     return b->fail(PXP_ERR_CUDA, "job upload");
-  for (auto &o : offs) {
+  // one stream per group (created as needed), each starting after the upload
+  // and joined back into the batch stream
+  if (!offs.empty()) {
+    if (!b->uploaded && cudaEventCreateWithFlags(&b->uploaded, cudaEventDisableTiming) != cudaSuccess)
+      return b->fail(PXP_ERR_CUDA, "batch event");
+    while (b->gstreams.size() < offs.size()) {
+      cudaStream_t st;
+      cudaEvent_t ev;
+      if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+        return b->fail(PXP_ERR_CUDA, "batch group stream");
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamDestroy(st);
+        return b->fail(PXP_ERR_CUDA, "batch group event");
+      }
+      b->gstreams.push_back(st);
+      b->gdone.push_back(ev);
+    }
+    if (cudaEventRecord(b->uploaded, b->stream) != cudaSuccess)
+      return b->fail(PXP_ERR_CUDA, "batch event record");
+  }
+  for (size_t gi = 0; gi < offs.size(); ++gi) {
+    auto &o = offs[gi];
+    cudaStream_t gst = b->gstreams[gi];
+    if (cudaStreamWaitEvent(gst, b->uploaded, 0) != cudaSuccess)
+      return b->fail(PXP_ERR_CUDA, "batch group wait");
     const Key &k = o.second->first;
     const auto &list = o.second->second;
     const void *jobs = (const char *)b->d_jobs + o.first;
@@ -2251,15 +2283,17 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
     cudaError_t e;
     if (k.kind == PXP_FFT_SOLVER_2D)
       e = pxp::launch_fft1d((pxp::Precision)k.prec, (const pxp::Fft1dJob *)jobs, (int)list.size(),
-                            k.n, -1, -1, b->stream, any_flux);
+                            k.n, -1, -1, gst, any_flux);
     else if (k.cpath)
       e = pxp::launch_cn_const((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
-                               pxp::cn_padded_n(k.n), -1, -1, b->stream, any_flux);
+                               pxp::cn_padded_n(k.n), -1, -1, gst, any_flux);
     else
       e = pxp::launch_cn((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
-                         pxp::cn_padded_n(k.n),
-                         -1, -1, b->stream, any_flux);
+                         pxp::cn_padded_n(k.n), -1, -1, gst, any_flux);
     if (e != cudaSuccess) return b->fail(PXP_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    if (cudaEventRecord(b->gdone[gi], gst) != cudaSuccess ||
+        cudaStreamWaitEvent(b->stream, b->gdone[gi], 0) != cudaSuccess)
+      return b->fail(PXP_ERR_CUDA, "batch group join");
     for (pxp_solver_s *h : list) {
       const int n = std::min(h->batch_remaining, max_steps);
       h->current_step += (unsigned)n;
