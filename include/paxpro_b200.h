@@ -89,8 +89,9 @@ unsigned pxp_node_count(double min, double max, double step);
  * Transverse sizes: CrankNicholson any Nx >= 16 up to 16384 (above 4096 in
  * FP64 and 8192 in FP32 for z-invariant media with Dirichlet ends only, on
  * clusters of CTAs; transparent ends need Nx / 8 to be a power of two); ADI
- * any Nx >= 4 up to 2048 (sizes other than powers of two from 64 to 1024
- * run on the general kernel, without the vacuum fast path); FFTSolver2D any
+ * any Nx >= 4 up to 2048 (vacuum planes of FP64 grids up to 1024 nodes of
+ * any size run the one-wave fast path, padded to 64 .. 1024 rows; other
+ * sizes that are not powers of two run the general kernel); FFTSolver2D any
  * Nx >= 8 up to 16384 for powers of two (FP64 16384 on a cluster of two
  * CTAs), and up to 4096 (FP64) / 8192 (FP32) for other sizes (Bluestein's
  * transform); FFTSolver3D powers of two from 64 to 8192 and other sizes up

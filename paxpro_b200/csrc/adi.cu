@@ -349,6 +349,10 @@ static cudaError_t adi_const_launch(const AdiHalf &h, const void *g, const void 
 
 // Vacuum half step, FP64, n <= 1024, one wave: G systems per CTA so that
 // ceil(n / G) CTAs cover the 148 SMs once (G = 7 at n = 1024: 147 CTAs).
+// Systems are solved with N rows, N the smallest of 64, 128, 256, 512, 768
+// and 1024 that holds the grid's n (h.n): rows n .. N-1 are decoupled (their
+// factors g = 1, h = 0, right-hand sides zero, nothing copied in or out),
+// so grids of any size up to 1024 take this path.
 // The G + 2 staged rows (G systems and their two stencil halos) arrive by
 // coalesced 16-byte cp.async copies, the factor tables (one 64 KB block at
 // n = 1024) by one TMA bulk copy counted on an mbarrier; results leave by
@@ -488,11 +492,11 @@ __device__ __forceinline__ void adi_group_solve(double2 (&r)[SCAP][M], const Adi
     for (int k = 0; k < S + 2; ++k) v[k] = tile[L::at(c, m, sys0 + k)];
 #pragma unroll
     for (int j = 0; j < S; ++j) {
-      const int s = s_base + sys0 + j;  // s >= N: padding system, all zero
+      const int s = s_base + sys0 + j;  // s >= h.n: padding system, all zero
       const double2 rr = cmul(coef, v[j + 1]);
       double2 nb = mk(0.0, 0.0);
       if (s > 0) nb = v[j];
-      if (s < N - 1) nb = cadd(nb, v[j + 2]);
+      if (s < h.n - 1) nb = cadd(nb, v[j + 2]);
       r[j][m] = mk(fma(-hk, nb.y, rr.x), fma(hk, nb.x, rr.y));
     }
   }
@@ -564,17 +568,19 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
   const int s_base = blockIdx.x * G;
   const double2 *in = reinterpret_cast<const double2 *>(h.in);
   double2 *out = reinterpret_cast<double2 *>(h.out);
+  const int nr = h.n;  // systems, and positions per system (N: rows solved)
   // staged systems s_base - 1 + g exist for g in [g_lo, g_hi)
   const int g_lo = s_base == 0 ? 1 : 0;
-  const int g_hi = N - s_base + 1 < RW ? N - s_base + 1 : RW;
+  const int g_hi = nr - s_base + 1 < RW ? nr - s_base + 1 : RW;
   if (tid == 0) {
     mbar_init(bar, 1);
     mbar_arrive_expect_tx(bar, (unsigned)(sizeof(double2) * 4 * N));
   }
-  // staged rows outside the grid (first and last CTA) are zero
+  // staged rows outside the grid (first and last CTA) and the padding
+  // positions nr .. N-1 are zero
   for (int g = 0; g < RW; ++g)
-    if (g < g_lo || g >= g_hi)
-      for (int p = tid; p < N; p += T) tile[L::at(p / M, p % M, g)] = mk(0.0, 0.0);
+    for (int p = (g < g_lo || g >= g_hi) ? tid : nr + tid; p < N; p += T)
+      tile[L::at(p / M, p % M, g)] = mk(0.0, 0.0);
   __syncthreads();
   if (tid == 0) bulk_load(gs, tabs, (unsigned)(sizeof(double2) * 4 * N), bar);
   // Programmatic dependent launch: everything above (barrier set-up, zero
@@ -591,14 +597,14 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
     const int g = tid % RW;
     if (tid < PPI * RW && g >= g_lo && g < g_hi) {
       const double2 *src = in + (s_base - 1 + g);
-      for (int p = tid / RW; p < N; p += PPI)
+      for (int p = tid / RW; p < nr; p += PPI)
         adi_cp_async16(tile + L::at(p / M, p % M, g), src + (long long)p * h.stride_pos);
     }
   } else {
 #pragma unroll 1
     for (int g = g_lo; g < g_hi; ++g) {
       const double2 *src = in + (long long)(s_base - 1 + g) * h.stride_sys;
-      for (int p = tid; p < N; p += T) adi_cp_async16(tile + L::at(p / M, p % M, g), src + p);
+      for (int p = tid; p < nr; p += T) adi_cp_async16(tile + L::at(p / M, p % M, g), src + p);
     }
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -632,13 +638,13 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
     }
   __syncthreads();
   double2 *save = reinterpret_cast<double2 *>(h.save);
-  const int nsys = N - s_base < G ? N - s_base : G;  // the last CTA may hold fewer
+  const int nsys = nr - s_base < G ? nr - s_base : G;  // the last CTA may hold fewer
   if constexpr (XH) {
     // consecutive threads write consecutive systems of a position
     constexpr int PPI = T / G;
     const int gg = tid % G;
     if (tid < PPI * G && gg < nsys) {
-      for (int p = tid / G; p < N; p += PPI) {
+      for (int p = tid / G; p < nr; p += PPI) {
         const double2 v = tile[L::at(p / M, p % M, gg + 1)];
         const long long off = (long long)p * h.stride_pos + s_base + gg;
         out[off] = v;
@@ -649,7 +655,7 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
 #pragma unroll 1
     for (int gg = 0; gg < nsys; ++gg) {
       const long long base = (long long)(s_base + gg) * h.stride_sys;
-      for (int p = tid; p < N; p += T) {
+      for (int p = tid; p < nr; p += T) {
         const double2 v = tile[L::at(p / M, p % M, gg + 1)];
         out[base + p] = v;
         if (save) save[base + p] = v;
@@ -707,16 +713,18 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
   const double2 *in = reinterpret_cast<const double2 *>(h.in);
   double2 *out = reinterpret_cast<double2 *>(h.out);
   double2 *save = reinterpret_cast<double2 *>(h.save);
+  const int nr = h.n;  // systems, and positions per system (N: rows solved)
   const int g_lo = s_base == 0 ? 1 : 0;
-  const int g_hi = N - s_base + 1 < RW ? N - s_base + 1 : RW;
+  const int g_hi = nr - s_base + 1 < RW ? nr - s_base + 1 : RW;
   if (tid == 0) {
     mbar_init(bar, 1);
     for (int k = 0; k < NG; ++k) mbar_init(bar + 1 + k, T);
     mbar_arrive_expect_tx(bar, (unsigned)(sizeof(double2) * 4 * N));
   }
+  // rows outside the grid and the padding positions nr .. N-1 are zero
   for (int g = 0; g < RW; ++g)
-    if (g < g_lo || g >= g_hi)
-      for (int p = tid; p < N; p += T) tile[L::at(p / M, p % M, g)] = mk(0.0, 0.0);
+    for (int p = (g < g_lo || g >= g_hi) ? tid : nr + tid; p < N; p += T)
+      tile[L::at(p / M, p % M, g)] = mk(0.0, 0.0);
   __syncthreads();
   if (tid == 0) bulk_load(gs, tabs, (unsigned)(sizeof(double2) * 4 * N), bar);
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
@@ -730,7 +738,7 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
     if constexpr (XH) {
       // the rows of a position are adjacent in memory: consecutive threads
       // take consecutive rows, then the next position
-      for (int i = tid; i < N * rows; i += T) {
+      for (int i = tid; i < nr * rows; i += T) {
         const int p = i / rows, g = lo + i % rows;
         if (g >= g_lo && g < g_hi)
           adi_cp_async16(tile + L::at(p / M, p % M, g),
@@ -740,7 +748,7 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
       for (int g = lo; g < hi; ++g) {
         if (g < g_lo || g >= g_hi) continue;
         const double2 *src = in + (long long)(s_base - 1 + g) * h.stride_sys;
-        for (int p = tid; p < N; p += T) adi_cp_async16(tile + L::at(p / M, p % M, g), src + p);
+        for (int p = tid; p < nr; p += T) adi_cp_async16(tile + L::at(p / M, p % M, g), src + p);
       }
     }
     cp_async_mbar_arrive(bar + 1 + k);
@@ -770,12 +778,14 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
   // results straight to global memory: position gtid*M + m of system
   // s_base + group*S + j
   const int ns = group < NG - 1 ? S : SL;
+  const int mr = nr - gtid * M;  // rows of this chunk inside the grid (padding after)
 #pragma unroll
   for (int j = 0; j < S; ++j) {
     const int sys = s_base + group * S + j;
-    if (j < ns && sys < N) {
+    if (j < ns && sys < nr) {
 #pragma unroll
       for (int m = 0; m < M; ++m) {
+        if (m >= mr) continue;
         const long long off =
             (long long)(gtid * M + m) * h.stride_pos + (long long)sys * h.stride_sys;
         out[off] = r[j][m];
@@ -813,7 +823,7 @@ static cudaError_t adi_const_wave_launch_x(const AdiHalf &h, const void *tabs, c
   // launched as a programmatic dependent of the previous kernel in the
   // stream (the kernel waits for it with griddepcontrol.wait)
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((N + G - 1) / G);
+  cfg.gridDim = dim3((h.n + G - 1) / G);
   cfg.blockDim = dim3(T);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
@@ -840,9 +850,18 @@ static bool adi_wave_config(int n, int *m, int *g) {
     case 128: *m = 4; *g = 2; return true;
     case 256: *m = 8; *g = 2; return true;
     case 512: *m = 8; *g = 4; return true;
+    case 768: *m = 8; *g = 6; return true;
     case 1024: *m = 8; *g = 7; return true;
     default: return false;
   }
+}
+
+int adi_wave_n(int n) {
+  static const int sizes[] = {64, 128, 256, 512, 768, 1024};
+  if (n < 4) return 0;
+  for (int w : sizes)
+    if (n <= w) return w;
+  return 0;
 }
 
 bool adi_const_staged_tables(int n, const double *g, const double *h, double *out) {
@@ -915,11 +934,12 @@ cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, 
     return p == kFP64 ? adi_const_launch<double, NN, GG>(h, g, hh, s)                   \
                       : adi_const_launch<float, NN, GG>(h, g, hh, s);
   if (p == kFP64) {
-    switch (h.n) {
+    switch (adi_wave_n(h.n)) {
       case 64: return adi_const_wave_launch<64, 2, 4, 2>(h, staged, s);
       case 128: return adi_const_wave_launch<128, 4, 2, 1>(h, staged, s);
       case 256: return adi_const_wave_launch<256, 8, 2, 1>(h, staged, s);
       case 512: return adi_const_wave_launch<512, 8, 4, 2>(h, staged, s);
+      case 768: return adi_const_wave_launch<768, 8, 6, 2>(h, staged, s);
       case 1024: return adi_const_wave_launch<1024, 8, 7, 2>(h, staged, s);
       default: break;
     }

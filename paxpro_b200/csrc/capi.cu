@@ -530,6 +530,14 @@ int cn_build_lu(pxp_solver_s *h, const double *delta, const double *beta) {
   return PXP_OK;
 }
 
+// Length of each staged table of the ADI vacuum half steps: the FP64
+// one-wave kernel's padded system length, or n where that kernel does not
+// run n (the tables are then not read).
+int adi_tab_len(unsigned n) {
+  const int w = pxp::adi_wave_n((int)n);
+  return w > 0 ? w : (int)n;
+}
+
 // ADI vacuum matrices of the x and y half steps (src/alternatingDirection
 // Solver.cpp:38, :103 with beta = delta = 0): tables [gx | hx | gy | hy].
 int adi_build_lu(pxp_solver_s *h) {
@@ -544,14 +552,23 @@ int adi_build_lu(pxp_solver_s *h) {
   thomas_factor(dgx, -0.5 * im / (k * dx * dx), gx);
   thomas_factor(dgy, -0.5 * im / (k * dy * dy), gy);
   // [gx | hx | gy | hy] in natural order, then the x and y tables staged for
-  // the one-wave kernel ([g | h | pf | pb] each, where its size runs it)
-  std::vector<cd> tabs(12 * (size_t)n);
+  // the FP64 one-wave kernel ([g | h | pf | pb] each, for its system length
+  // nw; rows n .. nw-1 decoupled: g = 1, h = 0)
+  const unsigned nw = (unsigned)adi_tab_len(n);
+  std::vector<cd> tabs(4 * (size_t)n + 8 * (size_t)nw);
   std::copy(gx.begin(), gx.end(), tabs.begin());
   std::copy(gy.begin(), gy.end(), tabs.begin() + 2 * n);
-  const double *t = reinterpret_cast<const double *>(tabs.data());
-  pxp::adi_const_staged_tables((int)n, t, t + 2 * n, reinterpret_cast<double *>(tabs.data() + 4 * n));
-  pxp::adi_const_staged_tables((int)n, t + 4 * n, t + 6 * n,
-                               reinterpret_cast<double *>(tabs.data() + 8 * n));
+  std::vector<cd> pad(2 * (size_t)nw);
+  for (int half = 0; half < 2; ++half) {
+    const std::vector<cd> &gv = half == 0 ? gx : gy;
+    for (unsigned i = 0; i < nw; ++i) {
+      pad[i] = i < n ? gv[i] : cd(1.0, 0.0);
+      pad[nw + i] = i < n ? gv[n + i] : cd(0.0, 0.0);
+    }
+    const double *t = reinterpret_cast<const double *>(pad.data());
+    pxp::adi_const_staged_tables((int)nw, t, t + 2 * nw,
+                                 reinterpret_cast<double *>(tabs.data() + 4 * n + 4 * half * nw));
+  }
   free_dev(h->d_lu, h->stream);
   int rc;
   if ((rc = alloc(h, &h->d_lu, sizeof(cd) * tabs.size(), "factor tables"))) return rc;
@@ -743,7 +760,8 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   adi_fill_spheres(h, a, a.z);
   planes3_at(h, step, 1, &a.plane_delta, &a.plane_beta);
   e = (a.nspheres == 0 && !a.csg.active && !a.plane_delta && !a.use_tbc && lu)
-          ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n, lu + 8 * n, h->stream)
+          ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n,
+                                       lu + 4 * n + 4 * adi_tab_len((unsigned)n), h->stream)
           : pxp::launch_adi_half(h->prec, a, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
   if (slot && h->d_save_stage) return save_downsample(h, slot);
@@ -1165,7 +1183,10 @@ int pxp_solver_create(const pxp_problem *problem, pxp_solver *out) {
       if ((rc = alloc(h, &h->d_field2, h->csize * h->npts, "second field buffer")))
         return cleanup_fail(rc);
       // vacuum factor tables for the step-invariant kernels (grids those run)
-      if (pxp::adi_supported(h->prec, (int)h->nx))
+      // the vacuum fast path: powers of two in both precisions, any size the
+      // FP64 one-wave kernel takes
+      if (pxp::adi_supported(h->prec, (int)h->nx) ||
+          (h->prec == pxp::kFP64 && pxp::adi_wave_n((int)h->nx) > 0))
         if ((rc = adi_build_lu(h))) return cleanup_fail(rc);
       break;
     case PXP_FFT_SOLVER_3D:

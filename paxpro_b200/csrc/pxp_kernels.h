@@ -174,17 +174,24 @@ int adi_padded_n(int n);
 bool adi_padded_supported(Precision p, int n);
 // Half step whose plane holds no material and no transparent boundary: the
 // matrix is the same for every system and every step; g/h are its Thomas
-// factor tables (n complex128 each, see scan_solve.cuh).
-// `staged`: the same tables with their in-chunk products in the layout the
-// FP64 one-wave kernel copies into shared memory (adi_const_staged_tables;
-// not read where that returns false for n).
+// factor tables (n complex128 each, see scan_solve.cuh; read by the FP32
+// kernel, which takes powers of two only).
+// `staged`: the factor tables of the FP64 one-wave kernel, for its padded
+// system length adi_wave_n(n), with their in-chunk products, in the layout
+// it copies into shared memory (adi_const_staged_tables).  FP64 runs any
+// n with adi_wave_n(n) > 0 here.
 cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, const void *hh,
                                   const void *staged, cudaStream_t s);
+// System length of the FP64 one-wave vacuum kernel for a grid of n nodes
+// (64, 128, 256, 512, 768 or 1024, the smallest that holds n), 0 when n is
+// outside 4 .. 1024.  Rows n .. length-1 are decoupled padding.
+int adi_wave_n(int n);
 // Host: fills out[0 .. 4n) complex128 with [g | h | pf | pb] in the
-// chunk-transposed slots of the one-wave vacuum kernel for size n (pf, pb:
-// products of h over each chunk's rows up to / from a row) and returns true;
-// false when size n runs the other kernel (out untouched).  g, h, out:
-// interleaved (re, im).
+// chunk-transposed slots of the one-wave vacuum kernel for system length n
+// (pf, pb: products of h over each chunk's rows up to / from a row) and
+// returns true; false when no one-wave kernel solves length n (out
+// untouched).  g, h, out: interleaved (re, im); for a padded grid, g and h
+// already hold the padding rows (g = 1, h = 0).
 bool adi_const_staged_tables(int n, const double *g, const double *h, double *out);
 // Saved-slice downsampling of the 3-D solvers (Solver3D::copyCurrentSolution,
 // src/solver3D.cpp:94-112): n x n field -> m x m block averages.

@@ -4,7 +4,7 @@ registers) against the unpipelined one (PXP_ADI_PIPE=0, run in a child
 process because the switch is read once per process): the two share the
 solve's arithmetic, so their fields are equal bit for bit, for both half
 steps (x: systems adjacent in memory; y: systems as rows), with saves, at
-every size the one-wave kernel takes."""
+every system length the one-wave kernel solves and on grids it pads."""
 import os
 import subprocess
 import sys
@@ -36,7 +36,7 @@ np.save(sys.argv[3], np.stack(out))
 """
 
 
-@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024])
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024, 33, 300, 513, 1000])
 def test_pipelined_wave_kernel_equals_unpipelined(n, tmp_path):
     res = {}
     for pipe in ("1", "0"):

@@ -98,11 +98,17 @@ def test_adi_fp32_served_intensity():
 
 
 @pytest.mark.parametrize("n,use_tbc,precision", [(100, False, 0), (300, False, 0), (129, True, 0),
-                                                 (200, False, 1)])
+                                                 (200, False, 1), (5, False, 0), (33, False, 0),
+                                                 (513, False, 0), (700, False, 0), (1000, False, 0),
+                                                 (1500, False, 0)])
 def test_adi_any_grid_size(n, use_tbc, precision):
-    """ADI on grids whose size is not a power of two (the general kernel
-    pads every system with decoupled rows): every save against the oracle,
-    with a sphere crossing the planes, Dirichlet and transparent ends."""
+    """ADI on grids whose size is not a power of two: every save against the
+    oracle, with a sphere crossing the planes, Dirichlet and transparent
+    ends.  The sphere planes run the general kernel (systems padded with
+    decoupled rows to adi_padded_n), the vacuum planes the FP64 one-wave
+    kernel (padded to 64 .. 1024 rows: 5 and 33 -> 64, 100 -> 128, 300 and
+    513 -> 512 and 768, 700 -> 768, 1000 -> 1024) up to 1024 nodes, the
+    general kernel above (1500) and in FP32 or with transparent ends."""
     sph = [(30.0, -20.0, 3000.0, 250.0, 4.5e-5, 3.6e-6)]
     x = -500.0 + wl.step_for_nodes(-500.0, 500.0, n) * np.arange(n)
     u0 = np.asfortranarray(np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / 300.0 ** 2)
