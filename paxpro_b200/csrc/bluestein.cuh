@@ -15,10 +15,14 @@ namespace pxp {
 // precomputed transform of the filter (1/m folded in).  The inverse
 // transform is conj(DFT(conj(X))).  The field stays resident in shared
 // memory beside the m-point work buffer, as in the power-of-two kernel.
+// Tables (chirp w, filter transform bf, Stockham twiddles tw): complex128
+// for FP64 data, split complex64 pairs for complex64 data (fft_smem.cuh).
 template <typename R, int M, int T>
 __device__ __forceinline__ void bluestein_dft(typename Cx<R>::T *x, typename Cx<R>::T *u, int n,
-                                              const double2 *w, const double2 *bf,
-                                              const double2 *tw, int lane, bool inverse) {
+                                              const Tw<typename Cx<R>::T> *w,
+                                              const Tw<typename Cx<R>::T> *bf,
+                                              const Tw<typename Cx<R>::T> *tw, int lane,
+                                              bool inverse) {
   using C = typename Cx<R>::T;
   for (int j = lane; j < M; j += T) {
     C a{};

@@ -221,12 +221,35 @@ int upload_complex(pxp_solver_s *h, void *dst, const cd *src, long long n) {
   return PXP_OK;
 }
 
-// Per-step factor tables and twiddles are complex128 in both precisions;
-// served mode rounds only the field to complex64.
+// Constant-factor tables of the FFT kernels (twiddles, propagators,
+// transmissions, Bluestein chirps): complex128 entries in FP64 mode; in FP32
+// served mode each complex128 value w split into two complex64 parts, hi =
+// fl32(w) and lo = fl32(w - hi), stored (hi.re, hi.im, lo.re, lo.im), which
+// the kernels multiply with one chain of FP32 FMAs (fft_smem.cuh).  Both
+// forms take 16 bytes an entry.
 size_t table_entry_bytes(const pxp_solver_s *) { return 16; }
 
+std::vector<float> split_table(const std::vector<cd> &t) {
+  std::vector<float> o(4 * t.size());
+  for (size_t i = 0; i < t.size(); ++i) {
+    const double re = t[i].real(), im = t[i].imag();
+    const float hr = (float)re, hi = (float)im;
+    o[4 * i] = hr;
+    o[4 * i + 1] = hi;
+    o[4 * i + 2] = (float)(re - (double)hr);
+    o[4 * i + 3] = (float)(im - (double)hi);
+  }
+  return o;
+}
+
 int upload_table(pxp_solver_s *h, void *dst, const cd *src, long long n) {
-  PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, sizeof(cd) * n, cudaMemcpyHostToDevice, h->stream));
+  if (h->prec == pxp::kFP64) {
+    PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, src, sizeof(cd) * n, cudaMemcpyHostToDevice, h->stream));
+  } else {
+    const std::vector<float> sp = split_table(std::vector<cd>(src, src + n));
+    PXP_TRY_CUDA(h, cudaMemcpyAsync(dst, sp.data(), sizeof(float) * sp.size(),
+                                    cudaMemcpyHostToDevice, h->stream));
+  }
   PXP_TRY_CUDA(h, cudaStreamSynchronize(h->stream));
   return PXP_OK;
 }
@@ -253,12 +276,37 @@ struct TableKey {
                      // column, 3: twiddles (radix 16), 4: exp(-2 pi i m / n), m < n
   unsigned n;
   double dx, dz, k;
+  int split;  // 1: the FP32 split form (split_table), 0: complex128 / doubles
   bool operator<(const TableKey &o) const {
-    return std::tie(device, kind, n, dx, dz, k) < std::tie(o.device, o.kind, o.n, o.dx, o.dz, o.k);
+    return std::tie(device, kind, n, dx, dz, k, split) <
+           std::tie(o.device, o.kind, o.n, o.dx, o.dz, o.k, o.split);
   }
 };
+
 std::mutex g_table_mutex;
 std::map<TableKey, void *> g_tables;
+
+// Upload a shared table (complex128 values, or their split form) and
+// register it under key; the caller holds g_table_mutex.
+int store_shared(pxp_solver_s *h, const TableKey &key, const std::vector<cd> &t, void **out,
+                 const char *what) {
+  std::vector<float> sp;
+  if (key.split) sp = split_table(t);
+  void *p = nullptr;
+  if (cudaMalloc(&p, sizeof(cd) * t.size()) != cudaSuccess) {
+    cudaGetLastError();
+    return h->fail(PXP_ERR_NOMEM, std::string(what) + " allocation");
+  }
+  const cudaError_t e = cudaMemcpy(p, key.split ? (const void *)sp.data() : (const void *)t.data(),
+                                   sizeof(cd) * t.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(p);
+    return h->cuda_fail(e, (std::string(what) + " upload").c_str());
+  }
+  g_tables[key] = p;
+  *out = p;
+  return PXP_OK;
+}
 
 int shared_table_n(pxp_solver_s *h, int kind, unsigned n, void **out);
 
@@ -268,7 +316,8 @@ int shared_table(pxp_solver_s *h, int kind, void **out) { return shared_table_n(
 // propagator and kx^2 tables).
 int shared_table_n(pxp_solver_s *h, int kind, unsigned n, void **out) {
   TableKey key{h->prob.device, kind, n, (kind == 1 || kind == 2) ? h->prob.x.step : 0.0,
-               kind == 1 ? h->prob.z.step : 0.0, kind == 1 ? h->prob.wavenumber : 0.0};
+               kind == 1 ? h->prob.z.step : 0.0, kind == 1 ? h->prob.wavenumber : 0.0,
+               (h->prec == pxp::kFP32 && kind != 2) ? 1 : 0};
   std::lock_guard<std::mutex> lk(g_table_mutex);
   auto it = g_tables.find(key);
   if (it != g_tables.end()) {
@@ -299,12 +348,11 @@ int shared_table_n(pxp_solver_s *h, int kind, unsigned n, void **out) {
       t2[i] = kx * kx;
     }
   }
-  const size_t bytes = kind == 2 ? sizeof(double) * n : sizeof(cd) * n;
+  if (kind != 2) return store_shared(h, key, t, out, "shared table");
   void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, bytes);
+  cudaError_t e = cudaMalloc(&p, sizeof(double) * n);
   if (e != cudaSuccess) return h->fail(PXP_ERR_NOMEM, "shared table allocation");
-  e = cudaMemcpy(p, kind == 2 ? (const void *)t2.data() : (const void *)t.data(), bytes,
-                 cudaMemcpyHostToDevice);
+  e = cudaMemcpy(p, t2.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return h->cuda_fail(e, "shared table upload");
   g_tables[key] = p;
   *out = p;
@@ -342,7 +390,7 @@ void fft_ld(std::vector<std::complex<long double>> &a, int sign) {
 int bluestein_table(pxp_solver_s *h, int kind, void **out) {
   const unsigned n = h->nx;
   const int m = pxp::fft1d_bluestein_m((int)n);
-  TableKey key{h->prob.device, kind, n, 0.0, 0.0, 0.0};
+  TableKey key{h->prob.device, kind, n, 0.0, 0.0, 0.0, h->prec == pxp::kFP32 ? 1 : 0};
   std::lock_guard<std::mutex> lk(g_table_mutex);
   auto it = g_tables.find(key);
   if (it != g_tables.end()) {
@@ -375,16 +423,7 @@ int bluestein_table(pxp_solver_s *h, int kind, void **out) {
   } else {
     t = twiddles(m);
   }
-  void *p = nullptr;
-  if (cudaMalloc(&p, sizeof(cd) * t.size()) != cudaSuccess) {
-    cudaGetLastError();
-    return h->fail(PXP_ERR_NOMEM, "Bluestein table allocation");
-  }
-  cudaError_t e = cudaMemcpy(p, t.data(), sizeof(cd) * t.size(), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return h->cuda_fail(e, "Bluestein table upload");
-  g_tables[key] = p;
-  *out = p;
-  return PXP_OK;
+  return store_shared(h, key, t, out, "Bluestein table");
 }
 
 int fft1d_setup(pxp_solver_s *h) {
@@ -1728,7 +1767,7 @@ unsigned ff_angle_index(double angle, unsigned size, double k, double step) {
 // kind 6 the split form of kind 4: lo[r] = exp(-2 pi i r / L) for
 // r < 2^b, then hi[q] = exp(-2 pi i q 2^b / L) for q < L / 2^b.
 int ff_table(pxp_solver_s *h, int kind, long long len, const double2 **out) {
-  TableKey key{h->prob.device, kind, (unsigned)len, 0.0, 0.0, 0.0};
+  TableKey key{h->prob.device, kind, (unsigned)len, 0.0, 0.0, 0.0, 0};  // FP64 kernels
   std::lock_guard<std::mutex> lk(g_table_mutex);
   auto it = g_tables.find(key);
   if (it == g_tables.end()) {

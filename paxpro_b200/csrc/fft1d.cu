@@ -10,8 +10,8 @@
 // FP64 mode reproduces the reference's pointwise arithmetic exactly:
 // curr *= kernel is a rounded complex product and the refraction update is
 // (prev * t) / N with t taken from a host table built with std::exp, as the
-// reference evaluates it.  FP32 mode multiplies by t/N, the product formed
-// in FP64 and rounded once.
+// reference evaluates it.  FP32 mode computes in FP32 with split
+// complex64 tables (fft_smem.cuh): twiddles, the propagator and t/N.
 #include "bluestein.cuh"
 #include "fft_smem.cuh"
 #include "flux.cuh"
@@ -19,26 +19,15 @@
 
 namespace pxp {
 
-// Per-step factor tables hold complex128 values in both precisions.  FP64
-// mode reproduces the reference's rounding (rounded complex product, then
-// division by N); FP32 served mode forms the product with t/N in FP64 and
-// rounds once to complex64.
-template <typename R> __device__ __forceinline__ void refract(typename Cx<R>::T &u, double2 t,
-                                                              R n);
-template <> __device__ __forceinline__ void refract<double>(double2 &u, double2 t, double n) {
+// Per-step factor tables: complex128 in FP64 mode, which reproduces the
+// reference's rounding (rounded complex product, then division by N);
+// split complex64 pairs of t/N in FP32 served mode (one FMA chain).
+__device__ __forceinline__ void refract(double2 &u, double2 t, double n) {
   u = cx_div_real_rn(cx_mul_rn(u, t), n);
 }
-template <> __device__ __forceinline__ void refract<float>(float2 &u, double2 t, float) {
-  u = tw_mul(u, t);
-}
-template <typename R> __device__ __forceinline__ typename Cx<R>::T kmul(typename Cx<R>::T u,
-                                                                       double2 k);
-template <> __device__ __forceinline__ double2 kmul<double>(double2 u, double2 k) {
-  return cx_mul_rn(u, k);
-}
-template <> __device__ __forceinline__ float2 kmul<float>(float2 u, double2 k) {
-  return tw_mul(u, k);
-}
+__device__ __forceinline__ void refract(float2 &u, float4 t, float) { u = tw_mul(u, t); }
+__device__ __forceinline__ double2 kmul(double2 u, double2 k) { return cx_mul_rn(u, k); }
+__device__ __forceinline__ float2 kmul(float2 u, float4 k) { return tw_mul(u, k); }
 
 template <typename R, int N, int T, bool TW_SMEM, bool FLUX>
 __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ jobs, int step0_ov,
@@ -53,19 +42,20 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     job.nsteps = nsteps_ov;
   }
   const int lane = threadIdx.x;
-  const double2 *gtw = reinterpret_cast<const double2 *>(job.twiddle);
-  const double2 *tw = gtw;
+  using W = Tw<C>;
+  const W *gtw = reinterpret_cast<const W *>(job.twiddle);
+  const W *tw = gtw;
   if constexpr (TW_SMEM) {
     // twiddles after the field, 16-byte aligned
-    double2 *stw = reinterpret_cast<double2 *>(smem_raw + ((sizeof(C) * N + 15) & ~size_t(15)));
+    W *stw = reinterpret_cast<W *>(smem_raw + ((sizeof(C) * N + 15) & ~size_t(15)));
     for (int i = lane; i < N; i += T) stw[i] = gtw[i];
     tw = stw;
   }
   C *field = reinterpret_cast<C *>(job.field);
   for (int i = lane; i < N; i += T) u[sw<C>(i)] = field[i];
   __syncthreads();
-  const double2 *kern = reinterpret_cast<const double2 *>(job.kern);
-  const double2 *trans0 = reinterpret_cast<const double2 *>(job.trans);
+  const W *kern = reinterpret_cast<const W *>(job.kern);
+  const W *trans0 = reinterpret_cast<const W *>(job.trans);
   C *saves = reinterpret_cast<C *>(job.saves);
   const R nreal = (R)N;
   for (int s = 0; s < job.nsteps; ++s) {
@@ -74,17 +64,17 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     int2 fw;
     const bool flux = FLUX && flux_window(job.flux, step, fw);
     fft_smem<C, N, T, -1>(u, tw, lane);
-    for (int i = lane; i < N; i += T) u[sw<C>(i)] = kmul<R>(u[sw<C>(i)], kern[i]);
+    for (int i = lane; i < N; i += T) u[sw<C>(i)] = kmul(u[sw<C>(i)], kern[i]);
     __syncthreads();
     fft_smem<C, N, T, +1>(u, tw, lane);
-    const double2 *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
+    const W *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * N : nullptr;
     double acc = 0.0;
     for (int i = lane; i < N; i += T) {
       C v = u[sw<C>(i)];
-      refract<R>(v, trans[i], nreal);
+      refract(v, trans[i], nreal);
       u[sw<C>(i)] = v;
       if (save) slot[i] = v;
       if (flux) flux_add(acc, i, fw, to_d(v));
@@ -111,14 +101,15 @@ __global__ void __launch_bounds__(T) fft1d_bluestein_kernel(const Fft1dJob *__re
   }
   const int n = job.n;
   const int lane = threadIdx.x;
-  const double2 *tw = reinterpret_cast<const double2 *>(job.twiddle);
-  const double2 *w = reinterpret_cast<const double2 *>(job.chirp);
-  const double2 *bf = reinterpret_cast<const double2 *>(job.bconv);
+  using W = Tw<C>;
+  const W *tw = reinterpret_cast<const W *>(job.twiddle);
+  const W *w = reinterpret_cast<const W *>(job.chirp);
+  const W *bf = reinterpret_cast<const W *>(job.bconv);
   C *field = reinterpret_cast<C *>(job.field);
   for (int i = lane; i < n; i += T) u[i] = field[i];
   __syncthreads();
-  const double2 *kern = reinterpret_cast<const double2 *>(job.kern);
-  const double2 *trans0 = reinterpret_cast<const double2 *>(job.trans);
+  const W *kern = reinterpret_cast<const W *>(job.kern);
+  const W *trans0 = reinterpret_cast<const W *>(job.trans);
   C *saves = reinterpret_cast<C *>(job.saves);
   const R nreal = (R)n;
   for (int s = 0; s < job.nsteps; ++s) {
@@ -126,17 +117,17 @@ __global__ void __launch_bounds__(T) fft1d_bluestein_kernel(const Fft1dJob *__re
     int2 fw;
     const bool flux = FLUX && flux_window(job.flux, step, fw);
     bluestein_dft<R, M, T>(x, u, n, w, bf, tw, lane, false);
-    for (int i = lane; i < n; i += T) u[i] = kmul<R>(u[i], kern[i]);
+    for (int i = lane; i < n; i += T) u[i] = kmul(u[i], kern[i]);
     __syncthreads();
     bluestein_dft<R, M, T>(x, u, n, w, bf, tw, lane, true);
-    const double2 *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
+    const W *trans = trans0 + job.trans_stride * (long long)(step - job.trans_step0);
     const bool save = job.save_every > 0 && saves != nullptr && (step % job.save_every) == 0 &&
                       (step / job.save_every - 1) < job.max_slots;
     C *slot = save ? saves + (long long)(step / job.save_every - 1) * n : nullptr;
     double acc = 0.0;
     for (int i = lane; i < n; i += T) {
       C v = u[i];
-      refract<R>(v, trans[i], nreal);
+      refract(v, trans[i], nreal);
       u[i] = v;
       if (save) slot[i] = v;
       if (flux) flux_add(acc, i, fw, to_d(v));
@@ -158,7 +149,7 @@ static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nstep
   using C = typename Cx<R>::T;
   constexpr int T = fft1d_threads<R>(N);
   constexpr size_t field_bytes = sizeof(C) * N;
-  constexpr size_t tw_bytes = sizeof(double2) * N;
+  constexpr size_t tw_bytes = sizeof(Tw<C>) * N;
   constexpr bool tw_smem = field_bytes + tw_bytes <= 200 * 1024;
   constexpr size_t smem = tw_smem ? field_bytes + tw_bytes : field_bytes;
   auto k = fft1d_kernel<R, N, T, tw_smem, FLUX>;

@@ -75,19 +75,20 @@ __device__ __forceinline__ void store_line(const C *src, C *field, int line, boo
 //               N/16 threads per line, single buffer.
 // The launcher times the variants on the first steps and keeps the fastest.
 template <typename R, int N, int T, bool DB, int MAXR>
-__global__ void __launch_bounds__(T, (DB || MAXR == 16 || T >= 1024) ? 1 : 2) fft3d_pass_kernel(const Fft3dPass q,
-                                                                  const double *__restrict__ gkx2,
-                                                                  const double2 *__restrict__ gtw) {
+__global__ void __launch_bounds__(T, (DB || MAXR == 16 || T >= 1024) ? 1 : 2)
+    fft3d_pass_kernel(const Fft3dPass q, const double *__restrict__ gkx2,
+                      const Tw<typename Cx<R>::T> *__restrict__ gtw) {
   using C = typename Cx<R>::T;
+  using W = Tw<C>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *buf0 = reinterpret_cast<C *>(smem_raw);
   C *buf1 = DB ? buf0 + N : buf0;
-  double2 *stw = reinterpret_cast<double2 *>(buf0 + (DB ? 2 * N : N));
+  W *stw = reinterpret_cast<W *>(buf0 + (DB ? 2 * N : N));
   double *skx2 = reinterpret_cast<double *>(stw + N);
   C *field = reinterpret_cast<C *>(q.field);
   const bool strided = q.mode == 1;
   const int tid = threadIdx.x;
-  const double2 *tw = gtw;
+  const W *tw = gtw;
   const double *kx2 = gkx2;
 
   int line = blockIdx.x;
@@ -164,11 +165,11 @@ constexpr int xpass_ld() { return N + (sizeof(C) == 16 ? 1 : 4); }
 template <typename R, int N, int T, int W>
 __global__ void __launch_bounds__(T, 1) fft3d_xpass_w_kernel(const Fft3dPass q,
                                                             const double *__restrict__ gkx2,
-                                                            const double2 *__restrict__ gtw) {
+                                                            const Tw<typename Cx<R>::T> *__restrict__ gtw) {
   using C = typename Cx<R>::T;
   constexpr int LD = xpass_ld<C, N>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2 *tw = reinterpret_cast<double2 *>(smem_raw);
+  Tw<C> *tw = reinterpret_cast<Tw<C> *>(smem_raw);
   double *kx2 = reinterpret_cast<double *>(tw + N);
   C *u = reinterpret_cast<C *>(kx2 + N);
   C *field = reinterpret_cast<C *>(q.field);
@@ -212,9 +213,10 @@ __global__ void __launch_bounds__(T, 1) fft3d_xpass_w_kernel(const Fft3dPass q,
 }
 
 template <typename R, int N>
-static cudaError_t fft3d_xpass_w_launch(const Fft3dPass &q, const double *kx2, const double2 *tw,
+static cudaError_t fft3d_xpass_w_launch(const Fft3dPass &q, const double *kx2, const void *twv,
                                         cudaStream_t s) {
   using C = typename Cx<R>::T;
+  const Tw<C> *tw = reinterpret_cast<const Tw<C> *>(twv);
   constexpr int W = 32 / (int)sizeof(C);
   constexpr int T = N / 8 < 32 ? 32 : (N / 8 > 1024 ? 1024 : N / 8);
   constexpr size_t smem = sizeof(double2) * N + sizeof(double) * N + sizeof(C) * W * xpass_ld<C, N>();
@@ -250,9 +252,10 @@ template <int N, int MAXR> constexpr int pass_threads() {
 }
 
 template <typename R, int N, bool DB, int MAXR>
-static cudaError_t fft3d_launch_v(const Fft3dPass &q, const double *kx2, const double2 *tw,
+static cudaError_t fft3d_launch_v(const Fft3dPass &q, const double *kx2, const void *twv,
                                   cudaStream_t s) {
   using C = typename Cx<R>::T;
+  const Tw<C> *tw = reinterpret_cast<const Tw<C> *>(twv);
   constexpr int T = pass_threads<N, MAXR>();
   constexpr size_t smem = DB ? 2 * sizeof(C) * N + sizeof(double2) * N + sizeof(double) * N
                              : sizeof(C) * N;
@@ -276,9 +279,9 @@ static cudaError_t fft3d_launch_v(const Fft3dPass &q, const double *kx2, const d
 
 template <typename R, int N>
 static cudaError_t fft3d_launch_n(const Fft3dPass &q, int variant, const double *kx2,
-                                  const double2 *tw16, cudaStream_t s) {
+                                  const void *tw16, cudaStream_t s) {
   using C = typename Cx<R>::T;
-  const double2 *tw8 = reinterpret_cast<const double2 *>(q.twiddle);
+  const void *tw8 = q.twiddle;
   // x pass: W adjacent columns per CTA where their buffer fits
   // (measured: faster from 1024 points, slower at 512)
   constexpr bool wide_fits = N >= 1024 && N <= 4096;
@@ -310,8 +313,8 @@ cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, cons
   }
 #define PXP_C3(NN)                                                                  \
   case NN:                                                                          \
-    return p == kFP64 ? fft3d_launch_n<double, NN>(q, variant, kx2, (const double2 *)tw16, s) \
-                      : fft3d_launch_n<float, NN>(q, variant, kx2, (const double2 *)tw16, s);
+    return p == kFP64 ? fft3d_launch_n<double, NN>(q, variant, kx2, tw16, s) \
+                      : fft3d_launch_n<float, NN>(q, variant, kx2, tw16, s);
   switch (q.n) {
     PXP_C3(64) PXP_C3(128) PXP_C3(256) PXP_C3(512) PXP_C3(1024) PXP_C3(2048) PXP_C3(4096)
     PXP_C3(8192)

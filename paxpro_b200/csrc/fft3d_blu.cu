@@ -18,9 +18,9 @@ namespace pxp {
 
 template <typename R, int M, int T>
 __global__ void __launch_bounds__(T) fft3d_blu_kernel(const Fft3dPass q, const double *__restrict__ kx2,
-                                                     const double2 *__restrict__ tw,
-                                                     const double2 *__restrict__ chirp,
-                                                     const double2 *__restrict__ bconv) {
+                                                     const Tw<typename Cx<R>::T> *__restrict__ tw,
+                                                     const Tw<typename Cx<R>::T> *__restrict__ chirp,
+                                                     const Tw<typename Cx<R>::T> *__restrict__ bconv) {
   using C = typename Cx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *x = reinterpret_cast<C *>(smem_raw);  // m-point work buffer (swizzled)
@@ -85,8 +85,9 @@ static cudaError_t blu_launch(const Fft3dPass &q, const double *kx2, cudaStream_
   const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, T, smem);
   if (e != cudaSuccess) return e;
   const int cap = sms * (per > 0 ? per : 1);
-  k<<<q.n < cap ? q.n : cap, T, smem, s>>>(q, kx2, (const double2 *)q.twiddle,
-                                         (const double2 *)q.chirp, (const double2 *)q.bconv);
+  using W = Tw<C>;
+  k<<<q.n < cap ? q.n : cap, T, smem, s>>>(q, kx2, (const W *)q.twiddle, (const W *)q.chirp,
+                                         (const W *)q.bconv);
   return cudaGetLastError();
 }
 

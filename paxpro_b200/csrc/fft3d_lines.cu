@@ -36,8 +36,8 @@
 // arithmetic (propagator argument and sincos, refraction, absorber, save) is
 // fft3d_point.cuh's, shared with fft3d.cu.  The transforms round like the
 // other kernels' up to the order of their passes (within the parity
-// tolerance); complex64 data keep every product with a twiddle or constant
-// in FP64 as fft_smem.cuh does.
+// tolerance); complex64 data compute in FP32 with split twiddles as
+// fft_smem.cuh does.
 #include <cuda.h>
 
 #include <cstdint>
@@ -86,7 +86,7 @@ template <typename R, int N, int LG> struct Cfg {
   static_assert(N % 8 == 0 && T <= 1024, "line slots");
 };
 
-template <typename C> __device__ __forceinline__ C twm(C v, double2 w, bool fwd) {
+template <typename C, typename W> __device__ __forceinline__ C twm(C v, W w, bool fwd) {
   return fwd ? tw_mul(v, w) : tw_mulc(v, w);
 }
 
@@ -126,7 +126,7 @@ __device__ __forceinline__ void first_pass(C (&v)[8], C *X, int j) {
 // (inputs j + r*n/8), twiddles tw[0..6], outputs to (j - k)*8 + k + r*NS,
 // k = j mod NS; the last pass (NS = n/8) keeps them in registers.
 template <int SIGN, int N, int NS, typename C>
-__device__ __forceinline__ void r8_pass(C (&v)[8], const C *Xin, C *Xout, const double2 (&tw)[7],
+__device__ __forceinline__ void r8_pass(C (&v)[8], const C *Xin, C *Xout, const Tw<C> (&tw)[7],
                                         int j) {
   constexpr int TL = N / 8;
 #pragma unroll
@@ -156,14 +156,14 @@ template <int R0, int P> __host__ __device__ constexpr int tws_offset() {
 template <int SIGN, typename R, int N, int LG, int P>
 __device__ __forceinline__ void r8_passes(typename Cx<R>::T (&v)[Cfg<R, N, LG>::LPT][8],
                                           typename Cx<R>::T *X0, typename Cx<R>::T *X1, int &cur,
-                                          const double2 (&twr)[Cfg<R, N, LG>::TWR][7],
-                                          const double2 *tws, int slot, int j) {
+                                          const Tw<typename Cx<R>::T> (&twr)[Cfg<R, N, LG>::TWR][7],
+                                          const Tw<typename Cx<R>::T> *tws, int slot, int j) {
   using K = Cfg<R, N, LG>;
   using C = typename Cx<R>::T;
   if constexpr (P < K::NP8) {
     constexpr int NS = K::R0 << (3 * P);
     constexpr int FIRST_REG = K::NP8 - K::TWR;
-    double2 tw[7];
+    Tw<C> tw[7];
     if constexpr (P >= FIRST_REG) {
 #pragma unroll
       for (int r = 0; r < 7; ++r) tw[r] = twr[P - FIRST_REG][r];
@@ -195,8 +195,8 @@ __device__ __forceinline__ void r8_passes(typename Cx<R>::T (&v)[Cfg<R, N, LG>::
 template <int SIGN, typename R, int N, int LG, typename Hook>
 __device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N, LG>::LPT][8],
                                          typename Cx<R>::T *X0, typename Cx<R>::T *X1, int &cur,
-                                         const double2 (&tw)[Cfg<R, N, LG>::TWR][7],
-                                         const double2 *tws, int slot, int j, Hook hook) {
+                                         const Tw<typename Cx<R>::T> (&tw)[Cfg<R, N, LG>::TWR][7],
+                                         const Tw<typename Cx<R>::T> *tws, int slot, int j, Hook hook) {
   using K = Cfg<R, N, LG>;
   using C = typename Cx<R>::T;
   C *out = cur ? X0 : X1;
@@ -212,7 +212,8 @@ __device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N, LG>::L
 template <typename R, int N, int LG>
 __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
     fft3d_lines_kernel(const Fft3dPass q, const __grid_constant__ CUtensorMap tmap,
-                       const double *__restrict__ gkx2, const double2 *__restrict__ wn) {
+                       const double *__restrict__ gkx2,
+                       const Tw<typename Cx<R>::T> *__restrict__ wn) {
   using K = Cfg<R, N, LG>;
   using C = typename Cx<R>::T;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
   C *S = reinterpret_cast<C *>(base);
   C *X0 = reinterpret_cast<C *>(base + K::STAGE);
   C *X1 = reinterpret_cast<C *>(base + K::STAGE + ((K::XBYTES + 127) & ~size_t(127)));
-  double2 *tws = reinterpret_cast<double2 *>(base + K::STAGE + 2 * ((K::XBYTES + 127) & ~size_t(127)));
+  Tw<C> *tws = reinterpret_cast<Tw<C> *>(base + K::STAGE + 2 * ((K::XBYTES + 127) & ~size_t(127)));
   uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<unsigned char *>(tws) +
                                                ((K::TWBYTES + 127) & ~size_t(127)));
   __shared__ int s_ok;
@@ -234,7 +235,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
 
   // twiddles of the last TWR radix-8 passes, constant for this thread, and
   // the shared table of the earlier passes' (entry (r-1)*NS + k of pass p)
-  double2 tw[K::TWR][7];
+  Tw<C> tw[K::TWR][7];
 #pragma unroll
   for (int pr = 0; pr < K::TWR; ++pr) {
     const int ns = K::R0 << (3 * (K::NP8 - K::TWR + pr));
@@ -404,7 +405,8 @@ cudaError_t make_tmap(void *field, CUtensorMap *out) {
 }
 
 template <typename R, int N, int LG>
-cudaError_t launch(const Fft3dPass &q, const double *kx2, const double2 *wn, cudaStream_t s) {
+cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaStream_t s) {
+  const Tw<typename Cx<R>::T> *wn = reinterpret_cast<const Tw<typename Cx<R>::T> *>(wnv);
   using K = Cfg<R, N, LG>;
   static_assert(K::SMEM <= 227 * 1024, "line pass exceeds shared memory");
   CUtensorMap tmap;
@@ -450,7 +452,7 @@ bool fft3d_lines_supported(Precision p, int n) {
 
 cudaError_t launch_fft3d_lines(Precision p, const Fft3dPass &q, const double *kx2,
                                const void *wn, cudaStream_t s) {
-  const double2 *w = (const double2 *)wn;
+  const void *w = wn;
 #define PXP_L3(NN, LGD, LGF)                                                          \
   case NN:                                                                            \
     return p == kFP64 ? lines::launch<double, NN, LGD>(q, kx2, w, s)                  \
