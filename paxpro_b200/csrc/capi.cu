@@ -359,6 +359,29 @@ int shared_table_n(pxp_solver_s *h, int kind, unsigned n, void **out) {
   return PXP_OK;
 }
 
+// FP32 FFTSolver3D: one factor of the separable propagator, exp(-i a k_i^2)
+// with k_i = spatialFreq(i) for the x (axis 0) or y (axis 1) step and
+// a = dz / (2k), the phase reduced in extended precision; split form.
+int prop3_table(pxp_solver_s *h, int axis, void **out) {
+  const unsigned n = h->nx;
+  const double step = axis == 0 ? h->prob.x.step : h->prob.y.step;
+  TableKey key{h->prob.device, 10, n, step, h->prob.z.step, h->prob.wavenumber, 1};
+  std::lock_guard<std::mutex> lk(g_table_mutex);
+  auto it = g_tables.find(key);
+  if (it != g_tables.end()) {
+    *out = it->second;
+    return PXP_OK;
+  }
+  const long double a = 0.5L * (long double)h->prob.z.step / (long double)h->prob.wavenumber;
+  std::vector<cd> t(n);
+  for (unsigned i = 0; i < n; ++i) {
+    const long double kx = spatial_freq(i, n, step);
+    const long double phi = a * kx * kx;
+    t[i] = cd((double)cosl(phi), -(double)sinl(phi));
+  }
+  return store_shared(h, key, t, out, "propagator table");
+}
+
 // ---- FFT 1-D -------------------------------------------------------------
 // In-place radix-2 FFT in extended precision (host tables only).
 void fft_ld(std::vector<std::complex<long double>> &a, int sign) {
@@ -969,6 +992,13 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   if (int rc = shared_table(h, 2, &kx2)) return rc;
   if (int rc = shared_table(h, 3, &tw16)) return rc;
   if (int rc = shared_table(h, 4, &wn)) return rc;
+  if (h->prec == pxp::kFP32) {
+    void *px = nullptr, *py = nullptr;
+    if (int rc = prop3_table(h, 0, &px)) return rc;
+    if (int rc = prop3_table(h, 1, &py)) return rc;
+    q.prop_x = px;
+    q.prop_y = py;
+  }
   int variant = 0;
   if (int rc = fft3d_variant(h, q, kx2, tw16, wn, &variant)) return rc;
   cudaError_t e;

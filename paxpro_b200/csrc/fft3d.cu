@@ -121,12 +121,7 @@ __global__ void __launch_bounds__(T, (DB || MAXR == 16 || T >= 1024) ? 1 : 2)
       fft_smem<C, N, T, -1, MAXR>(u, tw, tid);
       const double ky = kfreq(line, N, q.two_pi, q.stepn_y);
       const double ky2 = __dmul_rn(ky, ky);
-      for (int j = tid; j < N; j += T) {
-        const double phi = __dmul_rn(q.a, __dadd_rn(kx2[j], ky2));
-        double sn, cs;
-        sincos_cw(phi, &sn, &cs);
-        u[sw<C>(j)] = mul_k<R>(u[sw<C>(j)], mk(cs, -sn));
-      }
+      for (int j = tid; j < N; j += T) u[sw<C>(j)] = prop3(q, u[sw<C>(j)], kx2[j], ky2, j, line);
       __syncthreads();
       fft_smem<C, N, T, +1, MAXR>(u, tw, tid);
     } else {
@@ -195,12 +190,8 @@ __global__ void __launch_bounds__(T, 1) fft3d_xpass_w_kernel(const Fft3dPass q,
     for (int w = 0; w < W; ++w) {
       const double ky = kfreq(line0 + w, N, q.two_pi, q.stepn_y);
       const double ky2 = __dmul_rn(ky, ky);
-      for (int j = tid; j < N; j += T) {
-        const double phi = __dmul_rn(q.a, __dadd_rn(kx2[j], ky2));
-        double sn, cs;
-        sincos_cw(phi, &sn, &cs);
-        u[w * LD + sw<C>(j)] = mul_k<R>(u[w * LD + sw<C>(j)], mk(cs, -sn));
-      }
+      for (int j = tid; j < N; j += T)
+        u[w * LD + sw<C>(j)] = prop3(q, u[w * LD + sw<C>(j)], kx2[j], ky2, j, line0 + w);
     }
     __syncthreads();
     fft_smem_w<C, N, T, +1, W, LD>(u, tw, tid);

@@ -39,12 +39,7 @@ __global__ void __launch_bounds__(T) fft3d_blu_kernel(const Fft3dPass q, const d
       // propagator K = exp(-i a (kx^2 + ky^2)) (src/fftSolver3D.cpp:24-30, 87-120)
       const double ky = kfreq(line, n, q.two_pi, q.stepn_y);
       const double ky2 = __dmul_rn(ky, ky);
-      for (int j = lane; j < n; j += T) {
-        const double phi = __dmul_rn(q.a, __dadd_rn(kx2[j], ky2));
-        double sn, cs;
-        sincos_cw(phi, &sn, &cs);
-        u[j] = mul_k<R>(u[j], mk(cs, -sn));
-      }
+      for (int j = lane; j < n; j += T) u[j] = prop3(q, u[j], kx2[j], ky2, j, line);
       __syncthreads();
       bluestein_dft<R, M, T>(x, u, n, chirp, bconv, tw, lane, true);
     } else {

@@ -251,8 +251,8 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
       tws[off + i] = wn[r * k * (N / (8 * ns))];
     }
   }
-  double kx2[8];
-  if (xpass) {
+  double kx2[8] = {};
+  if (sizeof(R) == 8 && xpass) {  // FP64 forms the propagator's argument per point
 #pragma unroll
     for (int s = 0; s < 8; ++s) kx2[s] = gkx2[j + s * K::TL];
   }
@@ -326,12 +326,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
         const double ky = kfreq(line, N, q.two_pi, q.stepn_y);
         const double ky2 = __dmul_rn(ky, ky);
 #pragma unroll
-        for (int s = 0; s < 8; ++s) {
-          const double phi = __dmul_rn(q.a, __dadd_rn(kx2[s], ky2));
-          double sn, cs;
-          sincos_cw(phi, &sn, &cs);
-          v[t][s] = mul_k<R>(v[t][s], mk(cs, -sn));
-        }
+        for (int s = 0; s < 8; ++s) v[t][s] = prop3(q, v[t][s], kx2[s], ky2, j + s * K::TL, line);
       }
       line_fft<+1, R, N, LG>(v, X0, X1, cur, tw, tws, slot, j, nothing);
     } else if (q.mode == 0) {

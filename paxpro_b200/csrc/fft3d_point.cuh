@@ -66,6 +66,24 @@ __device__ __forceinline__ double kfreq(int idx, int n, double two_pi, double st
   return __ddiv_rn(__dmul_rn(two_pi, (double)idx), stepn);
 }
 
+// Propagator product of the x pass at column ix (kx2 = fl(kx*kx) there) of
+// row iy (ky2 = fl(ky*ky)): FP64 forms the reference's argument
+// fl(a * fl(kx2 + ky2)) and its sin/cos (src/fftSolver3D.cpp:24-30); FP32
+// multiplies by the split x and y factors of the propagator.
+__device__ __forceinline__ double2 prop3(const Fft3dPass &q, double2 u, double kx2, double ky2,
+                                         int, int) {
+  const double phi = __dmul_rn(q.a, __dadd_rn(kx2, ky2));
+  double sn, cs;
+  sincos_cw(phi, &sn, &cs);
+  return cx_mul_rn(u, mk(cs, -sn));
+}
+__device__ __forceinline__ float2 prop3(const Fft3dPass &q, float2 u, double, double, int ix,
+                                        int iy) {
+  const float4 *px = reinterpret_cast<const float4 *>(q.prop_x);
+  const float4 *py = reinterpret_cast<const float4 *>(q.prop_y);
+  return tw_mul(tw_mul(u, __ldg(px + ix)), __ldg(py + iy));
+}
+
 template <typename R> __device__ __forceinline__ typename Cx<R>::T mul_k(typename Cx<R>::T u,
                                                                         double2 k);
 template <> __device__ __forceinline__ double2 mul_k<double>(double2 u, double2 k) {

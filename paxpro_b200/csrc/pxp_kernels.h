@@ -301,6 +301,11 @@ struct Fft3dPass {
   // damping length per axis (0 thickness = off)
   int thick_x, thick_y;
   double inv_damp_x, inv_damp_y;
+  // FP32 served mode: the propagator as the product of its x and y factors,
+  // prop_x[i] = exp(-i a kx_i^2) and prop_y[i] = exp(-i a ky_i^2) (n split
+  // complex64 entries each, phases reduced on the host in extended
+  // precision); FP64 mode evaluates the reference's joint argument instead
+  const void *prop_x, *prop_y;
 };
 // variant: 0 = radix 8, double-buffered, tables in shared memory; 1 = radix
 // 8, single buffer, tables through L1; 2 = radix 16, single buffer; 3 =
