@@ -2309,6 +2309,17 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
     Key k{h->prob.kind, (int)h->nx, (int)h->prec, h->prob.kind == PXP_CRANK_NICHOLSON ? (int)cn_uses_const(h) : 0};
     groups[k].push_back(h);
   }
+  // Within a group the CTA index follows the job order, and the block
+  // scheduler starts CTAs in index order as SMs free up: with the jobs that
+  // have the most steps this round first (longest processing time first),
+  // a launch with more jobs than resident CTAs fills the freed slots with
+  // the shorter jobs and ends close to the longest job's time.
+  for (auto &g : groups)
+    std::stable_sort(g.second.begin(), g.second.end(),
+                     [max_steps](const pxp_solver_s *a, const pxp_solver_s *c) {
+                       return std::min(a->batch_remaining, max_steps) >
+                              std::min(c->batch_remaining, max_steps);
+                     });
   size_t total = 0;
   for (auto &g : groups)
     total += g.second.size() * (g.first.kind == PXP_FFT_SOLVER_2D ? sizeof(pxp::Fft1dJob) : sizeof(pxp::CnJob));
