@@ -892,7 +892,7 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
 // field (one untimed x+y pass pair, then three timed ones; the fastest kept),
 // and every solver with that key runs the winner from its first step on, so
 // a field never depends on when tuning happened (radix 8 and radix 16 round
-// differently).  PXP_FFT3D_VARIANT=0|1|2|3 pins the variant instead.
+// differently).  PXP_FFT3D_VARIANT=0..4 pins the variant instead.
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, int, unsigned>, int> g_fft3d_variant;
 

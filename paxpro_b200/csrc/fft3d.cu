@@ -302,6 +302,10 @@ cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, cons
     if (fft3d_lines_supported(p, q.n) && wn != nullptr) return launch_fft3d_lines(p, q, kx2, wn, s);
     variant = 0;
   }
+  if (variant == 4) {
+    if (fft3d_r16_supported(p, q.n) && wn != nullptr) return launch_fft3d_r16(p, q, kx2, wn, s);
+    variant = 0;
+  }
 #define PXP_C3(NN)                                                                  \
   case NN:                                                                          \
     return p == kFP64 ? fft3d_launch_n<double, NN>(q, variant, kx2, tw16, s) \

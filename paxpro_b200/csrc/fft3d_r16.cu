@@ -1,0 +1,325 @@
+// fft3d_r16.cu -- FFTSolver3D line passes with 16 points per thread
+// (n = 512 .. 4096), two line slots per CTA.
+//
+// The step is the two-pass scheme of fft3d.cu (src/fftSolver3D.cpp:52-156):
+//   x pass (mode 1): lines of fixed y (stride n): F_x, * K(kx, ky), F_x^-1
+//   y pass (mode 2): contiguous lines of fixed x: F_y^-1, refraction, F_y
+// (mode 0: F_y only; mode 3: F_y^-1 and refraction only).  What this
+// variant changes is how much shared memory a transform moves, the resource
+// that bounds the register-resident line kernels:
+//
+//  * Thread j of a line slot holds the 16 points j + s*n/16 (s = 0..15) in
+//    registers.  A transform is a first pass of radix R0 = 16, 8, 4 or 2 on
+//    the thread's own points (n = R0 * 16^k; 16/R0 butterflies, no
+//    twiddles) and k radix-16 Stockham passes, so a 4096-point transform
+//    crosses shared memory twice (radix 8 needs three crossings).  The last
+//    pass leaves thread j with outputs j + r*n/16 in natural order, the
+//    first pass's inputs of the next transform: the forward and inverse
+//    transforms meet in registers, and lines are loaded from and stored to
+//    global memory straight from registers (no staging copy through shared
+//    memory).
+//  * An exchange element is 16 bytes: one complex128 point, or the same
+//    point of two adjacent lines in complex64 (a complex64 thread carries
+//    two lines, which also makes each strided x-pass access 16 contiguous
+//    bytes).  The exchange buffer is XOR-swizzled, element i at
+//    i ^ (((i >> 3) ^ (i >> 4)) & 7), so that every access of 8 consecutive
+//    threads -- the reads at stride 1, the first-pass writes at stride 16,
+//    8, 4 or 2, the radix-16 passes' writes -- hits 8 different 16-byte bank
+//    groups.
+//  * Twiddles come from a shared table in pass order (entry (r-1)*NS + k of
+//    the pass with sub-transform length NS), built once per CTA from the
+//    exp(-2 pi i m / n) table; a complex64 thread applies each twiddle to
+//    both of its lines.
+//  * A CTA holds two line slots with their own exchange buffers and named
+//    barriers, each walking its own sequence of lines: while one slot waits
+//    for its loads or a barrier, the other computes.  No copy is
+//    asynchronous, so nothing waits on an mbarrier.
+//
+// Per-point arithmetic (propagator, refraction, absorber, save) is
+// fft3d_point.cuh's, shared with the other FFTSolver3D kernels.  The
+// transforms round like the radix-16 variant of fft3d.cu up to the order of
+// their passes (within the parity tolerance); complex64 data compute in FP32
+// with split twiddles and constants (fft_smem.cuh).
+#include "fft3d_point.cuh"
+
+namespace pxp {
+namespace r16 {
+
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+
+template <typename R, int N> struct Cfg {
+  using C = typename Cx<R>::T;
+  static constexpr int TL = N / 16;                       // threads per slot
+  static constexpr int S = 2;                             // line slots per CTA
+  static constexpr int T = S * TL;                        // threads per CTA
+  static constexpr int LPT = sizeof(C) == 8 ? 2 : 1;      // lines per slot
+  static constexpr int LOG = ilog2c(N);
+  static constexpr int R0 = 1 << (LOG % 4 == 0 ? 4 : LOG % 4);
+  static constexpr int NP16 = (LOG - ilog2c(R0)) / 4;     // radix-16 passes
+  static constexpr int TWN = R0 * ((1 << (4 * NP16)) - 1);  // twiddle entries
+  static constexpr int GROUPS = N / LPT;                  // line groups per pass
+  static constexpr size_t XBYTES = 16 * (size_t)N;        // one slot's buffer
+  static constexpr size_t SMEM = S * XBYTES + 16 * (size_t)TWN;
+  // CTAs per SM: as many as shared memory holds, at most 128 registers a
+  // thread
+  static constexpr int SMEM_FIT = (int)((227 * 1024) / SMEM);
+  static constexpr int REG_FIT = 65536 / (T * 128);
+  static constexpr int MINB = SMEM_FIT < REG_FIT ? SMEM_FIT : REG_FIT;
+  static_assert(N % 16 == 0 && TL % 32 == 0, "whole warps per slot");
+};
+
+// Exchange-buffer position of element i (16-byte elements).
+__device__ __forceinline__ int xsw(int i) { return i ^ (((i >> 3) ^ (i >> 4)) & 7); }
+
+__device__ __forceinline__ void slot_sync(int slot, int count) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(1 + slot), "r"(count) : "memory");
+}
+
+// 16-byte exchange element of a thread's LPT lines at one position.
+template <typename C> struct Xe;
+template <> struct Xe<double2> {
+  using T = double2;
+  static __device__ __forceinline__ T pack(const double2 (&v)[1][16], int s) { return v[0][s]; }
+  static __device__ __forceinline__ void unpack(double2 (&v)[1][16], int s, T e) { v[0][s] = e; }
+};
+template <> struct Xe<float2> {
+  using T = float4;
+  static __device__ __forceinline__ T pack(const float2 (&v)[2][16], int s) {
+    return make_float4(v[0][s].x, v[0][s].y, v[1][s].x, v[1][s].y);
+  }
+  static __device__ __forceinline__ void unpack(float2 (&v)[2][16], int s, T e) {
+    v[0][s] = make_float2(e.x, e.y);
+    v[1][s] = make_float2(e.z, e.w);
+  }
+};
+
+// Offset of the twiddles of radix-16 pass P (sub-transform length
+// NS = R0 * 16^P) in the shared table.
+template <int R0, int P> __host__ __device__ constexpr int tw_offset() {
+  int off = 0, ns = R0;
+  for (int p = 0; p < P; ++p, ns *= 16) off += 15 * ns;
+  return off;
+}
+
+// Radix-16 passes P .. NP16-1 of a transform: read the pass's inputs
+// j + r*TL, twiddles W_{16 NS}^(r k) (k = j mod NS), 16-point DFT, write the
+// outputs to (j - k)*16 + k + r*NS -- except the last pass, which keeps
+// them in registers (natural order).
+template <int SIGN, typename R, int N, int P>
+__device__ __forceinline__ void r16_passes(typename Cx<R>::T (&v)[Cfg<R, N>::LPT][16],
+                                           typename Xe<typename Cx<R>::T>::T *X,
+                                           const Tw<typename Cx<R>::T> *tws, int slot, int j) {
+  using K = Cfg<R, N>;
+  using C = typename Cx<R>::T;
+  using E = Xe<C>;
+  if constexpr (P < K::NP16) {
+    constexpr int NS = K::R0 << (4 * P);
+    constexpr int OFF = tw_offset<K::R0, P>();
+    slot_sync(slot, K::TL);  // the writes of the previous pass are done
+#pragma unroll
+    for (int r = 0; r < 16; ++r) E::unpack(v, r, X[xsw(j + r * K::TL)]);
+    const int k = j & (NS - 1);
+#pragma unroll
+    for (int r = 1; r < 16; ++r) {
+      const Tw<C> w = tws[OFF + (r - 1) * NS + k];
+#pragma unroll
+      for (int t = 0; t < K::LPT; ++t)
+        v[t][r] = SIGN < 0 ? tw_mul(v[t][r], w) : tw_mulc(v[t][r], w);
+    }
+#pragma unroll
+    for (int t = 0; t < K::LPT; ++t) dft16<SIGN>(v[t]);
+    if constexpr (P < K::NP16 - 1) {
+      slot_sync(slot, K::TL);  // every read of this pass is done
+      const int base = (j - k) * 16 + k;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) X[xsw(base + r * NS)] = E::pack(v, r);
+    }
+    r16_passes<SIGN, R, N, P + 1>(v, X, tws, slot, j);
+  }
+}
+
+// One transform of the thread's LPT lines, points v[t][s] = j + s*TL before
+// and after (natural order).  X: the slot's exchange buffer; every write to
+// it follows a barrier that ends the previous reads, every read follows the
+// barrier that ends the writes.
+template <int SIGN, typename R, int N>
+__device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N>::LPT][16],
+                                         typename Xe<typename Cx<R>::T>::T *X,
+                                         const Tw<typename Cx<R>::T> *tws, int slot, int j) {
+  using K = Cfg<R, N>;
+  using C = typename Cx<R>::T;
+  using E = Xe<C>;
+  constexpr int TL = K::TL, R0 = K::R0;
+  // first pass: radix R0 over the thread's own points; butterfly
+  // b = j + u*TL takes points s = u + r*(16/R0) and writes b*R0 + r
+#pragma unroll
+  for (int t = 0; t < K::LPT; ++t) {
+    if constexpr (R0 == 16) {
+      dft16<SIGN>(v[t]);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 16 / R0; ++u) {
+        C w[R0];
+#pragma unroll
+        for (int r = 0; r < R0; ++r) w[r] = v[t][u + r * (16 / R0)];
+        dft_r<R0, SIGN>(w);
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[t][u + r * (16 / R0)] = w[r];
+      }
+    }
+  }
+  slot_sync(slot, TL);  // the previous reads of X are done
+#pragma unroll
+  for (int u = 0; u < 16 / R0; ++u)
+#pragma unroll
+    for (int r = 0; r < R0; ++r) X[xsw((j + u * TL) * R0 + r)] = E::pack(v, u + r * (16 / R0));
+  r16_passes<SIGN, R, N, 0>(v, X, tws, slot, j);
+}
+
+template <typename R, int N>
+__global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
+    fft3d_r16_kernel(const Fft3dPass q, const double *__restrict__ gkx2,
+                     const Tw<typename Cx<R>::T> *__restrict__ wn) {
+  using K = Cfg<R, N>;
+  using C = typename Cx<R>::T;
+  using E = Xe<C>;
+  using W = Tw<C>;
+  constexpr int TL = K::TL, LPT = K::LPT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x;
+  const int slot = tid / TL, j = tid % TL;
+  typename E::T *X = reinterpret_cast<typename E::T *>(smem_raw + slot * K::XBYTES);
+  W *tws = reinterpret_cast<W *>(smem_raw + K::S * K::XBYTES);
+  // twiddles of every radix-16 pass: entry off + (r-1)*NS + k = W_{16 NS}^(r k)
+  {
+    int off = 0;
+    for (int ns = K::R0; ns < N; off += 15 * ns, ns *= 16)
+      for (int i = tid; i < 15 * ns; i += K::T) {
+        const int r = i / ns + 1, k = i % ns;
+        tws[off + i] = wn[r * k * (N / (16 * ns))];
+      }
+  }
+  __syncthreads();
+  // the field is read only after the previous kernel in the stream is done
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+
+  const bool xpass = q.mode == 1;
+  C *field = reinterpret_cast<C *>(q.field);
+  C *save = reinterpret_cast<C *>(q.save);
+  const double inv_norm = 1.0 / q.norm;  // n*n is a power of two: exact
+  const int nslots = gridDim.x * K::S;
+  for (int g = blockIdx.x * K::S + slot; g < K::GROUPS; g += nslots) {
+    const int line0 = g * LPT;
+    C v[LPT][16];
+    // load: x lines are columns (element e of line l at e*N + l; a complex64
+    // thread's two lines are adjacent), y lines are rows
+#pragma unroll
+    for (int s = 0; s < 16; ++s) {
+      const int e = j + s * TL;
+      if (xpass) {
+        E::unpack(v, s, *reinterpret_cast<const typename E::T *>(field + (long long)e * N + line0));
+      } else {
+#pragma unroll
+        for (int t = 0; t < LPT; ++t) v[t][s] = field[(long long)(line0 + t) * N + e];
+      }
+    }
+    if (xpass) {
+      line_fft<-1, R, N>(v, X, tws, slot, j);
+      // propagator K = exp(-i a (kx^2 + ky^2)) (src/fftSolver3D.cpp:24-30, 87-120)
+#pragma unroll
+      for (int t = 0; t < LPT; ++t) {
+        const int line = line0 + t;  // y index
+        double ky2 = 0.0;
+        if constexpr (sizeof(R) == 8) {
+          const double ky = kfreq(line, N, q.two_pi, q.stepn_y);
+          ky2 = __dmul_rn(ky, ky);
+        }
+#pragma unroll
+        for (int s = 0; s < 16; ++s) {
+          const int e = j + s * TL;
+          v[t][s] = prop3(q, v[t][s], sizeof(R) == 8 ? __ldg(gkx2 + e) : 0.0, ky2, e, line);
+        }
+      }
+      line_fft<+1, R, N>(v, X, tws, slot, j);
+    } else {
+      if (q.mode >= 2) {
+        line_fft<+1, R, N>(v, X, tws, slot, j);
+#pragma unroll
+        for (int t = 0; t < LPT; ++t) {
+          const int line = line0 + t;  // x index
+#pragma unroll
+          for (int s = 0; s < 16; ++s) {
+            const int e = j + s * TL;  // y index
+            v[t][s] = refract3<R>(q, v[t][s], line, e, inv_norm);
+            if (save) save[(long long)line * N + e] = v[t][s];
+          }
+        }
+      }
+      if (q.mode != 3) line_fft<-1, R, N>(v, X, tws, slot, j);
+    }
+#pragma unroll
+    for (int s = 0; s < 16; ++s) {
+      const int e = j + s * TL;
+      if (xpass) {
+        *reinterpret_cast<typename E::T *>(field + (long long)e * N + line0) = E::pack(v, s);
+      } else {
+#pragma unroll
+        for (int t = 0; t < LPT; ++t) field[(long long)(line0 + t) * N + e] = v[t][s];
+      }
+    }
+  }
+}
+
+template <typename R, int N>
+cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaStream_t s) {
+  using K = Cfg<R, N>;
+  using W = Tw<typename Cx<R>::T>;
+  static_assert(K::SMEM <= 227 * 1024, "line slots exceed shared memory");
+  auto k = fft3d_r16_kernel<R, N>;
+  {
+    const cudaError_t e = raise_dynamic_smem((const void *)k, (int)K::SMEM);
+    if (e != cudaSuccess) return e;
+  }
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, K::T, K::SMEM);
+  if (e != cudaSuccess) return e;
+  if (per < 1) per = 1;
+  const int ctas = (K::GROUPS + K::S - 1) / K::S;
+  const int grid = ctas < sms * per ? ctas : sms * per;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(K::T);
+  cfg.dynamicSmemBytes = K::SMEM;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, q, kx2, reinterpret_cast<const W *>(wnv));
+}
+
+}  // namespace r16
+
+bool fft3d_r16_supported(Precision p, int n) {
+  (void)p;
+  return n >= 512 && n <= 4096 && !(n & (n - 1));
+}
+
+cudaError_t launch_fft3d_r16(Precision p, const Fft3dPass &q, const double *kx2, const void *wn,
+                             cudaStream_t s) {
+#define PXP_R16(NN)                                                                     \
+  case NN:                                                                              \
+    return p == kFP64 ? r16::launch<double, NN>(q, kx2, wn, s) : r16::launch<float, NN>(q, kx2, wn, s);
+  switch (q.n) {
+    PXP_R16(512) PXP_R16(1024) PXP_R16(2048) PXP_R16(4096)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef PXP_R16
+}
+
+}  // namespace pxp

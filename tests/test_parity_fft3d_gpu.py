@@ -155,12 +155,15 @@ def _variant(monkeypatch):
 
 @pytest.mark.parametrize("n", [64, 128, 256, 512, 1024, 2048])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_fft3d_register_line_kernel_every_size(n, precision, _variant):
-    """Variant 3 (register-resident transforms, TMA-staged lines) at every
-    size it takes, FP64 and FP32: spheres crossing the sampling planes (the
-    refraction integral at their rims), the absorber, saves, and calls split
-    in chunks (the forward-only and inverse-only passes at call ends)."""
-    _variant(3)
+@pytest.mark.parametrize("variant", [3, 4])
+def test_fft3d_register_line_kernel_every_size(n, precision, variant, _variant):
+    """The register-resident line kernels -- variant 3 (8 points a thread,
+    TMA-staged lines) and variant 4 (16 points a thread, radix-16 passes, two
+    line slots a CTA; from 512 points) -- at every size they take, FP64 and
+    FP32: spheres crossing the sampling planes (the refraction integral at
+    their rims), the absorber, saves, and calls split in chunks (the
+    forward-only and inverse-only passes at call ends)."""
+    _variant(variant)
     sph = [(20.0, 10.0, 2500.0, 200.0, 3e-5, 6e-7), (-150.0, 120.0, 4100.0, 90.0, 2e-5, 4e-7)]
     out, saves, ref_out, ref_saves = _run_both(n, 1000.0, 0.0, 1000.0, 6, sph, save_every=2,
                                                chunks=2, precision=precision,
@@ -175,8 +178,9 @@ def test_fft3d_register_line_kernel_every_size(n, precision, _variant):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_fft3d_register_line_kernel_4096(precision, _variant):
-    _variant(3)
+@pytest.mark.parametrize("variant", [3, 4])
+def test_fft3d_register_line_kernel_4096(precision, variant, _variant):
+    _variant(variant)
     p = wl.spheres_fft3d()
     near = [s for s in p.spheres if s[2] + s[3] >= 86000.0 and s[2] - s[3] <= 92000.0]
     assert near  # step 44 of the workload samples a sphere
