@@ -62,6 +62,7 @@ struct pxp_solver_s {
   int save_every = 0;
   // FFT 1-D tables
   void *d_kern = nullptr, *d_trans = nullptr, *d_tw = nullptr;
+  void *d_wn = nullptr;  // exp(-2 pi i m / n) (shared table, not owned)
   void *d_chirp = nullptr, *d_bconv = nullptr;  // Bluestein tables (shared, not owned)
   long long trans_stride = 0;
   int trans_step0 = 1;
@@ -466,6 +467,7 @@ int fft1d_setup(pxp_solver_s *h) {
   } else if ((rc = shared_table(h, 0, &h->d_tw))) {
     return rc;
   }
+  if (pxp::fft1d_r16_enabled((int)h->nx) && (rc = shared_table(h, 4, &h->d_wn))) return rc;
   return alloc(h, &h->d_job, sizeof(pxp::Fft1dJob), "job descriptor");
 }
 
@@ -509,6 +511,7 @@ int fft1d_write_job(pxp_solver_s *h) {
   j.chirp = h->d_chirp;
   j.bconv = h->d_bconv;
   j.m = pxp::fft1d_bluestein_m((int)h->nx);
+  j.wn = h->d_wn;
   h->job_fft = j;
   if (int rc_ = h2d(h, h->d_job, &j, sizeof(j))) return rc_;
   return PXP_OK;
@@ -1284,6 +1287,7 @@ int pxp_solver_destroy(pxp_solver h) {
   h->d_kern = nullptr;  // shared table, not owned
   free_dev(h->d_trans, h->stream);
   h->d_tw = nullptr;  // shared table, not owned
+  h->d_wn = nullptr;  // shared table, not owned
   free_dev(h->d_mat, h->stream);
   free_dev(h->d_planes3, h->stream);
   free_dev(h->d_job, h->stream);

@@ -224,6 +224,7 @@ cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n, int
   if (nj <= 0) return cudaSuccess;
   if (n & (n - 1)) return launch_bluestein(p, d_jobs, nj, n, step0, nsteps, s, flux);
   if (fft1d_pair_size(p, n)) return launch_fft1d_pair(p, d_jobs, nj, n, step0, nsteps, s, flux);
+  if (fft1d_r16_enabled(n)) return launch_fft1d_r16(p, d_jobs, nj, n, step0, nsteps, s, flux);
 #define PXP_CASE(NN)                                                              \
   case NN:                                                                        \
     return p == kFP64 ? launch_nf<double, NN>(d_jobs, nj, step0, nsteps, s, flux)     \

@@ -41,11 +41,12 @@
 // their passes (within the parity tolerance); complex64 data compute in FP32
 // with split twiddles and constants (fft_smem.cuh).
 #include "fft3d_point.cuh"
+#include "fft_r16.cuh"
 
 namespace pxp {
 namespace r16 {
 
-__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+using r16c::tw_offset;
 
 template <typename R, int N> struct Cfg {
   using C = typename Cx<R>::T;
@@ -53,10 +54,9 @@ template <typename R, int N> struct Cfg {
   static constexpr int S = 2;                             // line slots per CTA
   static constexpr int T = S * TL;                        // threads per CTA
   static constexpr int LPT = sizeof(C) == 8 ? 2 : 1;      // lines per slot
-  static constexpr int LOG = ilog2c(N);
-  static constexpr int R0 = 1 << (LOG % 4 == 0 ? 4 : LOG % 4);
-  static constexpr int NP16 = (LOG - ilog2c(R0)) / 4;     // radix-16 passes
-  static constexpr int TWN = R0 * ((1 << (4 * NP16)) - 1);  // twiddle entries
+  static constexpr int R0 = r16c::Plan<N>::R0;             // first-pass radix
+  static constexpr int NP16 = r16c::Plan<N>::NP16;         // radix-16 passes
+  static constexpr int TWN = r16c::Plan<N>::TWN;           // twiddle entries
   static constexpr int GROUPS = N / LPT;                  // line groups per pass
   static constexpr size_t XBYTES = 16 * (size_t)N;        // one slot's buffer
   static constexpr size_t SMEM = S * XBYTES + 16 * (size_t)TWN;
@@ -69,7 +69,7 @@ template <typename R, int N> struct Cfg {
 };
 
 // Exchange-buffer position of element i (16-byte elements).
-__device__ __forceinline__ int xsw(int i) { return i ^ (((i >> 3) ^ (i >> 4)) & 7); }
+__device__ __forceinline__ int xsw(int i) { return r16c::xsw16(i); }
 
 __device__ __forceinline__ void slot_sync(int slot, int count) {
   asm volatile("bar.sync %0, %1;\n" ::"r"(1 + slot), "r"(count) : "memory");
@@ -93,13 +93,6 @@ template <> struct Xe<float2> {
   }
 };
 
-// Offset of the twiddles of radix-16 pass P (sub-transform length
-// NS = R0 * 16^P) in the shared table.
-template <int R0, int P> __host__ __device__ constexpr int tw_offset() {
-  int off = 0, ns = R0;
-  for (int p = 0; p < P; ++p, ns *= 16) off += 15 * ns;
-  return off;
-}
 
 // Radix-16 passes P .. NP16-1 of a transform: read the pass's inputs
 // j + r*TL, twiddles W_{16 NS}^(r k) (k = j mod NS), 16-point DFT, write the
@@ -153,21 +146,7 @@ __device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N>::LPT][
   // first pass: radix R0 over the thread's own points; butterfly
   // b = j + u*TL takes points s = u + r*(16/R0) and writes b*R0 + r
 #pragma unroll
-  for (int t = 0; t < K::LPT; ++t) {
-    if constexpr (R0 == 16) {
-      dft16<SIGN>(v[t]);
-    } else {
-#pragma unroll
-      for (int u = 0; u < 16 / R0; ++u) {
-        C w[R0];
-#pragma unroll
-        for (int r = 0; r < R0; ++r) w[r] = v[t][u + r * (16 / R0)];
-        dft_r<R0, SIGN>(w);
-#pragma unroll
-        for (int r = 0; r < R0; ++r) v[t][u + r * (16 / R0)] = w[r];
-      }
-    }
-  }
+  for (int t = 0; t < K::LPT; ++t) r16c::first_pass<SIGN, R0>(v[t]);
   slot_sync(slot, TL);  // the previous reads of X are done
 #pragma unroll
   for (int u = 0; u < 16 / R0; ++u)
@@ -191,14 +170,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
   typename E::T *X = reinterpret_cast<typename E::T *>(smem_raw + slot * K::XBYTES);
   W *tws = reinterpret_cast<W *>(smem_raw + K::S * K::XBYTES);
   // twiddles of every radix-16 pass: entry off + (r-1)*NS + k = W_{16 NS}^(r k)
-  {
-    int off = 0;
-    for (int ns = K::R0; ns < N; off += 15 * ns, ns *= 16)
-      for (int i = tid; i < 15 * ns; i += K::T) {
-        const int r = i / ns + 1, k = i % ns;
-        tws[off + i] = wn[r * k * (N / (16 * ns))];
-      }
-  }
+  r16c::load_twiddles<N>(tws, wn, tid, K::T);
   __syncthreads();
   // the field is read only after the previous kernel in the stream is done
   asm volatile("griddepcontrol.wait;\n" ::: "memory");

@@ -32,13 +32,14 @@ struct FluxSpec {
 
 struct Fft1dJob {
   void *field;             // N complex: field after the previous step
-  const void *kern;        // N complex128: propagator exp(-i (dz/2k) kx^2)
-  const void *trans;       // N complex128 per table: transmission (FP64: t,
-                           // applied as (u*t)/N; FP32: t/N, applied as u*t
-                           // with the product formed in FP64)
+  // Constant-factor tables hold complex128 entries in FP64 and split
+  // complex64 pairs (fft_smem.cuh) in FP32.
+  const void *kern;        // N entries: propagator exp(-i (dz/2k) kx^2)
+  const void *trans;       // N entries per table: transmission (FP64: t,
+                           // applied as (u*t)/N; FP32: t/N, applied as u*t)
   long long trans_stride;  // complex elements between per-step tables; 0 =
                            // z-invariant medium (one table)
-  const void *twiddle;     // N complex128: exp(-2 pi i m/N)
+  const void *twiddle;     // N entries: radix-8 Stockham twiddles (pass order)
   void *saves;             // save slots, N complex each (may be null)
   int n;                   // transverse points (power of two)
   int step0;               // 1-based index of the first step of this launch
@@ -54,11 +55,19 @@ struct Fft1dJob {
   const void *chirp;
   const void *bconv;
   int m;
+  // powers of two 512 .. 4096 (fft1d_r16.cu): N entries exp(-2 pi i m / N)
+  const void *wn;
 };
 
 // Launch nj jobs that all share one transform length n (one CTA per job).
 // step0/nsteps >= 0 override every job's own values (single-problem use).
 // flux: some job has flux windows (the kernel variant that sums them).
+// Register-resident radix-16 FFTSolver2D kernel (fft1d_r16.cu): whether it
+// runs size n (powers of two 512 .. 4096; PXP_FFT1D_R16=0 selects the
+// shared-memory kernel instead), and its launch.
+bool fft1d_r16_enabled(int n);
+cudaError_t launch_fft1d_r16(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
+                             int nsteps, cudaStream_t s, bool flux);
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n,
                          int step0, int nsteps, cudaStream_t s, bool flux = false);
 bool fft1d_supported(Precision p, int n);
