@@ -170,6 +170,7 @@ std::vector<cd> twiddles(int n, int maxr = 8) {
   int off = 0;
   for (int ns = 1; ns < n;) {
     const int r = n / ns >= maxr ? maxr : (n / ns >= 8 ? 8 : n / ns);
+    if (r < 2) break;  // n not a power of two: no further pass divides it
     for (int q = 1; q < r; ++q)
       for (int k = 0; k < ns; ++k) {
         long double a = -2.0L * pi_l * (long double)(q * k) / (long double)(ns * r);
@@ -993,8 +994,10 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   }
   void *kx2 = nullptr, *tw16 = nullptr, *wn = nullptr;
   if (int rc = shared_table(h, 2, &kx2)) return rc;
-  if (int rc = shared_table(h, 3, &tw16)) return rc;
-  if (int rc = shared_table(h, 4, &wn)) return rc;
+  if (!(n & (n - 1))) {  // the power-of-two variants' twiddle tables
+    if (int rc = shared_table(h, 3, &tw16)) return rc;
+    if (int rc = shared_table(h, 4, &wn)) return rc;
+  }
   if (h->prec == pxp::kFP32) {
     void *px = nullptr, *py = nullptr;
     if (int rc = prop3_table(h, 0, &px)) return rc;
