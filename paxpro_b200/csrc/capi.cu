@@ -965,6 +965,105 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
   return PXP_OK;
 }
 
+// Launch-variant tuner of the 2-D step kernels: FFTSolver2D at 512..4096
+// points (shared-memory Stockham kernel or register-resident radix-16
+// kernel) and CrankNicholson's step-invariant path at 4096 rows (one CTA or
+// a cluster of two).  As for FFTSolver3D, the first solver with a given
+// (device, precision, kind, size) times every variant on a scratch copy of
+// its own job (zeroed field; no saves, flux sums or per-step tables; 64
+// steps, one untimed launch and three timed, the fastest kept) and every
+// solver with that key -- alone or in a batch -- runs the winner from its
+// first step, so a field never depends on when tuning ran (the variants
+// agree within the FP64 tolerance, not bit for bit).  PXP_FFT1D_R16=0|1 and
+// PXP_CN_CLUSTER=0|1 pin the variant instead.
+std::map<std::tuple<int, int, int, unsigned>, int> g_2d_variant;
+
+bool cn_uses_const(const pxp_solver_s *h);
+
+int variant_2d(pxp_solver_s *h, int *out) {
+  *out = -1;
+  const bool fft = h->prob.kind == PXP_FFT_SOLVER_2D;
+  if (!fft && !(h->prob.kind == PXP_CRANK_NICHOLSON && cn_uses_const(h))) return PXP_OK;
+  const int n = fft ? (int)h->nx : pxp::cn_padded_n((int)h->nx);
+  const int nv = fft ? pxp::fft1d_variants(h->prec, n) : pxp::cn_const_variants(h->prec, n);
+  if (nv < 2) return PXP_OK;
+  if (const char *env = std::getenv(fft ? "PXP_FFT1D_R16" : "PXP_CN_CLUSTER")) {
+    if (env[0] == '0' || env[0] == '1') {
+      *out = env[0] - '0';
+      return PXP_OK;
+    }
+  }
+  const auto key = std::make_tuple(h->prob.device, (int)h->prec, (int)h->prob.kind, (unsigned)n);
+  std::lock_guard<std::mutex> lk(g_tune_mutex);
+  auto it = g_2d_variant.find(key);
+  if (it != g_2d_variant.end()) {
+    *out = it->second;
+    return PXP_OK;
+  }
+  const size_t job_bytes = fft ? sizeof(pxp::Fft1dJob) : sizeof(pxp::CnJob);
+  const size_t field_bytes = h->csize * (size_t)n;
+  void *scratch = nullptr, *djob = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, field_bytes, h->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&djob, job_bytes, h->stream);
+  if (e != cudaSuccess) {
+    if (scratch) cudaFreeAsync(scratch, h->stream);
+    return h->cuda_fail(e, "2-D kernel tuning scratch");
+  }
+  pxp::Fft1dJob jf = h->job_fft;
+  pxp::CnJob jc = h->job_cn;
+  if (fft) {
+    jf.field = scratch;
+    jf.saves = nullptr;
+    jf.save_every = 0;
+    jf.trans_stride = 0;
+    jf.flux = pxp::FluxSpec{};
+  } else {
+    jc.field = scratch;
+    jc.saves = nullptr;
+    jc.save_every = 0;
+    jc.flux = pxp::FluxSpec{};
+  }
+  e = cudaMemsetAsync(scratch, 0, field_bytes, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(djob, fft ? (const void *)&jf : (const void *)&jc, job_bytes,
+                        cudaMemcpyHostToDevice, h->stream);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  int best_v = 0;
+  float best = 1e30f;
+  constexpr int kTuneSteps = 64;
+  for (int v = 0; v < nv && e == cudaSuccess; ++v) {
+    float tmin = 1e30f;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+      cudaEventRecord(e0, h->stream);
+      e = fft ? pxp::launch_fft1d(h->prec, (const pxp::Fft1dJob *)djob, 1, n, 1, kTuneSteps,
+                                  h->stream, false, v)
+              : pxp::launch_cn_const(h->prec, (const pxp::CnJob *)djob, 1, n, 1, kTuneSteps,
+                                     h->stream, false, v);
+      cudaEventRecord(e1, h->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+        tmin = std::min(tmin, ms);
+    }
+    if (tmin < best) {
+      best = tmin;
+      best_v = v;
+    }
+  }
+  // the job descriptor must stay valid until the launches that read it ran
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFreeAsync(djob, h->stream);
+  cudaFreeAsync(scratch, h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "2-D kernel tuning");
+  g_2d_variant[key] = best_v;
+  *out = best_v;
+  return PXP_OK;
+}
+
 int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   const pxp_problem &p = h->prob;
   const int n = (int)h->nx;
@@ -1613,20 +1712,26 @@ int pxp_step(pxp_solver h, int nsteps) {
                                         " are outside the material planes provided");
   cudaError_t e = cudaSuccess;
   switch (h->prob.kind) {
-    case PXP_FFT_SOLVER_2D:
+    case PXP_FFT_SOLVER_2D: {
+      int v = -1;
+      if (int rc = variant_2d(h, &v)) return rc;
       e = pxp::launch_fft1d(h->prec, (const pxp::Fft1dJob *)h->d_job, 1, (int)h->nx,
-                            (int)first, nsteps, h->stream, h->flux_count > 0);
+                            (int)first, nsteps, h->stream, h->flux_count > 0, v);
       break;
+    }
     case PXP_CRANK_NICHOLSON:
       if (!(h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0) &&
           !pxp::cn_supported(h->prec, (int)h->nx))
         return h->fail(PXP_ERR_UNSUPPORTED,
                        "CrankNicholson at " + std::to_string(h->nx) +
                            " points runs with a z-invariant medium and Dirichlet ends only");
-      if (h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0)
+      if (h->cn_const && !h->prob.transparent_bc && h->mat_stride == 0) {
+        int v = -1;
+        if (int rc = variant_2d(h, &v)) return rc;
         e = pxp::launch_cn_const(h->prec, (const pxp::CnJob *)h->d_job, 1,
                                  pxp::cn_padded_n((int)h->nx), (int)first, nsteps, h->stream,
-                                 h->flux_count > 0);
+                                 h->flux_count > 0, v);
+      }
       else
         e = pxp::launch_cn(h->prec, (const pxp::CnJob *)h->d_job, 1, pxp::cn_padded_n((int)h->nx),
                            (int)first, nsteps, h->stream, h->flux_count > 0);
@@ -2327,6 +2432,15 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
                        return std::min(a->batch_remaining, max_steps) >
                               std::min(c->batch_remaining, max_steps);
                      });
+  // each group's kernel variant, the one every solver of its key runs alone
+  // (tuned here, before this round launches anything, if no solver of the
+  // key has stepped yet)
+  std::vector<int> gvariant;
+  for (auto &g : groups) {
+    int v = -1;
+    if (int rc = variant_2d(g.second.front(), &v)) return b->fail(rc, g.second.front()->err);
+    gvariant.push_back(v);
+  }
   size_t total = 0;
   for (auto &g : groups)
     total += g.second.size() * (g.first.kind == PXP_FFT_SOLVER_2D ? sizeof(pxp::Fft1dJob) : sizeof(pxp::CnJob));
@@ -2388,13 +2502,14 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
     const void *jobs = (const char *)b->d_jobs + o.first;
     bool any_flux = false;
     for (const pxp_solver_s *h : list) any_flux = any_flux || h->flux_count > 0;
+    const int variant = gvariant[gi];
     cudaError_t e;
     if (k.kind == PXP_FFT_SOLVER_2D)
       e = pxp::launch_fft1d((pxp::Precision)k.prec, (const pxp::Fft1dJob *)jobs, (int)list.size(),
-                            k.n, -1, -1, gst, any_flux);
+                            k.n, -1, -1, gst, any_flux, variant);
     else if (k.cpath)
       e = pxp::launch_cn_const((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
-                               pxp::cn_padded_n(k.n), -1, -1, gst, any_flux);
+                               pxp::cn_padded_n(k.n), -1, -1, gst, any_flux, variant);
     else
       e = pxp::launch_cn((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
                          pxp::cn_padded_n(k.n), -1, -1, gst, any_flux);

@@ -470,10 +470,10 @@ static cudaError_t cn_const_launch_t(const CnJob *d_jobs, int nj, int step0, int
               : cn_const_launch_f<R, M, T, false>(d_jobs, nj, step0, nsteps, s);
 }
 
-template <typename R, int K, bool FLUX>
+template <typename R, int M, int T, int K, bool FLUX>
 static cudaError_t cn_cluster_launch_f(const CnJob *d_jobs, int nj, int step0, int nsteps,
                                        cudaStream_t s) {
-  constexpr int M = 16, T = 256, NC = M * T;
+  constexpr int NC = M * T;
   constexpr size_t smem = sizeof(double2) * (3 * NC + 2 * T) + sizeof(Affine) * (T / 32 + 1);
   auto k = cn_const_cluster_kernel<R, M, T, K, FLUX>;
   {
@@ -495,19 +495,25 @@ static cudaError_t cn_cluster_launch_f(const CnJob *d_jobs, int nj, int step0, i
   return cudaLaunchKernelEx(&cfg, k, d_jobs, step0, nsteps);
 }
 
-template <typename R, int K>
+template <typename R, int K, int M = 16, int T = 256>
 static cudaError_t cn_cluster_launch_t(const CnJob *d_jobs, int nj, int step0, int nsteps,
                                        cudaStream_t s, bool flux) {
-  return flux ? cn_cluster_launch_f<R, K, true>(d_jobs, nj, step0, nsteps, s)
-              : cn_cluster_launch_f<R, K, false>(d_jobs, nj, step0, nsteps, s);
+  return flux ? cn_cluster_launch_f<R, M, T, K, true>(d_jobs, nj, step0, nsteps, s)
+              : cn_cluster_launch_f<R, M, T, K, false>(d_jobs, nj, step0, nsteps, s);
 }
+
+// 4096 rows on a cluster of two CTAs (2048 rows each) is variant 1: the
+// single-CTA step is bound by one SM's FP64 issue rate (about 36 FP64
+// operations a row) and its scans' latency, the pair halves the first and
+// adds two cluster barriers a step.
+int cn_const_variants(Precision, int n) { return n == 4096 ? 2 : 1; }
 
 bool cn_const_supported(Precision, int n) {
   return n >= 8 * kCnM && !(n & (n - 1)) && n <= 16384;  // 8192, 16384: clusters of 2, 4
 }
 
 cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0, int nsteps,
-                            cudaStream_t s, bool flux) {
+                            cudaStream_t s, bool flux, int variant) {
   if (nj <= 0) return cudaSuccess;
   if (n == 8192)
     return p == kFP64 ? cn_cluster_launch_t<double, 2>(d_jobs, nj, step0, nsteps, s, flux)
@@ -518,6 +524,9 @@ cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int
   // n >= 2048: 16 rows per thread (half the threads of 8 rows: fewer warps
   // in each scan's barriers and shuffles; measured 4.07 -> 3.08 us per step
   // at n = 4096)
+  if (n == 4096 && variant == 1)
+    return p == kFP64 ? cn_cluster_launch_t<double, 2, 16, 128>(d_jobs, nj, step0, nsteps, s, flux)
+                      : cn_cluster_launch_t<float, 2, 16, 128>(d_jobs, nj, step0, nsteps, s, flux);
   if (n == 4096)
     return p == kFP64 ? cn_const_launch_t<double, 16, 256>(d_jobs, nj, step0, nsteps, s, flux)
                       : cn_const_launch_t<float, 16, 256>(d_jobs, nj, step0, nsteps, s, flux);

@@ -219,12 +219,17 @@ static cudaError_t launch_nf(const Fft1dJob *d_jobs, int nj, int step0, int nste
               : launch_n<R, N, false>(d_jobs, nj, step0, nsteps, s);
 }
 
+int fft1d_variants(Precision p, int n) {
+  return !fft1d_pair_size(p, n) && fft1d_r16_enabled(n) ? 2 : 1;
+}
+
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
-                         int nsteps, cudaStream_t s, bool flux) {
+                         int nsteps, cudaStream_t s, bool flux, int variant) {
   if (nj <= 0) return cudaSuccess;
   if (n & (n - 1)) return launch_bluestein(p, d_jobs, nj, n, step0, nsteps, s, flux);
   if (fft1d_pair_size(p, n)) return launch_fft1d_pair(p, d_jobs, nj, n, step0, nsteps, s, flux);
-  if (fft1d_r16_enabled(n)) return launch_fft1d_r16(p, d_jobs, nj, n, step0, nsteps, s, flux);
+  if (variant != 0 && fft1d_r16_enabled(n))
+    return launch_fft1d_r16(p, d_jobs, nj, n, step0, nsteps, s, flux);
 #define PXP_CASE(NN)                                                              \
   case NN:                                                                        \
     return p == kFP64 ? launch_nf<double, NN>(d_jobs, nj, step0, nsteps, s, flux)     \

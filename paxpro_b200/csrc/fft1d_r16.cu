@@ -153,13 +153,7 @@ cudaError_t launch(const Fft1dJob *d_jobs, int nj, int step0, int nsteps, cudaSt
 
 }  // namespace r16_1d
 
-bool fft1d_r16_enabled(int n) {
-  static const bool on = [] {
-    const char *e = std::getenv("PXP_FFT1D_R16");
-    return !(e && e[0] == '0');
-  }();
-  return on && n >= 512 && n <= 4096 && !(n & (n - 1));
-}
+bool fft1d_r16_enabled(int n) { return n >= 512 && n <= 4096 && !(n & (n - 1)); }
 
 cudaError_t launch_fft1d_r16(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
                              int nsteps, cudaStream_t s, bool flux) {

@@ -63,13 +63,21 @@ struct Fft1dJob {
 // step0/nsteps >= 0 override every job's own values (single-problem use).
 // flux: some job has flux windows (the kernel variant that sums them).
 // Register-resident radix-16 FFTSolver2D kernel (fft1d_r16.cu): whether it
-// runs size n (powers of two 512 .. 4096; PXP_FFT1D_R16=0 selects the
-// shared-memory kernel instead), and its launch.
+// takes size n (powers of two 512 .. 4096), and its launch.
 bool fft1d_r16_enabled(int n);
 cudaError_t launch_fft1d_r16(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
                              int nsteps, cudaStream_t s, bool flux);
+// Launch variants of the 2-D step kernels, chosen per (device, precision,
+// size) by the tuner in capi.cu: FFTSolver2D 0 = shared-memory Stockham
+// kernel, 1 = register-resident radix-16 kernel; CrankNicholson's
+// step-invariant path at 4096 rows 0 = one CTA, 1 = a cluster of two CTAs.
+// *_variants returns how many a size has (1: nothing to choose); variant
+// -1 is the default (the radix-16 kernel where it runs; one CTA).
+int fft1d_variants(Precision p, int n);
+int cn_const_variants(Precision p, int n);
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n,
-                         int step0, int nsteps, cudaStream_t s, bool flux = false);
+                         int step0, int nsteps, cudaStream_t s, bool flux = false,
+                         int variant = -1);
 bool fft1d_supported(Precision p, int n);
 // complex128 lines of 16384 points (fft1d_pair.cu): a cluster of two CTAs per
 // job, each holding the points of one parity; the job's twiddle is the
@@ -110,7 +118,7 @@ constexpr double kCnPad = 1e30;
 // z-invariant medium and Dirichlet ends: the step matrix never changes; the
 // job's lu_g / lu_h hold its Thomas factor tables (n complex128 each).
 cudaError_t launch_cn_const(Precision p, const CnJob *d_jobs, int nj, int n, int step0,
-                            int nsteps, cudaStream_t s, bool flux = false);
+                            int nsteps, cudaStream_t s, bool flux = false, int variant = -1);
 bool cn_const_supported(Precision p, int n);
 
 // ------------------------------------------------------------- ADI ------

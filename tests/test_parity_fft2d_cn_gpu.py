@@ -328,3 +328,52 @@ def test_cn_cluster_size_rejects_planes_and_transparent_ends():
         s.set_material_planes(d, d, 1, 3)  # z-varying: the general kernel would be needed
         s.set_initial_conditions(np.ones(n, dtype=np.complex128))
         assert _capi.lib().pxp_step(s._h, 1) == _capi.PXP_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("n", [512, 1024, 2048, 4096])
+@pytest.mark.parametrize("variant", ["0", "1"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fft2d_kernel_variants(n, variant, precision, monkeypatch):
+    """Both FFTSolver2D kernels the tuner chooses between at 512..4096
+    points -- the shared-memory Stockham kernel (PXP_FFT1D_R16=0) and the
+    register-resident radix-16 kernel (=1) -- with saves and chunked calls:
+    FP64 within 1e-10 of the oracle at every save, FP32
+    intensity within 1e-4 (over 600 steps)."""
+    monkeypatch.setenv("PXP_FFT1D_R16", variant)
+    nsteps = 60 if precision == 0 else 600
+    p = wl.Problem2D("t", "fft", -250.0, 250.0, wl.step_for_nodes(-250.0, 250.0, n),
+                     0.0, 1e6, 1000.0, nsteps, 15.0, wl.Waveguide())
+    d, b = p.material()
+    rng = np.random.default_rng(n)
+    u0 = p.initial_field() + 0.01 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, nsteps, nsteps // 3)
+    out, saves = _gpu_2d(p, d, b, u0, nsteps, nsteps // 3, precision, chunks=3)
+    assert len(saves) == len(ref_saves) == 3
+    if precision == 0:
+        assert max(_rel(g, r) for g, r in zip(saves, ref_saves)) <= FP64_TOL
+        assert _rel(out, ref_out) <= FP64_TOL
+    else:
+        assert max(_int_rel(g, r) for g, r in zip(saves, ref_saves)) <= FP32_INT_TOL
+
+
+@pytest.mark.parametrize("variant", ["0", "1"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_cn_4096_kernel_variants(variant, precision, monkeypatch):
+    """Both launches of CrankNicholson's step-invariant path at 4096 rows
+    the tuner chooses between: one CTA (PXP_CN_CLUSTER=0) and a cluster of
+    two CTAs exchanging the halo and the recurrences' carries through
+    distributed shared memory (=1); every save against the oracle."""
+    monkeypatch.setenv("PXP_CN_CLUSTER", variant)
+    nsteps = 200
+    p = wl.Problem2D("cn4096", "cn", -250.0, 250.0, wl.step_for_nodes(-250.0, 250.0, 4096), 0.0,
+                     1e6, 500.0, nsteps, 15.0, wl.Waveguide())
+    d, b = p.material()
+    u0 = p.initial_field()
+    out, saves = _gpu_2d(p, d, b, u0, nsteps, 50, precision, chunks=2)
+    ref_out, ref_saves = _oracle_2d(p, d, b, u0, nsteps, 50)
+    assert len(saves) == len(ref_saves) == 4
+    if precision == 0:
+        assert max(_rel(a, r) for a, r in zip(saves, ref_saves)) <= FP64_TOL
+        assert _rel(out, ref_out) <= FP64_TOL
+    else:
+        assert max(_int_rel(a, r) for a, r in zip(saves, ref_saves)) <= FP32_INT_TOL
