@@ -211,7 +211,7 @@ __device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N, LG>::L
 
 template <typename R, int N, int LG>
 __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
-    fft3d_lines_kernel(const Fft3dPass q, const __grid_constant__ CUtensorMap tmap,
+    fft3d_lines_kernel(const __grid_constant__ Fft3dPass q, const __grid_constant__ CUtensorMap tmap,
                        const double *__restrict__ gkx2,
                        const Tw<typename Cx<R>::T> *__restrict__ wn) {
   using K = Cfg<R, N, LG>;
@@ -257,6 +257,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
     for (int s = 0; s < 8; ++s) kx2[s] = gkx2[j + s * K::TL];
   }
   const double inv_norm = 1.0 / q.norm;  // n*n is a power of two: exact
+  const bool scale_only = refract3_is_scale(q, inv_norm);
   if (tid == 0) mbar_init(bar, 1);
   __syncthreads();
   // the field is read only after the previous kernel in the stream is done
@@ -333,15 +334,40 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
       line_fft<-1, R, N, LG>(v, X0, X1, cur, tw, tws, slot, j, issue_next);
     } else {
       line_fft<+1, R, N, LG>(v, X0, X1, cur, tw, tws, slot, j, issue_next);
+      if (scale_only) {
 #pragma unroll
-      for (int t = 0; t < K::LPT; ++t) {
-        const int line = line0 + slot * K::LPT + t;  // x index
+        for (int t = 0; t < K::LPT; ++t)
 #pragma unroll
-        for (int s = 0; s < 8; ++s) {
-          const int e = j + s * K::TL;  // y index
-          v[t][s] = refract3<R>(q, v[t][s], line, e, inv_norm);
-          if (save) save[(long long)line * N + e] = v[t][s];
+          for (int s = 0; s < 8; ++s) v[t][s] = scale_point(v[t][s], inv_norm);
+      } else {
+        // material or absorber in this step: the thread's own points go
+        // through the exchange buffer the last pass did not read (every
+        // thread is past its reads) and one non-unrolled refract3 loop; the
+        // barrier after it keeps the next transform's first writes to that
+        // buffer behind every thread's use of it
+        C *scr = (cur ? X0 : X1) + slot * K::LPT * K::XS;
+#pragma unroll
+        for (int t = 0; t < K::LPT; ++t)
+#pragma unroll
+          for (int s = 0; s < 8; ++s) scr[t * K::XS + j + s * K::TL] = v[t][s];
+#pragma unroll 1
+        for (int i = 0; i < 8 * K::LPT; ++i) {
+          const int t = i / 8, e = j + (i % 8) * K::TL;  // e: y index
+          C *p = scr + t * K::XS + e;
+          *p = refract3<R>(q, *p, line0 + slot * K::LPT + t, e, inv_norm);
         }
+#pragma unroll
+        for (int t = 0; t < K::LPT; ++t)
+#pragma unroll
+          for (int s = 0; s < 8; ++s) v[t][s] = scr[t * K::XS + j + s * K::TL];
+        __syncthreads();
+      }
+      if (save) {
+#pragma unroll
+        for (int t = 0; t < K::LPT; ++t)
+#pragma unroll
+          for (int s = 0; s < 8; ++s)
+            save[(long long)(line0 + slot * K::LPT + t) * N + j + s * K::TL] = v[t][s];
       }
       if (q.mode != 3) line_fft<-1, R, N, LG>(v, X0, X1, cur, tw, tws, slot, j, nothing);
     }
@@ -439,6 +465,25 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
 }
 
 }  // namespace lines
+
+// Tensor map of an n x n complex field as rows of 2n reals (real_bytes 8:
+// complex128, 4: complex64), tiles of box_reals x box_rows; shared with the
+// radix-16 line kernel's L2 prefetches (fft3d_r16.cu).
+cudaError_t encode_field_tmap(void *field, int n, int real_bytes, int box_reals, int box_rows,
+                              CUtensorMap *out) {
+  lines::EncodeTiledFn enc = lines::encode_fn();
+  if (enc == nullptr) return cudaErrorNotSupported;
+  std::memset(out, 0, sizeof(*out));
+  const cuuint64_t dims[2] = {(cuuint64_t)2 * n, (cuuint64_t)n};
+  const cuuint64_t strides[1] = {(cuuint64_t)2 * n * real_bytes};
+  const cuuint32_t box[2] = {(cuuint32_t)box_reals, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r =
+      enc(out, real_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+          field, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
 
 bool fft3d_lines_supported(Precision p, int n) {
   (void)p;

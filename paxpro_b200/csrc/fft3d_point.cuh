@@ -148,3 +148,32 @@ __device__ __forceinline__ typename Cx<R>::T refract3(const Fft3dPass &q, typena
 }
 
 }  // namespace pxp
+
+namespace pxp {
+
+// Whether the y pass's refraction reduces to the scaling by 1/(n*n) at every
+// point: no material sample in the step (no sphere meets the slab, no CSG
+// or sampled plane), no absorber band, and n*n a power of two.
+__device__ __forceinline__ bool refract3_is_scale(const Fft3dPass &q, double inv_norm) {
+  return q.nspheres == 0 && !q.csg.active && q.plane_delta == nullptr && q.thick_x == 0 &&
+         q.thick_y == 0 && inv_norm != 0.0;
+}
+
+// The register-resident line kernels unroll their points; refract3 inlined
+// at every one of them (material lookups, refraction integral, exp and
+// sin/cos, absorber) makes the y pass's code outgrow the instruction cache,
+// and a call per point spills the caller's live registers.  So they apply
+// the scaling-only case inline (refract3_is_scale: the same rounding as
+// refract3, an exact power-of-two scale in either precision) and otherwise
+// stage their points through shared memory and run refract3 in one
+// non-unrolled loop over them.
+template <typename C> __device__ __forceinline__ C scale_point(C u, double inv_norm);
+template <> __device__ __forceinline__ double2 scale_point(double2 u, double inv_norm) {
+  return cx_scale_rn(u, inv_norm);
+}
+template <> __device__ __forceinline__ float2 scale_point(float2 u, double inv_norm) {
+  const float sc = (float)inv_norm;
+  return mk(u.x * sc, u.y * sc);
+}
+
+}  // namespace pxp

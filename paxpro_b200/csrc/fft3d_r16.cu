@@ -40,10 +40,17 @@
 // transforms round like the radix-16 variant of fft3d.cu up to the order of
 // their passes (within the parity tolerance); complex64 data compute in FP32
 // with split twiddles and constants (fft_smem.cuh).
+#include <cuda.h>
+
+#include <cstring>
+
 #include "fft3d_point.cuh"
 #include "fft_r16.cuh"
 
 namespace pxp {
+
+cudaError_t encode_field_tmap(void *field, int n, int real_bytes, int box_reals, int box_rows,
+                              CUtensorMap *out);
 namespace r16 {
 
 using r16c::tw_offset;
@@ -59,7 +66,10 @@ template <typename R, int N> struct Cfg {
   static constexpr int TWN = r16c::Plan<N>::TWN;           // twiddle entries
   static constexpr int GROUPS = N / LPT;                  // line groups per pass
   static constexpr size_t XBYTES = 16 * (size_t)N;        // one slot's buffer
-  static constexpr size_t SMEM = S * XBYTES + 16 * (size_t)TWN;
+  // FP64 keeps kx^2 per column in shared memory for the x pass
+  static constexpr size_t KXBYTES = sizeof(R) == 8 ? 8 * (size_t)N : 0;
+  static constexpr size_t SMEM = S * XBYTES + 16 * (size_t)TWN + KXBYTES;
+  static constexpr int BOX = N < 256 ? N : 256;  // rows of one L2 prefetch tile
   // CTAs per SM: as many as shared memory holds, at most 128 registers a
   // thread
   static constexpr int SMEM_FIT = (int)((227 * 1024) / SMEM);
@@ -157,7 +167,8 @@ __device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N>::LPT][
 
 template <typename R, int N>
 __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
-    fft3d_r16_kernel(const Fft3dPass q, const double *__restrict__ gkx2,
+    fft3d_r16_kernel(const __grid_constant__ Fft3dPass q,
+                     const __grid_constant__ CUtensorMap tmap, const double *__restrict__ gkx2,
                      const Tw<typename Cx<R>::T> *__restrict__ wn) {
   using K = Cfg<R, N>;
   using C = typename Cx<R>::T;
@@ -169,8 +180,13 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
   const int slot = tid / TL, j = tid % TL;
   typename E::T *X = reinterpret_cast<typename E::T *>(smem_raw + slot * K::XBYTES);
   W *tws = reinterpret_cast<W *>(smem_raw + K::S * K::XBYTES);
+  double *skx2 = reinterpret_cast<double *>(smem_raw + K::S * K::XBYTES + 16 * (size_t)K::TWN);
   // twiddles of every radix-16 pass: entry off + (r-1)*NS + k = W_{16 NS}^(r k)
   r16c::load_twiddles<N>(tws, wn, tid, K::T);
+  if constexpr (sizeof(R) == 8) {
+    if (q.mode == 1)
+      for (int i = tid; i < N; i += K::T) skx2[i] = gkx2[i];
+  }
   __syncthreads();
   // the field is read only after the previous kernel in the stream is done
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
@@ -180,9 +196,28 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
   C *field = reinterpret_cast<C *>(q.field);
   C *save = reinterpret_cast<C *>(q.save);
   const double inv_norm = 1.0 / q.norm;  // n*n is a power of two: exact
+  const bool scale_only = refract3_is_scale(q, inv_norm);
   const int nslots = gridDim.x * K::S;
+  // L2 prefetch of a slot's lines (one thread each): the y lines of a group
+  // are one contiguous block; the x lines are columns, N/BOX tiles of the
+  // tensor map (16-byte rows: one complex128 column, or two complex64)
+  auto prefetch = [&](int gp) {
+    if (gp >= K::GROUPS) return;
+    if (xpass) {
+      for (int b = 0; b < N / K::BOX; ++b)
+        asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];\n" ::"l"(&tmap),
+                     "r"(2 * gp * LPT), "r"(b * K::BOX)
+                     : "memory");
+    } else {
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(field + (long long)gp * LPT * N),
+                   "r"((unsigned)(sizeof(C) * LPT * N))
+                   : "memory");
+    }
+  };
+  if (j == 0) prefetch(blockIdx.x * K::S + slot);
   for (int g = blockIdx.x * K::S + slot; g < K::GROUPS; g += nslots) {
     const int line0 = g * LPT;
+    if (j == 0) prefetch(g + nslots);  // this slot's next group, while this one computes
     C v[LPT][16];
     // load: x lines are columns (element e of line l at e*N + l; a complex64
     // thread's two lines are adjacent), y lines are rows
@@ -210,22 +245,43 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
 #pragma unroll
         for (int s = 0; s < 16; ++s) {
           const int e = j + s * TL;
-          v[t][s] = prop3(q, v[t][s], sizeof(R) == 8 ? __ldg(gkx2 + e) : 0.0, ky2, e, line);
+          v[t][s] = prop3(q, v[t][s], sizeof(R) == 8 ? skx2[e] : 0.0, ky2, e, line);
         }
       }
       line_fft<+1, R, N>(v, X, tws, slot, j);
     } else {
       if (q.mode >= 2) {
         line_fft<+1, R, N>(v, X, tws, slot, j);
+        if (scale_only) {
 #pragma unroll
-        for (int t = 0; t < LPT; ++t) {
-          const int line = line0 + t;  // x index
+          for (int t = 0; t < LPT; ++t)
 #pragma unroll
+            for (int s = 0; s < 16; ++s) v[t][s] = scale_point(v[t][s], inv_norm);
+        } else {
+          // material or absorber in this step: the thread's own points go
+          // through its exchange-buffer slots (each thread touches only its
+          // own, so the one barrier ends the other threads' last reads) and
+          // one non-unrolled refract3 loop
+          slot_sync(slot, TL);
+#pragma unroll
+          for (int s = 0; s < 16; ++s) X[xsw(j + s * TL)] = E::pack(v, s);
+#pragma unroll 1
           for (int s = 0; s < 16; ++s) {
             const int e = j + s * TL;  // y index
-            v[t][s] = refract3<R>(q, v[t][s], line, e, inv_norm);
-            if (save) save[(long long)line * N + e] = v[t][s];
+            C w[LPT][16];
+            E::unpack(w, 0, X[xsw(e)]);
+#pragma unroll
+            for (int t = 0; t < LPT; ++t) w[t][0] = refract3<R>(q, w[t][0], line0 + t, e, inv_norm);
+            X[xsw(e)] = E::pack(w, 0);
           }
+#pragma unroll
+          for (int s = 0; s < 16; ++s) E::unpack(v, s, X[xsw(j + s * TL)]);
+        }
+        if (save) {
+#pragma unroll
+          for (int t = 0; t < LPT; ++t)
+#pragma unroll
+            for (int s = 0; s < 16; ++s) save[(long long)(line0 + t) * N + j + s * TL] = v[t][s];
         }
       }
       if (q.mode != 3) line_fft<-1, R, N>(v, X, tws, slot, j);
@@ -271,7 +327,14 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k, q, kx2, reinterpret_cast<const W *>(wnv));
+  // x pass: the tensor map of the field for the L2 prefetches (16-byte rows)
+  CUtensorMap tmap;
+  std::memset(&tmap, 0, sizeof(tmap));
+  if (q.mode == 1) {
+    const cudaError_t te = encode_field_tmap(q.field, N, (int)sizeof(R), 2 * K::LPT, K::BOX, &tmap);
+    if (te != cudaSuccess) return te;
+  }
+  return cudaLaunchKernelEx(&cfg, k, q, tmap, kx2, reinterpret_cast<const W *>(wnv));
 }
 
 }  // namespace r16

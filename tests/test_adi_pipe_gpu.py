@@ -1,6 +1,6 @@
 """The pipelined one-wave ADI vacuum kernel (staging in per-group stages,
-each system group solving as soon as its rows land, results stored from
-registers) against the unpipelined one (PXP_ADI_PIPE=0, run in a child
+each system group solving as soon as its rows land; PXP_ADI_PIPE=1)
+against the unpipelined one (PXP_ADI_PIPE=0, each run in a child
 process because the switch is read once per process): the two share the
 solve's arithmetic, so their fields are equal bit for bit, for both half
 steps (x: systems adjacent in memory; y: systems as rows), with saves, at
