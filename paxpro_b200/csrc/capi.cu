@@ -896,16 +896,21 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
 // field (one untimed x+y pass pair, then three timed ones; the fastest kept),
 // and every solver with that key runs the winner from its first step on, so
 // a field never depends on when tuning happened (radix 8 and radix 16 round
-// differently).  PXP_FFT3D_VARIANT=0..4 pins the variant instead.
+// differently).  The x and y passes are tuned separately (each its fastest
+// variant).  PXP_FFT3D_VARIANT=0..4 pins both passes' variant instead.
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, int, unsigned>, int> g_fft3d_variant;
+
+// A tuned choice: the x pass's variant and the y pass's (modes 0, 2, 3).
+int fft3d_variant_code(int vx, int vy) { return vx + 8 * vy; }
+int fft3d_variant_of(int code, int mode) { return mode == 1 ? code % 8 : code / 8; }
 
 int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, const void *tw16,
                   const void *wn, int *out) {
   if (const char *env = std::getenv("PXP_FFT3D_VARIANT")) {
     const int v = std::atoi(env);
     if (v >= 0 && v < pxp::kFft3dVariants) {
-      *out = v;
+      *out = fft3d_variant_code(v, v);
       return PXP_OK;
     }
   }
@@ -932,27 +937,29 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
   q.save = nullptr;
   q.nspheres = 0;
   q.spheres_all = nullptr;
-  int best_v = 0;
-  float best = 1e30f;
+  // the x pass (mode 1) and the y pass (mode 2) are separate launches with
+  // the same field layout before and after, so each takes its own fastest
+  // variant
+  int best_v[2] = {0, 0};
+  float best[2] = {1e30f, 1e30f};
   if ((e = cudaMemsetAsync(scratch, 0, bytes, h->stream)) == cudaSuccess) {
     for (int v = 0; v < pxp::kFft3dVariants && e == cudaSuccess; ++v) {
-      float tmin = 1e30f;
-      for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
-        cudaEventRecord(e0, h->stream);
-        q.mode = 1;
-        e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
-        q.mode = 2;
-        if (e == cudaSuccess)
+      for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
+        q.mode = pass == 0 ? 1 : 2;
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+          cudaEventRecord(e0, h->stream);
           e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
-        cudaEventRecord(e1, h->stream);
-        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-        float ms = 0.f;
-        if (e == cudaSuccess && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
-          tmin = std::min(tmin, ms);
-      }
-      if (tmin < best) {
-        best = tmin;
-        best_v = v;
+          cudaEventRecord(e1, h->stream);
+          if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+          float ms = 0.f;
+          if (e == cudaSuccess && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+            tmin = std::min(tmin, ms);
+        }
+        if (tmin < best[pass]) {
+          best[pass] = tmin;
+          best_v[pass] = v;
+        }
       }
     }
   }
@@ -960,8 +967,8 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
   cudaEventDestroy(e1);
   cudaFreeAsync(scratch, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "FFT3D tuning");
-  g_fft3d_variant[key] = best_v;
-  *out = best_v;
+  g_fft3d_variant[key] = fft3d_variant_code(best_v[0], best_v[1]);
+  *out = g_fft3d_variant[key];
   return PXP_OK;
 }
 
@@ -1108,7 +1115,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   if (int rc = fft3d_variant(h, q, kx2, tw16, wn, &variant)) return rc;
   cudaError_t e;
   q.mode = 0;  // forward transform along y of the real-space field
-  if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, wn, h->stream)) != cudaSuccess)
+  if ((e = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(variant, q.mode), (const double *)kx2, tw16, wn, h->stream)) != cudaSuccess)
     return h->cuda_fail(e, "FFT3D forward y pass");
   std::vector<pxp::Sphere> act;
   // step i of this call: x pass, then the y pass (mode 3 on the last step
@@ -1117,7 +1124,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     const unsigned step = first + (unsigned)i;
     q.mode = 1;
     q.save = nullptr;
-    if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, wn, h->stream)) !=
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(variant, q.mode), (const double *)kx2, tw16, wn, h->stream)) !=
         cudaSuccess)
       return h->cuda_fail(e, "FFT3D x pass");
     q.mode = (i == nsteps - 1) ? 3 : 2;
@@ -1136,7 +1143,7 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     }
     char *slot = save_at(h, step) ? save_slot(h, step) : nullptr;
     q.save = slot && h->d_save_stage ? h->d_save_stage : slot;
-    if ((e = pxp::launch_fft3d_pass(h->prec, q, variant, (const double *)kx2, tw16, wn, h->stream)) !=
+    if ((e = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(variant, q.mode), (const double *)kx2, tw16, wn, h->stream)) !=
         cudaSuccess)
       return h->cuda_fail(e, "FFT3D y pass");
     if (slot && h->d_save_stage) return save_downsample(h, slot);
