@@ -892,12 +892,14 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
 }
 
 // Launch-variant autotuner of the FFTSolver3D passes.  The first solver with
-// a given (device, precision, n) times every variant on a zeroed scratch
-// field (one untimed x+y pass pair, then three timed ones; the fastest kept),
-// and every solver with that key runs the winner from its first step on, so
-// a field never depends on when tuning happened (radix 8 and radix 16 round
-// differently).  The x and y passes are tuned separately (each its fastest
-// variant).  PXP_FFT3D_VARIANT=0..4 pins both passes' variant instead.
+// a given (device, precision, n) times every variant of each pass (x and y
+// separately: each takes its fastest) on a zeroed scratch field -- three
+// rounds of one untimed launch and three timed back to back, the best round
+// kept; the untimed launch keeps the device busy while the host prepares
+// the timed ones, so host-side launch set-up never counts -- and every
+// solver with that key runs the winners from its first step on, so a field
+// never depends on when tuning happened (the variants' transforms round
+// differently).  PXP_FFT3D_VARIANT=0..4 pins both passes' variant instead.
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, int, unsigned>, int> g_fft3d_variant;
 
@@ -947,14 +949,19 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
       for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
         q.mode = pass == 0 ? 1 : 2;
         float tmin = 1e30f;
-        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
-          cudaEventRecord(e0, h->stream);
+        for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+          // an untimed launch first keeps the device busy while the host
+          // prepares the timed ones (tensor maps, launch attributes), so the
+          // events bracket device time only
           e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
+          cudaEventRecord(e0, h->stream);
+          for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+            e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
           cudaEventRecord(e1, h->stream);
           if (e == cudaSuccess) e = cudaEventSynchronize(e1);
           float ms = 0.f;
-          if (e == cudaSuccess && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
-            tmin = std::min(tmin, ms);
+          if (e == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+            tmin = std::min(tmin, ms / 3.f);
         }
         if (tmin < best[pass]) {
           best[pass] = tmin;
@@ -978,7 +985,8 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
 // a cluster of two).  As for FFTSolver3D, the first solver with a given
 // (device, precision, kind, size) times every variant on a scratch copy of
 // its own job (zeroed field; no saves, flux sums or per-step tables; 64
-// steps, one untimed launch and three timed, the fastest kept) and every
+// steps a launch, three rounds of an untimed launch and a timed one, the
+// fastest kept) and every
 // solver with that key -- alone or in a batch -- runs the winner from its
 // first step, so a field never depends on when tuning ran (the variants
 // agree within the FP64 tolerance, not bit for bit).  PXP_FFT1D_R16=0|1 and
@@ -1040,18 +1048,22 @@ int variant_2d(pxp_solver_s *h, int *out) {
   int best_v = 0;
   float best = 1e30f;
   constexpr int kTuneSteps = 64;
+  auto launch_v = [&](int v) {
+    return fft ? pxp::launch_fft1d(h->prec, (const pxp::Fft1dJob *)djob, 1, n, 1, kTuneSteps,
+                                   h->stream, false, v)
+               : pxp::launch_cn_const(h->prec, (const pxp::CnJob *)djob, 1, n, 1, kTuneSteps,
+                                      h->stream, false, v);
+  };
   for (int v = 0; v < nv && e == cudaSuccess; ++v) {
     float tmin = 1e30f;
-    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+      e = launch_v(v);  // untimed: the device is busy while the timed launch is prepared
       cudaEventRecord(e0, h->stream);
-      e = fft ? pxp::launch_fft1d(h->prec, (const pxp::Fft1dJob *)djob, 1, n, 1, kTuneSteps,
-                                  h->stream, false, v)
-              : pxp::launch_cn_const(h->prec, (const pxp::CnJob *)djob, 1, n, 1, kTuneSteps,
-                                     h->stream, false, v);
+      if (e == cudaSuccess) e = launch_v(v);
       cudaEventRecord(e1, h->stream);
       if (e == cudaSuccess) e = cudaEventSynchronize(e1);
       float ms = 0.f;
-      if (e == cudaSuccess && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+      if (e == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
         tmin = std::min(tmin, ms);
     }
     if (tmin < best) {

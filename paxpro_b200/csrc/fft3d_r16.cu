@@ -309,12 +309,16 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
     const cudaError_t e = raise_dynamic_smem((const void *)k, (int)K::SMEM);
     if (e != cudaSuccess) return e;
   }
-  int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, K::T, K::SMEM);
-  if (e != cudaSuccess) return e;
-  if (per < 1) per = 1;
+  // CTAs per wave, once per instantiation (the same SM count on every B200)
+  static int per = 0, sms = 0;
+  if (per == 0) {
+    int dev = 0, p = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, k, K::T, K::SMEM);
+    if (e != cudaSuccess) return e;
+    per = p < 1 ? 1 : p;
+  }
   const int ctas = (K::GROUPS + K::S - 1) / K::S;
   const int grid = ctas < sms * per ? ctas : sms * per;
   cudaLaunchConfig_t cfg = {};
