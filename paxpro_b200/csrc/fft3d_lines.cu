@@ -26,7 +26,10 @@
 //  * Lines arrive by TMA into a staging buffer while the previous line group
 //    is transformed: a contiguous group of y lines is one bulk copy; a group
 //    of x lines (adjacent rows of the column-major field) is n/256 tiles of
-//    a 2-D tensor map over this GPU's own field (no multicast).  One thread
+//    a 2-D tensor map over this GPU's own field (no multicast).  x lines
+//    also leave by tile stores of the same map, from the exchange buffer
+//    the last pass did not read; y lines leave by coalesced stores from
+//    registers.  One thread
 //    arms an mbarrier for the group's bytes and issues the copies; it waits
 //    with a bounded wait (about 2 s; a wait that runs out is counted, the
 //    copy drained and the CTA leaves) and a CTA barrier publishes the line.
@@ -295,7 +298,10 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
       s_ok = ok;
     }
     __syncthreads();
-    if (!s_ok) return;
+    if (!s_ok) {
+      if (tid == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+      return;
+    }
     (void)mbar_try_wait(bar, it & 1);  // completed phase: orders the staged line for this thread
     const int line0 = g * K::L;
     C v[K::LPT][8];
@@ -371,20 +377,43 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
       }
       if (q.mode != 3) line_fft<-1, R, N, LG>(v, X0, X1, cur, tw, tws, slot, j, nothing);
     }
-    // natural-order outputs straight to global memory
+    if (xpass) {
+      // columns leave by TMA tile stores from the exchange buffer the last
+      // pass did not read (the staging layout: element e of line l at
+      // e*L + l), instead of 16-byte stores strided by the row length; the
+      // buffer is the next group's first-pass target, so thread 0 waits
+      // until the copies have read it before the CTA moves on
+      C *F = cur ? X0 : X1;
 #pragma unroll
-    for (int t = 0; t < K::LPT; ++t) {
-      const int line = line0 + slot * K::LPT + t;
+      for (int t = 0; t < K::LPT; ++t)
 #pragma unroll
-      for (int s = 0; s < 8; ++s) {
-        const int e = j + s * K::TL;
-        if (xpass)
-          field[(long long)e * N + line] = v[t][s];
-        else
-          field[(long long)line * N + e] = v[t][s];
+        for (int s = 0; s < 8; ++s) F[(j + s * K::TL) * K::L + slot * K::LPT + t] = v[t][s];
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        const unsigned src = smem_u32(F);
+        for (int b = 0; b < N / K::BC; ++b)
+          asm volatile(
+              "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                  &tmap),
+              "r"(2 * line0), "r"(b * K::BC), "r"(src + (unsigned)(b * K::BC * K::L * sizeof(C)))
+              : "memory");
+        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+      }
+      __syncthreads();
+    } else {
+      // rows: natural-order outputs straight to global memory (coalesced)
+#pragma unroll
+      for (int t = 0; t < K::LPT; ++t) {
+        const int line = line0 + slot * K::LPT + t;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) field[(long long)line * N + j + s * K::TL] = v[t][s];
       }
     }
   }
+  // the last group's tile stores complete before the CTA leaves
+  if (tid == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
 }
 
 // ---- host side -------------------------------------------------------------
