@@ -893,10 +893,12 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
 
 // Launch-variant autotuner of the FFTSolver3D passes.  The first solver with
 // a given (device, precision, n) times every variant of each pass (x and y
-// separately: each takes its fastest) on a zeroed scratch field -- three
-// rounds of one untimed launch and three timed back to back, the best round
-// kept; the untimed launch keeps the device busy while the host prepares
-// the timed ones, so host-side launch set-up never counts -- and every
+// separately) on a zeroed scratch field -- three rounds of one untimed
+// launch and three timed back to back, the best round kept; the untimed
+// launch keeps the device busy while the host prepares the timed ones, so
+// host-side launch set-up never counts -- then times whole steps (x and y
+// passes interleaved) of every variant and of the two per-pass winners
+// combined, and keeps the fastest step; every
 // solver with that key runs the winners from its first step on, so a field
 // never depends on when tuning happened (the variants' transforms round
 // differently).  PXP_FFT3D_VARIANT=0..4 pins both passes' variant instead.
@@ -970,12 +972,48 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
       }
     }
   }
+  // the per-pass winners against each variant for both passes, timed as
+  // whole steps (x pass, y pass, interleaved as the solver runs them): a
+  // pass timed in isolation meets the caches its own previous launch left
+  std::vector<int> cands;
+  for (int v = 0; v < pxp::kFft3dVariants; ++v) cands.push_back(fft3d_variant_code(v, v));
+  if (best_v[0] != best_v[1]) cands.push_back(fft3d_variant_code(best_v[0], best_v[1]));
+  int best_code = cands.back();
+  float best_step = 1e30f;
+  auto step_pair = [&](int code) {
+    q.mode = 1;
+    cudaError_t r = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(code, 1),
+                                           (const double *)kx2, tw16, wn, h->stream);
+    q.mode = 2;
+    if (r == cudaSuccess)
+      r = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(code, 2), (const double *)kx2,
+                                 tw16, wn, h->stream);
+    return r;
+  };
+  for (int code : cands) {
+    if (e != cudaSuccess) break;
+    float tmin = 1e30f;
+    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+      e = step_pair(code);  // untimed
+      cudaEventRecord(e0, h->stream);
+      for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = step_pair(code);
+      cudaEventRecord(e1, h->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+        tmin = std::min(tmin, ms / 3.f);
+    }
+    if (tmin < best_step) {
+      best_step = tmin;
+      best_code = code;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFreeAsync(scratch, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "FFT3D tuning");
-  g_fft3d_variant[key] = fft3d_variant_code(best_v[0], best_v[1]);
-  *out = g_fft3d_variant[key];
+  g_fft3d_variant[key] = best_code;
+  *out = best_code;
   return PXP_OK;
 }
 
