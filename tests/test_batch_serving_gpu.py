@@ -42,6 +42,29 @@ def test_batch_results_equal_alone(precision):
         assert np.array_equal(alone.intensities[i], mixed.intensities[i]), (i, jobs[i].kind, jobs[i].n)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_sizes_other_than_powers_of_two_equal_alone(precision):
+    """Batch groups on padded and Bluestein kernels (CrankNicholson at 300
+    and 600 rows on the step-invariant path padded to 512 and 1024;
+    FFTSolver2D at 1000 and 3000 points by Bluestein's transform) and the
+    largest lines (FFTSolver2D at 16384 points: a two-CTA cluster in FP64),
+    entering and leaving mid-batch: every exit intensity equal bit for bit
+    to the solver stepped alone."""
+    from paxpro_b200 import serving as sv
+    rng = np.random.default_rng(11)
+    jobs = []
+    for i, (kind, n) in enumerate([("cn", 300), ("cn", 300), ("cn", 600), ("fft2d", 1000),
+                                   ("fft2d", 3000), ("fft2d", 16384), ("fft2d", 1000)]):
+        j = sv.draw_2d(rng, kind, i)
+        j.n = n
+        j.nsteps = int(rng.integers(20, 90))
+        jobs.append(j)
+    alone = sv.run_plain(jobs, precision=precision)
+    mixed = sv.run_batched(jobs, precision=precision, max_steps=13)
+    for i in range(len(jobs)):
+        assert np.array_equal(alone.intensities[i], mixed.intensities[i]), (i, jobs[i].kind, jobs[i].n)
+
+
 def test_batch_budget_refuses_and_releases():
     import paxpro_b200 as pxp
     from paxpro_b200 import serving as sv
