@@ -2382,6 +2382,10 @@ struct pxp_batch_s {
   std::vector<cudaStream_t> gstreams;
   std::vector<cudaEvent_t> gdone;
   cudaEvent_t uploaded = nullptr;
+  // one job counter per group: FFTSolver2D groups run persistent CTAs that
+  // take their next job from it (persistent.cuh)
+  unsigned *d_queue = nullptr;
+  size_t queue_cap = 0;
   std::vector<pxp_solver_s *> active;
   void *d_jobs = nullptr;
   size_t d_jobs_cap = 0;
@@ -2451,6 +2455,7 @@ int pxp_batch_destroy(pxp_batch b) {
   if (b->d_jobs) cudaFreeAsync(b->d_jobs, b->stream);
   cudaStreamSynchronize(b->stream);
   if (b->h_jobs) cudaFreeHost(b->h_jobs);
+  if (b->d_queue) cudaFree(b->d_queue);
   for (cudaStream_t g : b->gstreams) cudaStreamDestroy(g);
   for (cudaEvent_t e : b->gdone) cudaEventDestroy(e);
   if (b->uploaded) cudaEventDestroy(b->uploaded);
@@ -2572,6 +2577,16 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
     if (cudaEventRecord(b->uploaded, b->stream) != cudaSuccess)
       return b->fail(PXP_ERR_CUDA, "batch event record");
   }
+  if (b->queue_cap < offs.size()) {
+    if (b->d_queue) cudaFree(b->d_queue);
+    b->d_queue = nullptr;
+    b->queue_cap = 0;
+    if (cudaMalloc(&b->d_queue, sizeof(unsigned) * offs.size()) != cudaSuccess) {
+      cudaGetLastError();
+      return b->fail(PXP_ERR_NOMEM, "batch job counters");
+    }
+    b->queue_cap = offs.size();
+  }
   for (size_t gi = 0; gi < offs.size(); ++gi) {
     auto &o = offs[gi];
     cudaStream_t gst = b->gstreams[gi];
@@ -2584,9 +2599,13 @@ int pxp_batch_round(pxp_batch b, int max_steps) {
     for (const pxp_solver_s *h : list) any_flux = any_flux || h->flux_count > 0;
     const int variant = gvariant[gi];
     cudaError_t e;
-    if (k.kind == PXP_FFT_SOLVER_2D)
-      e = pxp::launch_fft1d((pxp::Precision)k.prec, (const pxp::Fft1dJob *)jobs, (int)list.size(),
-                            k.n, -1, -1, gst, any_flux, variant);
+    if (k.kind == PXP_FFT_SOLVER_2D) {
+      e = cudaMemsetAsync(b->d_queue + gi, 0, sizeof(unsigned), gst);
+      if (e == cudaSuccess)
+        e = pxp::launch_fft1d((pxp::Precision)k.prec, (const pxp::Fft1dJob *)jobs,
+                              (int)list.size(), k.n, -1, -1, gst, any_flux, variant,
+                              b->d_queue + gi);
+    }
     else if (k.cpath)
       e = pxp::launch_cn_const((pxp::Precision)k.prec, (const pxp::CnJob *)jobs, (int)list.size(),
                                pxp::cn_padded_n(k.n), -1, -1, gst, any_flux, variant);

@@ -15,6 +15,7 @@
 #include "bluestein.cuh"
 #include "fft_smem.cuh"
 #include "flux.cuh"
+#include "persistent.cuh"
 #include "pxp_kernels.h"
 
 namespace pxp {
@@ -31,12 +32,14 @@ __device__ __forceinline__ float2 kmul(float2 u, float4 k) { return tw_mul(u, k)
 
 template <typename R, int N, int T, bool TW_SMEM, bool FLUX>
 __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ jobs, int step0_ov,
-                                                 int nsteps_ov) {
+                                                 int nsteps_ov, int njobs, unsigned *queue) {
   using C = typename Cx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double flux_red[2][flux_slots<T>()];
+  __shared__ int s_next;
   C *u = reinterpret_cast<C *>(smem_raw);
-  Fft1dJob job = jobs[blockIdx.x];
+  for (int jb = blockIdx.x; jb < njobs; jb = next_job(queue, &s_next)) {
+  Fft1dJob job = jobs[jb];
   if (nsteps_ov >= 0) {
     job.step0 = step0_ov;
     job.nsteps = nsteps_ov;
@@ -84,6 +87,7 @@ __global__ void __launch_bounds__(T) fft1d_kernel(const Fft1dJob *__restrict__ j
     if (flux) flux_store<T>(job.flux, step, flux_red[s & 1]);
   }
   for (int i = lane; i < N; i += T) field[i] = u[sw<C>(i)];
+  }
 }
 
 template <typename R, int M, int T, bool FLUX>
@@ -145,7 +149,7 @@ template <typename R> constexpr int fft1d_threads(int n) {
 
 template <typename R, int N, bool FLUX>
 static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nsteps,
-                            cudaStream_t s) {
+                            cudaStream_t s, unsigned *queue) {
   using C = typename Cx<R>::T;
   constexpr int T = fft1d_threads<R>(N);
   constexpr size_t field_bytes = sizeof(C) * N;
@@ -157,7 +161,8 @@ static cudaError_t launch_n(const Fft1dJob *d_jobs, int nj, int step0, int nstep
     const cudaError_t attr = raise_dynamic_smem((const void *)k, (int)smem);
     if (attr != cudaSuccess) return attr;
   }
-  k<<<nj, T, smem, s>>>(d_jobs, step0, nsteps);
+  const int grid = persistent_grid((const void *)k, T, smem, nj, queue);
+  k<<<grid, T, smem, s>>>(d_jobs, step0, nsteps, nj, queue);
   return cudaGetLastError();
 }
 
@@ -214,9 +219,9 @@ static cudaError_t launch_bluestein(Precision p, const Fft1dJob *d_jobs, int nj,
 
 template <typename R, int N>
 static cudaError_t launch_nf(const Fft1dJob *d_jobs, int nj, int step0, int nsteps, cudaStream_t s,
-                             bool flux) {
-  return flux ? launch_n<R, N, true>(d_jobs, nj, step0, nsteps, s)
-              : launch_n<R, N, false>(d_jobs, nj, step0, nsteps, s);
+                             bool flux, unsigned *queue) {
+  return flux ? launch_n<R, N, true>(d_jobs, nj, step0, nsteps, s, queue)
+              : launch_n<R, N, false>(d_jobs, nj, step0, nsteps, s, queue);
 }
 
 int fft1d_variants(Precision p, int n) {
@@ -224,21 +229,21 @@ int fft1d_variants(Precision p, int n) {
 }
 
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
-                         int nsteps, cudaStream_t s, bool flux, int variant) {
+                         int nsteps, cudaStream_t s, bool flux, int variant, unsigned *queue) {
   if (nj <= 0) return cudaSuccess;
   if (n & (n - 1)) return launch_bluestein(p, d_jobs, nj, n, step0, nsteps, s, flux);
   if (fft1d_pair_size(p, n)) return launch_fft1d_pair(p, d_jobs, nj, n, step0, nsteps, s, flux);
   if (variant != 0 && fft1d_r16_enabled(n))
-    return launch_fft1d_r16(p, d_jobs, nj, n, step0, nsteps, s, flux);
+    return launch_fft1d_r16(p, d_jobs, nj, n, step0, nsteps, s, flux, queue);
 #define PXP_CASE(NN)                                                              \
   case NN:                                                                        \
-    return p == kFP64 ? launch_nf<double, NN>(d_jobs, nj, step0, nsteps, s, flux)     \
-                      : launch_nf<float, NN>(d_jobs, nj, step0, nsteps, s, flux);
+    return p == kFP64 ? launch_nf<double, NN>(d_jobs, nj, step0, nsteps, s, flux, queue)     \
+                      : launch_nf<float, NN>(d_jobs, nj, step0, nsteps, s, flux, queue);
   switch (n) {
     PXP_CASE(8) PXP_CASE(16) PXP_CASE(32) PXP_CASE(64) PXP_CASE(128) PXP_CASE(256)
     PXP_CASE(512) PXP_CASE(1024) PXP_CASE(2048) PXP_CASE(4096) PXP_CASE(8192)
     case 16384:
-      if (p == kFP32) return launch_nf<float, 16384>(d_jobs, nj, step0, nsteps, s, flux);
+      if (p == kFP32) return launch_nf<float, 16384>(d_jobs, nj, step0, nsteps, s, flux, queue);
       return cudaErrorInvalidValue;
     default:
       return cudaErrorInvalidValue;

@@ -22,6 +22,7 @@
 // tables (kernel, t / N) with one FMA chain (fft_smem.cuh).
 #include "fft_r16.cuh"
 #include "flux.cuh"
+#include "persistent.cuh"
 #include "pxp_kernels.h"
 
 namespace pxp {
@@ -81,7 +82,8 @@ __device__ __forceinline__ void line_fft(C (&v)[16], C *X0, C *X1, const Tw<C> *
 
 template <typename R, int N, bool FLUX>
 __global__ void __launch_bounds__(N / 16) fft1d_r16_kernel(const Fft1dJob *__restrict__ jobs,
-                                                          int step0_ov, int nsteps_ov) {
+                                                          int step0_ov, int nsteps_ov, int njobs,
+                                                          unsigned *queue) {
   using C = typename Cx<R>::T;
   using W = Tw<C>;
   using P = r16c::Plan<N>;
@@ -91,7 +93,9 @@ __global__ void __launch_bounds__(N / 16) fft1d_r16_kernel(const Fft1dJob *__res
   C *X0 = reinterpret_cast<C *>(smem_raw);
   C *X1 = X0 + N;
   W *tws = reinterpret_cast<W *>(X1 + N);
-  Fft1dJob job = jobs[blockIdx.x];
+  __shared__ int s_next;
+  for (int jb = blockIdx.x; jb < njobs; jb = next_job(queue, &s_next)) {
+  Fft1dJob job = jobs[jb];
   if (nsteps_ov >= 0) {
     job.step0 = step0_ov;
     job.nsteps = nsteps_ov;
@@ -135,10 +139,12 @@ __global__ void __launch_bounds__(N / 16) fft1d_r16_kernel(const Fft1dJob *__res
   }
 #pragma unroll
   for (int s = 0; s < 16; ++s) field[j + s * TL] = v[s];
+  }
 }
 
 template <typename R, int N, bool FLUX>
-cudaError_t launch(const Fft1dJob *d_jobs, int nj, int step0, int nsteps, cudaStream_t s) {
+cudaError_t launch(const Fft1dJob *d_jobs, int nj, int step0, int nsteps, cudaStream_t s,
+                   unsigned *queue) {
   using C = typename Cx<R>::T;
   constexpr size_t smem = 2 * sizeof(C) * N + sizeof(Tw<C>) * r16c::Plan<N>::TWN;
   static_assert(smem <= 227 * 1024, "exchange buffers and twiddles exceed shared memory");
@@ -147,7 +153,8 @@ cudaError_t launch(const Fft1dJob *d_jobs, int nj, int step0, int nsteps, cudaSt
     const cudaError_t e = raise_dynamic_smem((const void *)k, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k<<<nj, N / 16, smem, s>>>(d_jobs, step0, nsteps);
+  const int grid = persistent_grid((const void *)k, N / 16, smem, nj, queue);
+  k<<<grid, N / 16, smem, s>>>(d_jobs, step0, nsteps, nj, queue);
   return cudaGetLastError();
 }
 
@@ -156,14 +163,14 @@ cudaError_t launch(const Fft1dJob *d_jobs, int nj, int step0, int nsteps, cudaSt
 bool fft1d_r16_enabled(int n) { return n >= 512 && n <= 4096 && !(n & (n - 1)); }
 
 cudaError_t launch_fft1d_r16(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
-                             int nsteps, cudaStream_t s, bool flux) {
+                             int nsteps, cudaStream_t s, bool flux, unsigned *queue) {
 #define PXP_1R(NN)                                                                              \
   case NN:                                                                                      \
     if (p == kFP64)                                                                             \
-      return flux ? r16_1d::launch<double, NN, true>(d_jobs, nj, step0, nsteps, s)              \
-                  : r16_1d::launch<double, NN, false>(d_jobs, nj, step0, nsteps, s);            \
-    return flux ? r16_1d::launch<float, NN, true>(d_jobs, nj, step0, nsteps, s)                 \
-                : r16_1d::launch<float, NN, false>(d_jobs, nj, step0, nsteps, s);
+      return flux ? r16_1d::launch<double, NN, true>(d_jobs, nj, step0, nsteps, s, queue)       \
+                  : r16_1d::launch<double, NN, false>(d_jobs, nj, step0, nsteps, s, queue);     \
+    return flux ? r16_1d::launch<float, NN, true>(d_jobs, nj, step0, nsteps, s, queue)          \
+                : r16_1d::launch<float, NN, false>(d_jobs, nj, step0, nsteps, s, queue);
   switch (n) {
     PXP_1R(512) PXP_1R(1024) PXP_1R(2048) PXP_1R(4096)
     default:

@@ -66,7 +66,7 @@ struct Fft1dJob {
 // takes size n (powers of two 512 .. 4096), and its launch.
 bool fft1d_r16_enabled(int n);
 cudaError_t launch_fft1d_r16(Precision p, const Fft1dJob *d_jobs, int nj, int n, int step0,
-                             int nsteps, cudaStream_t s, bool flux);
+                             int nsteps, cudaStream_t s, bool flux, unsigned *queue = nullptr);
 // Launch variants of the 2-D step kernels, chosen per (device, precision,
 // size) by the tuner in capi.cu: FFTSolver2D 0 = shared-memory Stockham
 // kernel, 1 = register-resident radix-16 kernel; CrankNicholson's
@@ -75,9 +75,12 @@ cudaError_t launch_fft1d_r16(Precision p, const Fft1dJob *d_jobs, int nj, int n,
 // -1 is the default (the radix-16 kernel where it runs; one CTA).
 int fft1d_variants(Precision p, int n);
 int cn_const_variants(Precision p, int n);
+// queue: a device counter (zero at launch) that makes the power-of-two
+// kernels persistent -- at most one wave of CTAs, each taking its next job
+// from the counter (persistent.cuh); null: one CTA per job.
 cudaError_t launch_fft1d(Precision p, const Fft1dJob *d_jobs, int nj, int n,
                          int step0, int nsteps, cudaStream_t s, bool flux = false,
-                         int variant = -1);
+                         int variant = -1, unsigned *queue = nullptr);
 bool fft1d_supported(Precision p, int n);
 // complex128 lines of 16384 points (fft1d_pair.cu): a cluster of two CTAs per
 // job, each holding the points of one parity; the job's twiddle is the
