@@ -474,28 +474,6 @@ __device__ __forceinline__ void multi_exclusive_scan(double2 &a, double2 (&b)[S]
 // for chunk c: r[j][m] holds the solution of row c*M + m of system sys0 + j.
 // Right-hand sides and solve of systems sys0 .. sys0+SC-1 of this CTA for
 // chunk c: r[j][m] holds the solution of row c*M + m of system sys0 + j.
-// Right-hand side of an ADI row (the explicit second difference across the
-// systems, src/alternatingDirectionSolver.cpp:28-36, 93-101 with vacuum):
-// coef * u + i*hk*(left + right), each neighbour outside the grid zero.  One
-// formula for the half step's own stencil and for the fused form, where the
-// previous half step forms it from its solutions, so both round alike.
-struct AdiRhsCoef {
-  double2 coef;
-  double hk;
-};
-__device__ __forceinline__ AdiRhsCoef adi_rhs_coef(double inv_dzh, double kd2_expl) {
-  const double inv_kd2_expl = __ddiv_rn(1.0, kd2_expl);
-  return {mk(inv_dzh, -inv_kd2_expl), 0.5 * inv_kd2_expl};
-}
-__device__ __forceinline__ double2 adi_rhs(const AdiRhsCoef &k, double2 center, bool has_left,
-                                           double2 left, bool has_right, double2 right) {
-  const double2 rr = cmul(k.coef, center);
-  double2 nb = mk(0.0, 0.0);
-  if (has_left) nb = left;
-  if (has_right) nb = cadd(nb, right);
-  return mk(fma(-k.hk, nb.y, rr.x), fma(k.hk, nb.x, rr.y));
-}
-
 template <int N, int M, int G, bool XH, int SCAP, int S>
 __device__ __forceinline__ void adi_group_solve(double2 (&r)[SCAP][M], const AdiHalf &h,
                                                 const double2 *tile, const double2 *gs,
@@ -504,24 +482,22 @@ __device__ __forceinline__ void adi_group_solve(double2 (&r)[SCAP][M], const Adi
                                                 int s_base, int c, int gtid, int bar) {
   using L = AdiWaveTile<N, M, G, XH>;
   constexpr int P = N / M;
-  if (h.in_rhs) {
-    // the staged rows are this half step's right-hand sides already
+  const double inv_kd2_expl = __ddiv_rn(1.0, h.kd2_expl);
+  const double hk = 0.5 * inv_kd2_expl;
+  const double2 coef = mk(h.inv_dzh, -inv_kd2_expl);
 #pragma unroll
-    for (int m = 0; m < M; ++m)
+  for (int m = 0; m < M; ++m) {
+    double2 v[S + 2];
 #pragma unroll
-      for (int j = 0; j < S; ++j) r[j][m] = tile[L::at(c, m, sys0 + j + 1)];
-  } else {
-    const AdiRhsCoef k = adi_rhs_coef(h.inv_dzh, h.kd2_expl);
+    for (int k = 0; k < S + 2; ++k) v[k] = tile[L::at(c, m, sys0 + k)];
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      double2 v[S + 2];
-#pragma unroll
-      for (int q = 0; q < S + 2; ++q) v[q] = tile[L::at(c, m, sys0 + q)];
-#pragma unroll
-      for (int j = 0; j < S; ++j) {
-        const int s = s_base + sys0 + j;  // s >= h.n: padding system, all zero
-        r[j][m] = adi_rhs(k, v[j + 1], s > 0, v[j], s < h.n - 1, v[j + 2]);
-      }
+    for (int j = 0; j < S; ++j) {
+      const int s = s_base + sys0 + j;  // s >= h.n: padding system, all zero
+      const double2 rr = cmul(coef, v[j + 1]);
+      double2 nb = mk(0.0, 0.0);
+      if (s > 0) nb = v[j];
+      if (s < h.n - 1) nb = cadd(nb, v[j + 2]);
+      r[j][m] = mk(fma(-hk, nb.y, rr.x), fma(hk, nb.x, rr.y));
     }
   }
   // forward, zero carry-in: y_i = g_i r_i + h_i y_{i-1}
@@ -619,18 +595,14 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
     // consecutive threads take consecutive systems
     constexpr int PPI = T / RW;  // positions per pass
     const int g = tid % RW;
-    // a fused right-hand side needs no halo systems (rows 0 and G + 1)
-    const bool need = !h.in_rhs || (g >= 1 && g <= G);
-    if (tid < PPI * RW && g >= g_lo && g < g_hi && need) {
+    if (tid < PPI * RW && g >= g_lo && g < g_hi) {
       const double2 *src = in + (s_base - 1 + g);
       for (int p = tid / RW; p < nr; p += PPI)
         adi_cp_async16(tile + L::at(p / M, p % M, g), src + (long long)p * h.stride_pos);
     }
   } else {
-    const int glo = h.in_rhs && g_lo < 1 ? 1 : g_lo;            // no halo rows when
-    const int ghi = h.in_rhs && g_hi > G + 1 ? G + 1 : g_hi;    // the input is fused
 #pragma unroll 1
-    for (int g = glo; g < ghi; ++g) {
+    for (int g = g_lo; g < g_hi; ++g) {
       const double2 *src = in + (long long)(s_base - 1 + g) * h.stride_sys;
       for (int p = tid; p < nr; p += T) adi_cp_async16(tile + L::at(p / M, p % M, g), src + p);
     }
@@ -667,24 +639,13 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
   __syncthreads();
   double2 *save = reinterpret_cast<double2 *>(h.save);
   const int nsys = nr - s_base < G ? nr - s_base : G;  // the last CTA may hold fewer
-  // the value stored at position p of system row g: the solution, or (fused
-  // output) the next half step's right-hand side, whose explicit difference
-  // runs along this half step's positions -- within the system's own row
-  const AdiRhsCoef knext = adi_rhs_coef(h.inv_dzh, h.next_kd2_expl);
-  auto stored = [&](int p, int g) {
-    const double2 v = tile[L::at(p / M, p % M, g)];
-    if (!h.out_rhs) return v;
-    const double2 lft = p > 0 ? tile[L::at((p - 1) / M, (p - 1) % M, g)] : mk(0.0, 0.0);
-    const double2 rgt = p < nr - 1 ? tile[L::at((p + 1) / M, (p + 1) % M, g)] : mk(0.0, 0.0);
-    return adi_rhs(knext, v, p > 0, lft, p < nr - 1, rgt);
-  };
   if constexpr (XH) {
     // consecutive threads write consecutive systems of a position
     constexpr int PPI = T / G;
     const int gg = tid % G;
     if (tid < PPI * G && gg < nsys) {
       for (int p = tid / G; p < nr; p += PPI) {
-        const double2 v = stored(p, gg + 1);
+        const double2 v = tile[L::at(p / M, p % M, gg + 1)];
         const long long off = (long long)p * h.stride_pos + s_base + gg;
         out[off] = v;
         if (save) save[off] = v;
@@ -695,7 +656,7 @@ __global__ void __launch_bounds__(((G + S - 1) / S) * (N / M), 1)
     for (int gg = 0; gg < nsys; ++gg) {
       const long long base = (long long)(s_base + gg) * h.stride_sys;
       for (int p = tid; p < nr; p += T) {
-        const double2 v = stored(p, gg + 1);
+        const double2 v = tile[L::at(p / M, p % M, gg + 1)];
         out[base + p] = v;
         if (save) save[base + p] = v;
       }
@@ -926,14 +887,6 @@ static bool adi_wave_config(int n, int *m, int *g) {
     case 1024: *m = 8; *g = 7; return true;
     default: return false;
   }
-}
-
-bool adi_fusion_supported(Precision p, int n) {
-  static const bool on = [] {
-    const char *e = std::getenv("PXP_ADI_FUSE");
-    return !(e && e[0] == '0');
-  }();
-  return on && p == kFP64 && adi_wave_n(n) > 0 && !adi_pipe_enabled();
 }
 
 int adi_wave_n(int n) {

@@ -778,15 +778,8 @@ int adi_fill_spheres(pxp_solver_s *h, pxp::AdiHalf &a, double z) {
   return PXP_OK;
 }
 
-// One ADI step (x half, then y half).  Fusion through right-hand sides
-// (AdiHalf::in_rhs/out_rhs; only where both half steps of a pair run the
-// FP64 one-wave vacuum kernel): fuse_in -- d_field holds this step's x-half
-// right-hand side, written by the previous step's y half; fuse_out -- the y
-// half writes the next step's x-half right-hand side instead of the field
-// (the caller guarantees the next step is vacuum on the same kernel and
-// that no save falls on this step).  Within the step the x half hands the y
-// half its right-hand side whenever both halves run that kernel.
-int adi_step(pxp_solver_s *h, unsigned step, bool fuse_in = false, bool fuse_out = false) {
+// One ADI step (x half, then y half) launched directly.
+int adi_step(pxp_solver_s *h, unsigned step) {
   const pxp_problem &p = h->prob;
   const double dzh = p.z.step / 2.0;  // ADI::xImplicit (src/alternatingDirectionSolver.cpp:18)
   const double k = p.wavenumber;
@@ -815,19 +808,7 @@ int adi_step(pxp_solver_s *h, unsigned step, bool fuse_in = false, bool fuse_out
   adi_fill_spheres(h, a, a.z);
   planes3_at(h, step, 0, &a.plane_delta, &a.plane_beta);
   const cd *lu = (const cd *)h->d_lu;
-  const bool x_const = a.nspheres == 0 && !a.csg.active && !a.plane_delta && !a.use_tbc && lu;
-  // whether the y half runs the vacuum kernel too (its plane: z + dz/2)
-  pxp::AdiHalf ay = a;
-  ay.z = get_z(h, step) + dzh;
-  adi_fill_spheres(h, ay, ay.z);
-  planes3_at(h, step, 1, &ay.plane_delta, &ay.plane_beta);
-  const bool y_const = ay.nspheres == 0 && !ay.csg.active && !ay.plane_delta && !ay.use_tbc && lu;
-  const bool fusable = pxp::adi_fusion_supported(h->prec, (int)n);
-  const bool fuse_mid = fusable && x_const && y_const;
-  a.in_rhs = fusable && x_const && fuse_in ? 1 : 0;
-  a.out_rhs = fuse_mid ? 1 : 0;
-  a.next_kd2_expl = kdx2;  // the y half's explicit direction is x
-  cudaError_t e = x_const
+  cudaError_t e = (a.nspheres == 0 && !a.csg.active && !a.plane_delta && !a.use_tbc && lu)
                       ? pxp::launch_adi_half_const(h->prec, a, lu, lu + n, lu + 4 * n, h->stream)
                       : pxp::launch_adi_half(h->prec, a, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "ADI x half step");
@@ -844,12 +825,10 @@ int adi_step(pxp_solver_s *h, unsigned step, bool fuse_in = false, bool fuse_out
   a.z = get_z(h, step) + dzh;
   adi_fill_spheres(h, a, a.z);
   planes3_at(h, step, 1, &a.plane_delta, &a.plane_beta);
-  a.in_rhs = fuse_mid ? 1 : 0;
-  a.out_rhs = fusable && y_const && fuse_out && !slot ? 1 : 0;
-  a.next_kd2_expl = kdy2;  // the next x half's explicit direction is y
-  e = y_const ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n,
-                                           lu + 4 * n + 4 * adi_tab_len((unsigned)n), h->stream)
-              : pxp::launch_adi_half(h->prec, a, h->stream);
+  e = (a.nspheres == 0 && !a.csg.active && !a.plane_delta && !a.use_tbc && lu)
+          ? pxp::launch_adi_half_const(h->prec, a, lu + 2 * n, lu + 3 * n,
+                                       lu + 4 * n + 4 * adi_tab_len((unsigned)n), h->stream)
+          : pxp::launch_adi_half(h->prec, a, h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "ADI y half step");
   if (slot && h->d_save_stage) return save_downsample(h, slot);
   return PXP_OK;
@@ -883,9 +862,7 @@ int adi_steps(pxp_solver_s *h, unsigned first, int nsteps) {
         const unsigned s0 = first + (unsigned)i;
         const int rc = replay_steps(h, sig, blocks, [&] {
           for (int j = 0; j < kGraphSteps; ++j)
-            // the block starts from the field and ends with it; inside it the
-            // half steps hand on their right-hand sides
-            if (int r = adi_step(h, s0 + (unsigned)j, j > 0, j < kGraphSteps - 1)) return r;
+            if (int r = adi_step(h, s0 + (unsigned)j)) return r;
           return (int)PXP_OK;
         });
         if (rc) return rc;

@@ -184,20 +184,8 @@ struct AdiHalf {
   const double *plane_delta, *plane_beta;
   const Sphere *spheres_all;
   Sphere spheres[kInlineSpheres];
-  // Half steps fused through their right-hand sides (FP64 one-wave vacuum
-  // kernel only, adi_fusion_supported): in_rhs = 1, `in` holds this half
-  // step's right-hand side (written by the previous half step) instead of
-  // the field; out_rhs = 1, `out` receives the next half step's right-hand
-  // side instead of the field (no save), formed with next_kd2_expl, the next
-  // half step's k*d*d along its explicit direction (this one's implicit).
-  int in_rhs, out_rhs;
-  double next_kd2_expl;
 };
 cudaError_t launch_adi_half(Precision p, const AdiHalf &h, cudaStream_t s);
-// Whether ADI half steps of this precision and grid size may be fused
-// through their right-hand sides (the FP64 one-wave vacuum kernel runs them,
-// the unpipelined form; PXP_ADI_FUSE=0 turns fusion off).
-bool adi_fusion_supported(Precision p, int n);
 bool adi_supported(Precision p, int n);
 // System length the general ADI kernel solves for Nx = n (n itself for the
 // powers of two adi_supported takes, else 8 times the next power of two),

@@ -49,30 +49,3 @@ def test_pipelined_wave_kernel_equals_unpipelined(n, tmp_path):
     assert res["1"].shape[0] == 1 + 30 // 7
     assert np.array_equal(res["1"].view(np.uint64), res["0"].view(np.uint64))
     assert np.std(np.abs(res["1"][0])) > 1e-3  # the sphere was crossed
-
-
-# 90 steps with saves at 40 and 80: runs of vacuum steps long enough for the
-# graph blocks (32 steps) in which consecutive steps fuse, the sphere's
-# planes near step 9 on the general kernel
-SCRIPT_LONG = (SCRIPT.replace("save_every=7", "save_every=40").replace("s.step(30)", "s.step(90)")
-               .replace("4e4", "1e5"))
-
-
-@pytest.mark.parametrize("n", [128, 512, 1000, 1024])
-def test_fused_right_hand_sides_equal_unfused(n, tmp_path):
-    """Half steps fused through their right-hand sides (each one-wave half
-    step stores the next one's right-hand side instead of the field inside
-    a graph block of vacuum steps) against PXP_ADI_FUSE=0: the same
-    arithmetic, so equal bit for bit, with the sphere's planes (general
-    kernel) and saves breaking the fused runs."""
-    res = {}
-    for fuse in ("1", "0"):
-        path = str(tmp_path / f"adi_fuse_{n}_{fuse}.npy")
-        env = dict(os.environ, PXP_ADI_FUSE=fuse, PXP_ADI_PIPE="0")
-        r = subprocess.run([sys.executable, "-c", SCRIPT_LONG, ROOT, str(n), path], env=env,
-                           capture_output=True, text=True)
-        assert r.returncode == 0, r.stderr
-        res[fuse] = np.load(path)
-    assert res["1"].shape[0] == 1 + 90 // 40
-    assert np.array_equal(res["1"].view(np.uint64), res["0"].view(np.uint64))
-    assert np.std(np.abs(res["1"][0])) > 1e-3
