@@ -901,7 +901,7 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
 // combined, and keeps the fastest step; every
 // solver with that key runs the winners from its first step on, so a field
 // never depends on when tuning happened (the variants' transforms round
-// differently).  PXP_FFT3D_VARIANT=0..4 pins both passes' variant instead.
+// differently).  PXP_FFT3D_VARIANT=0..5 pins both passes' variant instead.
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, int, unsigned>, int> g_fft3d_variant;
 

@@ -302,8 +302,10 @@ cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, cons
     if (fft3d_lines_supported(p, q.n) && wn != nullptr) return launch_fft3d_lines(p, q, kx2, wn, s);
     variant = 0;
   }
-  if (variant == 4) {
-    if (fft3d_r16_supported(p, q.n) && wn != nullptr) return launch_fft3d_r16(p, q, kx2, wn, s);
+  if (variant == 4 || variant == 5) {
+    const bool single = variant == 5;
+    if (fft3d_r16_supported(p, q.n, single) && wn != nullptr)
+      return launch_fft3d_r16(p, q, kx2, wn, s, single);
     variant = 0;
   }
 #define PXP_C3(NN)                                                                  \

@@ -55,44 +55,58 @@ namespace r16 {
 
 using r16c::tw_offset;
 
-template <typename R, int N> struct Cfg {
+// LP lines a slot (2 for complex64 by default, which makes every exchange
+// element 16 bytes; 1 gives complex64 8-byte elements and half the
+// registers), SL slots a CTA.
+template <typename R, int N, int LP = (sizeof(typename Cx<R>::T) == 8 ? 2 : 1), int SL = 2>
+struct Cfg {
   using C = typename Cx<R>::T;
   static constexpr int TL = N / 16;                       // threads per slot
-  static constexpr int S = 2;                             // line slots per CTA
+  static constexpr int S = SL;                            // line slots per CTA
   static constexpr int T = S * TL;                        // threads per CTA
-  static constexpr int LPT = sizeof(C) == 8 ? 2 : 1;      // lines per slot
+  static constexpr int LPT = LP;                          // lines per slot
+  static constexpr int EB = (int)sizeof(C) * LP;          // exchange element bytes
   static constexpr int R0 = r16c::Plan<N>::R0;             // first-pass radix
   static constexpr int NP16 = r16c::Plan<N>::NP16;         // radix-16 passes
   static constexpr int TWN = r16c::Plan<N>::TWN;           // twiddle entries
   static constexpr int GROUPS = N / LPT;                  // line groups per pass
-  static constexpr size_t XBYTES = 16 * (size_t)N;        // one slot's buffer
+  static constexpr size_t XBYTES = (size_t)EB * N;        // one slot's buffer
   // FP64 keeps kx^2 per column in shared memory for the x pass
   static constexpr size_t KXBYTES = sizeof(R) == 8 ? 8 * (size_t)N : 0;
   static constexpr size_t SMEM = S * XBYTES + 16 * (size_t)TWN + KXBYTES;
   static constexpr int BOX = N < 256 ? N : 256;  // rows of one L2 prefetch tile
+  // lines one prefetch tile covers (16-byte rows: complex64 single lines are
+  // prefetched in pairs)
+  static constexpr int PFL = EB == 8 ? 2 : LP;
   // CTAs per SM: as many as shared memory holds, at most 128 registers a
   // thread
   static constexpr int SMEM_FIT = (int)((227 * 1024) / SMEM);
-  static constexpr int REG_FIT = 65536 / (T * 128);
+  static constexpr int RPT = EB == 8 ? 64 : 128;          // registers a thread
+  static constexpr int REG_FIT = 65536 / (T * RPT);
   static constexpr int MINB = SMEM_FIT < REG_FIT ? SMEM_FIT : REG_FIT;
   static_assert(N % 16 == 0 && TL % 32 == 0, "whole warps per slot");
 };
 
-// Exchange-buffer position of element i (16-byte elements).
-__device__ __forceinline__ int xsw(int i) { return r16c::xsw16(i); }
+// Exchange-buffer position of element i (elements of EB bytes).
+template <int EB> __device__ __forceinline__ int xsw(int i) { return r16c::xsw<EB>(i); }
 
 __device__ __forceinline__ void slot_sync(int slot, int count) {
   asm volatile("bar.sync %0, %1;\n" ::"r"(1 + slot), "r"(count) : "memory");
 }
 
-// 16-byte exchange element of a thread's LPT lines at one position.
-template <typename C> struct Xe;
-template <> struct Xe<double2> {
+// Exchange element of a thread's LPT lines at one position.
+template <typename C, int LP> struct Xe;
+template <> struct Xe<double2, 1> {
   using T = double2;
   static __device__ __forceinline__ T pack(const double2 (&v)[1][16], int s) { return v[0][s]; }
   static __device__ __forceinline__ void unpack(double2 (&v)[1][16], int s, T e) { v[0][s] = e; }
 };
-template <> struct Xe<float2> {
+template <> struct Xe<float2, 1> {
+  using T = float2;
+  static __device__ __forceinline__ T pack(const float2 (&v)[1][16], int s) { return v[0][s]; }
+  static __device__ __forceinline__ void unpack(float2 (&v)[1][16], int s, T e) { v[0][s] = e; }
+};
+template <> struct Xe<float2, 2> {
   using T = float4;
   static __device__ __forceinline__ T pack(const float2 (&v)[2][16], int s) {
     return make_float4(v[0][s].x, v[0][s].y, v[1][s].x, v[1][s].y);
@@ -108,19 +122,19 @@ template <> struct Xe<float2> {
 // j + r*TL, twiddles W_{16 NS}^(r k) (k = j mod NS), 16-point DFT, write the
 // outputs to (j - k)*16 + k + r*NS -- except the last pass, which keeps
 // them in registers (natural order).
-template <int SIGN, typename R, int N, int P>
-__device__ __forceinline__ void r16_passes(typename Cx<R>::T (&v)[Cfg<R, N>::LPT][16],
-                                           typename Xe<typename Cx<R>::T>::T *X,
+template <int SIGN, typename R, int N, int LP, int SL, int P>
+__device__ __forceinline__ void r16_passes(typename Cx<R>::T (&v)[LP][16],
+                                           typename Xe<typename Cx<R>::T, LP>::T *X,
                                            const Tw<typename Cx<R>::T> *tws, int slot, int j) {
-  using K = Cfg<R, N>;
+  using K = Cfg<R, N, LP, SL>;
   using C = typename Cx<R>::T;
-  using E = Xe<C>;
+  using E = Xe<C, LP>;
   if constexpr (P < K::NP16) {
     constexpr int NS = K::R0 << (4 * P);
     constexpr int OFF = tw_offset<K::R0, P>();
     slot_sync(slot, K::TL);  // the writes of the previous pass are done
 #pragma unroll
-    for (int r = 0; r < 16; ++r) E::unpack(v, r, X[xsw(j + r * K::TL)]);
+    for (int r = 0; r < 16; ++r) E::unpack(v, r, X[xsw<K::EB>(j + r * K::TL)]);
     const int k = j & (NS - 1);
 #pragma unroll
     for (int r = 1; r < 16; ++r) {
@@ -135,9 +149,9 @@ __device__ __forceinline__ void r16_passes(typename Cx<R>::T (&v)[Cfg<R, N>::LPT
       slot_sync(slot, K::TL);  // every read of this pass is done
       const int base = (j - k) * 16 + k;
 #pragma unroll
-      for (int r = 0; r < 16; ++r) X[xsw(base + r * NS)] = E::pack(v, r);
+      for (int r = 0; r < 16; ++r) X[xsw<K::EB>(base + r * NS)] = E::pack(v, r);
     }
-    r16_passes<SIGN, R, N, P + 1>(v, X, tws, slot, j);
+    r16_passes<SIGN, R, N, LP, SL, P + 1>(v, X, tws, slot, j);
   }
 }
 
@@ -145,13 +159,13 @@ __device__ __forceinline__ void r16_passes(typename Cx<R>::T (&v)[Cfg<R, N>::LPT
 // and after (natural order).  X: the slot's exchange buffer; every write to
 // it follows a barrier that ends the previous reads, every read follows the
 // barrier that ends the writes.
-template <int SIGN, typename R, int N>
-__device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N>::LPT][16],
-                                         typename Xe<typename Cx<R>::T>::T *X,
+template <int SIGN, typename R, int N, int LP, int SL>
+__device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[LP][16],
+                                         typename Xe<typename Cx<R>::T, LP>::T *X,
                                          const Tw<typename Cx<R>::T> *tws, int slot, int j) {
-  using K = Cfg<R, N>;
+  using K = Cfg<R, N, LP, SL>;
   using C = typename Cx<R>::T;
-  using E = Xe<C>;
+  using E = Xe<C, LP>;
   constexpr int TL = K::TL, R0 = K::R0;
   // first pass: radix R0 over the thread's own points; butterfly
   // b = j + u*TL takes points s = u + r*(16/R0) and writes b*R0 + r
@@ -161,18 +175,18 @@ __device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N>::LPT][
 #pragma unroll
   for (int u = 0; u < 16 / R0; ++u)
 #pragma unroll
-    for (int r = 0; r < R0; ++r) X[xsw((j + u * TL) * R0 + r)] = E::pack(v, u + r * (16 / R0));
-  r16_passes<SIGN, R, N, 0>(v, X, tws, slot, j);
+    for (int r = 0; r < R0; ++r) X[xsw<K::EB>((j + u * TL) * R0 + r)] = E::pack(v, u + r * (16 / R0));
+  r16_passes<SIGN, R, N, LP, SL, 0>(v, X, tws, slot, j);
 }
 
-template <typename R, int N>
-__global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
+template <typename R, int N, int LP, int SL>
+__global__ void __launch_bounds__(Cfg<R, N, LP, SL>::T, Cfg<R, N, LP, SL>::MINB)
     fft3d_r16_kernel(const __grid_constant__ Fft3dPass q,
                      const __grid_constant__ CUtensorMap tmap, const double *__restrict__ gkx2,
                      const Tw<typename Cx<R>::T> *__restrict__ wn) {
-  using K = Cfg<R, N>;
+  using K = Cfg<R, N, LP, SL>;
   using C = typename Cx<R>::T;
-  using E = Xe<C>;
+  using E = Xe<C, LP>;
   using W = Tw<C>;
   constexpr int TL = K::TL, LPT = K::LPT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -206,7 +220,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
     if (xpass) {
       for (int b = 0; b < N / K::BOX; ++b)
         asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];\n" ::"l"(&tmap),
-                     "r"(2 * gp * LPT), "r"(b * K::BOX)
+                     "r"(2 * ((gp * LPT) & ~(K::PFL - 1))), "r"(b * K::BOX)
                      : "memory");
     } else {
       asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(field + (long long)gp * LPT * N),
@@ -232,7 +246,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
       }
     }
     if (xpass) {
-      line_fft<-1, R, N>(v, X, tws, slot, j);
+      line_fft<-1, R, N, LP, SL>(v, X, tws, slot, j);
       // propagator K = exp(-i a (kx^2 + ky^2)) (src/fftSolver3D.cpp:24-30, 87-120)
 #pragma unroll
       for (int t = 0; t < LPT; ++t) {
@@ -248,10 +262,10 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
           v[t][s] = prop3(q, v[t][s], sizeof(R) == 8 ? skx2[e] : 0.0, ky2, e, line);
         }
       }
-      line_fft<+1, R, N>(v, X, tws, slot, j);
+      line_fft<+1, R, N, LP, SL>(v, X, tws, slot, j);
     } else {
       if (q.mode >= 2) {
-        line_fft<+1, R, N>(v, X, tws, slot, j);
+        line_fft<+1, R, N, LP, SL>(v, X, tws, slot, j);
         if (scale_only) {
 #pragma unroll
           for (int t = 0; t < LPT; ++t)
@@ -264,18 +278,18 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
           // one non-unrolled refract3 loop
           slot_sync(slot, TL);
 #pragma unroll
-          for (int s = 0; s < 16; ++s) X[xsw(j + s * TL)] = E::pack(v, s);
+          for (int s = 0; s < 16; ++s) X[xsw<K::EB>(j + s * TL)] = E::pack(v, s);
 #pragma unroll 1
           for (int s = 0; s < 16; ++s) {
             const int e = j + s * TL;  // y index
             C w[LPT][16];
-            E::unpack(w, 0, X[xsw(e)]);
+            E::unpack(w, 0, X[xsw<K::EB>(e)]);
 #pragma unroll
             for (int t = 0; t < LPT; ++t) w[t][0] = refract3<R>(q, w[t][0], line0 + t, e, inv_norm);
-            X[xsw(e)] = E::pack(w, 0);
+            X[xsw<K::EB>(e)] = E::pack(w, 0);
           }
 #pragma unroll
-          for (int s = 0; s < 16; ++s) E::unpack(v, s, X[xsw(j + s * TL)]);
+          for (int s = 0; s < 16; ++s) E::unpack(v, s, X[xsw<K::EB>(j + s * TL)]);
         }
         if (save) {
 #pragma unroll
@@ -284,7 +298,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
             for (int s = 0; s < 16; ++s) save[(long long)(line0 + t) * N + j + s * TL] = v[t][s];
         }
       }
-      if (q.mode != 3) line_fft<-1, R, N>(v, X, tws, slot, j);
+      if (q.mode != 3) line_fft<-1, R, N, LP, SL>(v, X, tws, slot, j);
     }
 #pragma unroll
     for (int s = 0; s < 16; ++s) {
@@ -299,12 +313,12 @@ __global__ void __launch_bounds__(Cfg<R, N>::T, Cfg<R, N>::MINB)
   }
 }
 
-template <typename R, int N>
+template <typename R, int N, int LP, int SL>
 cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaStream_t s) {
-  using K = Cfg<R, N>;
+  using K = Cfg<R, N, LP, SL>;
   using W = Tw<typename Cx<R>::T>;
   static_assert(K::SMEM <= 227 * 1024, "line slots exceed shared memory");
-  auto k = fft3d_r16_kernel<R, N>;
+  auto k = fft3d_r16_kernel<R, N, LP, SL>;
   {
     const cudaError_t e = raise_dynamic_smem((const void *)k, (int)K::SMEM);
     if (e != cudaSuccess) return e;
@@ -335,7 +349,7 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
   CUtensorMap tmap;
   std::memset(&tmap, 0, sizeof(tmap));
   if (q.mode == 1) {
-    const cudaError_t te = encode_field_tmap(q.field, N, (int)sizeof(R), 2 * K::LPT, K::BOX, &tmap);
+    const cudaError_t te = encode_field_tmap(q.field, N, (int)sizeof(R), 2 * K::PFL, K::BOX, &tmap);
     if (te != cudaSuccess) return te;
   }
   return cudaLaunchKernelEx(&cfg, k, q, tmap, kx2, reinterpret_cast<const W *>(wnv));
@@ -343,16 +357,18 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
 
 }  // namespace r16
 
-bool fft3d_r16_supported(Precision p, int n) {
-  (void)p;
+bool fft3d_r16_supported(Precision p, int n, bool single) {
+  if (single && p != kFP32) return false;
   return n >= 512 && n <= 4096 && !(n & (n - 1));
 }
 
 cudaError_t launch_fft3d_r16(Precision p, const Fft3dPass &q, const double *kx2, const void *wn,
-                             cudaStream_t s) {
-#define PXP_R16(NN)                                                                     \
-  case NN:                                                                              \
-    return p == kFP64 ? r16::launch<double, NN>(q, kx2, wn, s) : r16::launch<float, NN>(q, kx2, wn, s);
+                             cudaStream_t s, bool single) {
+#define PXP_R16(NN)                                                                      \
+  case NN:                                                                               \
+    if (p == kFP64) return r16::launch<double, NN, 1, 2>(q, kx2, wn, s);                 \
+    return single ? r16::launch<float, NN, 1, 4>(q, kx2, wn, s)                          \
+                  : r16::launch<float, NN, 2, 2>(q, kx2, wn, s);
   switch (q.n) {
     PXP_R16(512) PXP_R16(1024) PXP_R16(2048) PXP_R16(4096)
     default:

@@ -331,19 +331,21 @@ struct Fft3dPass {
 // 8, single buffer, tables through L1; 2 = radix 16, single buffer; 3 =
 // register-resident transforms with TMA-staged lines (fft3d_lines.cu; n up
 // to 4096); 4 = 16 points per thread, radix-16 passes, two line slots per
-// CTA (fft3d_r16.cu; n = 512 .. 4096).  Sizes a variant does not take run
-// variant 0.
+// CTA (fft3d_r16.cu; n = 512 .. 4096); 5 = the same with complex64 lines
+// one a slot and four slots a CTA (FP32 only: half the registers, twice the
+// warps).  Sizes a variant does not take run variant 0.
 // kx2: n doubles, fl(kx*kx) per column index; q.twiddle / tw16: Stockham
 // twiddles for radix 8 / radix 16 pass orders; wn: n complex128
 // exp(-2 pi i m / n), m < n.
 cudaError_t launch_fft3d_pass(Precision p, const Fft3dPass &q, int variant, const double *kx2,
                               const void *tw16, const void *wn, cudaStream_t s);
-constexpr int kFft3dVariants = 5;
+constexpr int kFft3dVariants = 6;
 bool fft3d_supported(Precision p, int n);
 bool fft3d_lines_supported(Precision p, int n);
-bool fft3d_r16_supported(Precision p, int n);
+// single: complex64 lines one a slot, four slots a CTA (variant 5)
+bool fft3d_r16_supported(Precision p, int n, bool single = false);
 cudaError_t launch_fft3d_r16(Precision p, const Fft3dPass &q, const double *kx2, const void *wn,
-                             cudaStream_t s);
+                             cudaStream_t s, bool single = false);
 // Line passes of a size that is not a power of two (Bluestein transforms,
 // fft3d_blu.cu); q.chirp, q.bconv, q.m and q.twiddle as described above.
 cudaError_t launch_fft3d_bluestein(Precision p, const Fft3dPass &q, const double *kx2,

@@ -155,11 +155,13 @@ def _variant(monkeypatch):
 
 @pytest.mark.parametrize("n", [64, 128, 256, 512, 1024, 2048])
 @pytest.mark.parametrize("precision", [0, 1])
-@pytest.mark.parametrize("variant", [3, 4])
+@pytest.mark.parametrize("variant", [3, 4, 5])
 def test_fft3d_register_line_kernel_every_size(n, precision, variant, _variant):
     """The register-resident line kernels -- variant 3 (8 points a thread,
-    TMA-staged lines) and variant 4 (16 points a thread, radix-16 passes, two
-    line slots a CTA; from 512 points) -- at every size they take, FP64 and
+    TMA-staged lines), variant 4 (16 points a thread, radix-16 passes, two
+    line slots a CTA; from 512 points) and variant 5 (variant 4 with
+    complex64 lines one a slot, four slots a CTA; FP64 runs variant 0 there)
+    -- at every size they take, FP64 and
     FP32: spheres crossing the sampling planes (the refraction integral at
     their rims), the absorber, saves, and calls split in chunks (the
     forward-only and inverse-only passes at call ends)."""
@@ -178,7 +180,7 @@ def test_fft3d_register_line_kernel_every_size(n, precision, variant, _variant):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-@pytest.mark.parametrize("variant", [3, 4])
+@pytest.mark.parametrize("variant", [3, 4, 5])
 def test_fft3d_register_line_kernel_4096(precision, variant, _variant):
     _variant(variant)
     p = wl.spheres_fft3d()
