@@ -957,7 +957,7 @@ unsigned wait_timeouts(cudaStream_t s) {
           cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return 0;
-  return v + fft3d_lines_wait_timeouts(s);
+  return v + fft3d_lines_wait_timeouts(s) + fft3d_r16_wait_timeouts(s);
 }
 
 cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, const void *hh,

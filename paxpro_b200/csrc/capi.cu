@@ -893,12 +893,10 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
 
 // Launch-variant autotuner of the FFTSolver3D passes.  The first solver with
 // a given (device, precision, n) times every variant of each pass (x and y
-// separately) on a zeroed scratch field -- three rounds of one untimed
-// launch and three timed back to back, the best round kept; the untimed
-// launch keeps the device busy while the host prepares the timed ones, so
-// host-side launch set-up never counts -- then times whole steps (x and y
-// passes interleaved) of every variant and of the two per-pass winners
-// combined, and keeps the fastest step; every
+// separately) on a zeroed scratch field -- launches replayed from a CUDA
+// graph, so host-side launch set-up never counts -- then times whole steps
+// (x and y passes interleaved) of every variant and of the two per-pass
+// winners combined, and keeps the fastest step; every
 // solver with that key runs the winners from its first step on, so a field
 // never depends on when tuning happened (the variants' transforms round
 // differently).  PXP_FFT3D_VARIANT=0..5 pins both passes' variant instead.
@@ -944,29 +942,66 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
   // the x pass (mode 1) and the y pass (mode 2) are separate launches with
   // the same field layout before and after, so each takes its own fastest
   // variant
+  // Device time of `enqueue` (one launch or one step): four copies captured
+  // in a CUDA graph, the graph launched once untimed and then three times
+  // between events, the fastest kept -- no host-side launch set-up between
+  // the kernels (steps are replayed from graphs as well), however short
+  // they are.  A direct launch first sets up each kernel's one-time state.
+  auto graph_time = [&](auto enqueue) -> float {
+    float tmin = 1e30f;
+    if (e != cudaSuccess) return tmin;
+    if ((e = enqueue()) != cudaSuccess || (e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
+      return tmin;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ge = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (ge == cudaSuccess) {
+      cudaError_t ce = cudaSuccess;
+      for (int k = 0; k < 4 && ce == cudaSuccess; ++k) ce = enqueue();
+      ge = cudaStreamEndCapture(h->stream, &graph);
+      if (ge == cudaSuccess) ge = ce;
+    }
+    if (ge == cudaSuccess) ge = cudaGraphInstantiate(&exec, graph, 0);
+    if (ge == cudaSuccess) ge = cudaGraphLaunch(exec, h->stream);
+    for (int rep = 0; rep < 3 && ge == cudaSuccess; ++rep) {
+      cudaEventRecord(e0, h->stream);
+      ge = cudaGraphLaunch(exec, h->stream);
+      cudaEventRecord(e1, h->stream);
+      if (ge == cudaSuccess) ge = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (ge == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+        tmin = std::min(tmin, ms / 4.f);
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (ge == cudaSuccess) return tmin;
+    // no graph (capture refused): direct launches behind an untimed one
+    cudaGetLastError();
+    tmin = 1e30f;
+    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+      e = enqueue();
+      cudaEventRecord(e0, h->stream);
+      for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = enqueue();
+      cudaEventRecord(e1, h->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+        tmin = std::min(tmin, ms / 3.f);
+    }
+    return tmin;
+  };
   int best_v[2] = {0, 0};
   float best[2] = {1e30f, 1e30f};
   if ((e = cudaMemsetAsync(scratch, 0, bytes, h->stream)) == cudaSuccess) {
     for (int v = 0; v < pxp::kFft3dVariants && e == cudaSuccess; ++v) {
       for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
-        q.mode = pass == 0 ? 1 : 2;
-        float tmin = 1e30f;
-        for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
-          // an untimed launch first keeps the device busy while the host
-          // prepares the timed ones (tensor maps, launch attributes), so the
-          // events bracket device time only
-          e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
-          cudaEventRecord(e0, h->stream);
-          for (int k = 0; k < 3 && e == cudaSuccess; ++k)
-            e = pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
-          cudaEventRecord(e1, h->stream);
-          if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-          float ms = 0.f;
-          if (e == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
-            tmin = std::min(tmin, ms / 3.f);
-        }
-        if (tmin < best[pass]) {
-          best[pass] = tmin;
+        const int mode = pass == 0 ? 1 : 2;
+        const float t = graph_time([&] {
+          q.mode = mode;
+          return pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
+        });
+        if (t < best[pass]) {
+          best[pass] = t;
           best_v[pass] = v;
         }
       }
@@ -980,31 +1015,20 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
   if (best_v[0] != best_v[1]) cands.push_back(fft3d_variant_code(best_v[0], best_v[1]));
   int best_code = cands.back();
   float best_step = 1e30f;
-  auto step_pair = [&](int code) {
-    q.mode = 1;
-    cudaError_t r = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(code, 1),
-                                           (const double *)kx2, tw16, wn, h->stream);
-    q.mode = 2;
-    if (r == cudaSuccess)
-      r = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(code, 2), (const double *)kx2,
-                                 tw16, wn, h->stream);
-    return r;
-  };
   for (int code : cands) {
     if (e != cudaSuccess) break;
-    float tmin = 1e30f;
-    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
-      e = step_pair(code);  // untimed
-      cudaEventRecord(e0, h->stream);
-      for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = step_pair(code);
-      cudaEventRecord(e1, h->stream);
-      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-      float ms = 0.f;
-      if (e == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
-        tmin = std::min(tmin, ms / 3.f);
-    }
-    if (tmin < best_step) {
-      best_step = tmin;
+    const float t = graph_time([&] {
+      q.mode = 1;
+      cudaError_t r = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(code, 1),
+                                             (const double *)kx2, tw16, wn, h->stream);
+      q.mode = 2;
+      if (r == cudaSuccess)
+        r = pxp::launch_fft3d_pass(h->prec, q, fft3d_variant_of(code, 2), (const double *)kx2,
+                                   tw16, wn, h->stream);
+      return r;
+    });
+    if (t < best_step) {
+      best_step = t;
       best_code = code;
     }
   }

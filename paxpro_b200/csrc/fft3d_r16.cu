@@ -44,10 +44,15 @@
 
 #include <cstring>
 
+#include "bulk_copy.cuh"
 #include "fft3d_point.cuh"
 #include "fft_r16.cuh"
 
 namespace pxp {
+
+// waits of the radix-16 line kernel that ran out on this device, read by
+// the host
+__device__ unsigned int g_r16_wait_timeouts = 0;
 
 cudaError_t encode_field_tmap(void *field, int n, int real_bytes, int box_reals, int box_rows,
                               CUtensorMap *out);
@@ -73,7 +78,10 @@ struct Cfg {
   static constexpr size_t XBYTES = (size_t)EB * N;        // one slot's buffer
   // FP64 keeps kx^2 per column in shared memory for the x pass
   static constexpr size_t KXBYTES = sizeof(R) == 8 ? 8 * (size_t)N : 0;
-  static constexpr size_t SMEM = S * XBYTES + 16 * (size_t)TWN + KXBYTES;
+  // x lines by TMA tiles (loads into and stores from the slot's buffer)
+  // where an exchange element is 16 bytes
+  static constexpr bool XTMA = EB == 16;
+  static constexpr size_t SMEM = 128 + S * XBYTES + 16 * (size_t)TWN + KXBYTES + 16 * S;
   static constexpr int BOX = N < 256 ? N : 256;  // rows of one L2 prefetch tile
   // lines one prefetch tile covers (16-byte rows: complex64 single lines are
   // prefetched in pairs)
@@ -190,11 +198,20 @@ __global__ void __launch_bounds__(Cfg<R, N, LP, SL>::T, Cfg<R, N, LP, SL>::MINB)
   using W = Tw<C>;
   constexpr int TL = K::TL, LPT = K::LPT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char *base = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   const int tid = threadIdx.x;
   const int slot = tid / TL, j = tid % TL;
-  typename E::T *X = reinterpret_cast<typename E::T *>(smem_raw + slot * K::XBYTES);
-  W *tws = reinterpret_cast<W *>(smem_raw + K::S * K::XBYTES);
-  double *skx2 = reinterpret_cast<double *>(smem_raw + K::S * K::XBYTES + 16 * (size_t)K::TWN);
+  typename E::T *X = reinterpret_cast<typename E::T *>(base + slot * K::XBYTES);
+  W *tws = reinterpret_cast<W *>(base + K::S * K::XBYTES);
+  double *skx2 = reinterpret_cast<double *>(base + K::S * K::XBYTES + 16 * (size_t)K::TWN);
+  uint64_t *sbar = reinterpret_cast<uint64_t *>(base + K::S * K::XBYTES + 16 * (size_t)K::TWN +
+                                                K::KXBYTES) + 2 * slot;
+  __shared__ int slot_fail[K::S];
+  if (j == 0) {
+    mbar_init(sbar, 1);
+    slot_fail[slot] = 0;
+  }
   // twiddles of every radix-16 pass: entry off + (r-1)*NS + k = W_{16 NS}^(r k)
   r16c::load_twiddles<N>(tws, wn, tid, K::T);
   if constexpr (sizeof(R) == 8) {
@@ -229,20 +246,50 @@ __global__ void __launch_bounds__(Cfg<R, N, LP, SL>::T, Cfg<R, N, LP, SL>::MINB)
     }
   };
   if (j == 0) prefetch(blockIdx.x * K::S + slot);
-  for (int g = blockIdx.x * K::S + slot; g < K::GROUPS; g += nslots) {
+  int it = 0;
+  for (int g = blockIdx.x * K::S + slot; g < K::GROUPS; g += nslots, ++it) {
     const int line0 = g * LPT;
     if (j == 0) prefetch(g + nslots);  // this slot's next group, while this one computes
     C v[LPT][16];
-    // load: x lines are columns (element e of line l at e*N + l; a complex64
-    // thread's two lines are adjacent), y lines are rows
+    if (K::XTMA && xpass) {
+      // the columns arrive by N/BOX TMA tiles into the slot's buffer, in
+      // natural order (element e at X[e]), once every thread of the slot is
+      // past its reads of the buffer; one thread arms the slot's mbarrier
+      // and waits (bounded), a slot barrier publishes the line
+      slot_sync(slot, TL);
+      if (j == 0) {
+        mbar_arrive_expect_tx(sbar, (unsigned)(K::EB * N));
+        const unsigned dst = smem_u32(X);
+        for (int b = 0; b < N / K::BOX; ++b)
+          asm volatile(
+              "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+              " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst + (unsigned)(b * K::BOX * K::EB)),
+              "l"(&tmap), "r"(2 * line0), "r"(b * K::BOX), "r"(smem_u32(sbar))
+              : "memory");
+        if (!mbar_wait_bounded(sbar, it & 1, 2000000000ull)) {
+          atomicAdd(&g_r16_wait_timeouts, 1u);
+          mbar_wait_bounded(sbar, it & 1, 2000000000ull);  // the copy may still be in flight
+          slot_fail[slot] = 1;
+        }
+      }
+      slot_sync(slot, TL);
+      if (slot_fail[slot]) break;
+      (void)mbar_try_wait(sbar, it & 1);  // completed phase: orders the line for this thread
 #pragma unroll
-    for (int s = 0; s < 16; ++s) {
-      const int e = j + s * TL;
-      if (xpass) {
-        E::unpack(v, s, *reinterpret_cast<const typename E::T *>(field + (long long)e * N + line0));
-      } else {
+      for (int s = 0; s < 16; ++s) E::unpack(v, s, X[j + s * TL]);
+    } else {
+      // x lines are columns (element e of line l at e*N + l; a complex64
+      // thread's two lines are adjacent), y lines are rows
 #pragma unroll
-        for (int t = 0; t < LPT; ++t) v[t][s] = field[(long long)(line0 + t) * N + e];
+      for (int s = 0; s < 16; ++s) {
+        const int e = j + s * TL;
+        if (xpass) {
+          E::unpack(v, s,
+                    *reinterpret_cast<const typename E::T *>(field + (long long)e * N + line0));
+        } else {
+#pragma unroll
+          for (int t = 0; t < LPT; ++t) v[t][s] = field[(long long)(line0 + t) * N + e];
+        }
       }
     }
     if (xpass) {
@@ -300,17 +347,42 @@ __global__ void __launch_bounds__(Cfg<R, N, LP, SL>::T, Cfg<R, N, LP, SL>::MINB)
       }
       if (q.mode != 3) line_fft<-1, R, N, LP, SL>(v, X, tws, slot, j);
     }
+    if (K::XTMA && xpass) {
+      // the columns leave by TMA tile stores from the slot's buffer (natural
+      // order) once every thread is past the last pass's reads; the issuing
+      // thread waits until the copies have read the buffer before it joins
+      // the next line's first slot barrier
+      slot_sync(slot, TL);
 #pragma unroll
-    for (int s = 0; s < 16; ++s) {
-      const int e = j + s * TL;
-      if (xpass) {
-        *reinterpret_cast<typename E::T *>(field + (long long)e * N + line0) = E::pack(v, s);
-      } else {
+      for (int s = 0; s < 16; ++s) X[j + s * TL] = E::pack(v, s);
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      slot_sync(slot, TL);
+      if (j == 0) {
+        const unsigned src = smem_u32(X);
+        for (int b = 0; b < N / K::BOX; ++b)
+          asm volatile(
+              "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                  &tmap),
+              "r"(2 * line0), "r"(b * K::BOX), "r"(src + (unsigned)(b * K::BOX * K::EB))
+              : "memory");
+        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+      }
+    } else {
 #pragma unroll
-        for (int t = 0; t < LPT; ++t) field[(long long)(line0 + t) * N + e] = v[t][s];
+      for (int s = 0; s < 16; ++s) {
+        const int e = j + s * TL;
+        if (xpass) {
+          *reinterpret_cast<typename E::T *>(field + (long long)e * N + line0) = E::pack(v, s);
+        } else {
+#pragma unroll
+          for (int t = 0; t < LPT; ++t) field[(long long)(line0 + t) * N + e] = v[t][s];
+        }
       }
     }
   }
+  // the slot's last tile stores complete before its threads leave
+  if (j == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
 }
 
 template <typename R, int N, int LP, int SL>
@@ -356,6 +428,15 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
 }
 
 }  // namespace r16
+
+unsigned fft3d_r16_wait_timeouts(cudaStream_t s) {
+  unsigned v = 0;
+  if (cudaMemcpyFromSymbolAsync(&v, g_r16_wait_timeouts, sizeof(v), 0, cudaMemcpyDeviceToHost,
+                                s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return 0;
+  return v;
+}
 
 bool fft3d_r16_supported(Precision p, int n, bool single) {
   if (single && p != kFP32) return false;

@@ -354,5 +354,6 @@ cudaError_t launch_fft3d_lines(Precision p, const Fft3dPass &q, const double *kx
                                cudaStream_t s);
 // Bounded waits of the line-pass kernels that ran out on the current device.
 unsigned fft3d_lines_wait_timeouts(cudaStream_t s);
+unsigned fft3d_r16_wait_timeouts(cudaStream_t s);
 
 }  // namespace pxp
