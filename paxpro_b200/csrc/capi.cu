@@ -361,13 +361,15 @@ int shared_table_n(pxp_solver_s *h, int kind, unsigned n, void **out) {
   return PXP_OK;
 }
 
-// FP32 FFTSolver3D: one factor of the separable propagator, exp(-i a k_i^2)
-// with k_i = spatialFreq(i) for the x (axis 0) or y (axis 1) step and
-// a = dz / (2k), the phase reduced in extended precision; split form.
+// FFTSolver3D: one factor of the separable propagator, exp(-i a k_i^2) with
+// k_i = spatialFreq(i) for the x (axis 0) or y (axis 1) step and
+// a = dz / (2k), the phase reduced in extended precision; complex128 in
+// FP64, the split form in FP32.
 int prop3_table(pxp_solver_s *h, int axis, void **out) {
   const unsigned n = h->nx;
   const double step = axis == 0 ? h->prob.x.step : h->prob.y.step;
-  TableKey key{h->prob.device, 10, n, step, h->prob.z.step, h->prob.wavenumber, 1};
+  TableKey key{h->prob.device, 10, n, step, h->prob.z.step, h->prob.wavenumber,
+               h->prec == pxp::kFP32 ? 1 : 0};
   std::lock_guard<std::mutex> lk(g_table_mutex);
   auto it = g_tables.find(key);
   if (it != g_tables.end()) {
@@ -1178,7 +1180,10 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
     if (int rc = shared_table(h, 3, &tw16)) return rc;
     if (int rc = shared_table(h, 4, &wn)) return rc;
   }
-  if (h->prec == pxp::kFP32) {
+  // the propagator's x and y factor tables (FP32 always; FP64 unless
+  // PXP_FFT3D_JOINT_PROP=1 asks for the reference's joint argument)
+  const char *joint = std::getenv("PXP_FFT3D_JOINT_PROP");
+  if (h->prec == pxp::kFP32 || !(joint && joint[0] == '1')) {
     void *px = nullptr, *py = nullptr;
     if (int rc = prop3_table(h, 0, &px)) return rc;
     if (int rc = prop3_table(h, 1, &py)) return rc;

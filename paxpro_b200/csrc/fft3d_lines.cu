@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
     }
   }
   double kx2[8] = {};
-  if (sizeof(R) == 8 && xpass) {  // FP64 forms the propagator's argument per point
+  if (sizeof(R) == 8 && xpass && q.prop_x == nullptr) {  // FP64's joint argument per point
 #pragma unroll
     for (int s = 0; s < 8; ++s) kx2[s] = gkx2[j + s * K::TL];
   }

@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LP, SL>::T, Cfg<R, N, LP, SL>::MINB)
   // twiddles of every radix-16 pass: entry off + (r-1)*NS + k = W_{16 NS}^(r k)
   r16c::load_twiddles<N>(tws, wn, tid, K::T);
   if constexpr (sizeof(R) == 8) {
-    if (q.mode == 1)
+    if (q.mode == 1 && q.prop_x == nullptr)  // FP64's joint argument per point
       for (int i = tid; i < N; i += K::T) skx2[i] = gkx2[i];
   }
   __syncthreads();

@@ -213,3 +213,17 @@ def test_fft3d_sizes_other_than_powers_of_two(n, precision):
     else:
         assert max(_int_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP32_INT_TOL
     assert np.std(np.abs(out)) > 1e-5
+
+
+@pytest.mark.parametrize("n", [256, 1024])
+def test_fft3d_fp64_joint_propagator_argument(n, monkeypatch):
+    """PXP_FFT3D_JOINT_PROP=1: the x pass forms the reference's propagator
+    argument fl(a * fl(kx^2 + ky^2)) and its sin/cos at every point instead
+    of multiplying the x and y factor tables; every save within 1e-10 of the
+    oracle as with the tables."""
+    monkeypatch.setenv("PXP_FFT3D_JOINT_PROP", "1")
+    sph = [(20.0, 10.0, 2500.0, 200.0, 3e-5, 6e-7), (-150.0, 120.0, 4100.0, 90.0, 2e-5, 4e-7)]
+    out, saves, ref_out, ref_saves = _run_both(n, 1000.0, 0.0, 1000.0, 6, sph, save_every=2,
+                                               chunks=2, precision=0)
+    assert max(_rel(a, b) for a, b in zip(saves, ref_saves)) <= FP64_TOL
+    assert _rel(out, ref_out) <= FP64_TOL
