@@ -290,6 +290,8 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
   int cur = 1;
   for (int it = 0; g < K::GROUPS; ++it, g += gridDim.x) {
     if (tid == 0) {
+      // the previous group's tile stores have read their buffer (x pass)
+      asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
       const bool ok = mbar_wait_bounded(bar, it & 1, 2000000000ull);
       if (!ok) {
         atomicAdd(&g_lines_wait_timeouts, 1u);
@@ -378,12 +380,15 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
       if (q.mode != 3) line_fft<-1, R, N, LG>(v, X0, X1, cur, tw, tws, slot, j, nothing);
     }
     if (xpass) {
-      // columns leave by TMA tile stores from the exchange buffer the last
-      // pass did not read (the staging layout: element e of line l at
-      // e*L + l), instead of 16-byte stores strided by the row length; the
-      // buffer is the next group's first-pass target, so thread 0 waits
-      // until the copies have read it before the CTA moves on
-      C *F = cur ? X0 : X1;
+      // columns leave by TMA tile stores (the staging layout: element e of
+      // line l at e*L + l), instead of 16-byte stores strided by the row
+      // length, from the exchange buffer the last pass read, once every
+      // thread is past those reads: the next group writes that buffer only
+      // in its second pass, after its first-pass barrier, and thread 0 waits
+      // for the copies' reads at the top of the next group, beside its wait
+      // for the staged line -- off the critical path
+      __syncthreads();
+      C *F = cur ? X1 : X0;
 #pragma unroll
       for (int t = 0; t < K::LPT; ++t)
 #pragma unroll
@@ -399,9 +404,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
               "r"(2 * line0), "r"(b * K::BC), "r"(src + (unsigned)(b * K::BC * K::L * sizeof(C)))
               : "memory");
         asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
       }
-      __syncthreads();
     } else {
       // rows: natural-order outputs straight to global memory (coalesced)
 #pragma unroll
