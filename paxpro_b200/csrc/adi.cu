@@ -889,14 +889,6 @@ static bool adi_wave_config(int n, int *m, int *g) {
   }
 }
 
-static bool adi_wave_one_system() {
-  static const bool on = [] {
-    const char *e = std::getenv("PXP_ADI_S");
-    return e && e[0] == '1';
-  }();
-  return on;
-}
-
 int adi_wave_n(int n) {
   static const int sizes[] = {64, 128, 256, 512, 768, 1024};
   if (n < 4) return 0;
@@ -981,11 +973,7 @@ cudaError_t launch_adi_half_const(Precision p, const AdiHalf &h, const void *g, 
       case 256: return adi_const_wave_launch<256, 8, 2, 1>(h, staged, s);
       case 512: return adi_const_wave_launch<512, 8, 4, 2>(h, staged, s);
       case 768: return adi_const_wave_launch<768, 8, 6, 2>(h, staged, s);
-      case 1024:
-        // one system a thread group (seven groups, 28 warps at 72 registers)
-        // or two (four groups, 16 warps at 128): PXP_ADI_S=1 selects the first
-        return adi_wave_one_system() ? adi_const_wave_launch<1024, 8, 7, 1>(h, staged, s)
-                                     : adi_const_wave_launch<1024, 8, 7, 2>(h, staged, s);
+      case 1024: return adi_const_wave_launch<1024, 8, 7, 2>(h, staged, s);
       default: break;
     }
   }
