@@ -23,6 +23,7 @@
 // point of the plane.
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 
 #include "bulk_copy.cuh"
 #include "csg.cuh"
@@ -470,8 +471,6 @@ __device__ __forceinline__ void multi_exclusive_scan(double2 &a, double2 (&b)[S]
   for (int j = 0; j < S; ++j) b[j] = eb[j];
 }
 
-// Right-hand sides and solve of the S systems sys0 .. sys0+S-1 of this CTA
-// for chunk c: r[j][m] holds the solution of row c*M + m of system sys0 + j.
 // Right-hand sides and solve of systems sys0 .. sys0+SC-1 of this CTA for
 // chunk c: r[j][m] holds the solution of row c*M + m of system sys0 + j.
 template <int N, int M, int G, bool XH, int SCAP, int S>
@@ -485,6 +484,9 @@ __device__ __forceinline__ void adi_group_solve(double2 (&r)[SCAP][M], const Adi
   const double inv_kd2_expl = __ddiv_rn(1.0, h.kd2_expl);
   const double hk = 0.5 * inv_kd2_expl;
   const double2 coef = mk(h.inv_dzh, -inv_kd2_expl);
+  // table chunk: inside the run of identical chunks every thread reads the
+  // run's first chunk, so a warp's table reads there are broadcasts
+  const int ct = (c > h.tab_c0 && c < h.tab_c1) ? h.tab_c0 : c;
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     double2 v[S + 2];
@@ -503,22 +505,22 @@ __device__ __forceinline__ void adi_group_solve(double2 (&r)[SCAP][M], const Adi
   // forward, zero carry-in: y_i = g_i r_i + h_i y_{i-1}
   double2 y[S];
   {
-    const double2 g0 = gs[cslot<M, P>(c, 0)];
+    const double2 g0 = gs[cslot<M, P>(ct, 0)];
 #pragma unroll
     for (int j = 0; j < S; ++j) r[j][0] = y[j] = cmul(g0, r[j][0]);
   }
 #pragma unroll
   for (int m = 1; m < M; ++m) {
-    const int k = cslot<M, P>(c, m);
+    const int k = cslot<M, P>(ct, m);
     const double2 gm = gs[k], hm = hs[k];
 #pragma unroll
     for (int j = 0; j < S; ++j) r[j][m] = y[j] = cfma(hm, y[j], cmul(gm, r[j][m]));
   }
-  double2 a = pf[cslot<M, P>(c, M - 1)];
+  double2 a = pf[cslot<M, P>(ct, M - 1)];
   multi_exclusive_scan<P, S, false>(a, y, scratch, gtid, bar);
 #pragma unroll
   for (int m = 0; m < M; ++m) {
-    const double2 f = pf[cslot<M, P>(c, m)];
+    const double2 f = pf[cslot<M, P>(ct, m)];
 #pragma unroll
     for (int j = 0; j < S; ++j) r[j][m] = cfma(f, y[j], r[j][m]);
   }
@@ -528,15 +530,15 @@ __device__ __forceinline__ void adi_group_solve(double2 (&r)[SCAP][M], const Adi
   for (int j = 0; j < S; ++j) x[j] = r[j][M - 1];
 #pragma unroll
   for (int m = M - 2; m >= 0; --m) {
-    const double2 hm = hs[cslot<M, P>(c, m)];
+    const double2 hm = hs[cslot<M, P>(ct, m)];
 #pragma unroll
     for (int j = 0; j < S; ++j) r[j][m] = x[j] = cfma(hm, x[j], r[j][m]);
   }
-  a = pb[cslot<M, P>(c, 0)];
+  a = pb[cslot<M, P>(ct, 0)];
   multi_exclusive_scan<P, S, true>(a, x, scratch, gtid, bar);
 #pragma unroll
   for (int m = 0; m < M; ++m) {
-    const double2 f = pb[cslot<M, P>(c, m)];
+    const double2 f = pb[cslot<M, P>(ct, m)];
 #pragma unroll
     for (int j = 0; j < S; ++j) r[j][m] = cfma(f, x[j], r[j][m]);
   }
@@ -897,7 +899,7 @@ int adi_wave_n(int n) {
   return 0;
 }
 
-bool adi_const_staged_tables(int n, const double *g, const double *h, double *out) {
+bool adi_const_staged_tables(int n, const double *g, const double *h, double *out, int run[2]) {
   int M = 0, G = 0;
   if (!adi_wave_config(n, &M, &G)) return false;
   const int P = n / M;
@@ -931,6 +933,28 @@ bool adi_const_staged_tables(int n, const double *g, const double *h, double *ou
       pb[2 * k + 1] = prod[1];
     }
   }
+  // Thomas factors of a constant-coefficient matrix reach their limit to the
+  // last bit after a few dozen rows, so most chunks' entries coincide
+  auto same_chunk = [&](int c0, int c1) {
+    for (int t = 0; t < 4; ++t)
+      for (int m = 0; m < M; ++m) {
+        const double *e0 = out + 2 * ((size_t)t * n + slot(c0, m));
+        const double *e1 = out + 2 * ((size_t)t * n + slot(c1, m));
+        if (std::memcmp(e0, e1, 2 * sizeof(double)) != 0) return false;
+      }
+    return true;
+  };
+  run[0] = run[1] = 0;
+  for (int c = 0; c < P;) {
+    int e = c + 1;
+    while (e < P && same_chunk(c, e)) ++e;
+    if (e - c > run[1] - run[0]) {
+      run[0] = c;
+      run[1] = e;
+    }
+    c = e;
+  }
+  if (run[1] - run[0] < 2) run[0] = run[1] = 0;
   return true;
 }
 

@@ -76,6 +76,7 @@ struct pxp_solver_s {
   // 2-transverse-dim solvers
   void *d_field2 = nullptr;                  // ping-pong buffer
   void *d_lu = nullptr;                      // factor tables of step-invariant matrices
+  int adi_tab_run[2][2] = {};                // x / y staged ADI tables: identical chunks
   bool cn_const = false;                     // CN matrix step-invariant
   size_t dev_bytes = 0;                      // device memory held by the handle
   pxp::Fft1dJob job_fft{};                   // host copies of the job descriptors
@@ -634,8 +635,10 @@ int adi_build_lu(pxp_solver_s *h) {
       pad[nw + i] = i < n ? gv[n + i] : cd(0.0, 0.0);
     }
     const double *t = reinterpret_cast<const double *>(pad.data());
-    pxp::adi_const_staged_tables((int)nw, t, t + 2 * nw,
-                                 reinterpret_cast<double *>(tabs.data() + 4 * n + 4 * half * nw));
+    if (!pxp::adi_const_staged_tables((int)nw, t, t + 2 * nw,
+                                      reinterpret_cast<double *>(tabs.data() + 4 * n + 4 * half * nw),
+                                      h->adi_tab_run[half]))
+      h->adi_tab_run[half][0] = h->adi_tab_run[half][1] = 0;
   }
   free_dev(h->d_lu, h->stream);
   int rc;
@@ -807,6 +810,8 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   a.kd2_impl = kdx2;
   a.kd2_expl = kdy2;
   a.z = get_z(h, step);
+  a.tab_c0 = h->adi_tab_run[0][0];
+  a.tab_c1 = h->adi_tab_run[0][1];
   adi_fill_spheres(h, a, a.z);
   planes3_at(h, step, 0, &a.plane_delta, &a.plane_beta);
   const cd *lu = (const cd *)h->d_lu;
@@ -825,6 +830,8 @@ int adi_step(pxp_solver_s *h, unsigned step) {
   a.kd2_impl = kdy2;
   a.kd2_expl = kdx2;
   a.z = get_z(h, step) + dzh;
+  a.tab_c0 = h->adi_tab_run[1][0];
+  a.tab_c1 = h->adi_tab_run[1][1];
   adi_fill_spheres(h, a, a.z);
   planes3_at(h, step, 1, &a.plane_delta, &a.plane_beta);
   e = (a.nspheres == 0 && !a.csg.active && !a.plane_delta && !a.use_tbc && lu)

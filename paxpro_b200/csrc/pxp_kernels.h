@@ -177,6 +177,9 @@ struct AdiHalf {
   double k;
   double xmin, dx, ymin, dy;
   double z;                // material plane of this half step
+  // one-wave vacuum kernel: chunks tab_c0 < c < tab_c1 of the staged tables
+  // hold bit for bit the entries of chunk tab_c0 and read those (0, 0: none)
+  int tab_c0, tab_c1;
   Csg csg;                 // CSG material (instead of spheres) when csg.active
   // sampled material of this half step's plane (instead of spheres or CSG)
   // when plane_delta is set: n*n doubles each, the field's layout (x index *
@@ -211,8 +214,10 @@ int adi_wave_n(int n);
 // (pf, pb: products of h over each chunk's rows up to / from a row) and
 // returns true; false when no one-wave kernel solves length n (out
 // untouched).  g, h, out: interleaved (re, im); for a padded grid, g and h
-// already hold the padding rows (g = 1, h = 0).
-bool adi_const_staged_tables(int n, const double *g, const double *h, double *out);
+// already hold the padding rows (g = 1, h = 0).  run[0..1]: the longest
+// run [c0, c1) of consecutive chunks whose entries (g, h, pf and pb at every
+// row of the chunk) are bit for bit equal, for AdiHalf::tab_c0 / tab_c1.
+bool adi_const_staged_tables(int n, const double *g, const double *h, double *out, int run[2]);
 // Saved-slice downsampling of the 3-D solvers (Solver3D::copyCurrentSolution,
 // src/solver3D.cpp:94-112): n x n field -> m x m block averages.
 cudaError_t launch_block_average(Precision p, const void *full, void *out, int n, int m,
