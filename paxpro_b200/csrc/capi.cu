@@ -276,7 +276,8 @@ int alloc(pxp_solver_s *h, void **p, size_t bytes, const char *what) {
 // with the same grids).  The handles do not own these copies.
 struct TableKey {
   int device, kind;  // kind 0: twiddles (radix 8), 1: 1-D propagator, 2: kx^2 per
-                     // column, 3: twiddles (radix 16), 4: exp(-2 pi i m / n), m < n
+                     // column, 3: twiddles (radix 16), 4: exp(-2 pi i m / n), m < n,
+                     // 11: the FFTSolver3D register-line kernel's twiddle table
   unsigned n;
   double dx, dz, k;
   int split;  // 1: the FP32 split form (split_table), 0: complex128 / doubles
@@ -338,6 +339,21 @@ int shared_table_n(pxp_solver_s *h, int kind, unsigned n, void **out) {
     for (unsigned m = 0; m < n; ++m) {
       const long double a = -2.0L * pi_l * (long double)m / (long double)n;
       t[m] = cd((double)cosl(a), (double)sinl(a));
+    }
+  } else if (kind == 11) {
+    // the register-line kernel's twiddles of its earlier radix-8 passes:
+    // exp(-2 pi i m / n) at the exponents that kernel lists
+    std::vector<int> ex(n);
+    const int cnt = pxp::fft3d_lines_tw_exponents((int)n, ex.data(), (int)n);
+    if (cnt <= 0) {
+      *out = nullptr;
+      return PXP_OK;
+    }
+    t.resize(cnt);
+    const long double pi_l = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < cnt; ++i) {
+      const long double a = -2.0L * pi_l * (long double)ex[i] / (long double)n;
+      t[i] = cd((double)cosl(a), (double)sinl(a));
     }
   } else if (kind == 1) {
     t.resize(n);
@@ -1186,6 +1202,9 @@ int fft3d_steps(pxp_solver_s *h, unsigned first, int nsteps) {
   if (!(n & (n - 1))) {  // the power-of-two variants' twiddle tables
     if (int rc = shared_table(h, 3, &tw16)) return rc;
     if (int rc = shared_table(h, 4, &wn)) return rc;
+    void *twl = nullptr;
+    if (int rc = shared_table(h, 11, &twl)) return rc;
+    q.tw_lines = twl;
   }
   // the propagator's x and y factor tables (FP32 always; FP64 unless
   // PXP_FFT3D_JOINT_PROP=1 asks for the reference's joint argument)

@@ -74,7 +74,9 @@ template <typename R, int N, int LG> struct Cfg {
   // radix-8 passes whose twiddles sit in registers: all of them, except at
   // 512 threads per CTA (128 registers a thread), where the earlier passes'
   // twiddles -- few distinct values, 7 * NS of them -- are read from a small
-  // shared table instead
+  // table in global memory (Fft3dPass::tw_lines) through L1 instead: in
+  // shared memory it would push the CTA past 196 KB and the L1 left beside
+  // it from 60 KB to 28 KB, too little for the propagator's x factors
   static constexpr int TWR = T >= 512 ? 1 : NP8;
   static constexpr int TWS_N = [] {  // entries of that table
     int n = 0;
@@ -83,9 +85,7 @@ template <typename R, int N, int LG> struct Cfg {
   }();
   static constexpr size_t STAGE = sizeof(C) * (size_t)L * N;
   static constexpr size_t XBYTES = sizeof(C) * (size_t)L * XS;
-  static constexpr size_t TWBYTES = sizeof(double2) * (size_t)(TWS_N > 0 ? TWS_N : 1);
-  static constexpr size_t SMEM =
-      128 + STAGE + 2 * ((XBYTES + 127) & ~size_t(127)) + ((TWBYTES + 127) & ~size_t(127)) + 128;
+  static constexpr size_t SMEM = 128 + STAGE + 2 * ((XBYTES + 127) & ~size_t(127)) + 128;
   static_assert(N % 8 == 0 && T <= 1024, "line slots");
 };
 
@@ -225,9 +225,9 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
   C *S = reinterpret_cast<C *>(base);
   C *X0 = reinterpret_cast<C *>(base + K::STAGE);
   C *X1 = reinterpret_cast<C *>(base + K::STAGE + ((K::XBYTES + 127) & ~size_t(127)));
-  Tw<C> *tws = reinterpret_cast<Tw<C> *>(base + K::STAGE + 2 * ((K::XBYTES + 127) & ~size_t(127)));
-  uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<unsigned char *>(tws) +
-                                               ((K::TWBYTES + 127) & ~size_t(127)));
+  uint64_t *bar =
+      reinterpret_cast<uint64_t *>(base + K::STAGE + 2 * ((K::XBYTES + 127) & ~size_t(127)));
+  const Tw<C> *tws = reinterpret_cast<const Tw<C> *>(q.tw_lines);
   __shared__ int s_ok;
 
   const int tid = threadIdx.x;
@@ -236,8 +236,8 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
   C *field = reinterpret_cast<C *>(q.field);
   C *save = reinterpret_cast<C *>(q.save);
 
-  // twiddles of the last TWR radix-8 passes, constant for this thread, and
-  // the shared table of the earlier passes' (entry (r-1)*NS + k of pass p)
+  // twiddles of the last TWR radix-8 passes, constant for this thread (the
+  // earlier passes' come from tws, entry (r-1)*NS + k of pass p)
   Tw<C> tw[K::TWR][7];
 #pragma unroll
   for (int pr = 0; pr < K::TWR; ++pr) {
@@ -246,13 +246,6 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
     const int stride = N / (8 * ns);
 #pragma unroll
     for (int r = 1; r < 8; ++r) tw[pr][r - 1] = wn[r * k * stride];
-  }
-  for (int p = 0, off = 0; p < K::NP8 - K::TWR; off += 7 * (K::R0 << (3 * p)), ++p) {
-    const int ns = K::R0 << (3 * p);
-    for (int i = tid; i < 7 * ns; i += K::T) {
-      const int r = i / ns + 1, k = i % ns;
-      tws[off + i] = wn[r * k * (N / (8 * ns))];
-    }
   }
   double kx2[8] = {};
   if (sizeof(R) == 8 && xpass && q.prop_x == nullptr) {  // FP64's joint argument per point
@@ -468,9 +461,27 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
     const cudaError_t e = make_tmap<R, N, LG>(q.field, &tmap);
     if (e != cudaSuccess) return e;
   }
+  if (K::TWS_N > 0 && q.tw_lines == nullptr) return cudaErrorInvalidValue;
   auto k = fft3d_lines_kernel<R, N, LG>;
   {
     const cudaError_t e = raise_dynamic_smem((const void *)k, (int)K::SMEM);
+    if (e != cudaSuccess) return e;
+  }
+  if constexpr (K::T >= 512) {
+    // one CTA an SM: ask for the smallest shared-memory carve-out that
+    // holds it, so that the rest of the SM's 256 KB serves as L1 (the
+    // propagator's x factors and the twiddle table are read through it)
+    static int pct = -1;
+    if (pct < 0) {
+      int dev = 0, per_sm_max = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&per_sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+      const long long need = (long long)K::SMEM + 1024;  // + the driver's reserve per CTA
+      pct = per_sm_max > 0 ? (int)((100 * need + per_sm_max - 1) / per_sm_max) : 100;
+      if (pct > 100) pct = 100;
+    }
+    const cudaError_t e =
+        cudaFuncSetAttribute((const void *)k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
     if (e != cudaSuccess) return e;
   }
   static int per_sm = 0, sms = 0;
@@ -515,6 +526,31 @@ cudaError_t encode_field_tmap(void *field, int n, int real_bytes, int box_reals,
           field, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+namespace lines {
+template <int N, int LG> int tw_exponents(int *out, int cap) {
+  using K = Cfg<double, N, LG>;  // the complex64 kernel has the same passes
+  static_assert(Cfg<float, N, LG>::TWS_N == K::TWS_N, "one table for both precisions");
+  if (K::TWS_N > cap) return -1;
+  int i = 0;
+  for (int p = 0; p < K::NP8 - K::TWR; ++p) {
+    const int ns = K::R0 << (3 * p);
+    for (int e = 0; e < 7 * ns; ++e) {
+      const int r = e / ns + 1, kk = e % ns;
+      out[i++] = r * kk * (N / (8 * ns));
+    }
+  }
+  return i;
+}
+}  // namespace lines
+
+int fft3d_lines_tw_exponents(int n, int *out, int cap) {
+  switch (n) {  // the line slots launch_fft3d_lines uses for n
+    case 2048: return lines::tw_exponents<2048, 1>(out, cap);
+    case 4096: return lines::tw_exponents<4096, 1>(out, cap);
+    default: return 0;
+  }
 }
 
 bool fft3d_lines_supported(Precision p, int n) {

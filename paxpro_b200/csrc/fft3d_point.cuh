@@ -60,6 +60,11 @@ __device__ __forceinline__ void step_material(const Fft3dPass &q, double x, doub
   }
 }
 
+// The index spatialFreq folds to: the propagator factor tables hold equal
+// entries at idx and n - idx, and reading entries 0 .. n/2 only halves the
+// part of a table a line pass keeps in L1.
+__device__ __forceinline__ int kfold(int idx, int n) { return idx > n / 2 ? n - idx : idx; }
+
 // spatialFreq: fold, then 2*PI*indx / (step*size)
 __device__ __forceinline__ double kfreq(int idx, int n, double two_pi, double stepn) {
   if (idx > n / 2) idx = n - idx;
@@ -82,7 +87,7 @@ __device__ __forceinline__ double2 prop3(const Fft3dPass &q, double2 u, double k
   if (q.prop_x != nullptr) {
     const double2 *px = reinterpret_cast<const double2 *>(q.prop_x);
     const double2 *py = reinterpret_cast<const double2 *>(q.prop_y);
-    return cx_mul_rn(u, cx_mul_rn(__ldg(px + ix), __ldg(py + iy)));
+    return cx_mul_rn(u, cx_mul_rn(__ldg(px + kfold(ix, q.n)), __ldg(py + kfold(iy, q.n))));
   }
   const double phi = __dmul_rn(q.a, __dadd_rn(kx2, ky2));
   double sn, cs;
@@ -93,7 +98,7 @@ __device__ __forceinline__ float2 prop3(const Fft3dPass &q, float2 u, double, do
                                         int iy) {
   const float4 *px = reinterpret_cast<const float4 *>(q.prop_x);
   const float4 *py = reinterpret_cast<const float4 *>(q.prop_y);
-  return tw_mul(tw_mul(u, __ldg(px + ix)), __ldg(py + iy));
+  return tw_mul(tw_mul(u, __ldg(px + kfold(ix, q.n))), __ldg(py + kfold(iy, q.n)));
 }
 
 template <typename R> __device__ __forceinline__ typename Cx<R>::T mul_k(typename Cx<R>::T u,

@@ -326,12 +326,22 @@ struct Fft3dPass {
   // damping length per axis (0 thickness = off)
   int thick_x, thick_y;
   double inv_damp_x, inv_damp_y;
-  // FP32 served mode: the propagator as the product of its x and y factors,
-  // prop_x[i] = exp(-i a kx_i^2) and prop_y[i] = exp(-i a ky_i^2) (n split
-  // complex64 entries each, phases reduced on the host in extended
-  // precision); FP64 mode evaluates the reference's joint argument instead
+  // the propagator as the product of its x and y factors, prop_x[i] =
+  // exp(-i a kx_i^2) and prop_y[i] = exp(-i a ky_i^2) (n entries each,
+  // complex128 in FP64, split complex64 in FP32; phases reduced on the host
+  // in extended precision; k_i folds, so entry i equals entry n - i and the
+  // kernels read entries 0 .. n/2 only); null in FP64 when the reference's
+  // joint argument is asked for (PXP_FFT3D_JOINT_PROP=1)
   const void *prop_x, *prop_y;
+  // twiddles of the register-line kernel's radix-8 passes before its last
+  // (fft3d_lines.cu, n = 4096): entry i = exp(-2 pi i m_i / n) with m_i from
+  // fft3d_lines_tw_exponents, in the solver's table form
+  const void *tw_lines;
 };
+// Exponents m_i of the twiddle table Fft3dPass::tw_lines for length n (out:
+// room for cap entries); returns the entry count (0: the kernel for n reads
+// no table).
+int fft3d_lines_tw_exponents(int n, int *out, int cap);
 // variant: 0 = radix 8, double-buffered, tables in shared memory; 1 = radix
 // 8, single buffer, tables through L1; 2 = radix 16, single buffer; 3 =
 // register-resident transforms with TMA-staged lines (fft3d_lines.cu; n up
