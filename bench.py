@@ -564,6 +564,10 @@ def run_ours(args, rank, world, device):
                     "unit": "GB/s", "frac": round(achieved / peak, 4),
                     "peak_kind": peak_kind,
                     "traffic": profiled_traffic("adi_const_wave_kernel_1024.md"),
+                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                                      "from one ncu capture of this kernel at this size "
+                                      "(profiles/adi_const_wave_kernel_1024.md; ncu flushes "
+                                      "the caches before each replayed launch)",
                     "residency": "L2: the 16 MB field and its 16 MB half-step copy stay in the "
                                  "126 MB L2 across half steps, so `achieved` is effective "
                                  "bandwidth against the HBM copy peak, not an HBM-bound figure",

@@ -71,6 +71,11 @@ template <typename R, int N, int LG> struct Cfg {
   static constexpr int XS = N + 16 / (int)sizeof(C);        // exchange stride per line
   static constexpr int BC = N < 256 ? N : 256;              // tensor tile: positions
   static constexpr int GROUPS = N / L;
+  // x pass stores by warp (one complex128 line a group, n >= 256): see the
+  // kernel's epilogue
+  static constexpr bool WARP_ST = L == 1 && N >= 256;
+  static constexpr int BCS = 32;                            // rows a warp's tile store
+
   // radix-8 passes whose twiddles sit in registers: all of them, except at
   // 512 threads per CTA (128 registers a thread), where the earlier passes'
   // twiddles -- few distinct values, 7 * NS of them -- are read from a small
@@ -215,6 +220,7 @@ __device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N, LG>::L
 template <typename R, int N, int LG>
 __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
     fft3d_lines_kernel(const __grid_constant__ Fft3dPass q, const __grid_constant__ CUtensorMap tmap,
+                       const __grid_constant__ CUtensorMap tmap_st,
                        const double *__restrict__ gkx2,
                        const Tw<typename Cx<R>::T> *__restrict__ wn) {
   using K = Cfg<R, N, LG>;
@@ -282,9 +288,11 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
   if (tid == 0 && g < K::GROUPS) issue(g);
   int cur = 1;
   for (int it = 0; g < K::GROUPS; ++it, g += gridDim.x) {
-    if (tid == 0) {
-      // the previous group's tile stores have read their buffer (x pass)
+    // the previous group's tile stores have read their buffer (x pass; with
+    // per-warp stores each warp's lane 0 issued its own)
+    if (K::WARP_ST ? (tid & 31) == 0 : tid == 0)
       asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+    if (tid == 0) {
       const bool ok = mbar_wait_bounded(bar, it & 1, 2000000000ull);
       if (!ok) {
         atomicAdd(&g_lines_wait_timeouts, 1u);
@@ -294,7 +302,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
     }
     __syncthreads();
     if (!s_ok) {
-      if (tid == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+      if ((tid & 31) == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
       return;
     }
     (void)mbar_try_wait(bar, it & 1);  // completed phase: orders the staged line for this thread
@@ -372,7 +380,32 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
       }
       if (q.mode != 3) line_fft<-1, R, N, LG>(v, X0, X1, cur, tw, tws, slot, j, nothing);
     }
-    if (xpass) {
+    if (xpass && K::WARP_ST) {
+      // one line a group: the last pass left thread j with outputs j + s*TL
+      // and read them from F at sw(j + s*TL), which stays inside the aligned
+      // 8-element block of j + s*TL, so a warp's outputs go back to exactly
+      // the slots that warp read -- no CTA barrier, only the warp's own --
+      // and leave by the warp's tile stores of its 8 runs of 32 rows
+      C *F = cur ? X1 : X0;
+      const int lane = tid & 31, w0 = tid & ~31;
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 8; ++s) F[j + s * K::TL] = v[0][s];
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+          const int e0 = w0 + s * K::TL;
+          asm volatile(
+              "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                  &tmap_st),
+              "r"(2 * line0), "r"(e0), "r"(smem_u32(F + e0))
+              : "memory");
+        }
+        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+      }
+    } else if (xpass) {
       // columns leave by TMA tile stores (the staging layout: element e of
       // line l at e*L + l), instead of 16-byte stores strided by the row
       // length, from the exchange buffer the last pass read, once every
@@ -409,7 +442,7 @@ __global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
     }
   }
   // the last group's tile stores complete before the CTA leaves
-  if (tid == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+  if ((tid & 31) == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
 }
 
 // ---- host side -------------------------------------------------------------
@@ -433,15 +466,16 @@ EncodeTiledFn encode_fn() {
 }
 
 // Tensor map of the field as rows of 2n reals (re, im) x n columns; tiles
-// of 2L reals x BC positions (the x lines row0 .. row0+L-1 at BC positions).
+// of 2L reals x rows positions (the x lines row0 .. row0+L-1 at that many
+// positions: BC for the loads and the CTA's stores, BCS for a warp's).
 template <typename R, int N, int LG>
-cudaError_t make_tmap(void *field, CUtensorMap *out) {
+cudaError_t make_tmap(void *field, CUtensorMap *out, int rows) {
   using K = Cfg<R, N, LG>;
   EncodeTiledFn enc = encode_fn();
   if (enc == nullptr) return cudaErrorNotSupported;
   const cuuint64_t dims[2] = {(cuuint64_t)2 * N, (cuuint64_t)N};
   const cuuint64_t strides[1] = {(cuuint64_t)2 * N * sizeof(R)};
-  const cuuint32_t box[2] = {(cuuint32_t)(2 * K::L), (cuuint32_t)K::BC};
+  const cuuint32_t box[2] = {(cuuint32_t)(2 * K::L), (cuuint32_t)rows};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = enc(out, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                          2, field, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -455,10 +489,12 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
   const Tw<typename Cx<R>::T> *wn = reinterpret_cast<const Tw<typename Cx<R>::T> *>(wnv);
   using K = Cfg<R, N, LG>;
   static_assert(K::SMEM <= 227 * 1024, "line pass exceeds shared memory");
-  CUtensorMap tmap;
+  CUtensorMap tmap, tmap_st;
   std::memset(&tmap, 0, sizeof(tmap));
+  std::memset(&tmap_st, 0, sizeof(tmap_st));
   if (q.mode == 1) {
-    const cudaError_t e = make_tmap<R, N, LG>(q.field, &tmap);
+    cudaError_t e = make_tmap<R, N, LG>(q.field, &tmap, K::BC);
+    if (e == cudaSuccess && K::WARP_ST) e = make_tmap<R, N, LG>(q.field, &tmap_st, K::BCS);
     if (e != cudaSuccess) return e;
   }
   if (K::TWS_N > 0 && q.tw_lines == nullptr) return cudaErrorInvalidValue;
@@ -504,7 +540,7 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k, q, tmap, kx2, wn);
+  return cudaLaunchKernelEx(&cfg, k, q, tmap, tmap_st, kx2, wn);
 }
 
 }  // namespace lines
