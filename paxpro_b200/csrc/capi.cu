@@ -928,6 +928,15 @@ void slab_spheres(const pxp_solver_s *h, double z0, double z1, std::vector<pxp::
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, int, unsigned>, int> g_fft3d_variant;
 
+// PXP_TUNE_LOG=1: the tuners print each candidate's time to stderr.
+bool tune_log() {
+  static const bool on = [] {
+    const char *e = std::getenv("PXP_TUNE_LOG");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 // A tuned choice: the x pass's variant and the y pass's (modes 0, 2, 3).
 int fft3d_variant_code(int vx, int vy) { return vx + 8 * vy; }
 int fft3d_variant_of(int code, int mode) { return mode == 1 ? code % 8 : code / 8; }
@@ -1025,6 +1034,9 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
           q.mode = mode;
           return pxp::launch_fft3d_pass(h->prec, q, v, (const double *)kx2, tw16, wn, h->stream);
         });
+        if (tune_log())
+          std::fprintf(stderr, "pxp fft3d tune n=%u prec=%d variant %d %s pass: %.2f us\n", h->nx,
+                       (int)h->prec, v, mode == 1 ? "x" : "y", t * 1e3f);
         if (t < best[pass]) {
           best[pass] = t;
           best_v[pass] = v;
@@ -1052,6 +1064,9 @@ int fft3d_variant(pxp_solver_s *h, const pxp::Fft3dPass &q0, const void *kx2, co
                                    tw16, wn, h->stream);
       return r;
     });
+    if (tune_log())
+      std::fprintf(stderr, "pxp fft3d tune n=%u prec=%d step x v%d + y v%d: %.2f us\n", h->nx,
+                   (int)h->prec, fft3d_variant_of(code, 1), fft3d_variant_of(code, 2), t * 1e3f);
     if (t < best_step) {
       best_step = t;
       best_code = code;

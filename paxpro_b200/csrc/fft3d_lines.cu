@@ -77,12 +77,17 @@ template <typename R, int N, int LG> struct Cfg {
   static constexpr int BCS = 32;                            // rows a warp's tile store
 
   // radix-8 passes whose twiddles sit in registers: all of them, except at
-  // 512 threads per CTA (128 registers a thread), where the earlier passes'
-  // twiddles -- few distinct values, 7 * NS of them -- are read from a small
-  // table in global memory (Fft3dPass::tw_lines) through L1 instead: in
-  // shared memory it would push the CTA past 196 KB and the L1 left beside
-  // it from 60 KB to 28 KB, too little for the propagator's x factors
-  static constexpr int TWR = T >= 512 ? 1 : NP8;
+  // 512 threads per CTA and for complex128 lines at 256, where only the
+  // last pass's do and the earlier passes' -- few distinct values, 7 * NS
+  // of them -- come from a small table in global memory
+  // (Fft3dPass::tw_lines) through L1.  That keeps a thread at 128
+  // registers: one CTA an SM at 512 threads, two at 256 (16 warps instead
+  // of 8; complex64 lines, two a thread, would spill there); and outside
+  // shared memory the table leaves the SM 60 KB of L1 (a 196 KB carve-out)
+  // for it and the propagator's x factors
+  static constexpr bool TW_TABLE = T >= 512 || (T == 256 && sizeof(C) == 16);
+  static constexpr int TWR = TW_TABLE ? 1 : NP8;
+  static constexpr int MINB = T == 256 && TW_TABLE ? 2 : 1;  // CTAs an SM
   static constexpr int TWS_N = [] {  // entries of that table
     int n = 0;
     for (int p = 0; p < NP8 - TWR; ++p) n += 7 * (R0 << (3 * p));
@@ -218,7 +223,7 @@ __device__ __forceinline__ void line_fft(typename Cx<R>::T (&v)[Cfg<R, N, LG>::L
 }
 
 template <typename R, int N, int LG>
-__global__ void __launch_bounds__(Cfg<R, N, LG>::T, 1)
+__global__ void __launch_bounds__(Cfg<R, N, LG>::T, Cfg<R, N, LG>::MINB)
     fft3d_lines_kernel(const __grid_constant__ Fft3dPass q, const __grid_constant__ CUtensorMap tmap,
                        const __grid_constant__ CUtensorMap tmap_st,
                        const double *__restrict__ gkx2,
@@ -503,21 +508,10 @@ cudaError_t launch(const Fft3dPass &q, const double *kx2, const void *wnv, cudaS
     const cudaError_t e = raise_dynamic_smem((const void *)k, (int)K::SMEM);
     if (e != cudaSuccess) return e;
   }
-  if constexpr (K::T >= 512) {
-    // one CTA an SM: ask for the smallest shared-memory carve-out that
-    // holds it, so that the rest of the SM's 256 KB serves as L1 (the
+  if constexpr (K::TW_TABLE) {
+    // MINB CTAs an SM: the rest of the SM's 256 KB serves as L1 (the
     // propagator's x factors and the twiddle table are read through it)
-    static int pct = -1;
-    if (pct < 0) {
-      int dev = 0, per_sm_max = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&per_sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-      const long long need = (long long)K::SMEM + 1024;  // + the driver's reserve per CTA
-      pct = per_sm_max > 0 ? (int)((100 * need + per_sm_max - 1) / per_sm_max) : 100;
-      if (pct > 100) pct = 100;
-    }
-    const cudaError_t e =
-        cudaFuncSetAttribute((const void *)k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    const cudaError_t e = prefer_smem_carveout((const void *)k, (int)K::SMEM, K::MINB);
     if (e != cudaSuccess) return e;
   }
   static int per_sm = 0, sms = 0;
@@ -566,8 +560,9 @@ cudaError_t encode_field_tmap(void *field, int n, int real_bytes, int box_reals,
 
 namespace lines {
 template <int N, int LG> int tw_exponents(int *out, int cap) {
-  using K = Cfg<double, N, LG>;  // the complex64 kernel has the same passes
-  static_assert(Cfg<float, N, LG>::TWS_N == K::TWS_N, "one table for both precisions");
+  using K = Cfg<double, N, LG>;  // the complex64 kernel reads the same table or none
+  static_assert(Cfg<float, N, LG>::TWS_N == 0 || Cfg<float, N, LG>::TWS_N == K::TWS_N,
+                "one table for both precisions");
   if (K::TWS_N > cap) return -1;
   int i = 0;
   for (int p = 0; p < K::NP8 - K::TWR; ++p) {
@@ -583,6 +578,7 @@ template <int N, int LG> int tw_exponents(int *out, int cap) {
 
 int fft3d_lines_tw_exponents(int n, int *out, int cap) {
   switch (n) {  // the line slots launch_fft3d_lines uses for n
+    case 1024: return lines::tw_exponents<1024, 2>(out, cap);
     case 2048: return lines::tw_exponents<2048, 1>(out, cap);
     case 4096: return lines::tw_exponents<4096, 1>(out, cap);
     default: return 0;

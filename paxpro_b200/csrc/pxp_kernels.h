@@ -17,6 +17,10 @@ void set_last_error(const char *msg);
 // process driving several GPUs needs it set on each; this records what was
 // set per (kernel, device) and calls cudaFuncSetAttribute only when needed.
 cudaError_t raise_dynamic_smem(const void *kernel, int bytes);
+// Ask, once per kernel and device, for the smallest shared-memory carve-out
+// that holds `ctas` CTAs of `bytes` dynamic shared memory each, leaving the
+// rest of the SM's unified L1/shared storage to L1.
+cudaError_t prefer_smem_carveout(const void *kernel, int bytes, int ctas);
 
 // ---------------------------------------------------------------- FFT 1-D --
 // One split-step problem with one transverse dimension (FFTSolver2D).
@@ -334,7 +338,7 @@ struct Fft3dPass {
   // joint argument is asked for (PXP_FFT3D_JOINT_PROP=1)
   const void *prop_x, *prop_y;
   // twiddles of the register-line kernel's radix-8 passes before its last
-  // (fft3d_lines.cu, n = 4096): entry i = exp(-2 pi i m_i / n) with m_i from
+  // (fft3d_lines.cu, n = 1024 .. 4096): entry i = exp(-2 pi i m_i / n), m_i from
   // fft3d_lines_tw_exponents, in the solver's table form
   const void *tw_lines;
 };

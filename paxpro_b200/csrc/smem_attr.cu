@@ -34,3 +34,28 @@ cudaError_t pxp::raise_dynamic_smem(const void *kernel, int bytes) {
   g_set[key] = bytes;
   return cudaSuccess;
 }
+
+namespace {
+std::map<std::pair<const void *, int>, int> g_carve;  // (kernel, device) -> percent set
+}  // namespace
+
+cudaError_t pxp::prefer_smem_carveout(const void *kernel, int bytes, int ctas) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_mutex);
+  auto key = std::make_pair(kernel, dev);
+  if (g_carve.count(key)) return cudaSuccess;
+  int per_sm = 0;
+  e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (e != cudaSuccess) return e;
+  // the driver adds 1 KB a CTA and rounds the percentage up to a carve-out
+  // it supports
+  const long long need = ((long long)bytes + 1024) * (ctas > 0 ? ctas : 1);
+  int pct = per_sm > 0 ? (int)((100 * need + per_sm - 1) / per_sm) : 100;
+  if (pct > 100) pct = 100;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  if (e != cudaSuccess) return e;
+  g_carve[key] = pct;
+  return cudaSuccess;
+}
