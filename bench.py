@@ -428,8 +428,17 @@ def precision_sweep(device, kind: str = "fft3d", every: int = 100):
         rows.append({"step": (i + 1) * every, **{key: float(f"{v:.3e}") for key, v in r.items()}})
     for s in solvers:
         s.close()
+    # FFTSolver3D: a step's two line passes each read and write the whole
+    # field once (complex128: 16 B a point in FP64, complex64 in FP32); an
+    # ADI half step does too (two a step)
+    peak, peak_kind = measured_peaks()
+    step_bytes = [4.0 * p.nx * p.nx * 16, 4.0 * p.nx * p.nx * 8]
+    gbs = [b / (t * 1e-6) / 1e9 if t > 0 else 0.0 for b, t in zip(step_bytes, us)]
     return {"workload": f"{p.name}: {p.nx}^2, {p.nsteps} steps, {len(p.spheres)} spheres",
             "us_per_step_fp64": round(us[0], 2), "us_per_step_fp32": round(us[1], 2),
+            "step_gbs_fp64": round(gbs[0], 1), "step_gbs_fp32": round(gbs[1], 1),
+            "frac_of_hbm_fp64": round(gbs[0] / peak, 4), "frac_of_hbm_fp32": round(gbs[1] / peak, 4),
+            "hbm_peak_gbs": peak, "hbm_peak_kind": peak_kind,
             "max_intensity_rel_l2": max(r["intensity_rel_l2"] for r in rows),
             "max_phase_rms_rad": max(r["phase_rms_rad"] for r in rows), "every": rows}
 
