@@ -49,10 +49,17 @@ cudaError_t pxp::prefer_smem_carveout(const void *kernel, int bytes, int ctas) {
   int per_sm = 0;
   e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   if (e != cudaSuccess) return e;
-  // the driver adds 1 KB a CTA and rounds the percentage up to a carve-out
-  // it supports
+  // the driver adds 1 KB a CTA and rounds the percentage up to the next
+  // carve-out it supports: ask for the largest percentage that still rounds
+  // to the smallest supported carve-out holding the CTAs
+  static const int kCarveKB[] = {0, 8, 16, 32, 64, 100, 132, 164, 196, 228};
   const long long need = ((long long)bytes + 1024) * (ctas > 0 ? ctas : 1);
-  int pct = per_sm > 0 ? (int)((100 * need + per_sm - 1) / per_sm) : 100;
+  int pct = 100;
+  for (int kb : kCarveKB)
+    if (1024LL * kb >= need && per_sm > 0) {
+      pct = (int)((100LL * 1024 * kb) / per_sm);
+      break;
+    }
   if (pct > 100) pct = 100;
   e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
   if (e != cudaSuccess) return e;
