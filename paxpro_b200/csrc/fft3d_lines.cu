@@ -27,20 +27,21 @@
 //    is transformed: a contiguous group of y lines is one bulk copy; a group
 //    of x lines (adjacent rows of the column-major field) is n/256 tiles of
 //    a 2-D tensor map over this GPU's own field (no multicast).  x lines
-//    also leave by tile stores of the same map, from the exchange buffer
-//    the last pass did not read; y lines leave by coalesced stores from
-//    registers.  One thread
-//    arms an mbarrier for the group's bytes and issues the copies; it waits
-//    with a bounded wait (about 2 s; a wait that runs out is counted, the
-//    copy drained and the CTA leaves) and a CTA barrier publishes the line.
+//    also leave by tile stores, from the exchange buffer the last pass
+//    read (issued by one thread for the CTA, or, with one complex128 line a
+//    group, by each warp for its own rows); y lines leave by coalesced
+//    stores from registers.  One thread arms an mbarrier for the group's
+//    bytes and issues the copies; it waits with a bounded wait (about 2 s;
+//    a wait that runs out is counted, the copy drained and the CTA leaves)
+//    and a CTA barrier publishes the line.
 //
 // A CTA holds LG line slots of n/8 threads; a complex64 thread carries two
 // lines (the tensor tiles then start on 16-byte boundaries).  Per-point
-// arithmetic (propagator argument and sincos, refraction, absorber, save) is
-// fft3d_point.cuh's, shared with fft3d.cu.  The transforms round like the
-// other kernels' up to the order of their passes (within the parity
-// tolerance); complex64 data compute in FP32 with split twiddles as
-// fft_smem.cuh does.
+// arithmetic (propagator factors or argument and sincos, refraction,
+// absorber, save) is fft3d_point.cuh's, shared with fft3d.cu.  The
+// transforms round like the other kernels' up to the order of their passes
+// (within the parity tolerance); complex64 data compute in FP32 with split
+// twiddles as fft_smem.cuh does.
 #include <cuda.h>
 
 #include <cstdint>
